@@ -1,0 +1,625 @@
+// Element kernels: hyperelastic internal force, tangent stiffness fused with
+// the colored CSR scatter, and the consistent mass matrix (FP64).
+//
+// Reference: fenris/src/assembly.rs:618-797 (element mass / elliptic term /
+// stiffness), :252-314 + :1042-1075 (colored CSR scatter), :915-966 (colored
+// force scatter); materials in fenris/src/solid/materials.rs.
+//
+// Layout: connectivity is SoA (conn[I * ne + e]) so that the lanes that own
+// the nodes of one element read it with one transaction per node.  One warp
+// owns a Tet10 element (4 elements per 128-thread CTA); one 128-thread CTA
+// owns a Hex27 element.  Per quadrature point the owning warp builds the
+// per-node vectors a_I = sqrt(w |det J|) J^-T grad N_I, b_I = F a_I and
+// c_I = Cof(F) a_I (SNH) or S a_I (StVK); the stiffness block of a node pair
+// is then a closed-form rank-structured expression of those vectors (the
+// contraction sum_kl C[3k+i,3l+j] a_I[k] a_J[l] of materials.rs:689-743
+// evaluated without forming the 9x9 tensor), accumulated in registers over
+// the quadrature points.  The element matrix is scattered straight into the
+// CSR values with the precomputed element-to-nnz map; colors are launched in
+// sequence so no two concurrent elements touch the same node (no atomics,
+// and every CSR entry receives its contributions in color order).
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace hoefem {
+
+namespace {
+
+constexpr int TPB = 128;
+
+__constant__ signed char c_hex27_alpha[27][3] = {
+    {-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1}, {-1, -1, 1}, {1, -1, 1}, {1, 1, 1}, {-1, 1, 1},
+    {0, -1, -1},  {-1, 0, -1}, {-1, -1, 0}, {1, 0, -1}, {1, -1, 0}, {0, 1, -1}, {1, 1, 0}, {-1, 1, 0},
+    {0, -1, 1},   {-1, 0, 1},  {1, 0, 1},   {0, 1, 1},  {0, 0, -1}, {0, -1, 0}, {-1, 0, 0}, {1, 0, 0},
+    {0, 1, 0},    {0, 0, 1},   {0, 0, 0}};
+__constant__ signed char c_tet10_edge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {2, 3}, {1, 3}};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void set_error(int* err, int code) { atomicCAS(err, 0, code); }
+
+// ---- reference elements ----------------------------------------------------
+__device__ __forceinline__ void tet4_psi(const double* xi, double* p) {
+  p[0] = -0.5 * xi[0] - 0.5 * xi[1] - 0.5 * xi[2] - 0.5;
+  p[1] = 0.5 * xi[0] + 0.5;
+  p[2] = 0.5 * xi[1] + 0.5;
+  p[3] = 0.5 * xi[2] + 0.5;
+}
+// gradient of Tet4 basis function I (constant): column I of [[-.5,.5,0,0],[-.5,0,.5,0],[-.5,0,0,.5]]
+__device__ __forceinline__ void tet4_g(int I, double* g) {
+  g[0] = (I == 0) ? -0.5 : (I == 1 ? 0.5 : 0.0);
+  g[1] = (I == 0) ? -0.5 : (I == 2 ? 0.5 : 0.0);
+  g[2] = (I == 0) ? -0.5 : (I == 3 ? 0.5 : 0.0);
+}
+// Tet10 reference gradient of node I (element.rs:1921-1947)
+__device__ __forceinline__ void tet10_grad(int I, const double* xi, double* g) {
+  double p[4];
+  tet4_psi(xi, p);
+  if (I < 4) {
+    double gi[3];
+    tet4_g(I, gi);
+    double f = 4.0 * p[I] - 1.0;
+    g[0] = gi[0] * f; g[1] = gi[1] * f; g[2] = gi[2] * f;
+  } else {
+    int a = c_tet10_edge[I - 4][0], b = c_tet10_edge[I - 4][1];
+    double ga[3], gb[3];
+    tet4_g(a, ga);
+    tet4_g(b, gb);
+    double fb = 4.0 * p[b], fa = 4.0 * p[a];
+    g[0] = ga[0] * fb + gb[0] * fa;
+    g[1] = ga[1] * fb + gb[1] * fa;
+    g[2] = ga[2] * fb + gb[2] * fa;
+  }
+}
+__device__ __forceinline__ double tet10_phi(int I, const double* xi) {
+  double p[4];
+  tet4_psi(xi, p);
+  if (I < 4) return p[I] * (2.0 * p[I] - 1.0);
+  return 4.0 * p[c_tet10_edge[I - 4][0]] * p[c_tet10_edge[I - 4][1]];
+}
+__device__ __forceinline__ double phi_q(double a, double x) {
+  double a2 = a * a, x2 = x * x;
+  return (3.0 / 2.0 * a2 - 1.0) * x2 + 0.5 * a * x + 1.0 - a2;
+}
+__device__ __forceinline__ double dphi_q(double a, double x) {
+  double a2 = a * a;
+  return 2.0 * (3.0 / 2.0 * a2 - 1.0) * x + 0.5 * a;
+}
+__device__ __forceinline__ void hex27_grad(int I, const double* xi, double* g) {
+  double a0 = c_hex27_alpha[I][0], a1 = c_hex27_alpha[I][1], a2 = c_hex27_alpha[I][2];
+  double p0 = phi_q(a0, xi[0]), p1 = phi_q(a1, xi[1]), p2 = phi_q(a2, xi[2]);
+  g[0] = dphi_q(a0, xi[0]) * p1 * p2;
+  g[1] = p0 * dphi_q(a1, xi[1]) * p2;
+  g[2] = p0 * p1 * dphi_q(a2, xi[2]);
+}
+__device__ __forceinline__ double hex27_phi(int I, const double* xi) {
+  return phi_q(c_hex27_alpha[I][0], xi[0]) * phi_q(c_hex27_alpha[I][1], xi[1]) * phi_q(c_hex27_alpha[I][2], xi[2]);
+}
+// Jacobian of the trilinear Hex8 geometry from the 8 corners (smem, xyz per corner).
+__device__ __forceinline__ void hex8_jacobian(const double* Xc, const double* xi, double* J) {
+#pragma unroll
+  for (int k = 0; k < 9; ++k) J[k] = 0.0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    double a0 = c_hex27_alpha[c][0], a1 = c_hex27_alpha[c][1], a2 = c_hex27_alpha[c][2];
+    double l0 = (1.0 + a0 * xi[0]) / 2.0, l1 = (1.0 + a1 * xi[1]) / 2.0, l2 = (1.0 + a2 * xi[2]) / 2.0;
+    double g0 = a0 / 2.0 * l1 * l2, g1 = l0 * a1 / 2.0 * l2, g2 = l0 * l1 * a2 / 2.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      double x = Xc[3 * c + i];
+      J[3 * i + 0] += x * g0;
+      J[3 * i + 1] += x * g1;
+      J[3 * i + 2] += x * g2;
+    }
+  }
+}
+// Jacobian of the affine Tet4 geometry: J(:,j) = 0.5 (X_{j+1} - X_0)
+__device__ __forceinline__ void tet4_jacobian(const double* Xc, double* J) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) J[3 * i + j] = -0.5 * Xc[i] + 0.5 * Xc[3 * (j + 1) + i];
+}
+
+__device__ __forceinline__ double det3(const double* m) {
+  return m[0] * (m[4] * m[8] - m[7] * m[5]) - m[1] * (m[3] * m[8] - m[6] * m[5]) + m[2] * (m[3] * m[7] - m[6] * m[4]);
+}
+// inverse (row-major), returns det; out undefined when det == 0
+__device__ __forceinline__ double inv3(const double* m, double* o) {
+  double d = det3(m);
+  o[0] = (m[4] * m[8] - m[7] * m[5]) / d;
+  o[1] = -(m[1] * m[8] - m[7] * m[2]) / d;
+  o[2] = (m[1] * m[5] - m[4] * m[2]) / d;
+  o[3] = -(m[3] * m[8] - m[6] * m[5]) / d;
+  o[4] = (m[0] * m[8] - m[6] * m[2]) / d;
+  o[5] = -(m[0] * m[5] - m[3] * m[2]) / d;
+  o[6] = (m[3] * m[7] - m[6] * m[4]) / d;
+  o[7] = -(m[0] * m[7] - m[6] * m[1]) / d;
+  o[8] = (m[0] * m[4] - m[3] * m[1]) / d;
+  return d;
+}
+
+// ---- materials (materials.rs) -----------------------------------------------
+// Per quadrature point state.  M1 / M2 are the two matrices the pair
+// contraction needs: SNH: M1 = Cof(F) = J F^-T, StVK: M1 = S, M2 = F F^T.
+struct QpState {
+  double F[9];
+  double M1[9];
+  double M2[9];
+  double s1, s2, s3, s4;
+  double P[9];
+};
+
+__device__ __forceinline__ bool snh_state(const double* F, double mu0, double lam0, QpState& q, bool need_stress) {
+  const double d = 3.0;
+  double mu = (d + 1.0) / d * mu0;
+  double lam = lam0 + (1.0 - 2.0 / (d * (d + 1.0))) * mu0;
+  double alpha = 1.0 + mu / lam * (d / (d + 1.0));
+  double IC = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) IC += F[k] * F[k];
+  double Fi[9];
+  double J = inv3(F, Fi);
+  if (J == 0.0) return false;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) q.M1[3 * i + j] = Fi[3 * j + i] * J;  // dJ/dF = F^-T J
+  double beta = IC + 1.0;
+  q.s1 = mu * (1.0 - 1.0 / beta);
+  q.s2 = mu * 2.0 / (beta * beta);
+  q.s3 = lam * (J - alpha);
+  q.s4 = lam;
+  if (need_stress) {
+    double cf = mu * (1.0 - 1.0 / (IC + 1.0)), cj = lam * (J - alpha);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) q.P[k] = F[k] * cf + q.M1[k] * cj;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void stvk_state(const double* F, double mu, double lam, QpState& q, bool need_stress) {
+  double E[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      double s = F[i] * F[j] + F[3 + i] * F[3 + j] + F[6 + i] * F[6 + j];  // (F^T F)(i,j)
+      E[3 * i + j] = (s - (i == j ? 1.0 : 0.0)) * 0.5;
+    }
+  double tr = E[0] + E[4] + E[8];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) q.M1[k] = E[k] * 2.0 * mu + ((k % 4 == 0) ? lam * tr : 0.0);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) q.M2[3 * i + j] = F[3 * i] * F[3 * j] + F[3 * i + 1] * F[3 * j + 1] + F[3 * i + 2] * F[3 * j + 2];
+  q.s1 = mu;
+  q.s4 = lam;
+  if (need_stress) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        q.P[3 * i + j] = F[3 * i] * q.M1[j] + F[3 * i + 1] * q.M1[3 + j] + F[3 * i + 2] * q.M1[6 + j];
+  }
+}
+
+__device__ __forceinline__ bool material_state(int kind, const double* F, double mu, double lam, QpState& q,
+                                               bool need_stress) {
+#pragma unroll
+  for (int k = 0; k < 9; ++k) q.F[k] = F[k];
+  if (kind == HOEFEM_MAT_SNH) return snh_state(F, mu, lam, q, need_stress);
+  stvk_state(F, mu, lam, q, need_stress);
+  return true;
+}
+
+__device__ __forceinline__ void mat3vec(const double* M, const double* a, double* o) {
+  o[0] = M[0] * a[0] + M[1] * a[1] + M[2] * a[2];
+  o[1] = M[3] * a[0] + M[4] * a[1] + M[5] * a[2];
+  o[2] = M[6] * a[0] + M[7] * a[1] + M[8] * a[2];
+}
+
+// Stiffness block of node pair (I row, J column), added into acc (3x3 row-major).
+// Per-node vectors: v[0..2] = a, v[3..5] = F a, v[6..8] = M1 a.
+//  SNH : s1 (aI.aJ) I + s2 (F aI)(F aJ)^T + lam (Cof aI)(Cof aJ)^T + s3 eps_ijm (F (aI x aJ))_m
+//  StVK: (aJ . S aI) I + mu (F aJ)(F aI)^T + mu (aI.aJ) F F^T + lam (F aI)(F aJ)^T
+__device__ __forceinline__ void pair_block(int kind, const QpState& q, const double* vI, const double* vJ,
+                                           double* acc) {
+  double dot = vI[0] * vJ[0] + vI[1] * vJ[1] + vI[2] * vJ[2];
+  if (kind == HOEFEM_MAT_SNH) {
+    double cr[3] = {vI[1] * vJ[2] - vI[2] * vJ[1], vI[2] * vJ[0] - vI[0] * vJ[2], vI[0] * vJ[1] - vI[1] * vJ[0]};
+    double w[3];
+    mat3vec(q.F, cr, w);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) acc[3 * i + j] += q.s2 * vI[3 + i] * vJ[3 + j] + q.s4 * vI[6 + i] * vJ[6 + j];
+    double d1 = q.s1 * dot;
+    acc[0] += d1; acc[4] += d1; acc[8] += d1;
+    // eps_ijm w_m: (0,1)=w2 (0,2)=-w1 (1,0)=-w2 (1,2)=w0 (2,0)=w1 (2,1)=-w0
+    double s3 = q.s3;
+    acc[1] += s3 * w[2]; acc[2] -= s3 * w[1];
+    acc[3] -= s3 * w[2]; acc[5] += s3 * w[0];
+    acc[6] += s3 * w[1]; acc[7] -= s3 * w[0];
+  } else {
+    double d0 = vJ[0] * vI[6] + vJ[1] * vI[7] + vJ[2] * vI[8];  // aJ . S aI
+    double mu = q.s1, lam = q.s4;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        acc[3 * i + j] += mu * vJ[3 + i] * vI[3 + j] + mu * dot * q.M2[3 * i + j] + lam * vI[3 + i] * vJ[3 + j];
+    acc[0] += d0; acc[4] += d0; acc[8] += d0;
+  }
+}
+
+__device__ __forceinline__ void quad_rule(const BlockDev& b, int e, int& q0, int& nq) {
+  if (b.uniform) { q0 = 0; nq = b.nq; }
+  else { q0 = b.qoff[e]; nq = b.qoff[e + 1] - q0; }
+}
+
+// ============================================================================
+// Internal force: warp per element (nodes <= 32), per-color launch.
+// f_e(:, I) += -(P J^-T grad N_I) w |det J|  (assembly.rs:695-708)
+// ============================================================================
+template <int NN>
+__global__ void __launch_bounds__(TPB) k_forces(const BlockDev b, const int* __restrict__ elems, int count,
+                                                const double* __restrict__ X, const double* __restrict__ u,
+                                                double* __restrict__ f, MatDev mat, int* err) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int idx = blockIdx.x * (TPB / 32) + warp;
+  __shared__ double s_corner[TPB / 32][24];
+  if (idx >= count) return;
+  const int e = elems[idx];
+  const bool own = lane < NN;
+  int g = own ? b.conn[lane * b.ne + e] : 0;
+  double Xl[3] = {0, 0, 0}, ul[3] = {0, 0, 0};
+  if (own) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { Xl[k] = X[3 * g + k]; ul[k] = u[3 * g + k]; }
+  }
+  constexpr int NC = (NN == 10) ? 4 : 8;
+  if (lane < NC) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s_corner[warp][3 * lane + k] = Xl[k];
+  }
+  __syncwarp();
+  double J[9], Ji[9], detJ = 0.0;
+  if (NN == 10) {
+    tet4_jacobian(s_corner[warp], J);
+    detJ = inv3(J, Ji);
+  }
+  double fl[3] = {0, 0, 0};
+  int q0, nq;
+  quad_rule(b, e, q0, nq);
+  bool ok = true;
+  for (int q = 0; q < nq; ++q) {
+    const double xi[3] = {b.qp[3 * (q0 + q)], b.qp[3 * (q0 + q) + 1], b.qp[3 * (q0 + q) + 2]};
+    const double w = b.qw[q0 + q];
+    if (NN == 27) {
+      hex8_jacobian(s_corner[warp], xi, J);
+      detJ = inv3(J, Ji);
+    }
+    if (detJ == 0.0) { ok = false; break; }
+    double gr[3] = {0, 0, 0}, G[3] = {0, 0, 0};
+    if (own) {
+      if (NN == 10) tet10_grad(lane, xi, gr); else hex27_grad(lane, xi, gr);
+      // G = J^-T gr
+#pragma unroll
+      for (int k = 0; k < 3; ++k) G[k] = Ji[k] * gr[0] + Ji[3 + k] * gr[1] + Ji[6 + k] * gr[2];
+    }
+    // F(c,k) = delta + sum_I u_I[c] G_I[k]
+    double F[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) F[3 * c + k] = warp_sum(ul[c] * G[k]) + (c == k ? 1.0 : 0.0);
+    QpState st;
+    if (!material_state(mat.kind, F, mat.mu, mat.lambda, st, true)) { ok = false; break; }
+    if (own) {
+      double sc = w * fabs(detJ);
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        fl[i] += -(st.P[3 * i] * G[0] + st.P[3 * i + 1] * G[1] + st.P[3 * i + 2] * G[2]) * sc;
+    }
+  }
+  if (!ok) {
+    if (lane == 0) set_error(err, HOEFEM_ERR_SINGULAR);
+    return;
+  }
+  if (own) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) f[3 * g + i] += fl[i];
+  }
+}
+
+// ============================================================================
+// Stiffness + scatter.  GROUP threads own one element; the first warp of the
+// group builds the per-node vectors, all GROUP threads accumulate node pairs.
+// ============================================================================
+template <int NN>
+struct PairTable {
+  static constexpr int NP = NN * (NN + 1) / 2;
+};
+__constant__ unsigned char c_pairs10[55][2];
+__constant__ unsigned char c_pairs27[378][2];
+
+template <int NN>
+__device__ __forceinline__ void pair_of(int p, int& I, int& J) {
+  if (NN == 10) { I = c_pairs10[p][0]; J = c_pairs10[p][1]; }
+  else { I = c_pairs27[p][0]; J = c_pairs27[p][1]; }
+}
+
+template <int NN, int GROUP>
+__global__ void __launch_bounds__(TPB) k_stiffness(const BlockDev b, const int* __restrict__ elems, int count,
+                                                   const double* __restrict__ X, const double* __restrict__ u,
+                                                   const int* __restrict__ adj_off, double* __restrict__ vals,
+                                                   MatDev mat, int* err) {
+  constexpr int EPC = TPB / GROUP;                 // elements per CTA
+  constexpr int NP = PairTable<NN>::NP;            // node pairs I >= J
+  constexpr int PPT = (NP + GROUP - 1) / GROUP;    // pairs per thread
+  const int grp = threadIdx.x / GROUP, t = threadIdx.x % GROUP;
+  const int lane = threadIdx.x & 31;
+  const int idx = blockIdx.x * EPC + grp;
+  __shared__ double s_vec[EPC][NN][9];
+  __shared__ double s_corner[EPC][24];
+  __shared__ QpState s_q[EPC];
+  __shared__ int s_g[EPC][NN];
+  __shared__ int s_ok[EPC];
+  const bool active = idx < count;
+  const int e = active ? elems[idx] : 0;
+  const bool nodewarp = (t < 32);
+  const bool own = nodewarp && lane < NN && active;
+  int g = own ? b.conn[lane * b.ne + e] : 0;
+  double Xl[3] = {0, 0, 0}, ul[3] = {0, 0, 0};
+  if (own) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { Xl[k] = X[3 * g + k]; ul[k] = u[3 * g + k]; }
+    s_g[grp][lane] = g;
+  }
+  constexpr int NC = (NN == 10) ? 4 : 8;
+  if (own && lane < NC) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s_corner[grp][3 * lane + k] = Xl[k];
+  }
+  if (t == 0) s_ok[grp] = 1;
+  __syncthreads();
+  double J[9], Ji[9], detJ = 0.0;
+  if (NN == 10) {
+    tet4_jacobian(s_corner[grp], J);
+    detJ = inv3(J, Ji);
+  }
+  double acc[PPT][9];
+#pragma unroll
+  for (int k = 0; k < PPT; ++k)
+#pragma unroll
+    for (int m = 0; m < 9; ++m) acc[k][m] = 0.0;
+  int q0 = 0, nq = 0;
+  if (active) quad_rule(b, e, q0, nq);
+  // uniform trip count across the CTA: the max over its elements
+  __shared__ int s_nq[EPC];
+  if (t == 0) s_nq[grp] = nq;
+  __syncthreads();
+  int nq_max = 0;
+#pragma unroll
+  for (int k = 0; k < EPC; ++k) nq_max = max(nq_max, s_nq[k]);
+  for (int q = 0; q < nq_max; ++q) {
+    const bool live = q < nq;
+    if (nodewarp && live) {
+      const double xi[3] = {b.qp[3 * (q0 + q)], b.qp[3 * (q0 + q) + 1], b.qp[3 * (q0 + q) + 2]};
+      const double w = b.qw[q0 + q];
+      if (NN == 27) {
+        hex8_jacobian(s_corner[grp], xi, J);
+        detJ = inv3(J, Ji);
+      }
+      double gr[3] = {0, 0, 0}, G[3] = {0, 0, 0};
+      if (lane < NN) {
+        if (NN == 10) tet10_grad(lane, xi, gr); else hex27_grad(lane, xi, gr);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) G[k] = Ji[k] * gr[0] + Ji[3 + k] * gr[1] + Ji[6 + k] * gr[2];
+      }
+      double F[9];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[3 * c + k] = warp_sum(ul[c] * G[k]) + (c == k ? 1.0 : 0.0);
+      QpState st;
+      bool okq = (detJ != 0.0) && material_state(mat.kind, F, mat.mu, mat.lambda, st, false);
+      if (!okq) {
+        if (lane == 0) s_ok[grp] = 0;
+      } else if (lane < NN) {
+        double sc = sqrt(w * fabs(detJ));
+        double a[3] = {G[0] * sc, G[1] * sc, G[2] * sc};
+        double* v = s_vec[grp][lane];
+        v[0] = a[0]; v[1] = a[1]; v[2] = a[2];
+        mat3vec(st.F, a, v + 3);
+        mat3vec(st.M1, a, v + 6);
+      }
+      if (lane == 0) s_q[grp] = st;
+    }
+    __syncthreads();
+    if (live) {
+      const QpState& st = s_q[grp];
+#pragma unroll
+      for (int k = 0; k < PPT; ++k) {
+        int p = t + k * GROUP;
+        if (p < NP) {
+          int I, Jn;
+          pair_of<NN>(p, I, Jn);
+          pair_block(mat.kind, st, s_vec[grp][I], s_vec[grp][Jn], acc[k]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!active) return;
+  if (!s_ok[grp]) {
+    if (t == 0) set_error(err, HOEFEM_ERR_SINGULAR);
+    return;
+  }
+  const int* em = b.emap + (size_t)e * NN * NN;
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    int p = t + k * GROUP;
+    if (p < NP) {
+      int I, Jn;
+      pair_of<NN>(p, I, Jn);
+      int gI = s_g[grp][I], gJ = s_g[grp][Jn];
+      int rlI = 3 * (adj_off[gI + 1] - adj_off[gI]);
+      int bIJ = em[I * NN + Jn];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) vals[bIJ + i * rlI + j] += acc[k][3 * i + j];
+      if (I != Jn) {
+        int rlJ = 3 * (adj_off[gJ + 1] - adj_off[gJ]);
+        int bJI = em[Jn * NN + I];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) vals[bJI + j * rlJ + i] += acc[k][3 * i + j];
+      }
+    }
+  }
+}
+
+// ============================================================================
+// Mass: warp per element, scalar mass m_IJ = sum rho |det J| w phi_I phi_J
+// replicated on the three components (assembly.rs:624-671).
+// ============================================================================
+template <int NN>
+__global__ void __launch_bounds__(TPB) k_mass(const BlockDev b, const int* __restrict__ elems, int count,
+                                              const double* __restrict__ X, const int* __restrict__ adj_off,
+                                              double* __restrict__ vals, double density, int* err) {
+  constexpr int NE = NN * NN;
+  constexpr int EPT = (NE + 31) / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int idx = blockIdx.x * (TPB / 32) + warp;
+  __shared__ double s_corner[TPB / 32][24];
+  __shared__ double s_phi[TPB / 32][32];
+  __shared__ int s_g[TPB / 32][32];
+  if (idx >= count) return;
+  const int e = elems[idx];
+  int g = lane < NN ? b.conn[lane * b.ne + e] : 0;
+  s_g[warp][lane] = g;
+  constexpr int NC = (NN == 10) ? 4 : 8;
+  if (lane < NC)
+    for (int k = 0; k < 3; ++k) s_corner[warp][3 * lane + k] = X[3 * g + k];
+  __syncwarp();
+  double acc[EPT];
+#pragma unroll
+  for (int k = 0; k < EPT; ++k) acc[k] = 0.0;
+  double J[9];
+  int q0, nq;
+  quad_rule(b, e, q0, nq);
+  for (int q = 0; q < nq; ++q) {
+    const double xi[3] = {b.qp[3 * (q0 + q)], b.qp[3 * (q0 + q) + 1], b.qp[3 * (q0 + q) + 2]};
+    const double w = b.qw[q0 + q];
+    if (NN == 10) tet4_jacobian(s_corner[warp], J); else hex8_jacobian(s_corner[warp], xi, J);
+    double dJ = det3(J);
+    if (lane < NN) s_phi[warp][lane] = (NN == 10) ? tet10_phi(lane, xi) : hex27_phi(lane, xi);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < EPT; ++k) {
+      int p = lane + 32 * k;
+      if (p < NE) {
+        int I = p / NN, Jn = p % NN;
+        acc[k] += density * fabs(dJ) * w * s_phi[warp][I] * s_phi[warp][Jn];
+      }
+    }
+    __syncwarp();
+  }
+  const int* em = b.emap + (size_t)e * NE;
+#pragma unroll
+  for (int k = 0; k < EPT; ++k) {
+    int p = lane + 32 * k;
+    if (p < NE) {
+      int I = p / NN, Jn = p % NN;
+      int gI = s_g[warp][I];
+      int rl = 3 * (adj_off[gI + 1] - adj_off[gI]);
+      int base = em[p];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) vals[base + c * rl + c] += acc[k];
+    }
+  }
+  (void)err;
+}
+
+bool g_pairs_ready = false;
+void init_pairs() {
+  if (g_pairs_ready) return;
+  unsigned char p10[55][2], p27[378][2];
+  int k = 0;
+  for (int J = 0; J < 10; ++J)
+    for (int I = J; I < 10; ++I) { p10[k][0] = (unsigned char)I; p10[k][1] = (unsigned char)J; ++k; }
+  k = 0;
+  for (int J = 0; J < 27; ++J)
+    for (int I = J; I < 27; ++I) { p27[k][0] = (unsigned char)I; p27[k][1] = (unsigned char)J; ++k; }
+  HOEFEM_CUDA(cudaMemcpyToSymbol(c_pairs10, p10, sizeof(p10)));
+  HOEFEM_CUDA(cudaMemcpyToSymbol(c_pairs27, p27, sizeof(p27)));
+  g_pairs_ready = true;
+}
+
+template <class F>
+void for_each_color(const Block& blk, F&& fn) {
+  const int nc = (int)blk.color_off.size() - 1;
+  for (int c = 0; c < nc; ++c) {
+    int begin = (int)blk.color_off[c];
+    int cnt = (int)(blk.color_off[c + 1] - begin);
+    if (cnt > 0) fn(blk.d_color_elems.p + begin, cnt);
+  }
+}
+
+}  // namespace
+
+void launch_forces(const Model& m, const MatDev& mat, const double* u, double* f, cudaStream_t s) {
+  for (const Block* bp : m.blocks) {
+    BlockDev bd = bp->dev();
+    for_each_color(*bp, [&](const int* elems, int cnt) {
+      int grid = (cnt + TPB / 32 - 1) / (TPB / 32);
+      if (bp->kind == HOEFEM_ELEM_TET10)
+        k_forces<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p);
+      else
+        k_forces<27><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p);
+    });
+  }
+  HOEFEM_CUDA(cudaGetLastError());
+}
+
+void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s) {
+  init_pairs();
+  for (const Block* bp : m.blocks) {
+    BlockDev bd = bp->dev();
+    for_each_color(*bp, [&](const int* elems, int cnt) {
+      if (bp->kind == HOEFEM_ELEM_TET10) {
+        int grid = (cnt + TPB / 32 - 1) / (TPB / 32);
+        k_stiffness<10, 32><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p, vals, mat, m.d_err.p);
+      } else {
+        k_stiffness<27, TPB><<<cnt, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p, vals, mat, m.d_err.p);
+      }
+    });
+  }
+  HOEFEM_CUDA(cudaGetLastError());
+}
+
+void launch_mass(const Model& m, double density, double* vals, cudaStream_t s) {
+  for (const Block* bp : m.blocks) {
+    BlockDev bd = bp->dev();
+    for_each_color(*bp, [&](const int* elems, int cnt) {
+      int grid = (cnt + TPB / 32 - 1) / (TPB / 32);
+      if (bp->kind == HOEFEM_ELEM_TET10)
+        k_mass<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, m.d_adj_off.p, vals, density, m.d_err.p);
+      else
+        k_mass<27><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, m.d_adj_off.p, vals, density, m.d_err.p);
+    });
+  }
+  HOEFEM_CUDA(cudaGetLastError());
+}
+
+}  // namespace hoefem

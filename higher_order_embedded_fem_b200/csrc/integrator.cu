@@ -1,0 +1,363 @@
+// Newton-CG backward Euler integrator.
+//
+// Reference: NewtonCgIntegrator3d / integrate_model_with_substeps /
+// integrate_model / NewtonCgDynamicSystem (simulation_toolbox/src/fem/
+// newton_cg.rs:43-295,413-802), backward_euler_step +
+// BackwardEulerImplicitFunction (hamilton2/src/integrators/euler.rs:76-199),
+// newton_line_search + BacktrackingLineSearch (hamilton2/src/newton.rs:
+// 76-248), system_assembly.rs:30-235, fe_model.rs:423-431,489-515.
+//
+// The control flow (Newton iterations, line-search trials, substep retries)
+// stays on the host, as in the reference; every vector / matrix operation is
+// a device kernel on the model's stream.  Host round trips per Newton
+// iteration: one norm per residual evaluation and one state read per CG chunk.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <memory>
+
+#include "internal.h"
+#include "kernels_common.cuh"
+#include "solver.h"
+
+namespace hoefem {
+
+int spmv_grid(int nv);
+
+namespace {
+
+constexpr int TPB = 256;
+
+__global__ void k_be_init(int n, const double* __restrict__ u, const double* __restrict__ v, double dt,
+                          double* __restrict__ up, double* __restrict__ vn, double* __restrict__ w) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    vn[i] = v[i];
+    up[i] = u[i] + v[i] * dt;
+    w[i] = 0.0;
+  }
+}
+
+// u = u_p + dt w, v = v_n + w, Dirichlet values (homogeneous) applied.
+__global__ void k_be_state(int n, const double* __restrict__ up, const double* __restrict__ vn,
+                           const double* __restrict__ w, double dt, const unsigned char* __restrict__ bc,
+                           double* __restrict__ us, double* __restrict__ vs) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double uu = up[i] + w[i] * dt, vv = vn[i] + w[i];
+    if (bc && bc[i]) { uu = 0.0; vv = 0.0; }
+    us[i] = uu;
+    vs[i] = vv;
+  }
+}
+
+__global__ void k_copy(int n, const double* __restrict__ a, double* __restrict__ b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
+}
+
+// F = -dt * f with Dirichlet rows of f zeroed first (eval_f + eval_into)
+__global__ void k_F(int n, const double* __restrict__ f, const unsigned char* __restrict__ bc, double dt,
+                    double* __restrict__ F) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double fi = (bc && bc[i]) ? 0.0 : f[i];
+    F[i] = fi * (dt * -1.0);
+  }
+}
+
+__global__ void k_zero_bc(int n, const unsigned char* __restrict__ bc, double* __restrict__ f) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (bc[i]) f[i] = 0.0;
+}
+
+__global__ void k_axpy_w(int n, double da, const double* __restrict__ dx, double* __restrict__ w) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) w[i] = da * dx[i] + 1.0 * w[i];
+}
+
+__global__ void k_neg(int n, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] *= -1.0;
+}
+
+__global__ void k_be_final(int n, const double* __restrict__ w, double dt, const unsigned char* __restrict__ bc,
+                           double* __restrict__ u, double* __restrict__ v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double vv = v[i] + w[i];
+    double uu = u[i] + vv * dt;
+    if (bc && bc[i]) { uu = 0.0; vv = 0.0; }
+    v[i] = vv;
+    u[i] = uu;
+  }
+}
+
+__global__ void k_bc_uv(int n, const unsigned char* __restrict__ bc, double* __restrict__ u, double* __restrict__ v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (bc[i]) { u[i] = 0.0; v[i] = 0.0; }
+}
+
+__global__ void k_fill(int n, double v, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = v;
+}
+
+__global__ void k_gravity_density(int n, double g, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = (i % 3 == 2) ? g : 0.0;
+}
+
+}  // namespace
+
+struct Integrator {
+  Model* m = nullptr;
+  MatDev mat{};
+  double density = 1000.0;
+  std::vector<i64> bc_nodes;
+  bool gravity_enabled = true;
+  double gravity = -9.81;
+  Precond* P = nullptr;
+  std::unique_ptr<Precond> own;
+  double cg_tol = 1e-5;
+  i64 cg_max = 500, newton_max = 100;
+  double rep_force = 0.0;
+  DBuf<unsigned char> bc;
+  DBuf<double> M, K, J, gforce, up, vn, w, F, dx, us, vs, f, u, v, partials, scalars;
+  DBuf<unsigned> counter;
+  double* h_scalar = nullptr;
+  CgWork cg;
+  hoefem_step_stats stats{};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+
+  ~Integrator() {
+    if (h_scalar) cudaFreeHost(h_scalar);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+
+  int grid() const { return reduce_blocks_for(m->ndof); }
+
+  double norm_sq(const double* a) {
+    dot_device(a, a, m->ndof, scalars.p, partials.p, counter.p, m->stream);
+    HOEFEM_CUDA(cudaMemcpyAsync(h_scalar, scalars.p, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    HOEFEM_CUDA(cudaStreamSynchronize(m->stream));
+    return *h_scalar;
+  }
+
+  void setup() {
+    cudaStream_t s = m->stream;
+    const int n = (int)m->ndof;
+    bc.alloc(n);
+    std::vector<unsigned char> hb(n, 0);
+    for (i64 a : bc_nodes) {
+      HOEFEM_REQUIRE(a >= 0 && a < m->nv, HOEFEM_ERR_INVALID_ARGUMENT, "boundary node out of range");
+      for (int i = 0; i < 3; ++i) hb[3 * a + i] = 1;
+    }
+    HOEFEM_CUDA(cudaMemcpyAsync(bc.p, hb.data(), n, cudaMemcpyHostToDevice, s));
+    for (auto* b : {&M, &K, &J}) b->alloc(m->nnz);
+    for (auto* b : {&gforce, &up, &vn, &w, &F, &dx, &us, &vs, &f, &u, &v}) b->alloc(n);
+    partials.alloc(4 * 148 * 16);
+    scalars.alloc(8);
+    counter.alloc(1);
+    counter.zero(s);
+    HOEFEM_CUDA(cudaMallocHost(&h_scalar, 8 * sizeof(double)));
+    for (auto& e : ev) HOEFEM_CUDA(cudaEventCreate(&e));
+    cg.init(m);
+    // mass matrix with Dirichlet (fe_model.rs:489-515)
+    K.zero(s);
+    launch_mass(*m, density, K.p, s);
+    jacobian_combination(*m, 0.0, nullptr, 1.0, K.p, bc_nodes.empty() ? nullptr : bc.p, M.p, scalars.p, s);
+    check_device_error(*m);
+    // representative force ||M a||, a_i = sqrt(a^2 / 3), a = 10 (fe_model.rs:423-431)
+    k_fill<<<grid(), TPB, 0, s>>>(n, std::sqrt((10.0 * 10.0) / 3.0), us.p);
+    spmv_node_rows(m->rows(), M.p, us.p, vs.p, 1.0, 0.0, s);
+    rep_force = std::sqrt(norm_sq(vs.p));
+    // gravity force M g (system_assembly.rs:30-75, newton_cg.rs:248-255)
+    if (gravity_enabled) k_gravity_density<<<grid(), TPB, 0, s>>>(n, gravity, us.p);
+    else k_fill<<<grid(), TPB, 0, s>>>(n, 0.0, us.p);
+    spmv_node_rows(m->rows(), M.p, us.p, gforce.p, 1.0, 0.0, s);
+    HOEFEM_CUDA(cudaStreamSynchronize(s));
+    if (!P) {
+      own.reset(new Precond());
+      own->kind = PREC_DIAGONAL;
+      own->m = m;
+      P = own.get();
+    }
+  }
+
+  float elapsed() {
+    float ms = 0.f;
+    HOEFEM_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    return ms;
+  }
+
+  // f = M g + f_int(u) with Dirichlet rows zeroed (eval_f, newton_cg.rs:441-478)
+  void eval_f(const double* ud, const double* vd, double* out) {
+    cudaStream_t s = m->stream;
+    const int n = (int)m->ndof;
+    k_copy<<<grid(), TPB, 0, s>>>(n, ud, us.p);
+    k_copy<<<grid(), TPB, 0, s>>>(n, vd, vs.p);
+    if (!bc_nodes.empty()) k_bc_uv<<<grid(), TPB, 0, s>>>(n, bc.p, us.p, vs.p);
+    k_copy<<<grid(), TPB, 0, s>>>(n, gforce.p, out);
+    launch_forces(*m, mat, us.p, out, s);
+    if (!bc_nodes.empty()) k_zero_bc<<<grid(), TPB, 0, s>>>(n, bc.p, out);
+    check_device_error(*m);
+  }
+
+  // F(w) = M w - dt f(t + dt, u_p + dt w, v_n + w); returns ||F||^2
+  double eval_F(double dt) {
+    cudaStream_t s = m->stream;
+    const int n = (int)m->ndof;
+    const unsigned char* bcp = bc_nodes.empty() ? nullptr : bc.p;
+    HOEFEM_CUDA(cudaEventRecord(ev[0], s));
+    k_be_state<<<grid(), TPB, 0, s>>>(n, up.p, vn.p, w.p, dt, bcp, us.p, vs.p);
+    k_copy<<<grid(), TPB, 0, s>>>(n, gforce.p, f.p);
+    launch_forces(*m, mat, us.p, f.p, s);
+    HOEFEM_CUDA(cudaEventRecord(ev[1], s));
+    k_F<<<grid(), TPB, 0, s>>>(n, f.p, bcp, dt, F.p);
+    spmv_node_rows(m->rows(), M.p, w.p, F.p, 1.0, 1.0, s);
+    double r = norm_sq(F.p);
+    stats.ms_assemble_forces += elapsed();
+    check_device_error(*m);
+    return r;
+  }
+
+  int solve_jacobian(double dt) {
+    cudaStream_t s = m->stream;
+    const int n = (int)m->ndof;
+    const unsigned char* bcp = bc_nodes.empty() ? nullptr : bc.p;
+    HOEFEM_CUDA(cudaEventRecord(ev[0], s));
+    k_be_state<<<grid(), TPB, 0, s>>>(n, up.p, vn.p, w.p, dt, bcp, us.p, vs.p);
+    K.zero(s);
+    launch_stiffness(*m, mat, us.p, K.p, s);
+    // J = gamma M - beta D - alpha K with alpha = -dt^2, gamma = 1, no damping
+    jacobian_combination(*m, -(-dt * dt), K.p, 1.0, M.p, bcp, J.p, scalars.p + 4, s);
+    HOEFEM_CUDA(cudaEventRecord(ev[1], s));
+    check_device_error(*m);
+    stats.ms_assemble_stiffness += elapsed();
+    HOEFEM_CUDA(cudaEventRecord(ev[0], s));
+    precond_update(*P, J.p, s);
+    HOEFEM_CUDA(cudaEventRecord(ev[1], s));
+    HOEFEM_CUDA(cudaEventSynchronize(ev[1]));
+    stats.ms_precond_update += elapsed();
+    HOEFEM_CUDA(cudaMemsetAsync(cg.x.p, 0, sizeof(double) * n, s));
+    k_copy<<<grid(), TPB, 0, s>>>(n, F.p, cg.b.p);
+    i64 it = 0;
+    HOEFEM_CUDA(cudaEventRecord(ev[0], s));
+    int st = cg_solve(cg, J.p, P, cg_tol, cg_max, &it, s);
+    HOEFEM_CUDA(cudaEventRecord(ev[1], s));
+    HOEFEM_CUDA(cudaEventSynchronize(ev[1]));
+    stats.ms_cg += elapsed();
+    stats.num_cg_solves += 1;
+    stats.total_cg_iterations += it;
+    if (it > stats.max_cg_iterations) stats.max_cg_iterations = it;
+    stats.last_cg_status = st;
+    k_copy<<<grid(), TPB, 0, s>>>(n, cg.x.p, dx.p);
+    // MaxIterationsReached and IndefiniteOperator are tolerated (newton_cg.rs:776-797)
+    if (st == HOEFEM_OK || st == HOEFEM_CG_MAX_ITERATIONS || st == HOEFEM_CG_INDEFINITE_OPERATOR) return HOEFEM_OK;
+    return st;
+  }
+
+  int be_step(double dt) {
+    cudaStream_t s = m->stream;
+    const int n = (int)m->ndof;
+    k_be_init<<<grid(), TPB, 0, s>>>(n, u.p, v.p, dt, up.p, vn.p, w.p);
+    const double tol = dt * (1e-5 * rep_force);
+    double fsq = eval_F(dt);
+    i64 iter = 0;
+    while (std::sqrt(fsq) > tol) {
+      if (iter == newton_max) return HOEFEM_NEWTON_MAX_ITERATIONS;
+      int st = solve_jacobian(dt);
+      if (st != HOEFEM_OK) return st;
+      k_neg<<<grid(), TPB, 0, s>>>(n, dx.p);
+      const double c = 1e-4, alpha_min = 1e-6;
+      const double g0 = 0.5 * fsq;
+      const double initial[4] = {0.0, 1.0, 0.75, 0.5};
+      double alpha_prev = 0.0, alpha = 1.0, tail = 0.25;
+      int k = 1;
+      for (;;) {
+        k_axpy_w<<<grid(), TPB, 0, s>>>(n, alpha - alpha_prev, dx.p, w.p);
+        fsq = eval_F(dt);
+        double g = 0.5 * fsq;
+        if (g <= (1.0 - c * alpha) * g0) break;
+        if (alpha < alpha_min) return HOEFEM_LINE_SEARCH_FAILED;
+        alpha_prev = alpha;
+        ++k;
+        if (k < 4) alpha = initial[k];
+        else { alpha = tail; tail *= 0.25; }
+      }
+      ++iter;
+    }
+    stats.newton_iterations = iter;
+    stats.residual_norm = std::sqrt(fsq);
+    k_be_final<<<grid(), TPB, 0, s>>>(n, w.p, dt, bc_nodes.empty() ? nullptr : bc.p, u.p, v.p);
+    HOEFEM_CUDA(cudaGetLastError());
+    return HOEFEM_OK;
+  }
+
+  // integrate_model_with_substeps: u, v device pointers (length ndof)
+  int step(double* ud, double* vd, double t, double dt) {
+    (void)t;
+    cudaStream_t s = m->stream;
+    const int n = (int)m->ndof;
+    stats = hoefem_step_stats{};
+    stats.representative_force = rep_force;
+    cudaEvent_t t0, t1;
+    HOEFEM_CUDA(cudaEventCreate(&t0));
+    HOEFEM_CUDA(cudaEventCreate(&t1));
+    HOEFEM_CUDA(cudaEventRecord(t0, s));
+    if (!bc_nodes.empty()) k_bc_uv<<<grid(), TPB, 0, s>>>(n, bc.p, ud, vd);
+    i64 num = 1;
+    int result = HOEFEM_OK;
+    for (;;) {
+      k_copy<<<grid(), TPB, 0, s>>>(n, ud, u.p);
+      k_copy<<<grid(), TPB, 0, s>>>(n, vd, v.p);
+      double sdt = dt / (double)num;
+      bool failed = false;
+      for (i64 k = 0; k < num; ++k) {
+        int r;
+        try {
+          r = be_step(sdt);
+        } catch (Error& e) {
+          if (e.code == HOEFEM_ERR_CUDA || e.code == HOEFEM_ERR_OUT_OF_MEMORY) throw;
+          r = e.code;
+        }
+        if (r != HOEFEM_OK) { failed = true; result = r; break; }
+      }
+      if (!failed) { result = HOEFEM_OK; break; }
+      num *= 5;
+      if (num >= 1000) { result = HOEFEM_SUBSTEPPING_FAILED; break; }
+    }
+    stats.substeps = num;
+    if (result == HOEFEM_OK) {
+      k_copy<<<grid(), TPB, 0, s>>>(n, u.p, ud);
+      k_copy<<<grid(), TPB, 0, s>>>(n, v.p, vd);
+    }
+    HOEFEM_CUDA(cudaEventRecord(t1, s));
+    HOEFEM_CUDA(cudaEventSynchronize(t1));
+    float ms = 0.f;
+    HOEFEM_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    stats.ms_total = ms;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return result;
+  }
+};
+
+Integrator* integrator_new(Model* m, const hoefem_material* mat, double density, const i64* bc_nodes, i64 nbc,
+                           int gravity_enabled, double gravity, Precond* P) {
+  std::unique_ptr<Integrator> it(new Integrator());
+  it->m = m;
+  it->mat = MatDev{mat->kind, mat->mu, mat->lambda};
+  it->density = density;
+  it->bc_nodes.assign(bc_nodes, bc_nodes + nbc);
+  it->gravity_enabled = gravity_enabled != 0;
+  it->gravity = gravity;
+  it->P = P;
+  it->setup();
+  return it.release();
+}
+void integrator_delete(Integrator* it) { delete it; }
+void integrator_set_tolerances(Integrator* it, double tol, i64 cg_max, i64 newton_max) {
+  it->cg_tol = tol;
+  it->cg_max = cg_max;
+  it->newton_max = newton_max;
+}
+int integrator_step(Integrator* it, double* ud, double* vd, double t, double dt) { return it->step(ud, vd, t, dt); }
+hoefem_step_stats integrator_stats(Integrator* it) { return it->stats; }
+const double* integrator_mass(Integrator* it) { return it->M.p; }
+void integrator_eval_f(Integrator* it, const double* ud, const double* vd, double* f) { it->eval_f(ud, vd, f); }
+
+}  // namespace hoefem

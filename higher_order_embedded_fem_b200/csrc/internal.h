@@ -1,0 +1,157 @@
+// Internal declarations shared by the libhoefem sources (host + device).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "hoefem.h"
+
+namespace hoefem {
+
+using i64 = int64_t;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define HOEFEM_CUDA(x)                                                                                   \
+  do {                                                                                                   \
+    cudaError_t e_ = (x);                                                                                \
+    if (e_ != cudaSuccess)                                                                               \
+      throw ::hoefem::Error(e_ == cudaErrorMemoryAllocation ? HOEFEM_ERR_OUT_OF_MEMORY : HOEFEM_ERR_CUDA, \
+                            std::string(#x) + ": " + cudaGetErrorString(e_));                            \
+  } while (0)
+
+#define HOEFEM_REQUIRE(cond, code, msg) \
+  do {                                  \
+    if (!(cond)) throw ::hoefem::Error((code), (msg)); \
+  } while (0)
+
+// Device buffer owned by a handle (plain cudaMalloc, freed on destruction).
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    release();
+    if (count == 0) count = 1;
+    HOEFEM_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void upload(const T* h, size_t count, cudaStream_t s) {
+    alloc(count);
+    if (count) HOEFEM_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void upload(const std::vector<T>& h, cudaStream_t s) { upload(h.data(), h.size(), s); }
+  void zero(cudaStream_t s) {
+    if (n) HOEFEM_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+};
+
+// Node-row description of a CSR matrix whose three rows per node share the
+// same column structure, with three consecutive columns per neighbour node:
+// entry (3a+i, 3b+j) is at base[a] + i * 3 * deg(a) + 3 * slot(b in adj(a)) + j.
+// Rows of `diag_only` nodes hold a single diagonal entry each (base[a] + i).
+struct NodeRows {
+  int nv = 0;
+  const long long* base = nullptr;  // row_offsets[3a]
+  const int* adj_off = nullptr;     // nv + 1
+  const int* adj = nullptr;         // sorted neighbour nodes
+  const int* diag_slot = nullptr;   // slot of a in adj(a) (-1 for diag_only nodes)
+  const unsigned char* diag_only = nullptr;  // may be null
+};
+
+// Per-block device data.
+struct BlockDev {
+  int kind = 0;     // HOEFEM_ELEM_*
+  int nn = 0;       // nodes per element
+  int ne = 0;
+  const int* conn = nullptr;   // SoA: conn[I * ne + e]
+  int uniform = 1;
+  int nq = 0;                  // points of the uniform rule
+  const int* qoff = nullptr;   // ne + 1 (non-uniform)
+  const double* qw = nullptr;
+  const double* qp = nullptr;  // xyz interleaved
+  const int* emap = nullptr;   // [e * nn * nn + I * nn + J] = nnz index of (3 gI, 3 gJ)
+};
+
+struct Block {
+  int kind = 0, nn = 0;
+  i64 ne = 0;
+  std::vector<i64> conn;  // row-major ne x nn (host)
+  bool uniform = true;
+  std::vector<i64> qoff;
+  std::vector<double> qw, qp;
+  std::vector<i64> color_off;   // ncolors + 1
+  std::vector<int> color_elems;  // elements ordered by color
+  DBuf<int> d_conn, d_qoff, d_emap, d_color_elems;
+  DBuf<double> d_qw, d_qp;
+  BlockDev dev() const;
+};
+
+struct Model {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  i64 nv = 0;
+  std::vector<double> X;
+  std::vector<Block*> blocks;
+  bool finalized = false;
+  bool on_device = false;
+  i64 ndof = 0, nnz = 0, num_elements = 0;
+  // node structure of the shared pattern (host)
+  std::vector<int> adj_off, adj, diag_slot;
+  std::vector<long long> base;
+  // device
+  DBuf<double> d_X;
+  DBuf<int> d_adj_off, d_adj, d_diag_slot, d_err;
+  DBuf<long long> d_base;
+  NodeRows rows() const;
+  ~Model();
+};
+
+struct MatDev {
+  int kind;
+  double mu, lambda;
+};
+
+// ---- element kernels (elements.cu) -----------------------------------------
+void launch_forces(const Model& m, const MatDev& mat, const double* u, double* f, cudaStream_t s);
+void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s);
+void launch_mass(const Model& m, double density, double* vals, cudaStream_t s);
+
+// ---- sparse / vector kernels (linalg.cu) -----------------------------------
+// y = beta*y + alpha*A x on a node-row matrix.
+void spmv_node_rows(const NodeRows& A, const double* vals, const double* x, double* y, double alpha, double beta,
+                    cudaStream_t s);
+// Fills out = c_k * K + c_m * M (either may be null) and applies homogeneous
+// Dirichlet rows / columns for the dof mask (may be null).
+void jacobian_combination(const Model& m, double ck, const double* K, double cm, const double* M,
+                          const unsigned char* bc_dof, double* out, double* d_scratch, cudaStream_t s);
+// Deterministic reductions: result written to *out (device).
+void dot_device(const double* a, const double* b, i64 n, double* out, double* partials, unsigned* counter,
+                cudaStream_t s);
+int reduce_blocks_for(i64 n);
+
+void finalize_model(Model& m);
+void ensure_device(Model& m);
+void export_pattern(const std::vector<int>& adj_off, const std::vector<int>& adj, const std::vector<long long>& base,
+                    const std::vector<unsigned char>* diag_only, i64 nv, int64_t* ro, int64_t* ci);
+
+// ---- errors ----------------------------------------------------------------
+void check_device_error(const Model& m);  // reads and clears d_err
+
+}  // namespace hoefem

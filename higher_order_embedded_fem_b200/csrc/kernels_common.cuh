@@ -1,0 +1,112 @@
+// Device helpers shared by the sparse, CG and Schwarz kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace hoefem {
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Three row sums of node a (warp cooperative; result valid in every lane).
+__device__ __forceinline__ void node_row_dot(const NodeRows& A, const double* __restrict__ vals,
+                                             const double* __restrict__ x, int a, int lane, double& s0, double& s1,
+                                             double& s2) {
+  s0 = s1 = s2 = 0.0;
+  const long long b = A.base[a];
+  if (A.diag_only && A.diag_only[a]) {
+    if (lane == 0) {
+      s0 = vals[b] * x[3 * a];
+      s1 = vals[b + 1] * x[3 * a + 1];
+      s2 = vals[b + 2] * x[3 * a + 2];
+    }
+  } else {
+    const int o = A.adj_off[a], d = A.adj_off[a + 1] - o;
+    const long long rl = 3LL * d;
+    for (int s = lane; s < d; s += 32) {
+      const int nb = A.adj[o + s];
+      const double x0 = x[3 * nb], x1 = x[3 * nb + 1], x2 = x[3 * nb + 2];
+      const double* r0 = vals + b + 3 * s;
+      s0 += r0[0] * x0 + r0[1] * x1 + r0[2] * x2;
+      const double* r1 = r0 + rl;
+      s1 += r1[0] * x0 + r1[1] * x1 + r1[2] * x2;
+      const double* r2 = r1 + rl;
+      s2 += r2[0] * x0 + r2[1] * x1 + r2[2] * x2;
+    }
+  }
+  s0 = warp_sum_d(s0);
+  s1 = warp_sum_d(s1);
+  s2 = warp_sum_d(s2);
+}
+
+// Block sum of K values (blockDim.x multiple of 32, <= 1024); result in
+// thread 0.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K]) {
+  __shared__ double sh[K][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = warp_sum_d(v[k]);
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) sh[k][w] = v[k];
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double t = lane < nw ? sh[k][lane] : 0.0;
+      v[k] = warp_sum_d(t);
+    }
+  }
+  __syncthreads();
+}
+
+// Grid-wide deterministic reduction of K values: every block writes its
+// partials, the last block to finish sums them in block order.  Returns true
+// in the last block (all threads); `tot` is valid in its thread 0.
+template <int K>
+__device__ __forceinline__ bool grid_reduce_last_k(double (&v)[K], double* partials, unsigned* counter,
+                                                   double (&tot)[K]) {
+  __shared__ bool s_last;
+  block_sum<K>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) partials[(size_t)k * gridDim.x + blockIdx.x] = v[k];
+    __threadfence();
+    unsigned t = atomicAdd(counter, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0.0;
+  // fixed order: thread t sums blocks t, t+blockDim, ... then a tree
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] += __ldcg(partials + (size_t)k * gridDim.x + i);
+  block_sum<K>(acc);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) tot[k] = acc[k];
+    *counter = 0u;
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool grid_reduce_last(double v, double* partials, unsigned* counter, double& tot) {
+  double a[1] = {v}, t[1];
+  bool last = grid_reduce_last_k<1>(a, partials, counter, t);
+  tot = t[0];
+  return last;
+}
+
+}  // namespace hoefem

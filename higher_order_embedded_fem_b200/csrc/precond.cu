@@ -1,0 +1,437 @@
+// Preconditioners: diagonal (Jacobi) and element-wise additive Schwarz.
+//
+// Reference: DiagonalPreconditioner (simulation_toolbox/src/fem/
+// newton_cg.rs:534-593); SchwarzPreconditioner / build_preconditioner_pattern /
+// build_schwarz_preconditioner_into / SchwarzElementAssembler /
+// invert_element_block (simulation_toolbox/src/fem/schwarz_precond.rs:
+// 134-216,250-342, newton_cg.rs:297-370).
+//
+// Schwarz update on the device, in three steps:
+//  1. k_schwarz_factor: one CTA per subdomain gathers its 3n x 3n principal
+//     block of the system matrix (element-to-nnz map, no searches), runs a
+//     parallel cyclic Jacobi eigensolver in shared memory (round-robin
+//     ordering: m/2 disjoint rotations per round, rows then columns), applies
+//     the reference's spectrum rule (1/|lambda|, floor 1e-12 max|lambda|) and
+//     writes the recomposed block V f(L) V^T to a staging buffer.  All
+//     subdomains are factored in one launch.
+//  2. k_schwarz_scatter: per subdomain color (greedy coloring of the subdomain
+//     node lists, as the reference), the staged blocks are added into the
+//     preconditioner's own CSR values, so every entry receives its
+//     contributions in color order without atomics.
+//  3. k_schwarz_untreated: scalar Jacobi 1/a_ii on the untreated nodes.
+// The eigen-decomposition replaces LAPACK dsyev (nalgebra-lapack over MKL);
+// eigenpairs are not unique, the recomposed block is.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "internal.h"
+#include "kernels_common.cuh"
+#include "solver.h"
+
+namespace hoefem {
+
+void greedy_coloring(const i64* conn, i64 ne, int nn, i64 nv, std::vector<i64>& color_off,
+                     std::vector<int>& color_elems);
+void node_adjacency(i64 nv, const std::vector<const std::vector<i64>*>& conns, const std::vector<int>& nns,
+                    std::vector<int>& adj_off, std::vector<int>& adj);
+
+NodeRows Precond::rows() const {
+  NodeRows r;
+  r.nv = (int)m->nv;
+  r.base = d_base.p;
+  r.adj_off = d_adj_off.p;
+  r.adj = d_adj.p;
+  r.diag_slot = d_diag_slot.p;
+  r.diag_only = d_diag_only.p;
+  return r;
+}
+
+namespace {
+
+constexpr int FACTOR_TPB = 256;
+
+// Jacobi rotation parameters zeroing A[p][q] (same formulas as the oracle).
+__device__ __forceinline__ void jacobi_cs(double app, double aqq, double apq, double& c, double& s) {
+  if (apq == 0.0) { c = 1.0; s = 0.0; return; }
+  double theta = (aqq - app) / (2.0 * apq);
+  double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+  c = 1.0 / sqrt(t * t + 1.0);
+  s = t * c;
+}
+
+__global__ void __launch_bounds__(FACTOR_TPB) k_schwarz_factor(
+    int nsub, const int* __restrict__ sub_off, const int* __restrict__ sub_nodes, const long long* __restrict__ gmap_off,
+    const int* __restrict__ gmap, const int* __restrict__ adj_off, const double* __restrict__ J,
+    const long long* __restrict__ stage_off, double* __restrict__ stage, int* err) {
+  extern __shared__ double smem[];
+  const int sidx = blockIdx.x;
+  const int n = sub_off[sidx + 1] - sub_off[sidx];
+  const int dim = 3 * n;
+  const int m = (dim + 1) & ~1;  // even, padded with a dummy index
+  double* A = smem;              // m x m
+  double* V = A + m * m;         // m x m
+  double* cs = V + m * m;        // m/2 cosines
+  double* sn = cs + m / 2;       // m/2 sines
+  __shared__ int s_g[27];
+  __shared__ int s_rl[27];
+  __shared__ double s_red[2];
+  const int* nodes = sub_nodes + sub_off[sidx];
+  for (int I = threadIdx.x; I < n; I += blockDim.x) {
+    int g = nodes[I];
+    s_g[I] = g;
+    s_rl[I] = 3 * (adj_off[g + 1] - adj_off[g]);
+  }
+  __syncthreads();
+  // gather the principal block
+  const int* gm = gmap + gmap_off[sidx];
+  for (int k = threadIdx.x; k < m * m; k += blockDim.x) {
+    int r = k / m, c = k % m;
+    double v = 0.0;
+    if (r < dim && c < dim) {
+      int I = r / 3, i = r % 3, Jn = c / 3, j = c % 3;
+      v = J[gm[I * n + Jn] + i * s_rl[I] + j];
+    }
+    A[k] = v;
+    V[k] = (r == c) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const int half = m / 2;
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    // convergence test on the off-diagonal mass
+    double off = 0.0, tot = 0.0;
+    for (int k = threadIdx.x; k < m * m; k += blockDim.x) {
+      double x = A[k] * A[k];
+      tot += x;
+      if (k / m != k % m) off += x;
+    }
+    double vv[2] = {off, tot};
+    block_sum<2>(vv);
+    if (threadIdx.x == 0) { s_red[0] = vv[0]; s_red[1] = vv[1]; }
+    __syncthreads();
+    if (s_red[0] == 0.0 || s_red[0] <= 1e-32 * s_red[1]) break;
+    for (int round = 0; round < m - 1; ++round) {
+      for (int k = threadIdx.x; k < half; k += blockDim.x) {
+        int p, q;
+        if (k == 0) { p = round; q = m - 1; }
+        else { p = (round + k) % (m - 1); q = (round - k + (m - 1)) % (m - 1); }
+        if (p > q) { int t = p; p = q; q = t; }
+        double c = 1.0, s = 0.0;
+        if (q < dim) jacobi_cs(A[p * m + p], A[q * m + q], A[p * m + q], c, s);
+        cs[k] = c;
+        sn[k] = s;
+      }
+      __syncthreads();
+      // rows p, q of A
+      for (int it = threadIdx.x; it < half * m; it += blockDim.x) {
+        int k = it / m, j = it % m;
+        double s = sn[k];
+        if (s == 0.0) continue;
+        int p, q;
+        if (k == 0) { p = round; q = m - 1; }
+        else { p = (round + k) % (m - 1); q = (round - k + (m - 1)) % (m - 1); }
+        if (p > q) { int t = p; p = q; q = t; }
+        double c = cs[k];
+        double a = A[p * m + j], b = A[q * m + j];
+        A[p * m + j] = c * a - s * b;
+        A[q * m + j] = s * a + c * b;
+      }
+      __syncthreads();
+      // columns p, q of A and V
+      for (int it = threadIdx.x; it < half * m; it += blockDim.x) {
+        int k = it % half, i = it / half;
+        double s = sn[k];
+        if (s == 0.0) continue;
+        int p, q;
+        if (k == 0) { p = round; q = m - 1; }
+        else { p = (round + k) % (m - 1); q = (round - k + (m - 1)) % (m - 1); }
+        if (p > q) { int t = p; p = q; q = t; }
+        double c = cs[k];
+        double a = A[i * m + p], b = A[i * m + q];
+        A[i * m + p] = c * a - s * b;
+        A[i * m + q] = s * a + c * b;
+        double va = V[i * m + p], vb = V[i * m + q];
+        V[i * m + p] = c * va - s * vb;
+        V[i * m + q] = s * va + c * vb;
+      }
+      __syncthreads();
+    }
+  }
+  // spectrum rule of invert_element_block: f = 1/|l| if |l| >= 1e-12 max|l| else 1/(1e-12 max|l|)
+  double amax = 0.0;
+  for (int k = threadIdx.x; k < dim; k += blockDim.x) amax = fmax(amax, fabs(A[k * m + k]));
+  double am[1] = {amax};
+  // block max of |lambda| (warp shuffles, then the warp maxima)
+  for (int o = 16; o > 0; o >>= 1) am[0] = fmax(am[0], __shfl_xor_sync(0xffffffffu, am[0], o));
+  __shared__ double s_max[FACTOR_TPB / 32];
+  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = am[0];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mx = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mx = fmax(mx, s_max[w]);
+    s_red[0] = mx;
+  }
+  __syncthreads();
+  const double lower = 1e-12 * s_red[0];
+  for (int k = threadIdx.x; k < dim; k += blockDim.x) {
+    double l = A[k * m + k];
+    A[k * m + k] = (fabs(l) >= lower) ? 1.0 / fabs(l) : 1.0 / lower;
+  }
+  __syncthreads();
+  if (!(s_red[0] > 0.0) || !isfinite(s_red[0])) {
+    if (threadIdx.x == 0) atomicCAS(err, 0, HOEFEM_ERR_NONFINITE);
+  }
+  // recompose P = V f V^T into the staging buffer (row-major dim x dim)
+  double* out = stage + stage_off[sidx];
+  for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) {
+    int i = k / dim, j = k % dim;
+    double s = 0.0;
+    for (int t = 0; t < dim; ++t) s += V[i * m + t] * A[t * m + t] * V[j * m + t];
+    out[k] = s;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_schwarz_scatter(const int* __restrict__ subs, int count,
+                                                         const int* __restrict__ sub_off,
+                                                         const int* __restrict__ sub_nodes,
+                                                         const long long* __restrict__ gmap_off,
+                                                         const int* __restrict__ smap, const int* __restrict__ padj_off,
+                                                         const long long* __restrict__ stage_off,
+                                                         const double* __restrict__ stage, double* __restrict__ pv) {
+  const int sidx = subs[blockIdx.x];
+  const int n = sub_off[sidx + 1] - sub_off[sidx];
+  const int dim = 3 * n;
+  const int* nodes = sub_nodes + sub_off[sidx];
+  const int* sm = smap + gmap_off[sidx];
+  const double* blk = stage + stage_off[sidx];
+  for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) {
+    int r = k / dim, c = k % dim;
+    int I = r / 3, i = r % 3, Jn = c / 3, j = c % 3;
+    int g = nodes[I];
+    int rl = 3 * (padj_off[g + 1] - padj_off[g]);
+    pv[sm[I * n + Jn] + i * rl + j] += blk[k];
+  }
+}
+
+__global__ void k_schwarz_untreated(int nun, const int* __restrict__ untreated, const long long* __restrict__ pbase,
+                                    NodeRows A, const double* __restrict__ J, double* __restrict__ pv, int* err) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3 * nun) return;
+  int a = untreated[t / 3], i = t % 3;
+  double v = 0.0;
+  int s = A.diag_slot[a];
+  if (s >= 0) {
+    int d = A.adj_off[a + 1] - A.adj_off[a];
+    v = J[A.base[a] + (long long)i * 3 * d + 3 * s + i];
+  }
+  if (v != 0.0) pv[pbase[a] + i] = 1.0 / v;
+  else atomicCAS(err, 0, HOEFEM_ERR_ZERO_DIAGONAL);
+}
+
+__global__ void k_diag_inverse(NodeRows A, const double* __restrict__ J, double* __restrict__ d, int* err) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3 * A.nv) return;
+  int a = t / 3, i = t % 3;
+  double v = 0.0;
+  int s = A.diag_slot[a];
+  if (s >= 0) {
+    int dd = A.adj_off[a + 1] - A.adj_off[a];
+    v = J[A.base[a] + (long long)i * 3 * dd + 3 * s + i];
+  }
+  if (v != 0.0) d[t] = 1.0 / v;
+  else {
+    d[t] = 0.0;
+    atomicCAS(err, 0, HOEFEM_ERR_ZERO_DIAGONAL);
+  }
+}
+
+__global__ void k_mul(int n, const double* __restrict__ d, const double* __restrict__ r, double* __restrict__ z) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = d[i] * r[i];
+}
+
+__global__ void k_spmv_plain(NodeRows A, const double* __restrict__ vals, const double* __restrict__ x,
+                             double* __restrict__ y) {
+  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  for (int a = blockIdx.x * wpb + (threadIdx.x >> 5); a < A.nv; a += gridDim.x * wpb) {
+    double s0, s1, s2;
+    node_row_dot(A, vals, x, a, lane, s0, s1, s2);
+    if (lane == 0) { y[3 * a] = s0; y[3 * a + 1] = s1; y[3 * a + 2] = s2; }
+  }
+}
+
+}  // namespace
+
+int spmv_grid(int nv);
+
+void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes, i64 nsub, const i64* untreated,
+                            i64 nun) {
+  Model& m = *p.m;
+  p.kind = PREC_SCHWARZ;
+  p.nsub = nsub;
+  p.sub_off.assign(sub_off, sub_off + nsub + 1);
+  p.sub_nodes.assign(sub_nodes, sub_nodes + sub_off[nsub]);
+  p.untreated.assign(untreated, untreated + nun);
+  p.max_nodes = 0;
+  for (i64 s = 0; s < nsub; ++s) {
+    int n = (int)(sub_off[s + 1] - sub_off[s]);
+    HOEFEM_REQUIRE(n >= 1 && n <= 27, HOEFEM_ERR_INVALID_ARGUMENT, "Schwarz subdomains must have 1..27 nodes");
+    p.max_nodes = std::max(p.max_nodes, n);
+    for (i64 k = sub_off[s]; k < sub_off[s + 1]; ++k)
+      HOEFEM_REQUIRE(sub_nodes[k] >= 0 && sub_nodes[k] < m.nv, HOEFEM_ERR_INVALID_ARGUMENT, "node out of range");
+  }
+  // pattern of build_preconditioner_pattern: subdomain blocks + untreated diagonal
+  // Ragged subdomains: gather per-size groups for node_adjacency.
+  std::vector<std::vector<i64>> bysize(28);
+  for (i64 s = 0; s < nsub; ++s) {
+    int n = (int)(sub_off[s + 1] - sub_off[s]);
+    bysize[n].insert(bysize[n].end(), sub_nodes + sub_off[s], sub_nodes + sub_off[s + 1]);
+  }
+  std::vector<const std::vector<i64>*> conns;
+  std::vector<int> nns;
+  for (int n = 1; n <= 27; ++n)
+    if (!bysize[n].empty()) { conns.push_back(&bysize[n]); nns.push_back(n); }
+  node_adjacency(m.nv, conns, nns, p.adj_off, p.adj);
+  p.diag_only.assign(m.nv, 0);
+  for (i64 a : p.untreated) {
+    HOEFEM_REQUIRE(a >= 0 && a < m.nv, HOEFEM_ERR_INVALID_ARGUMENT, "untreated node out of range");
+    HOEFEM_REQUIRE(p.adj_off[a + 1] == p.adj_off[a], HOEFEM_ERR_INVALID_ARGUMENT,
+                   "untreated node belongs to a subdomain");
+    p.diag_only[a] = 1;
+  }
+  p.base.assign(m.nv + 1, 0);
+  p.diag_slot.assign(m.nv, -1);
+  for (i64 a = 0; a < m.nv; ++a) {
+    i64 d = p.adj_off[a + 1] - p.adj_off[a];
+    p.base[a + 1] = p.base[a] + (p.diag_only[a] ? 3 : 9 * d);
+    const int* b0 = p.adj.data() + p.adj_off[a];
+    const int* e0 = p.adj.data() + p.adj_off[a + 1];
+    const int* it = std::lower_bound(b0, e0, (int)a);
+    if (it != e0 && *it == a) p.diag_slot[a] = (int)(it - b0);
+  }
+  p.nnz = p.base[m.nv];
+  // gather map (system pattern) and scatter map (preconditioner pattern)
+  std::vector<long long> gmap_off(nsub + 1, 0), stage_off(nsub + 1, 0);
+  for (i64 s = 0; s < nsub; ++s) {
+    i64 n = sub_off[s + 1] - sub_off[s];
+    gmap_off[s + 1] = gmap_off[s] + n * n;
+    stage_off[s + 1] = stage_off[s] + 9 * n * n;
+  }
+  std::vector<int> gmap(gmap_off[nsub]), smap(gmap_off[nsub]);
+  for (i64 s = 0; s < nsub; ++s) {
+    i64 n = sub_off[s + 1] - sub_off[s];
+    const i64* nd = sub_nodes + sub_off[s];
+    for (i64 I = 0; I < n; ++I)
+      for (i64 J = 0; J < n; ++J) {
+        i64 a = nd[I], b = nd[J];
+        const int* m0 = m.adj.data() + m.adj_off[a];
+        const int* m1 = m.adj.data() + m.adj_off[a + 1];
+        const int* it = std::lower_bound(m0, m1, (int)b);
+        HOEFEM_REQUIRE(it != m1 && *it == b, HOEFEM_ERR_PATTERN, "subdomain block not in the system pattern");
+        gmap[gmap_off[s] + I * n + J] = (int)(m.base[a] + 3 * (it - m0));
+        const int* p0 = p.adj.data() + p.adj_off[a];
+        const int* p1 = p.adj.data() + p.adj_off[a + 1];
+        const int* jt = std::lower_bound(p0, p1, (int)b);
+        smap[gmap_off[s] + I * n + J] = (int)(p.base[a] + 3 * (jt - p0));
+      }
+  }
+  // colors of the subdomains (sequential_greedy_coloring of the node lists)
+  {
+    // ragged greedy coloring: pad to a dense layout with repeated first node
+    int mx = p.max_nodes;
+    std::vector<i64> dense(nsub * (size_t)mx);
+    for (i64 s = 0; s < nsub; ++s)
+      for (int k = 0; k < mx; ++k) {
+        i64 n = sub_off[s + 1] - sub_off[s];
+        dense[s * mx + k] = sub_nodes[sub_off[s] + std::min<i64>(k, n - 1)];
+      }
+    greedy_coloring(dense.data(), nsub, mx, m.nv, p.color_off, p.color_subs);
+  }
+  cudaStream_t st = m.stream;
+  std::vector<int> so(p.sub_off.begin(), p.sub_off.end()), sn(p.sub_nodes.begin(), p.sub_nodes.end());
+  std::vector<int> un(p.untreated.begin(), p.untreated.end());
+  p.d_sub_off.upload(so, st);
+  p.d_sub_nodes.upload(sn, st);
+  p.d_untreated.upload(un, st);
+  p.d_gmap_off.upload(gmap_off, st);
+  p.d_gmap.upload(gmap, st);
+  p.d_smap.upload(smap, st);
+  p.d_color_subs.upload(p.color_subs, st);
+  p.d_adj_off.upload(p.adj_off, st);
+  p.d_adj.upload(p.adj, st);
+  p.d_diag_slot.upload(p.diag_slot, st);
+  p.d_base.upload(p.base, st);
+  p.d_diag_only.upload(p.diag_only, st);
+  p.d_stage_off.upload(stage_off, st);
+  p.vals.alloc(p.nnz);
+  p.vals.zero(st);
+  p.staging.alloc(stage_off[nsub]);
+  p.d_err.alloc(1);
+  p.d_err.zero(st);
+  HOEFEM_CUDA(cudaStreamSynchronize(st));
+  int m_max = (3 * p.max_nodes + 1) & ~1;
+  size_t smem = (size_t)(2 * m_max * m_max + m_max) * sizeof(double);
+  HOEFEM_CUDA(cudaFuncSetAttribute(k_schwarz_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+}
+
+static void check_err(DBuf<int>& e, cudaStream_t s) {
+  int v = 0;
+  HOEFEM_CUDA(cudaMemcpyAsync(&v, e.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  HOEFEM_CUDA(cudaStreamSynchronize(s));
+  if (v) {
+    HOEFEM_CUDA(cudaMemsetAsync(e.p, 0, sizeof(int), s));
+    throw Error(v, v == HOEFEM_ERR_ZERO_DIAGONAL ? "Can not construct preconditioner: diagonal entry is zero"
+                                                 : "non-finite Schwarz block");
+  }
+}
+
+void precond_update(Precond& p, const double* J, cudaStream_t s) {
+  Model& m = *p.m;
+  NodeRows A = m.rows();
+  if (p.kind == PREC_DIAGONAL) {
+    if (p.diag.n < (size_t)m.ndof) p.diag.alloc(m.ndof);
+    if (!p.d_err.p) { p.d_err.alloc(1); p.d_err.zero(s); }
+    k_diag_inverse<<<(int)((m.ndof + 255) / 256), 256, 0, s>>>(A, J, p.diag.p, p.d_err.p);
+    HOEFEM_CUDA(cudaGetLastError());
+    check_err(p.d_err, s);
+    p.ready = true;
+    return;
+  }
+  p.vals.zero(s);
+  if (p.nsub > 0) {
+    int m_max = (3 * p.max_nodes + 1) & ~1;
+    size_t smem = (size_t)(2 * m_max * m_max + m_max) * sizeof(double);
+    k_schwarz_factor<<<(int)p.nsub, FACTOR_TPB, smem, s>>>((int)p.nsub, p.d_sub_off.p, p.d_sub_nodes.p,
+                                                           p.d_gmap_off.p, p.d_gmap.p, m.d_adj_off.p, J,
+                                                           p.d_stage_off.p, p.staging.p, p.d_err.p);
+    HOEFEM_CUDA(cudaGetLastError());
+    const int nc = (int)p.color_off.size() - 1;
+    for (int c = 0; c < nc; ++c) {
+      int b = (int)p.color_off[c], cnt = (int)(p.color_off[c + 1] - b);
+      if (cnt)
+        k_schwarz_scatter<<<cnt, 256, 0, s>>>(p.d_color_subs.p + b, cnt, p.d_sub_off.p, p.d_sub_nodes.p,
+                                              p.d_gmap_off.p, p.d_smap.p, p.d_adj_off.p, p.d_stage_off.p,
+                                              p.staging.p, p.vals.p);
+    }
+  }
+  if (!p.untreated.empty())
+    k_schwarz_untreated<<<(int)((3 * p.untreated.size() + 255) / 256), 256, 0, s>>>(
+        (int)p.untreated.size(), p.d_untreated.p, p.d_base.p, A, J, p.vals.p, p.d_err.p);
+  HOEFEM_CUDA(cudaGetLastError());
+  check_err(p.d_err, s);
+  p.ready = true;
+}
+
+void precond_apply(const Precond& p, const double* r, double* z, cudaStream_t s) {
+  HOEFEM_REQUIRE(p.ready, HOEFEM_ERR_INVALID_ARGUMENT, "preconditioner has not been updated");
+  if (p.kind == PREC_DIAGONAL) {
+    int n = (int)p.m->ndof;
+    k_mul<<<reduce_blocks_for(n), 256, 0, s>>>(n, p.diag.p, r, z);
+  } else {
+    NodeRows PR = p.rows();
+    k_spmv_plain<<<spmv_grid(PR.nv), 256, 0, s>>>(PR, p.vals.p, r, z);
+  }
+  HOEFEM_CUDA(cudaGetLastError());
+}
+
+}  // namespace hoefem

@@ -1,0 +1,64 @@
+// Preconditioner and CG declarations (internal).
+#pragma once
+
+#include "internal.h"
+
+namespace hoefem {
+
+enum PrecondKind { PREC_NONE = 0, PREC_DIAGONAL = 1, PREC_SCHWARZ = 2 };
+
+struct Precond {
+  int kind = PREC_DIAGONAL;
+  Model* m = nullptr;
+  bool ready = false;
+  DBuf<double> diag;  // inverse diagonal (DIAGONAL) or scratch
+  // ---- Schwarz ----
+  i64 nsub = 0;
+  int max_nodes = 0;
+  std::vector<i64> sub_off, sub_nodes, untreated;
+  std::vector<i64> color_off;
+  std::vector<int> color_subs;
+  std::vector<int> adj_off, adj, diag_slot;
+  std::vector<long long> base;
+  std::vector<unsigned char> diag_only;
+  DBuf<int> d_adj_off, d_adj, d_diag_slot, d_sub_off, d_sub_nodes, d_gmap, d_smap, d_color_subs, d_untreated;
+  DBuf<long long> d_base, d_gmap_off;
+  DBuf<unsigned char> d_diag_only;
+  DBuf<double> vals, staging;
+  DBuf<long long> d_stage_off;
+  DBuf<int> d_err;
+  i64 nnz = 0;
+  NodeRows rows() const;
+};
+
+void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes, i64 nsub, const i64* untreated,
+                            i64 nun);
+void precond_update(Precond& p, const double* system_vals, cudaStream_t s);
+void precond_apply(const Precond& p, const double* r, double* z, cudaStream_t s);
+
+struct CgState {
+  double bnorm, tol, zTr, pAp, rr, alpha, beta;
+  long long iters, max_iter;
+  int done, status;
+};
+
+struct CgWork {
+  Model* m = nullptr;
+  i64 n = 0;
+  DBuf<double> x, b, r, z, p, Ap, partials;
+  DBuf<CgState> st;
+  DBuf<unsigned> counter;
+  CgState* h_st = nullptr;  // pinned
+  cudaGraphExec_t graph = nullptr;
+  const void* graph_key[3] = {nullptr, nullptr, nullptr};
+  int graph_kind = -1;
+  int chunk = 8;
+  void init(Model* model);
+  ~CgWork();
+};
+
+// Solves A x = b with x = work.x (initial guess) and b = work.b on the model
+// pattern values `vals`.  Returns HOEFEM_OK or a HOEFEM_CG_* status.
+int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 max_iter, i64* iters, cudaStream_t s);
+
+}  // namespace hoefem

@@ -1,0 +1,223 @@
+"""Preconditioners, conjugate gradient and the Newton-CG backward Euler
+integrator, mirroring:
+
+  SystemPreconditioner, DiagonalPreconditioner, SchwarzPreconditioner
+      simulation_toolbox/src/fem/newton_cg.rs:297-411,534-593
+  SchwarzPreconditionerComponent::from_embedded_model
+      simulation_toolbox/src/fem/schwarz_precond.rs:65-127
+  ConjugateGradient, RelativeResidualCriterion, SolveError(Kind), CgOutput
+      fenris/src/cg.rs:62-124,195-482
+  NewtonCgIntegrator3d
+      simulation_toolbox/src/fem/newton_cg.rs:43-295
+"""
+import ctypes as C
+import enum
+
+import numpy as np
+
+from . import _capi
+from ._capi import HoefemError, check, host_f64, host_i64, lib, ptr
+from .model import _same_space
+
+
+class DiagonalPreconditioner:
+    """z = r / diag(A); update() fails with ZERO_DIAGONAL like the reference."""
+
+    def __init__(self, model):
+        self.model = model
+        h = C.c_void_p()
+        check(lib().hoefem_precond_create_diagonal(model._h, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().hoefem_precond_destroy(h)
+            self._h = None
+
+    def update(self, system_values):
+        check(lib().hoefem_precond_update(self._h, ptr(system_values)[0], _same_space(system_values)))
+
+    def apply(self, r, z=None):
+        if z is None:
+            z = np.zeros_like(r) if not _capi.is_device_array(r) else r.new_zeros(r.shape)
+        check(lib().hoefem_precond_apply(self._h, ptr(r)[0], ptr(z)[0], _same_space(r, z)))
+        return z
+
+    def values(self):
+        nnz = C.c_int64()
+        check(lib().hoefem_precond_nnz(self._h, C.byref(nnz)))
+        v = np.zeros(nnz.value)
+        check(lib().hoefem_precond_values(self._h, v.ctypes.data))
+        return v
+
+
+class SchwarzPreconditioner(DiagonalPreconditioner):
+    """Element-wise additive Schwarz on `subdomains` (node lists), scalar
+    Jacobi on `untreated_nodes` (build_schwarz_preconditioner_into)."""
+
+    def __init__(self, model, subdomains, untreated_nodes):
+        self.model = model
+        subs = [np.asarray(s, dtype=np.int64) for s in subdomains]
+        off = np.zeros(len(subs) + 1, dtype=np.int64)
+        for i, s in enumerate(subs):
+            off[i + 1] = off[i] + s.size
+        flat = np.concatenate(subs) if subs else np.zeros(0, dtype=np.int64)
+        un = host_i64(untreated_nodes)
+        h = C.c_void_p()
+        check(lib().hoefem_precond_create_schwarz(model._h, off.ctypes.data, flat.ctypes.data if flat.size else None,
+                                                  len(subs), un.ctypes.data if un.size else None, un.size,
+                                                  C.byref(h)))
+        self._h = h
+        self.num_subdomains = len(subs)
+
+    def pattern(self):
+        nnz = C.c_int64()
+        check(lib().hoefem_precond_nnz(self._h, C.byref(nnz)))
+        ro = np.zeros(self.model.ndof() + 1, dtype=np.int64)
+        ci = np.zeros(max(nnz.value, 1), dtype=np.int64)
+        check(lib().hoefem_precond_pattern(self._h, ro.ctypes.data, ci.ctypes.data))
+        return ro, ci[: nnz.value]
+
+
+class SchwarzPreconditionerComponent:
+    """Subdomain selection of the reference: interface elements whose embedded
+    volume fraction is <= threshold become subdomains, every node outside them
+    is untreated (schwarz_precond.rs:65-127)."""
+
+    def __init__(self, subdomains, untreated_nodes):
+        self.schwarz_connectivity = subdomains
+        self.untreated_nodes = untreated_nodes
+
+    @staticmethod
+    def from_embedded_model(model, volume_fractions, volume_fraction_threshold):
+        conn = model.interface_connectivity
+        sel = [conn[i] for i in range(conn.shape[0]) if volume_fractions[i] <= volume_fraction_threshold]
+        is_iface = np.zeros(model.num_vertices, dtype=bool)
+        for s in sel:
+            is_iface[s] = True
+        untreated = np.nonzero(~is_iface)[0].astype(np.int64)
+        return SchwarzPreconditionerComponent(sel, untreated)
+
+    def build(self, model):
+        return SchwarzPreconditioner(model, self.schwarz_connectivity, self.untreated_nodes)
+
+
+class RelativeResidualCriterion:
+    """||r|| <= tol ||b|| on the CG recurrence residual (cg.rs:77-124)."""
+
+    def __init__(self, tol=1e-8):
+        self.tol = float(tol)
+
+
+class SolveErrorKind(enum.Enum):
+    IndefiniteOperator = _capi.STATUS[10]
+    IndefinitePreconditioner = _capi.STATUS[11]
+    MaxIterationsReached = _capi.STATUS[12]
+
+
+class CgOutput:
+    def __init__(self, num_iterations):
+        self.num_iterations = num_iterations
+
+
+class SolveError(Exception):
+    def __init__(self, kind, output):
+        super().__init__("CG solve failed after %d iterations: %s" % (output.num_iterations, kind.name))
+        self.kind = kind
+        self.output = output
+
+
+_CG_KIND = {10: SolveErrorKind.IndefiniteOperator, 11: SolveErrorKind.IndefinitePreconditioner,
+            12: SolveErrorKind.MaxIterationsReached}
+
+
+class ConjugateGradient:
+    """Builder as in cg.rs:195-275: with_operator / with_preconditioner /
+    with_stopping_criterion / with_max_iter, then solve_with_guess(b, x)."""
+
+    def __init__(self, model):
+        self.model = model
+        self.values = None
+        self.preconditioner = None
+        self.criterion = RelativeResidualCriterion()
+        self.max_iter = -1
+
+    def with_operator(self, values):
+        self.values = values
+        return self
+
+    def with_preconditioner(self, p):
+        self.preconditioner = p
+        return self
+
+    def with_stopping_criterion(self, c):
+        self.criterion = c
+        return self
+
+    def with_max_iter(self, n):
+        self.max_iter = int(n)
+        return self
+
+    def solve_with_guess(self, b, x):
+        it = C.c_int64()
+        mem = _same_space(self.values, b, x)
+        st = lib().hoefem_cg_solve(self.model._h, ptr(self.values)[0],
+                                   self.preconditioner._h if self.preconditioner is not None else None, ptr(b)[0],
+                                   ptr(x)[0], self.criterion.tol, self.max_iter, C.byref(it), mem)
+        if st in _CG_KIND:
+            raise SolveError(_CG_KIND[st], CgOutput(it.value))
+        check(st)
+        return CgOutput(it.value)
+
+
+class NewtonCgIntegrator3d:
+    """One backward-Euler step per call, solved by Newton with backtracking line
+    search and preconditioned CG (homogeneous Dirichlet nodes, scalar gravity
+    on z, no damping).  `preconditioner` is a SchwarzPreconditioner of the same
+    model or None (diagonal, the reference's fallback)."""
+
+    def __init__(self, model, material, density, dirichlet_nodes=(), gravity=-9.81, gravity_enabled=True,
+                 preconditioner=None):
+        self.model = model
+        self.material = material
+        self.preconditioner = preconditioner
+        bc = host_i64(dirichlet_nodes)
+        self._bc = bc
+        h = C.c_void_p()
+        check(lib().hoefem_integrator_create(model._h, C.byref(material.descriptor()), float(density),
+                                             bc.ctypes.data if bc.size else None, bc.size,
+                                             1 if gravity_enabled else 0, float(gravity),
+                                             preconditioner._h if preconditioner is not None else None, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().hoefem_integrator_destroy(h)
+            self._h = None
+
+    def set_tolerances(self, cg_tol=1e-5, cg_max_iter=500, newton_max_iter=100):
+        check(lib().hoefem_integrator_set_tolerances(self._h, cg_tol, cg_max_iter, newton_max_iter))
+
+    def step(self, u, v, t, dt):
+        """Advances (u, v) in place by dt; returns the step statistics."""
+        mem = _same_space(u, v)
+        check(lib().hoefem_integrator_step(self._h, ptr(u)[0], ptr(v)[0], float(t), float(dt), mem))
+        return self.stats()
+
+    def stats(self):
+        s = _capi.StepStats()
+        check(lib().hoefem_integrator_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def mass(self):
+        v = np.zeros(self.model.nnz)
+        check(lib().hoefem_integrator_mass(self._h, v.ctypes.data))
+        return v
+
+    def eval_f(self, u, v, f=None):
+        if f is None:
+            f = np.zeros(self.model.ndof()) if not _capi.is_device_array(u) else u.new_zeros(self.model.ndof())
+        check(lib().hoefem_integrator_eval_f(self._h, ptr(u)[0], ptr(v)[0], ptr(f)[0], _same_space(u, v, f)))
+        return f

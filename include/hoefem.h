@@ -1,0 +1,277 @@
+/*
+ * hoefem.h — C ABI of the B200 (sm_100a) implementation of the per-step hot
+ * path of the higher-order embedded FEM method (reference project:
+ * InteractiveComputerGraphics/higher_order_embedded_fem, Rust).
+ *
+ * The reference exposes this path as Rust traits called by its integrator.
+ * Every entry point below replaces one of those trait methods; the comment of
+ * each cites the reference item (path inside the reference project : line).
+ * All arithmetic is IEEE FP64 unless an entry point says otherwise.
+ *
+ * Conventions
+ *  - Returns: every function returns a hoefem_status (0 = success).  The
+ *    reference panics or returns Box<dyn Error>; this ABI never aborts.
+ *  - Memory: vectors / value arrays passed to compute entry points live in the
+ *    space named by the `mem` argument (HOEFEM_MEM_HOST: host memory, copied
+ *    in/out inside the call; HOEFEM_MEM_DEVICE: device pointers on the current
+ *    CUDA device, used in place).  Setup arrays (meshes, quadrature, patterns)
+ *    are always host memory.
+ *  - Indices are int64 (the reference uses usize); DOF numbering is node-major
+ *    (dof = 3 * node + component), as in the reference.
+ *  - Accumulation: "_into" entry points ADD into their output, like the
+ *    reference's `*_into` / `*_into_par` methods.
+ *  - Threading: a handle is used by one host thread at a time; calls on one
+ *    handle are ordered on that handle's CUDA stream and synchronous on return.
+ */
+#ifndef HOEFEM_H
+#define HOEFEM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HOEFEM_ABI_VERSION 1
+
+typedef enum {
+  HOEFEM_OK = 0,
+  HOEFEM_ERR_INVALID_ARGUMENT = 1,
+  HOEFEM_ERR_CUDA = 2,
+  HOEFEM_ERR_OUT_OF_MEMORY = 3,
+  /* singular reference Jacobian or deformation gradient: the reference panics
+     ("Jacobian must be invertible", "TODO: Handle singular F?") */
+  HOEFEM_ERR_SINGULAR = 4,
+  HOEFEM_ERR_NONFINITE = 5,
+  /* an element entry is missing from the CSR pattern or an element repeats a
+     node (reference: "Could not find column index associated with node") */
+  HOEFEM_ERR_PATTERN = 6,
+  /* zero diagonal while building a preconditioner (newton_cg.rs:560-576,
+     schwarz_precond.rs:203-210) */
+  HOEFEM_ERR_ZERO_DIAGONAL = 7,
+  HOEFEM_ERR_NOT_FINALIZED = 8,
+  /* CG outcomes, fenris/src/cg.rs:277-286 SolveErrorKind */
+  HOEFEM_CG_INDEFINITE_OPERATOR = 10,
+  HOEFEM_CG_INDEFINITE_PRECONDITIONER = 11,
+  HOEFEM_CG_MAX_ITERATIONS = 12,
+  /* Newton / integrator outcomes, hamilton2/src/newton.rs:26-33 and
+     simulation_toolbox/src/fem/newton_cg.rs:146-228 */
+  HOEFEM_NEWTON_MAX_ITERATIONS = 20,
+  HOEFEM_LINE_SEARCH_FAILED = 21,
+  HOEFEM_SUBSTEPPING_FAILED = 22,
+  HOEFEM_ERR_NO_DEVICE = 31
+} hoefem_status;
+
+typedef enum { HOEFEM_MEM_HOST = 0, HOEFEM_MEM_DEVICE = 1 } hoefem_mem;
+
+/* Element kinds (fenris/src/element.rs: Tet10 :1790-1972, Hex27 :1244-1444). */
+typedef enum { HOEFEM_ELEM_TET10 = 1, HOEFEM_ELEM_HEX27 = 3 } hoefem_element_kind;
+
+/* Material models (fenris/src/solid/materials.rs: StVK :177-219, Stable
+   Neo-Hookean :221-377).  Lame parameters are the un-reparametrised ones; the
+   SNH re-parametrisation (materials.rs:242-253) happens inside the kernels. */
+typedef enum { HOEFEM_MAT_STVK = 0, HOEFEM_MAT_SNH = 1 } hoefem_material_kind;
+
+/* An ElasticMaterialModel<f64, U3> (fenris/src/solid/mod.rs:21-87) as a POD
+   descriptor passed to the kernels instead of a trait object. */
+typedef struct {
+  int32_t kind;  /* hoefem_material_kind */
+  double mu;
+  double lambda;
+} hoefem_material;
+
+const char* hoefem_last_error(void);
+int hoefem_abi_version(void);
+/* Selects the CUDA device used by handles created afterwards on this thread. */
+int hoefem_set_device(int device);
+
+/* LameParameters::from(YoungPoisson), fenris/src/solid/materials.rs:27-38.
+   Reproduces the reference's lambda = 0.5*mu*nu/(1-2nu) (documented erratum,
+   a factor 4 below the textbook value) so results match the reference. */
+int hoefem_lame_from_young_poisson(double young, double poisson, double* mu, double* lambda);
+
+/* ------------------------------------------------------------------------ */
+/* Model: NodalModel3d (fenris/src/model.rs:32-117) / EmbeddedModel3d
+   (fenris/src/embedding/mod.rs:39-59,243-283).  A model is a vertex array
+   plus one or more element blocks assembled in order; each block has its own
+   greedy coloring (paradis/src/coloring.rs:48-72).  A NodalModel is one block;
+   an EmbeddedModel is an interior block (uniform rule) followed by an
+   interface block (one rule per element). */
+typedef struct hoefem_model_s* hoefem_model;
+
+int hoefem_model_create(const double* vertices /* num_vertices x 3 */, int64_t num_vertices, hoefem_model* out);
+/* connectivity: num_elements x nodes_per_element (row-major).  quadrature:
+   when quad_offsets == NULL every element uses the same rule of
+   num_quad_points points; otherwise element e uses points
+   [quad_offsets[e], quad_offsets[e+1]) (num_elements+1 offsets).
+   Weights are in reference measure (sum w |det J| = element volume). */
+int hoefem_model_add_block(hoefem_model m, int element_kind, const int64_t* connectivity, int64_t num_elements,
+                           const int64_t* quad_offsets, const double* quad_weights,
+                           const double* quad_points /* x3 */, int64_t num_quad_points);
+/* Builds the shared CSR pattern (CsrParAssembler::assemble_pattern,
+   fenris/src/assembly.rs:177-249), the colorings, the element-to-nnz maps and
+   uploads everything to the device. */
+int hoefem_model_finalize(hoefem_model m);
+int hoefem_model_destroy(hoefem_model m);
+int hoefem_model_sizes(hoefem_model m, int64_t* ndof, int64_t* nnz, int64_t* num_elements, int64_t* num_blocks);
+/* row_offsets: ndof+1, column_indices: nnz (SparsityPattern, sparse.rs:297-410) */
+int hoefem_model_pattern(hoefem_model m, int64_t* row_offsets, int64_t* column_indices);
+int hoefem_model_num_colors(hoefem_model m, int block, int64_t* num_colors);
+/* DisjointSubsets labels per color (paradis/src/lib.rs:78-190): color_offsets
+   has num_colors+1 entries, element_labels are block-local element indices. */
+int hoefem_model_colors(hoefem_model m, int block, int64_t* color_offsets, int64_t* element_labels);
+
+/* ElasticityModelParallel::assemble_elastic_pseudo_forces_into_par
+   (fenris/src/solid/mod.rs:129-134; impls solid/impl_model.rs:111-127,
+   embedding/mod.rs:516-554): f += f_int(u), f_e = -sum_q P J^-T grad N w|det J|. */
+int hoefem_assemble_elastic_pseudo_forces_into(hoefem_model m, const hoefem_material* mat, const double* u, double* f,
+                                               int mem);
+/* ElasticityModelParallel::assemble_stiffness_into_par
+   (fenris/src/solid/mod.rs:144-151, assembly.rs:252-314): values += K(u) on the
+   model pattern; colored scatter without atomics, one launch per color. */
+int hoefem_assemble_stiffness_into(hoefem_model m, const hoefem_material* mat, const double* u, double* values,
+                                   int mem);
+/* ElasticityModel::assemble_mass(density).to_csr (solid/mod.rs:106,
+   assembly.rs:624-671): values += M on the model pattern. */
+int hoefem_assemble_mass_into(hoefem_model m, double density, double* values, int mem);
+/* apply_homogeneous_dirichlet_bc_csr (fenris/src/assembly.rs:799-869) on
+   values of the model pattern; nodes are host indices. */
+int hoefem_apply_dirichlet_bc_csr(hoefem_model m, const int64_t* nodes, int64_t num_nodes, double* values, int mem);
+/* compute_jacobian_combination_into (simulation_toolbox/src/fem/
+   system_assembly.rs:196-235) without damping: out = (0 + c_k K) + c_m M,
+   then Dirichlet rows/columns. */
+int hoefem_jacobian_combination(hoefem_model m, double c_stiffness, const double* stiffness_values, double c_mass,
+                                const double* mass_values, const int64_t* bc_nodes, int64_t num_bc, double* out,
+                                int mem);
+/* spmv_csr (fenris/src/sparse.rs:1164-1199) / LinearOperator::apply for the
+   model pattern (cg.rs:15-17): y = beta*y + alpha*A x. */
+int hoefem_spmv(hoefem_model m, double beta, double* y, double alpha, const double* values, const double* x, int mem);
+
+/* ------------------------------------------------------------------------ */
+/* SystemPreconditioner (simulation_toolbox/src/fem/newton_cg.rs:397-411). */
+typedef struct hoefem_precond_s* hoefem_precond;
+
+/* DiagonalPreconditioner (newton_cg.rs:534-593). */
+int hoefem_precond_create_diagonal(hoefem_model m, hoefem_precond* out);
+/* SchwarzPreconditioner (newton_cg.rs:297-370; schwarz_precond.rs:26-216):
+   one subdomain per node list (the reference uses the interface elements whose
+   embedded volume fraction is below a threshold), scalar Jacobi for untreated
+   nodes.  Builds build_preconditioner_pattern (schwarz_precond.rs:134-169). */
+int hoefem_precond_create_schwarz(hoefem_model m, const int64_t* subdomain_offsets, const int64_t* subdomain_nodes,
+                                  int64_t num_subdomains, const int64_t* untreated_nodes, int64_t num_untreated,
+                                  hoefem_precond* out);
+/* SystemPreconditioner::update (newton_cg.rs:352-365 / 556-571): system values
+   on the model pattern. */
+int hoefem_precond_update(hoefem_precond p, const double* system_values, int mem);
+/* LinearOperator::apply of the preconditioner: z = P r. */
+int hoefem_precond_apply(hoefem_precond p, const double* r, double* z, int mem);
+/* Schwarz pattern / values for inspection (nnz first, then the arrays). */
+int hoefem_precond_nnz(hoefem_precond p, int64_t* nnz);
+int hoefem_precond_pattern(hoefem_precond p, int64_t* row_offsets, int64_t* column_indices);
+int hoefem_precond_values(hoefem_precond p, double* values /* host */);
+int hoefem_precond_destroy(hoefem_precond p);
+
+/* ------------------------------------------------------------------------ */
+/* ConjugateGradient::solve_with_guess (fenris/src/cg.rs:368-482) with a
+   RelativeResidualCriterion (cg.rs:77-124): stops when ||r|| <= tol ||b||.
+   x holds the initial guess on entry.  p == NULL means no preconditioner.
+   Returns HOEFEM_OK or one of the HOEFEM_CG_* outcomes; *iterations is always
+   written (CgOutput::num_iterations). */
+int hoefem_cg_solve(hoefem_model m, const double* system_values, hoefem_precond p, const double* b, double* x,
+                    double tol, int64_t max_iter, int64_t* iterations, int mem);
+
+/* ------------------------------------------------------------------------ */
+/* NewtonCgIntegrator3d (simulation_toolbox/src/fem/newton_cg.rs:43-295):
+   backward Euler (hamilton2/src/integrators/euler.rs:155-199) solved by
+   Newton with backtracking line search (hamilton2/src/newton.rs:76-248), the
+   Jacobian M + dt^2 K solved by preconditioned CG; failures retried with
+   5x substeps up to 1000.  Homogeneous Dirichlet nodes (u = v = 0), scalar
+   gravity on the last component (system_assembly.rs:30-75), no damping. */
+typedef struct hoefem_integrator_s* hoefem_integrator;
+
+typedef struct {
+  int64_t newton_iterations;     /* of the last backward Euler solve */
+  int64_t num_cg_solves;         /* over all substeps */
+  int64_t total_cg_iterations;
+  int64_t max_cg_iterations;
+  int64_t substeps;
+  int32_t last_cg_status;
+  double residual_norm;          /* ||F(w)|| at exit */
+  double representative_force;   /* fe_model.rs:423-431 */
+  double ms_assemble_forces;     /* device time per phase, last step */
+  double ms_assemble_stiffness;
+  double ms_precond_update;
+  double ms_cg;
+  double ms_total;
+} hoefem_step_stats;
+
+/* precond: a preconditioner of this model (ownership stays with the caller),
+   or NULL for the diagonal preconditioner.  The mass matrix (with Dirichlet),
+   representative force and gravity force are built here (fe_model.rs:489-515). */
+int hoefem_integrator_create(hoefem_model m, const hoefem_material* mat, double density, const int64_t* bc_nodes,
+                             int64_t num_bc, int gravity_enabled, double gravity, hoefem_precond precond,
+                             hoefem_integrator* out);
+/* Defaults follow the reference: cg_tol 1e-5, cg_max_iter 500,
+   newton_max_iter 100 (newton_cg.rs:282-286,761-773). */
+int hoefem_integrator_set_tolerances(hoefem_integrator it, double cg_tol, int64_t cg_max_iter,
+                                     int64_t newton_max_iter);
+/* One time step: u, v (ndof) updated in place. */
+int hoefem_integrator_step(hoefem_integrator it, double* u, double* v, double t, double dt, int mem);
+int hoefem_integrator_stats(hoefem_integrator it, hoefem_step_stats* out);
+/* Mass matrix values (model pattern, Dirichlet applied) for inspection. */
+int hoefem_integrator_mass(hoefem_integrator it, double* values /* host */);
+/* NewtonCgDynamicSystem::eval_f (newton_cg.rs:441-478): f = M g + f_int(u)
+   with Dirichlet rows zeroed. */
+int hoefem_integrator_eval_f(hoefem_integrator it, const double* u, const double* v, double* f, int mem);
+int hoefem_integrator_destroy(hoefem_integrator it);
+
+/* ------------------------------------------------------------------------ */
+/* Synthetic scenes (input construction; not part of the reference hot path).
+   Restates the reference's procedural meshes and refinements:
+   create_rectangular_uniform_hex_mesh (fenris/src/geometry/procedural.rs:
+   191-250), Max triangulation (geometry/polymesh.rs:402-500) + Tet4
+   conversion (mesh_convert.rs:639-727) + Tet10 / Hex27 refinement
+   (mesh_convert.rs:41-75,163-244,296-406), keep_cells (mesh.rs:321-366). */
+typedef struct hoefem_scene_s* hoefem_scene;
+
+/* Box [0, unit*ux] x [0, unit*uy] x [0, unit*uz], cells_per_unit cells per unit,
+   each hex split into 6 Tet10; one uniform block with tet_quadrature_strength_5. */
+int hoefem_scene_create_tet10_box(double unit, int64_t ux, int64_t uy, int64_t uz, int64_t cells_per_unit,
+                                  hoefem_scene* out);
+/* Unit-box Hex27 grid (n^3 cells) clipped to the hollow cylinder with axis z
+   through (0.5, 0.5), radii [r_inner, r_outer], full height.  Cells with volume
+   fraction < 1e-4 are removed, >= 0.999 are interior (hex_quadrature_strength_5),
+   the rest are interface cells with Q ~ U{q_min..q_max} seeded uniform points
+   and Dirichlet(1) weights summing to 8*phi (reference measure). */
+int hoefem_scene_create_embedded_cylinder(int64_t n, double r_inner, double r_outer, int q_min, int q_max,
+                                          uint64_t seed, hoefem_scene* out);
+
+typedef struct {
+  int64_t num_vertices;
+  int64_t num_blocks;
+  int32_t block_kind[2];
+  int64_t block_elements[2];
+  int64_t block_quad_points[2]; /* total points stored for the block */
+  int32_t block_uniform[2];     /* 1: one rule for all elements */
+  double cell_size;
+} hoefem_scene_info;
+
+int hoefem_scene_info_get(hoefem_scene s, hoefem_scene_info* info);
+int hoefem_scene_vertices(hoefem_scene s, double* vertices);
+/* quad_offsets is written only for non-uniform blocks (num_elements+1). */
+int hoefem_scene_block(hoefem_scene s, int block, int64_t* connectivity, int64_t* quad_offsets, double* quad_weights,
+                       double* quad_points);
+/* Volume fraction of each interface element from its quadrature
+   (schwarz_precond.rs:65-127): sum_q w |det J| / cell volume. */
+int hoefem_scene_volume_fractions(hoefem_scene s, double* fractions /* interface elements */);
+/* Nodes with coordinate `axis` <= value (sorted ascending); count first with nodes == NULL. */
+int hoefem_scene_nodes_below(hoefem_scene s, int axis, double value, int64_t* nodes, int64_t* count);
+int hoefem_scene_destroy(hoefem_scene s);
+
+/* Seeded N(0, sigma^2) samples (splitmix64 + Box-Muller), identical on all hosts. */
+int hoefem_random_normal(uint64_t seed, int64_t n, double sigma, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HOEFEM_H */
