@@ -63,12 +63,14 @@ class SceneInfo(C.Structure):
 SIGNATURES = {
     "hoefem_last_error": (C.c_char_p, []),
     "hoefem_abi_version": (C.c_int, []),
+    "hoefem_launch_count": (C.c_int, [pi64]),
     "hoefem_set_device": (C.c_int, [C.c_int]),
     "hoefem_lame_from_young_poisson": (C.c_int, [dbl, dbl, pdbl, pdbl]),
     "hoefem_model_create": (C.c_int, [vp, i64, C.POINTER(vp)]),
     "hoefem_model_add_block": (C.c_int, [vp, C.c_int, vp, i64, vp, vp, vp, i64]),
     "hoefem_model_finalize": (C.c_int, [vp]),
     "hoefem_model_destroy": (C.c_int, [vp]),
+    "hoefem_model_set_stream": (C.c_int, [vp, vp]),
     "hoefem_model_sizes": (C.c_int, [vp, pi64, pi64, pi64, pi64]),
     "hoefem_model_pattern": (C.c_int, [vp, vp, vp]),
     "hoefem_model_num_colors": (C.c_int, [vp, C.c_int, pi64]),
@@ -121,6 +123,12 @@ def lib():
             fn.argtypes = args
         _lib = L
     return _lib
+
+
+def launch_count():
+    n = C.c_int64()
+    check(lib().hoefem_launch_count(C.byref(n)))
+    return n.value
 
 
 def check(status):

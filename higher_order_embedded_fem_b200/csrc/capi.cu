@@ -27,11 +27,20 @@ void greedy_coloring(const i64* conn, i64 ne, int nn, i64 nv, std::vector<i64>& 
                      std::vector<int>& color_elems);
 }  // namespace hoefem
 
+namespace hoefem {
+std::atomic<long long> g_launch_count{0};
+thread_local long long g_capture_count = -1;
+}  // namespace hoefem
+
 using namespace hoefem;
 
 struct hoefem_model_s {
   Model m;
   std::unique_ptr<CgWork> cg;
+  cudaStream_t own_stream = nullptr;
+  ~hoefem_model_s() {
+    if (own_stream) m.stream = own_stream;  // the Model destroys its own stream only
+  }
 };
 struct hoefem_precond_s {
   Precond p;
@@ -124,6 +133,12 @@ extern "C" {
 const char* hoefem_last_error(void) { return g_error.c_str(); }
 int hoefem_abi_version(void) { return HOEFEM_ABI_VERSION; }
 
+int hoefem_launch_count(int64_t* count) {
+  if (!count) return fail(HOEFEM_ERR_INVALID_ARGUMENT, "null output");
+  *count = g_launch_count.load();
+  return HOEFEM_OK;
+}
+
 int hoefem_set_device(int device) {
   API_BEGIN
   HOEFEM_CUDA(cudaSetDevice(device));
@@ -190,6 +205,15 @@ int hoefem_model_finalize(hoefem_model m) {
 int hoefem_model_destroy(hoefem_model m) {
   API_BEGIN
   delete m;
+  API_END
+}
+
+int hoefem_model_set_stream(hoefem_model m, void* stream) {
+  API_BEGIN
+  Model& mm = device_model(m);
+  if (!m->own_stream) m->own_stream = mm.stream;
+  HOEFEM_CUDA(cudaStreamSynchronize(mm.stream));
+  mm.stream = stream ? (cudaStream_t)stream : m->own_stream;
   API_END
 }
 

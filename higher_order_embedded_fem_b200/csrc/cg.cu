@@ -220,19 +220,19 @@ static void enqueue_iteration(CgWork& w, const double* vals, const Precond* P, c
   NodeRows A = w.m->rows();
   const int n = (int)w.n;
   const int sg = spmv_grid(A.nv), vg = vec_grid(n);
-  k_cg_Ap<<<sg, TPB, 0, s>>>(A, vals, w.p.p, w.Ap.p, w.partials.p, w.counter.p, w.st.p);
+  (note_launch(), k_cg_Ap<<<sg, TPB, 0, s>>>(A, vals, w.p.p, w.Ap.p, w.partials.p, w.counter.p, w.st.p));
   const int kind = P ? P->kind : PREC_NONE;
   if (kind == PREC_SCHWARZ) {
-    k_cg_update<<<vg, TPB, 0, s>>>(n, 0, nullptr, w.x.p, w.r.p, w.p.p, w.Ap.p, w.z.p, w.partials.p, w.counter.p,
-                                   w.st.p);
+    (note_launch(), k_cg_update<<<vg, TPB, 0, s>>>(n, 0, nullptr, w.x.p, w.r.p, w.p.p, w.Ap.p, w.z.p, w.partials.p, w.counter.p,
+                                   w.st.p));
     NodeRows PR = P->rows();
-    k_cg_prec_spmv<<<spmv_grid(PR.nv), TPB, 0, s>>>(PR, P->vals.p, w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, 0);
+    (note_launch(), k_cg_prec_spmv<<<spmv_grid(PR.nv), TPB, 0, s>>>(PR, P->vals.p, w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, 0));
   } else {
     int mode = kind == PREC_DIAGONAL ? 2 : 1;
-    k_cg_update<<<vg, TPB, 0, s>>>(n, mode, kind == PREC_DIAGONAL ? P->diag.p : nullptr, w.x.p, w.r.p, w.p.p, w.Ap.p,
-                                   w.z.p, w.partials.p, w.counter.p, w.st.p);
+    (note_launch(), k_cg_update<<<vg, TPB, 0, s>>>(n, mode, kind == PREC_DIAGONAL ? P->diag.p : nullptr, w.x.p, w.r.p, w.p.p, w.Ap.p,
+                                   w.z.p, w.partials.p, w.counter.p, w.st.p));
   }
-  k_cg_p<<<vg, TPB, 0, s>>>(n, w.z.p, w.p.p, w.st.p);
+  (note_launch(), k_cg_p<<<vg, TPB, 0, s>>>(n, w.z.p, w.p.p, w.st.p));
 }
 
 int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 max_iter, i64* iters, cudaStream_t s) {
@@ -246,16 +246,16 @@ int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 ma
   init.max_iter = max_iter;
   HOEFEM_CUDA(cudaMemcpyAsync(w.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
   const int sg = spmv_grid(A.nv), vg = vec_grid(n);
-  k_cg_init<<<sg, TPB, 0, s>>>(A, vals, w.x.p, w.b.p, w.r.p, w.partials.p, w.counter.p, w.st.p);
+  (note_launch(), k_cg_init<<<sg, TPB, 0, s>>>(A, vals, w.x.p, w.b.p, w.r.p, w.partials.p, w.counter.p, w.st.p));
   if (kind == PREC_SCHWARZ) {
     NodeRows PR = P->rows();
-    k_cg_prec_spmv<<<spmv_grid(PR.nv), TPB, 0, s>>>(PR, P->vals.p, w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, 1);
+    (note_launch(), k_cg_prec_spmv<<<spmv_grid(PR.nv), TPB, 0, s>>>(PR, P->vals.p, w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, 1));
   } else {
-    k_cg_prec_vec<<<vg, TPB, 0, s>>>(n, kind == PREC_DIAGONAL ? 1 : 0, kind == PREC_DIAGONAL ? P->diag.p : nullptr,
-                                     w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, 1);
+    (note_launch(), k_cg_prec_vec<<<vg, TPB, 0, s>>>(n, kind == PREC_DIAGONAL ? 1 : 0, kind == PREC_DIAGONAL ? P->diag.p : nullptr,
+                                     w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, 1));
   }
-  k_cg_copy<<<vg, TPB, 0, s>>>(n, w.z.p, w.p.p);
-  k_cg_init_check<<<1, 1, 0, s>>>(w.st.p);
+  (note_launch(), k_cg_copy<<<vg, TPB, 0, s>>>(n, w.z.p, w.p.p));
+  (note_launch(), k_cg_init_check<<<1, 1, 0, s>>>(w.st.p));
   HOEFEM_CUDA(cudaGetLastError());
   HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
   HOEFEM_CUDA(cudaStreamSynchronize(s));
@@ -278,7 +278,10 @@ int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 ma
     HOEFEM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaGraph_t g;
     HOEFEM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    g_capture_count = 0;
     for (int k = 0; k < w.chunk; ++k) enqueue_iteration(w, vals, P, cs);
+    w.graph_kernels = g_capture_count;
+    g_capture_count = -1;
     HOEFEM_CUDA(cudaStreamEndCapture(cs, &g));
     HOEFEM_CUDA(cudaGraphInstantiate(&w.graph, g, 0));
     cudaGraphDestroy(g);
@@ -291,6 +294,7 @@ int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 ma
   const i64 max_chunks = max_iter >= 0 ? (max_iter + w.chunk - 1) / w.chunk + 2 : (i64)1 << 40;
   for (i64 c = 0; c < max_chunks; ++c) {
     HOEFEM_CUDA(cudaGraphLaunch(w.graph, s));
+    g_launch_count.fetch_add(w.graph_kernels, std::memory_order_relaxed);
     HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
     HOEFEM_CUDA(cudaStreamSynchronize(s));
     if (w.h_st->done) break;

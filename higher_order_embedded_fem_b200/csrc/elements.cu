@@ -584,9 +584,9 @@ void launch_forces(const Model& m, const MatDev& mat, const double* u, double* f
     for_each_color(*bp, [&](const int* elems, int cnt) {
       int grid = (cnt + TPB / 32 - 1) / (TPB / 32);
       if (bp->kind == HOEFEM_ELEM_TET10)
-        k_forces<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p);
+        (note_launch(), k_forces<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p));
       else
-        k_forces<27><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p);
+        (note_launch(), k_forces<27><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p));
     });
   }
   HOEFEM_CUDA(cudaGetLastError());
@@ -599,9 +599,9 @@ void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double
     for_each_color(*bp, [&](const int* elems, int cnt) {
       if (bp->kind == HOEFEM_ELEM_TET10) {
         int grid = (cnt + TPB / 32 - 1) / (TPB / 32);
-        k_stiffness<10, 32><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p, vals, mat, m.d_err.p);
+        (note_launch(), k_stiffness<10, 32><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p, vals, mat, m.d_err.p));
       } else {
-        k_stiffness<27, TPB><<<cnt, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p, vals, mat, m.d_err.p);
+        (note_launch(), k_stiffness<27, TPB><<<cnt, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p, vals, mat, m.d_err.p));
       }
     });
   }
@@ -614,9 +614,9 @@ void launch_mass(const Model& m, double density, double* vals, cudaStream_t s) {
     for_each_color(*bp, [&](const int* elems, int cnt) {
       int grid = (cnt + TPB / 32 - 1) / (TPB / 32);
       if (bp->kind == HOEFEM_ELEM_TET10)
-        k_mass<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, m.d_adj_off.p, vals, density, m.d_err.p);
+        (note_launch(), k_mass<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, m.d_adj_off.p, vals, density, m.d_err.p));
       else
-        k_mass<27><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, m.d_adj_off.p, vals, density, m.d_err.p);
+        (note_launch(), k_mass<27><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, m.d_adj_off.p, vals, density, m.d_err.p));
     });
   }
   HOEFEM_CUDA(cudaGetLastError());

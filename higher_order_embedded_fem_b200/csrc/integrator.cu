@@ -161,12 +161,12 @@ struct Integrator {
     jacobian_combination(*m, 0.0, nullptr, 1.0, K.p, bc_nodes.empty() ? nullptr : bc.p, M.p, scalars.p, s);
     check_device_error(*m);
     // representative force ||M a||, a_i = sqrt(a^2 / 3), a = 10 (fe_model.rs:423-431)
-    k_fill<<<grid(), TPB, 0, s>>>(n, std::sqrt((10.0 * 10.0) / 3.0), us.p);
+    (note_launch(), k_fill<<<grid(), TPB, 0, s>>>(n, std::sqrt((10.0 * 10.0) / 3.0), us.p));
     spmv_node_rows(m->rows(), M.p, us.p, vs.p, 1.0, 0.0, s);
     rep_force = std::sqrt(norm_sq(vs.p));
     // gravity force M g (system_assembly.rs:30-75, newton_cg.rs:248-255)
-    if (gravity_enabled) k_gravity_density<<<grid(), TPB, 0, s>>>(n, gravity, us.p);
-    else k_fill<<<grid(), TPB, 0, s>>>(n, 0.0, us.p);
+    if (gravity_enabled) (note_launch(), k_gravity_density<<<grid(), TPB, 0, s>>>(n, gravity, us.p));
+    else (note_launch(), k_fill<<<grid(), TPB, 0, s>>>(n, 0.0, us.p));
     spmv_node_rows(m->rows(), M.p, us.p, gforce.p, 1.0, 0.0, s);
     HOEFEM_CUDA(cudaStreamSynchronize(s));
     if (!P) {
@@ -187,12 +187,12 @@ struct Integrator {
   void eval_f(const double* ud, const double* vd, double* out) {
     cudaStream_t s = m->stream;
     const int n = (int)m->ndof;
-    k_copy<<<grid(), TPB, 0, s>>>(n, ud, us.p);
-    k_copy<<<grid(), TPB, 0, s>>>(n, vd, vs.p);
-    if (!bc_nodes.empty()) k_bc_uv<<<grid(), TPB, 0, s>>>(n, bc.p, us.p, vs.p);
-    k_copy<<<grid(), TPB, 0, s>>>(n, gforce.p, out);
+    (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, ud, us.p));
+    (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, vd, vs.p));
+    if (!bc_nodes.empty()) (note_launch(), k_bc_uv<<<grid(), TPB, 0, s>>>(n, bc.p, us.p, vs.p));
+    (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, gforce.p, out));
     launch_forces(*m, mat, us.p, out, s);
-    if (!bc_nodes.empty()) k_zero_bc<<<grid(), TPB, 0, s>>>(n, bc.p, out);
+    if (!bc_nodes.empty()) (note_launch(), k_zero_bc<<<grid(), TPB, 0, s>>>(n, bc.p, out));
     check_device_error(*m);
   }
 
@@ -202,11 +202,11 @@ struct Integrator {
     const int n = (int)m->ndof;
     const unsigned char* bcp = bc_nodes.empty() ? nullptr : bc.p;
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
-    k_be_state<<<grid(), TPB, 0, s>>>(n, up.p, vn.p, w.p, dt, bcp, us.p, vs.p);
-    k_copy<<<grid(), TPB, 0, s>>>(n, gforce.p, f.p);
+    (note_launch(), k_be_state<<<grid(), TPB, 0, s>>>(n, up.p, vn.p, w.p, dt, bcp, us.p, vs.p));
+    (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, gforce.p, f.p));
     launch_forces(*m, mat, us.p, f.p, s);
     HOEFEM_CUDA(cudaEventRecord(ev[1], s));
-    k_F<<<grid(), TPB, 0, s>>>(n, f.p, bcp, dt, F.p);
+    (note_launch(), k_F<<<grid(), TPB, 0, s>>>(n, f.p, bcp, dt, F.p));
     spmv_node_rows(m->rows(), M.p, w.p, F.p, 1.0, 1.0, s);
     double r = norm_sq(F.p);
     stats.ms_assemble_forces += elapsed();
@@ -219,7 +219,7 @@ struct Integrator {
     const int n = (int)m->ndof;
     const unsigned char* bcp = bc_nodes.empty() ? nullptr : bc.p;
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
-    k_be_state<<<grid(), TPB, 0, s>>>(n, up.p, vn.p, w.p, dt, bcp, us.p, vs.p);
+    (note_launch(), k_be_state<<<grid(), TPB, 0, s>>>(n, up.p, vn.p, w.p, dt, bcp, us.p, vs.p));
     K.zero(s);
     launch_stiffness(*m, mat, us.p, K.p, s);
     // J = gamma M - beta D - alpha K with alpha = -dt^2, gamma = 1, no damping
@@ -233,7 +233,7 @@ struct Integrator {
     HOEFEM_CUDA(cudaEventSynchronize(ev[1]));
     stats.ms_precond_update += elapsed();
     HOEFEM_CUDA(cudaMemsetAsync(cg.x.p, 0, sizeof(double) * n, s));
-    k_copy<<<grid(), TPB, 0, s>>>(n, F.p, cg.b.p);
+    (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, F.p, cg.b.p));
     i64 it = 0;
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
     int st = cg_solve(cg, J.p, P, cg_tol, cg_max, &it, s);
@@ -244,7 +244,7 @@ struct Integrator {
     stats.total_cg_iterations += it;
     if (it > stats.max_cg_iterations) stats.max_cg_iterations = it;
     stats.last_cg_status = st;
-    k_copy<<<grid(), TPB, 0, s>>>(n, cg.x.p, dx.p);
+    (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, cg.x.p, dx.p));
     // MaxIterationsReached and IndefiniteOperator are tolerated (newton_cg.rs:776-797)
     if (st == HOEFEM_OK || st == HOEFEM_CG_MAX_ITERATIONS || st == HOEFEM_CG_INDEFINITE_OPERATOR) return HOEFEM_OK;
     return st;
@@ -253,7 +253,7 @@ struct Integrator {
   int be_step(double dt) {
     cudaStream_t s = m->stream;
     const int n = (int)m->ndof;
-    k_be_init<<<grid(), TPB, 0, s>>>(n, u.p, v.p, dt, up.p, vn.p, w.p);
+    (note_launch(), k_be_init<<<grid(), TPB, 0, s>>>(n, u.p, v.p, dt, up.p, vn.p, w.p));
     const double tol = dt * (1e-5 * rep_force);
     double fsq = eval_F(dt);
     i64 iter = 0;
@@ -261,14 +261,14 @@ struct Integrator {
       if (iter == newton_max) return HOEFEM_NEWTON_MAX_ITERATIONS;
       int st = solve_jacobian(dt);
       if (st != HOEFEM_OK) return st;
-      k_neg<<<grid(), TPB, 0, s>>>(n, dx.p);
+      (note_launch(), k_neg<<<grid(), TPB, 0, s>>>(n, dx.p));
       const double c = 1e-4, alpha_min = 1e-6;
       const double g0 = 0.5 * fsq;
       const double initial[4] = {0.0, 1.0, 0.75, 0.5};
       double alpha_prev = 0.0, alpha = 1.0, tail = 0.25;
       int k = 1;
       for (;;) {
-        k_axpy_w<<<grid(), TPB, 0, s>>>(n, alpha - alpha_prev, dx.p, w.p);
+        (note_launch(), k_axpy_w<<<grid(), TPB, 0, s>>>(n, alpha - alpha_prev, dx.p, w.p));
         fsq = eval_F(dt);
         double g = 0.5 * fsq;
         if (g <= (1.0 - c * alpha) * g0) break;
@@ -282,7 +282,7 @@ struct Integrator {
     }
     stats.newton_iterations = iter;
     stats.residual_norm = std::sqrt(fsq);
-    k_be_final<<<grid(), TPB, 0, s>>>(n, w.p, dt, bc_nodes.empty() ? nullptr : bc.p, u.p, v.p);
+    (note_launch(), k_be_final<<<grid(), TPB, 0, s>>>(n, w.p, dt, bc_nodes.empty() ? nullptr : bc.p, u.p, v.p));
     HOEFEM_CUDA(cudaGetLastError());
     return HOEFEM_OK;
   }
@@ -298,12 +298,12 @@ struct Integrator {
     HOEFEM_CUDA(cudaEventCreate(&t0));
     HOEFEM_CUDA(cudaEventCreate(&t1));
     HOEFEM_CUDA(cudaEventRecord(t0, s));
-    if (!bc_nodes.empty()) k_bc_uv<<<grid(), TPB, 0, s>>>(n, bc.p, ud, vd);
+    if (!bc_nodes.empty()) (note_launch(), k_bc_uv<<<grid(), TPB, 0, s>>>(n, bc.p, ud, vd));
     i64 num = 1;
     int result = HOEFEM_OK;
     for (;;) {
-      k_copy<<<grid(), TPB, 0, s>>>(n, ud, u.p);
-      k_copy<<<grid(), TPB, 0, s>>>(n, vd, v.p);
+      (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, ud, u.p));
+      (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, vd, v.p));
       double sdt = dt / (double)num;
       bool failed = false;
       for (i64 k = 0; k < num; ++k) {
@@ -322,8 +322,8 @@ struct Integrator {
     }
     stats.substeps = num;
     if (result == HOEFEM_OK) {
-      k_copy<<<grid(), TPB, 0, s>>>(n, u.p, ud);
-      k_copy<<<grid(), TPB, 0, s>>>(n, v.p, vd);
+      (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, u.p, ud));
+      (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, v.p, vd));
     }
     HOEFEM_CUDA(cudaEventRecord(t1, s));
     HOEFEM_CUDA(cudaEventSynchronize(t1));

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -13,6 +14,16 @@
 namespace hoefem {
 
 using i64 = int64_t;
+
+// Launch accounting: every kernel launch site calls note_launch(); launches
+// recorded while a CUDA graph is being captured are counted into the graph
+// (capture_count) and added per replay instead.
+extern std::atomic<long long> g_launch_count;
+extern thread_local long long g_capture_count;  // -1 when not capturing
+inline void note_launch() {
+  if (g_capture_count >= 0) ++g_capture_count;
+  else g_launch_count.fetch_add(1, std::memory_order_relaxed);
+}
 
 struct Error : std::runtime_error {
   int code;

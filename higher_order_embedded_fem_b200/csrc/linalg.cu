@@ -114,22 +114,22 @@ int spmv_grid(int nv) {
 
 void spmv_node_rows(const NodeRows& A, const double* vals, const double* x, double* y, double alpha, double beta,
                     cudaStream_t s) {
-  k_spmv<<<spmv_grid(A.nv), 256, 0, s>>>(A, vals, x, y, alpha, beta);
+  (note_launch(), k_spmv<<<spmv_grid(A.nv), 256, 0, s>>>(A, vals, x, y, alpha, beta));
   HOEFEM_CUDA(cudaGetLastError());
 }
 
 void jacobian_combination(const Model& m, double ck, const double* K, double cm, const double* M,
                           const unsigned char* bc_dof, double* out, double* d_scratch, cudaStream_t s) {
   NodeRows A = m.rows();
-  k_combine<<<148 * 8, 256, 0, s>>>(A, ck, K, cm, M, out);
+  (note_launch(), k_combine<<<148 * 8, 256, 0, s>>>(A, ck, K, cm, M, out));
   if (bc_dof) {
     unsigned long long* first = reinterpret_cast<unsigned long long*>(d_scratch);
-    k_fill_u64<<<1, 1, 0, s>>>(first, ~0ull);
-    k_first_nonzero_diag<<<(A.nv + 255) / 256, 256, 0, s>>>(A, out, first);
+    (note_launch(), k_fill_u64<<<1, 1, 0, s>>>(first, ~0ull));
+    (note_launch(), k_first_nonzero_diag<<<(A.nv + 255) / 256, 256, 0, s>>>(A, out, first));
     // The scale entry is read before any thread writes: k_dirichlet reads it
     // at entry, and a Dirichlet diagonal entry is overwritten with `scale`
     // itself, so the race is benign (all writers store the same value).
-    k_dirichlet<<<spmv_grid(A.nv), 256, 0, s>>>(A, bc_dof, out, first);
+    (note_launch(), k_dirichlet<<<spmv_grid(A.nv), 256, 0, s>>>(A, bc_dof, out, first));
   }
   HOEFEM_CUDA(cudaGetLastError());
 }
@@ -155,7 +155,7 @@ int reduce_blocks_for(i64 n) {
 
 void dot_device(const double* a, const double* b, i64 n, double* out, double* partials, unsigned* counter,
                 cudaStream_t s) {
-  k_dot<<<reduce_blocks_for(n), 256, 0, s>>>(a, b, n, out, partials, counter);
+  (note_launch(), k_dot<<<reduce_blocks_for(n), 256, 0, s>>>(a, b, n, out, partials, counter));
   HOEFEM_CUDA(cudaGetLastError());
 }
 

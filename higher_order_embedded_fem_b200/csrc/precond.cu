@@ -391,7 +391,7 @@ void precond_update(Precond& p, const double* J, cudaStream_t s) {
   if (p.kind == PREC_DIAGONAL) {
     if (p.diag.n < (size_t)m.ndof) p.diag.alloc(m.ndof);
     if (!p.d_err.p) { p.d_err.alloc(1); p.d_err.zero(s); }
-    k_diag_inverse<<<(int)((m.ndof + 255) / 256), 256, 0, s>>>(A, J, p.diag.p, p.d_err.p);
+    (note_launch(), k_diag_inverse<<<(int)((m.ndof + 255) / 256), 256, 0, s>>>(A, J, p.diag.p, p.d_err.p));
     HOEFEM_CUDA(cudaGetLastError());
     check_err(p.d_err, s);
     p.ready = true;
@@ -401,22 +401,22 @@ void precond_update(Precond& p, const double* J, cudaStream_t s) {
   if (p.nsub > 0) {
     int m_max = (3 * p.max_nodes + 1) & ~1;
     size_t smem = (size_t)(2 * m_max * m_max + m_max) * sizeof(double);
-    k_schwarz_factor<<<(int)p.nsub, FACTOR_TPB, smem, s>>>((int)p.nsub, p.d_sub_off.p, p.d_sub_nodes.p,
+    (note_launch(), k_schwarz_factor<<<(int)p.nsub, FACTOR_TPB, smem, s>>>((int)p.nsub, p.d_sub_off.p, p.d_sub_nodes.p,
                                                            p.d_gmap_off.p, p.d_gmap.p, m.d_adj_off.p, J,
-                                                           p.d_stage_off.p, p.staging.p, p.d_err.p);
+                                                           p.d_stage_off.p, p.staging.p, p.d_err.p));
     HOEFEM_CUDA(cudaGetLastError());
     const int nc = (int)p.color_off.size() - 1;
     for (int c = 0; c < nc; ++c) {
       int b = (int)p.color_off[c], cnt = (int)(p.color_off[c + 1] - b);
       if (cnt)
-        k_schwarz_scatter<<<cnt, 256, 0, s>>>(p.d_color_subs.p + b, cnt, p.d_sub_off.p, p.d_sub_nodes.p,
+        (note_launch(), k_schwarz_scatter<<<cnt, 256, 0, s>>>(p.d_color_subs.p + b, cnt, p.d_sub_off.p, p.d_sub_nodes.p,
                                               p.d_gmap_off.p, p.d_smap.p, p.d_adj_off.p, p.d_stage_off.p,
-                                              p.staging.p, p.vals.p);
+                                              p.staging.p, p.vals.p));
     }
   }
   if (!p.untreated.empty())
-    k_schwarz_untreated<<<(int)((3 * p.untreated.size() + 255) / 256), 256, 0, s>>>(
-        (int)p.untreated.size(), p.d_untreated.p, p.d_base.p, A, J, p.vals.p, p.d_err.p);
+    (note_launch(), k_schwarz_untreated<<<(int)((3 * p.untreated.size() + 255) / 256), 256, 0, s>>>(
+        (int)p.untreated.size(), p.d_untreated.p, p.d_base.p, A, J, p.vals.p, p.d_err.p));
   HOEFEM_CUDA(cudaGetLastError());
   check_err(p.d_err, s);
   p.ready = true;
@@ -426,10 +426,10 @@ void precond_apply(const Precond& p, const double* r, double* z, cudaStream_t s)
   HOEFEM_REQUIRE(p.ready, HOEFEM_ERR_INVALID_ARGUMENT, "preconditioner has not been updated");
   if (p.kind == PREC_DIAGONAL) {
     int n = (int)p.m->ndof;
-    k_mul<<<reduce_blocks_for(n), 256, 0, s>>>(n, p.diag.p, r, z);
+    (note_launch(), k_mul<<<reduce_blocks_for(n), 256, 0, s>>>(n, p.diag.p, r, z));
   } else {
     NodeRows PR = p.rows();
-    k_spmv_plain<<<spmv_grid(PR.nv), 256, 0, s>>>(PR, p.vals.p, r, z);
+    (note_launch(), k_spmv_plain<<<spmv_grid(PR.nv), 256, 0, s>>>(PR, p.vals.p, r, z));
   }
   HOEFEM_CUDA(cudaGetLastError());
 }

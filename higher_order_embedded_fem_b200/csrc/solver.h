@@ -53,6 +53,7 @@ struct CgWork {
   const void* graph_key[3] = {nullptr, nullptr, nullptr};
   int graph_kind = -1;
   int chunk = 8;
+  long long graph_kernels = 0;
   void init(Model* model);
   ~CgWork();
 };

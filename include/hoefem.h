@@ -82,6 +82,9 @@ typedef struct {
 
 const char* hoefem_last_error(void);
 int hoefem_abi_version(void);
+/* Number of kernels this library has launched in this process (graph
+   replays counted per kernel).  Instrumentation; no reference counterpart. */
+int hoefem_launch_count(int64_t* count);
 /* Selects the CUDA device used by handles created afterwards on this thread. */
 int hoefem_set_device(int device);
 
@@ -113,6 +116,11 @@ int hoefem_model_add_block(hoefem_model m, int element_kind, const int64_t* conn
    uploads everything to the device. */
 int hoefem_model_finalize(hoefem_model m);
 int hoefem_model_destroy(hoefem_model m);
+/* Runs the model's work (and that of its preconditioners / integrator) on a
+   caller stream (a cudaStream_t, e.g. torch.cuda.current_stream().cuda_stream);
+   NULL restores the model's own stream.  Calls stay synchronous on return.
+   No counterpart in the reference (its path is synchronous host code). */
+int hoefem_model_set_stream(hoefem_model m, void* stream);
 int hoefem_model_sizes(hoefem_model m, int64_t* ndof, int64_t* nnz, int64_t* num_elements, int64_t* num_blocks);
 /* row_offsets: ndof+1, column_indices: nnz (SparsityPattern, sparse.rs:297-410) */
 int hoefem_model_pattern(hoefem_model m, int64_t* row_offsets, int64_t* column_indices);
