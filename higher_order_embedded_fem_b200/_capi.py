@@ -77,6 +77,7 @@ SIGNATURES = {
     "hoefem_model_colors": (C.c_int, [vp, C.c_int, vp, vp]),
     "hoefem_assemble_elastic_pseudo_forces_into": (C.c_int, [vp, C.POINTER(Material), vp, vp, C.c_int]),
     "hoefem_assemble_stiffness_into": (C.c_int, [vp, C.POINTER(Material), vp, vp, C.c_int]),
+    "hoefem_assemble_stiffness_into_precision": (C.c_int, [vp, C.POINTER(Material), vp, vp, C.c_int, C.c_int]),
     "hoefem_assemble_mass_into": (C.c_int, [vp, dbl, vp, C.c_int]),
     "hoefem_apply_dirichlet_bc_csr": (C.c_int, [vp, vp, i64, vp, C.c_int]),
     "hoefem_jacobian_combination": (C.c_int, [vp, dbl, vp, dbl, vp, vp, i64, vp, C.c_int]),
@@ -90,8 +91,10 @@ SIGNATURES = {
     "hoefem_precond_values": (C.c_int, [vp, vp]),
     "hoefem_precond_destroy": (C.c_int, [vp]),
     "hoefem_cg_solve": (C.c_int, [vp, vp, vp, vp, vp, dbl, i64, pi64, C.c_int]),
+    "hoefem_cg_solve_mixed": (C.c_int, [vp, vp, vp, vp, vp, dbl, i64, dbl, pi64, C.c_int]),
     "hoefem_integrator_create": (C.c_int, [vp, C.POINTER(Material), dbl, vp, i64, C.c_int, dbl, vp, C.POINTER(vp)]),
     "hoefem_integrator_set_tolerances": (C.c_int, [vp, dbl, i64, i64]),
+    "hoefem_integrator_set_precision": (C.c_int, [vp, C.c_int, dbl]),
     "hoefem_integrator_step": (C.c_int, [vp, vp, vp, dbl, dbl, C.c_int]),
     "hoefem_integrator_stats": (C.c_int, [vp, C.POINTER(StepStats)]),
     "hoefem_integrator_mass": (C.c_int, [vp, vp]),

@@ -19,6 +19,7 @@ Integrator* integrator_new(Model* m, const hoefem_material* mat, double density,
                            int gravity_enabled, double gravity, Precond* P);
 void integrator_delete(Integrator* it);
 void integrator_set_tolerances(Integrator* it, double tol, i64 cg_max, i64 newton_max);
+void integrator_set_precision(Integrator* it, int precision, double inner_tol);
 int integrator_step(Integrator* it, double* ud, double* vd, double t, double dt);
 hoefem_step_stats integrator_stats(Integrator* it);
 const double* integrator_mass(Integrator* it);
@@ -284,6 +285,21 @@ int hoefem_assemble_stiffness_into(hoefem_model m, const hoefem_material* mat, c
   API_END
 }
 
+int hoefem_assemble_stiffness_into_precision(hoefem_model m, const hoefem_material* mat, const double* u,
+                                             double* values, int precision, int mem) {
+  API_BEGIN
+  Model& mm = device_model(m);
+  MatDev md = mat_of(mat);
+  HOEFEM_REQUIRE(precision == HOEFEM_PRECISION_FP64 || precision == HOEFEM_PRECISION_MIXED,
+                 HOEFEM_ERR_INVALID_ARGUMENT, "bad precision");
+  View U(u, mm.ndof, mem, mm.stream, true), V(values, mm.nnz, mem, mm.stream, true);
+  launch_stiffness(mm, md, U.d, V.d, mm.stream, precision == HOEFEM_PRECISION_MIXED ? PRECISION_FP32 : PRECISION_FP64);
+  V.copy_out();
+  sync(mm);
+  check_device_error(mm);
+  API_END
+}
+
 int hoefem_assemble_mass_into(hoefem_model m, double density, double* values, int mem) {
   API_BEGIN
   Model& mm = device_model(m);
@@ -465,6 +481,39 @@ int hoefem_cg_solve(hoefem_model m, const double* system_values, hoefem_precond 
   API_END
 }
 
+int hoefem_cg_solve_mixed(hoefem_model m, const double* system_values, hoefem_precond p, const double* b, double* x,
+                          double tol, int64_t max_iter, double inner_tol, int64_t* iterations, int mem) {
+  API_BEGIN
+  Model& mm = device_model(m);
+  HOEFEM_REQUIRE(iterations && inner_tol > 0.0 && inner_tol < 1.0, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  HOEFEM_REQUIRE(!p || p->p.m == &mm, HOEFEM_ERR_INVALID_ARGUMENT, "preconditioner of another model");
+  if (!m->cg) {
+    m->cg.reset(new CgWork());
+    m->cg->init(&mm);
+  }
+  CgWork& w = *m->cg;
+  View A(system_values, mm.nnz, mem, mm.stream, true);
+  View B(b, mm.ndof, mem, mm.stream, true), X(x, mm.ndof, mem, mm.stream, true);
+  DBuf<float> A32;
+  A32.alloc(mm.nnz);
+  to_f32(A.d, A32.p, mm.nnz, mm.stream);
+  if (p && p->p.kind == PREC_SCHWARZ && p->p.ready && (!p->p.vals32.p || !p->p.want_fp32)) {
+    p->p.want_fp32 = true;
+    p->p.vals32.alloc(p->p.nnz);
+    to_f32(p->p.vals.p, p->p.vals32.p, p->p.nnz, mm.stream);
+  }
+  HOEFEM_CUDA(cudaMemcpyAsync(w.b.p, B.d, mm.ndof * sizeof(double), cudaMemcpyDeviceToDevice, mm.stream));
+  HOEFEM_CUDA(cudaMemcpyAsync(w.x.p, X.d, mm.ndof * sizeof(double), cudaMemcpyDeviceToDevice, mm.stream));
+  i64 it = 0, outer = 0;
+  int st = cg_solve_ir(w, A.d, A32.p, p ? &p->p : nullptr, tol, max_iter, inner_tol, &it, &outer, mm.stream);
+  HOEFEM_CUDA(cudaMemcpyAsync(X.d, w.x.p, mm.ndof * sizeof(double), cudaMemcpyDeviceToDevice, mm.stream));
+  X.copy_out();
+  sync(mm);
+  *iterations = it;
+  if (st != HOEFEM_OK) return fail(st, "CG did not converge");
+  API_END
+}
+
 // ---- integrator ----------------------------------------------------------------
 int hoefem_integrator_create(hoefem_model m, const hoefem_material* mat, double density, const int64_t* bc_nodes,
                              int64_t num_bc, int gravity_enabled, double gravity, hoefem_precond precond,
@@ -487,6 +536,15 @@ int hoefem_integrator_set_tolerances(hoefem_integrator it, double cg_tol, int64_
   API_BEGIN
   HOEFEM_REQUIRE(it && cg_tol > 0.0, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
   integrator_set_tolerances(it->it, cg_tol, cg_max_iter, newton_max_iter);
+  API_END
+}
+
+int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double inner_tol) {
+  API_BEGIN
+  HOEFEM_REQUIRE(it && (precision == HOEFEM_PRECISION_FP64 || precision == HOEFEM_PRECISION_MIXED) &&
+                     inner_tol > 0.0 && inner_tol < 1.0,
+                 HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  integrator_set_precision(it->it, precision == HOEFEM_PRECISION_MIXED ? PRECISION_FP32 : PRECISION_FP64, inner_tol);
   API_END
 }
 

@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdint>
 
 #include "internal.h"
 #include "kernels_common.cuh"
@@ -29,7 +31,8 @@ namespace {
 constexpr int TPB = 256;
 
 // r = b - A x ; partial b.b, r.r
-__global__ void __launch_bounds__(TPB) k_cg_init(NodeRows A, const double* __restrict__ vals,
+template <class VA>
+__global__ void __launch_bounds__(TPB) k_cg_init(NodeRows A, const VA* __restrict__ vals,
                                                  const double* __restrict__ x, const double* __restrict__ b,
                                                  double* __restrict__ r, double* partials, unsigned* counter,
                                                  CgState* st) {
@@ -80,7 +83,8 @@ __global__ void __launch_bounds__(TPB) k_cg_prec_vec(int n, int mode, const doub
 }
 
 // z = P r with P a node-row matrix (Schwarz) ; partial z.r.
-__global__ void __launch_bounds__(TPB) k_cg_prec_spmv(NodeRows P, const double* __restrict__ pv,
+template <class VP>
+__global__ void __launch_bounds__(TPB) k_cg_prec_spmv(NodeRows P, const VP* __restrict__ pv,
                                                       const double* __restrict__ r, double* __restrict__ z,
                                                       double* partials, unsigned* counter, CgState* st, int init) {
   if (!init && st->done) return;
@@ -125,7 +129,8 @@ __global__ void k_cg_init_check(CgState* st) {
 }
 
 // Ap = A p ; pAp ; checks ; alpha
-__global__ void __launch_bounds__(TPB) k_cg_Ap(NodeRows A, const double* __restrict__ vals,
+template <class VA>
+__global__ void __launch_bounds__(TPB) k_cg_Ap(NodeRows A, const VA* __restrict__ vals,
                                                const double* __restrict__ p, double* __restrict__ Ap,
                                                double* partials, unsigned* counter, CgState* st) {
   if (st->done) return;
@@ -198,12 +203,22 @@ __global__ void __launch_bounds__(TPB) k_cg_p(int n, const double* __restrict__ 
 
 int vec_grid(i64 n) { return reduce_blocks_for(n); }
 
+__global__ void k_axpy(int n, double a, const double* __restrict__ x, double* __restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += a * x[i];
+}
+
+__global__ void k_to_f32(long long n, const double* __restrict__ a, float* __restrict__ b) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
 }  // namespace
 
 void CgWork::init(Model* model) {
   m = model;
   n = model->ndof;
   x.alloc(n); b.alloc(n); r.alloc(n); z.alloc(n); p.alloc(n); Ap.alloc(n);
+  xo.alloc(n); bo.alloc(n); ro.alloc(n);
   partials.alloc(4 * 148 * 16);
   st.alloc(1);
   counter.alloc(1);
@@ -212,47 +227,118 @@ void CgWork::init(Model* model) {
 }
 
 CgWork::~CgWork() {
-  if (graph) cudaGraphExecDestroy(graph);
+  for (auto& g : graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   if (h_st) cudaFreeHost(h_st);
 }
 
-static void enqueue_iteration(CgWork& w, const double* vals, const Precond* P, cudaStream_t s) {
-  NodeRows A = w.m->rows();
+void to_f32(const double* a, float* b, long long n, cudaStream_t s) {
+  (note_launch(), k_to_f32<<<148 * 8, 256, 0, s>>>(n, a, b));
+  HOEFEM_CUDA(cudaGetLastError());
+}
+
+namespace {
+
+// Operator values: FP64 or FP32 (exactly one set).
+struct Operator {
+  const double* v64;
+  const float* v32;
+};
+
+const void* prec_key(const Precond* P, bool p32) {
+  if (!P) return nullptr;
+  if (P->kind == PREC_SCHWARZ) return p32 ? (const void*)P->vals32.p : (const void*)P->vals.p;
+  return (const void*)P->diag.p;
+}
+
+void enqueue_Ap(CgWork& w, Operator A, cudaStream_t s) {
+  NodeRows R = w.m->rows();
+  const int sg = spmv_grid(R.nv);
+  if (A.v32)
+    (note_launch(), k_cg_Ap<float><<<sg, TPB, 0, s>>>(R, A.v32, w.p.p, w.Ap.p, w.partials.p, w.counter.p, w.st.p));
+  else
+    (note_launch(), k_cg_Ap<double><<<sg, TPB, 0, s>>>(R, A.v64, w.p.p, w.Ap.p, w.partials.p, w.counter.p, w.st.p));
+}
+
+void enqueue_prec_spmv(CgWork& w, const Precond* P, bool p32, int init, cudaStream_t s) {
+  NodeRows PR = P->rows();
+  const int g = spmv_grid(PR.nv);
+  if (p32)
+    (note_launch(), k_cg_prec_spmv<float><<<g, TPB, 0, s>>>(PR, P->vals32.p, w.r.p, w.z.p, w.partials.p, w.counter.p,
+                                                            w.st.p, init));
+  else
+    (note_launch(), k_cg_prec_spmv<double><<<g, TPB, 0, s>>>(PR, P->vals.p, w.r.p, w.z.p, w.partials.p, w.counter.p,
+                                                             w.st.p, init));
+}
+
+void enqueue_iteration(CgWork& w, Operator A, const Precond* P, bool p32, cudaStream_t s) {
   const int n = (int)w.n;
-  const int sg = spmv_grid(A.nv), vg = vec_grid(n);
-  (note_launch(), k_cg_Ap<<<sg, TPB, 0, s>>>(A, vals, w.p.p, w.Ap.p, w.partials.p, w.counter.p, w.st.p));
+  const int vg = vec_grid(n);
+  enqueue_Ap(w, A, s);
   const int kind = P ? P->kind : PREC_NONE;
   if (kind == PREC_SCHWARZ) {
-    (note_launch(), k_cg_update<<<vg, TPB, 0, s>>>(n, 0, nullptr, w.x.p, w.r.p, w.p.p, w.Ap.p, w.z.p, w.partials.p, w.counter.p,
-                                   w.st.p));
-    NodeRows PR = P->rows();
-    (note_launch(), k_cg_prec_spmv<<<spmv_grid(PR.nv), TPB, 0, s>>>(PR, P->vals.p, w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, 0));
+    (note_launch(), k_cg_update<<<vg, TPB, 0, s>>>(n, 0, nullptr, w.x.p, w.r.p, w.p.p, w.Ap.p, w.z.p, w.partials.p,
+                                                   w.counter.p, w.st.p));
+    enqueue_prec_spmv(w, P, p32, 0, s);
   } else {
     int mode = kind == PREC_DIAGONAL ? 2 : 1;
-    (note_launch(), k_cg_update<<<vg, TPB, 0, s>>>(n, mode, kind == PREC_DIAGONAL ? P->diag.p : nullptr, w.x.p, w.r.p, w.p.p, w.Ap.p,
-                                   w.z.p, w.partials.p, w.counter.p, w.st.p));
+    (note_launch(), k_cg_update<<<vg, TPB, 0, s>>>(n, mode, kind == PREC_DIAGONAL ? P->diag.p : nullptr, w.x.p, w.r.p,
+                                                   w.p.p, w.Ap.p, w.z.p, w.partials.p, w.counter.p, w.st.p));
   }
   (note_launch(), k_cg_p<<<vg, TPB, 0, s>>>(n, w.z.p, w.p.p, w.st.p));
 }
 
-int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 max_iter, i64* iters, cudaStream_t s) {
-  NodeRows A = w.m->rows();
+CgWork::Graph& graph_for(CgWork& w, Operator A, const Precond* P, bool p32) {
+  const void* key[4] = {A.v32 ? (const void*)A.v32 : (const void*)A.v64, (const void*)P, prec_key(P, p32),
+                        (const void*)(intptr_t)((P ? P->kind : 0) * 2 + (p32 ? 1 : 0))};
+  for (auto& g : w.graphs)
+    if (g.exec && std::equal(key, key + 4, g.key)) return g;
+  if (w.graphs.size() >= 4) {
+    cudaGraphExecDestroy(w.graphs.front().exec);
+    w.graphs.erase(w.graphs.begin());
+  }
+  CgWork::Graph G;
+  std::copy(key, key + 4, G.key);
+  cudaStream_t cs;
+  HOEFEM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t g;
+  HOEFEM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  g_capture_count = 0;
+  for (int k = 0; k < w.chunk; ++k) enqueue_iteration(w, A, P, p32, cs);
+  G.kernels = g_capture_count;
+  g_capture_count = -1;
+  HOEFEM_CUDA(cudaStreamEndCapture(cs, &g));
+  HOEFEM_CUDA(cudaGraphInstantiate(&G.exec, g, 0));
+  cudaGraphDestroy(g);
+  cudaStreamDestroy(cs);
+  w.graphs.push_back(G);
+  return w.graphs.back();
+}
+
+// PCG on A with preconditioner P: x = w.x (initial guess), b = w.b.
+int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 max_iter, i64* iters,
+            cudaStream_t s) {
+  NodeRows R = w.m->rows();
   const int n = (int)w.n;
   const int kind = P ? P->kind : PREC_NONE;
   HOEFEM_REQUIRE(!P || P->ready, HOEFEM_ERR_INVALID_ARGUMENT, "preconditioner has not been updated");
-  // state
   CgState init{};
   init.tol = tol;
   init.max_iter = max_iter;
   HOEFEM_CUDA(cudaMemcpyAsync(w.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
-  const int sg = spmv_grid(A.nv), vg = vec_grid(n);
-  (note_launch(), k_cg_init<<<sg, TPB, 0, s>>>(A, vals, w.x.p, w.b.p, w.r.p, w.partials.p, w.counter.p, w.st.p));
+  const int sg = spmv_grid(R.nv), vg = vec_grid(n);
+  if (A.v32)
+    (note_launch(), k_cg_init<float><<<sg, TPB, 0, s>>>(R, A.v32, w.x.p, w.b.p, w.r.p, w.partials.p, w.counter.p,
+                                                        w.st.p));
+  else
+    (note_launch(), k_cg_init<double><<<sg, TPB, 0, s>>>(R, A.v64, w.x.p, w.b.p, w.r.p, w.partials.p, w.counter.p,
+                                                         w.st.p));
   if (kind == PREC_SCHWARZ) {
-    NodeRows PR = P->rows();
-    (note_launch(), k_cg_prec_spmv<<<spmv_grid(PR.nv), TPB, 0, s>>>(PR, P->vals.p, w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, 1));
+    enqueue_prec_spmv(w, P, p32, 1, s);
   } else {
-    (note_launch(), k_cg_prec_vec<<<vg, TPB, 0, s>>>(n, kind == PREC_DIAGONAL ? 1 : 0, kind == PREC_DIAGONAL ? P->diag.p : nullptr,
-                                     w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, 1));
+    (note_launch(), k_cg_prec_vec<<<vg, TPB, 0, s>>>(n, kind == PREC_DIAGONAL ? 1 : 0,
+                                                     kind == PREC_DIAGONAL ? P->diag.p : nullptr, w.r.p, w.z.p,
+                                                     w.partials.p, w.counter.p, w.st.p, 1));
   }
   (note_launch(), k_cg_copy<<<vg, TPB, 0, s>>>(n, w.z.p, w.p.p));
   (note_launch(), k_cg_init_check<<<1, 1, 0, s>>>(w.st.p));
@@ -268,33 +354,13 @@ int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 ma
     *iters = w.h_st->iters;
     return w.h_st->status;
   }
-  // (re)build the chunk graph when the operator / preconditioner changed
-  const void* key0 = vals;
-  const void* key1 = P ? (const void*)P : nullptr;
-  const void* key2 = P ? (kind == PREC_SCHWARZ ? (const void*)P->vals.p : (const void*)P->diag.p) : nullptr;
-  if (!w.graph || w.graph_key[0] != key0 || w.graph_key[1] != key1 || w.graph_key[2] != key2 || w.graph_kind != kind) {
-    if (w.graph) { cudaGraphExecDestroy(w.graph); w.graph = nullptr; }
-    cudaStream_t cs;
-    HOEFEM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    cudaGraph_t g;
-    HOEFEM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    g_capture_count = 0;
-    for (int k = 0; k < w.chunk; ++k) enqueue_iteration(w, vals, P, cs);
-    w.graph_kernels = g_capture_count;
-    g_capture_count = -1;
-    HOEFEM_CUDA(cudaStreamEndCapture(cs, &g));
-    HOEFEM_CUDA(cudaGraphInstantiate(&w.graph, g, 0));
-    cudaGraphDestroy(g);
-    cudaStreamDestroy(cs);
-    w.graph_key[0] = key0;
-    w.graph_key[1] = key1;
-    w.graph_key[2] = key2;
-    w.graph_kind = kind;
-  }
-  const i64 max_chunks = max_iter >= 0 ? (max_iter + w.chunk - 1) / w.chunk + 2 : (i64)1 << 40;
+  CgWork::Graph& G = graph_for(w, A, P, p32);
+  // without an iteration limit CG is still bounded: 10 n iterations
+  const i64 cap = max_iter >= 0 ? max_iter : 10 * (i64)n;
+  const i64 max_chunks = (cap + w.chunk - 1) / w.chunk + 2;
   for (i64 c = 0; c < max_chunks; ++c) {
-    HOEFEM_CUDA(cudaGraphLaunch(w.graph, s));
-    g_launch_count.fetch_add(w.graph_kernels, std::memory_order_relaxed);
+    HOEFEM_CUDA(cudaGraphLaunch(G.exec, s));
+    g_launch_count.fetch_add(G.kernels, std::memory_order_relaxed);
     HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
     HOEFEM_CUDA(cudaStreamSynchronize(s));
     if (w.h_st->done) break;
@@ -302,6 +368,67 @@ int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 ma
   *iters = w.h_st->iters;
   if (!w.h_st->done) return HOEFEM_CG_MAX_ITERATIONS;
   return w.h_st->status;
+}
+
+}  // namespace
+
+int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 max_iter, i64* iters, cudaStream_t s) {
+  return run_pcg(w, Operator{vals, nullptr}, P, false, tol, max_iter, iters, s);
+}
+
+// Mixed precision: FP64 iterative refinement around an inner PCG whose
+// operator and preconditioner values are FP32 (vectors, dot products and
+// residual updates stay FP64).  Outer: r = b - A64 x (FP64), stop when
+// ||r|| <= tol ||b||; inner: A32 d = r to a relative tolerance, x += d.
+int cg_solve_ir(CgWork& w, const double* A64, const float* A32, const Precond* P, double tol, i64 max_iter,
+                double inner_tol, i64* iters, i64* outer, cudaStream_t s) {
+  NodeRows R = w.m->rows();
+  const int n = (int)w.n;
+  const int sg = spmv_grid(R.nv), vg = vec_grid(n);
+  const bool p32 = P && P->kind == PREC_SCHWARZ && P->vals32.p;
+  HOEFEM_CUDA(cudaMemcpyAsync(w.xo.p, w.x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  HOEFEM_CUDA(cudaMemcpyAsync(w.bo.p, w.b.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  auto residual = [&](double* rnorm, double* bnorm) {
+    CgState init{};
+    HOEFEM_CUDA(cudaMemcpyAsync(w.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
+    (note_launch(), k_cg_init<double><<<sg, TPB, 0, s>>>(R, A64, w.xo.p, w.bo.p, w.ro.p, w.partials.p, w.counter.p,
+                                                         w.st.p));
+    HOEFEM_CUDA(cudaGetLastError());
+    HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+    HOEFEM_CUDA(cudaStreamSynchronize(s));
+    *rnorm = std::sqrt(w.h_st->rr);
+    *bnorm = w.h_st->bnorm;
+  };
+  double rn, bn;
+  residual(&rn, &bn);
+  *iters = 0;
+  *outer = 0;
+  int status = HOEFEM_OK;
+  if (bn == 0.0) {
+    HOEFEM_CUDA(cudaMemsetAsync(w.x.p, 0, sizeof(double) * n, s));
+    return HOEFEM_OK;
+  }
+  for (int k = 0; k < 40; ++k) {
+    if (rn <= tol * bn) { status = HOEFEM_OK; break; }
+    const i64 left = max_iter >= 0 ? max_iter - *iters : -1;
+    if (left == 0) { status = HOEFEM_CG_MAX_ITERATIONS; break; }
+    // inner solve A32 d = r, relative tolerance: the larger of inner_tol and
+    // what is still needed to reach the outer target
+    HOEFEM_CUDA(cudaMemcpyAsync(w.b.p, w.ro.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    HOEFEM_CUDA(cudaMemsetAsync(w.x.p, 0, sizeof(double) * n, s));
+    double tin = std::max(inner_tol, 0.5 * tol * bn / rn);
+    i64 it = 0;
+    int st = run_pcg(w, Operator{nullptr, A32}, P, p32, tin, left, &it, s);
+    *iters += it;
+    *outer += 1;
+    if (it > 0) (note_launch(), k_axpy<<<vg, TPB, 0, s>>>(n, 1.0, w.x.p, w.xo.p));
+    residual(&rn, &bn);
+    if (st != HOEFEM_OK && st != HOEFEM_CG_MAX_ITERATIONS) { status = st; break; }
+    if (st == HOEFEM_CG_MAX_ITERATIONS && rn > tol * bn) { status = st; break; }
+    status = rn <= tol * bn ? HOEFEM_OK : HOEFEM_CG_MAX_ITERATIONS;
+  }
+  HOEFEM_CUDA(cudaMemcpyAsync(w.x.p, w.xo.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  return status;
 }
 
 }  // namespace hoefem

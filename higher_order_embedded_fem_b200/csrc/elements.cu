@@ -35,7 +35,8 @@ __constant__ signed char c_hex27_alpha[27][3] = {
     {0, 1, 0},    {0, 0, 1},   {0, 0, 0}};
 __constant__ signed char c_tet10_edge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {2, 3}, {1, 3}};
 
-__device__ __forceinline__ double warp_sum(double v) {
+template <class R>
+__device__ __forceinline__ R warp_sum(R v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
@@ -44,94 +45,107 @@ __device__ __forceinline__ double warp_sum(double v) {
 __device__ __forceinline__ void set_error(int* err, int code) { atomicCAS(err, 0, code); }
 
 // ---- reference elements ----------------------------------------------------
-__device__ __forceinline__ void tet4_psi(const double* xi, double* p) {
-  p[0] = -0.5 * xi[0] - 0.5 * xi[1] - 0.5 * xi[2] - 0.5;
-  p[1] = 0.5 * xi[0] + 0.5;
-  p[2] = 0.5 * xi[1] + 0.5;
-  p[3] = 0.5 * xi[2] + 0.5;
+template <class R>
+__device__ __forceinline__ void tet4_psi(const R* xi, R* p) {
+  p[0] = -R(0.5) * xi[0] - R(0.5) * xi[1] - R(0.5) * xi[2] - R(0.5);
+  p[1] = R(0.5) * xi[0] + R(0.5);
+  p[2] = R(0.5) * xi[1] + R(0.5);
+  p[3] = R(0.5) * xi[2] + R(0.5);
 }
 // gradient of Tet4 basis function I (constant): column I of [[-.5,.5,0,0],[-.5,0,.5,0],[-.5,0,0,.5]]
-__device__ __forceinline__ void tet4_g(int I, double* g) {
-  g[0] = (I == 0) ? -0.5 : (I == 1 ? 0.5 : 0.0);
-  g[1] = (I == 0) ? -0.5 : (I == 2 ? 0.5 : 0.0);
-  g[2] = (I == 0) ? -0.5 : (I == 3 ? 0.5 : 0.0);
+template <class R>
+__device__ __forceinline__ void tet4_g(int I, R* g) {
+  g[0] = (I == 0) ? -R(0.5) : (I == 1 ? R(0.5) : R(0.0));
+  g[1] = (I == 0) ? -R(0.5) : (I == 2 ? R(0.5) : R(0.0));
+  g[2] = (I == 0) ? -R(0.5) : (I == 3 ? R(0.5) : R(0.0));
 }
 // Tet10 reference gradient of node I (element.rs:1921-1947)
-__device__ __forceinline__ void tet10_grad(int I, const double* xi, double* g) {
-  double p[4];
+template <class R>
+__device__ __forceinline__ void tet10_grad(int I, const R* xi, R* g) {
+  R p[4];
   tet4_psi(xi, p);
   if (I < 4) {
-    double gi[3];
+    R gi[3];
     tet4_g(I, gi);
-    double f = 4.0 * p[I] - 1.0;
+    R f = R(4.0) * p[I] - R(1.0);
     g[0] = gi[0] * f; g[1] = gi[1] * f; g[2] = gi[2] * f;
   } else {
     int a = c_tet10_edge[I - 4][0], b = c_tet10_edge[I - 4][1];
-    double ga[3], gb[3];
+    R ga[3], gb[3];
     tet4_g(a, ga);
     tet4_g(b, gb);
-    double fb = 4.0 * p[b], fa = 4.0 * p[a];
+    R fb = R(4.0) * p[b], fa = R(4.0) * p[a];
     g[0] = ga[0] * fb + gb[0] * fa;
     g[1] = ga[1] * fb + gb[1] * fa;
     g[2] = ga[2] * fb + gb[2] * fa;
   }
 }
-__device__ __forceinline__ double tet10_phi(int I, const double* xi) {
-  double p[4];
+template <class R>
+__device__ __forceinline__ R tet10_phi(int I, const R* xi) {
+  R p[4];
   tet4_psi(xi, p);
-  if (I < 4) return p[I] * (2.0 * p[I] - 1.0);
-  return 4.0 * p[c_tet10_edge[I - 4][0]] * p[c_tet10_edge[I - 4][1]];
+  if (I < 4) return p[I] * (R(2.0) * p[I] - R(1.0));
+  return R(4.0) * p[c_tet10_edge[I - 4][0]] * p[c_tet10_edge[I - 4][1]];
 }
-__device__ __forceinline__ double phi_q(double a, double x) {
-  double a2 = a * a, x2 = x * x;
-  return (3.0 / 2.0 * a2 - 1.0) * x2 + 0.5 * a * x + 1.0 - a2;
+template <class R>
+__device__ __forceinline__ R phi_q(R a, R x) {
+  R a2 = a * a, x2 = x * x;
+  return (R(3.0) / R(2.0) * a2 - R(1.0)) * x2 + R(0.5) * a * x + R(1.0) - a2;
 }
-__device__ __forceinline__ double dphi_q(double a, double x) {
-  double a2 = a * a;
-  return 2.0 * (3.0 / 2.0 * a2 - 1.0) * x + 0.5 * a;
+template <class R>
+__device__ __forceinline__ R dphi_q(R a, R x) {
+  R a2 = a * a;
+  return R(2.0) * (R(3.0) / R(2.0) * a2 - R(1.0)) * x + R(0.5) * a;
 }
-__device__ __forceinline__ void hex27_grad(int I, const double* xi, double* g) {
-  double a0 = c_hex27_alpha[I][0], a1 = c_hex27_alpha[I][1], a2 = c_hex27_alpha[I][2];
-  double p0 = phi_q(a0, xi[0]), p1 = phi_q(a1, xi[1]), p2 = phi_q(a2, xi[2]);
+template <class R>
+__device__ __forceinline__ void hex27_grad(int I, const R* xi, R* g) {
+  R a0 = c_hex27_alpha[I][0], a1 = c_hex27_alpha[I][1], a2 = c_hex27_alpha[I][2];
+  R p0 = phi_q(a0, xi[0]), p1 = phi_q(a1, xi[1]), p2 = phi_q(a2, xi[2]);
   g[0] = dphi_q(a0, xi[0]) * p1 * p2;
   g[1] = p0 * dphi_q(a1, xi[1]) * p2;
   g[2] = p0 * p1 * dphi_q(a2, xi[2]);
 }
-__device__ __forceinline__ double hex27_phi(int I, const double* xi) {
-  return phi_q(c_hex27_alpha[I][0], xi[0]) * phi_q(c_hex27_alpha[I][1], xi[1]) * phi_q(c_hex27_alpha[I][2], xi[2]);
+template <class R>
+__device__ __forceinline__ R hex27_phi(int I, const R* xi) {
+  return phi_q((R)c_hex27_alpha[I][0], xi[0]) * phi_q((R)c_hex27_alpha[I][1], xi[1]) *
+         phi_q((R)c_hex27_alpha[I][2], xi[2]);
 }
 // Jacobian of the trilinear Hex8 geometry from the 8 corners (smem, xyz per corner).
-__device__ __forceinline__ void hex8_jacobian(const double* Xc, const double* xi, double* J) {
+template <class R>
+__device__ __forceinline__ void hex8_jacobian(const R* Xc, const R* xi, R* J) {
 #pragma unroll
-  for (int k = 0; k < 9; ++k) J[k] = 0.0;
+  for (int k = 0; k < 9; ++k) J[k] = R(0.0);
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
-    double a0 = c_hex27_alpha[c][0], a1 = c_hex27_alpha[c][1], a2 = c_hex27_alpha[c][2];
-    double l0 = (1.0 + a0 * xi[0]) / 2.0, l1 = (1.0 + a1 * xi[1]) / 2.0, l2 = (1.0 + a2 * xi[2]) / 2.0;
-    double g0 = a0 / 2.0 * l1 * l2, g1 = l0 * a1 / 2.0 * l2, g2 = l0 * l1 * a2 / 2.0;
+    R a0 = c_hex27_alpha[c][0], a1 = c_hex27_alpha[c][1], a2 = c_hex27_alpha[c][2];
+    R l0 = (R(1.0) + a0 * xi[0]) / R(2.0), l1 = (R(1.0) + a1 * xi[1]) / R(2.0), l2 = (R(1.0) + a2 * xi[2]) / R(2.0);
+    R g0 = a0 / R(2.0) * l1 * l2, g1 = l0 * a1 / R(2.0) * l2, g2 = l0 * l1 * a2 / R(2.0);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      double x = Xc[3 * c + i];
+      R x = Xc[3 * c + i];
       J[3 * i + 0] += x * g0;
       J[3 * i + 1] += x * g1;
       J[3 * i + 2] += x * g2;
     }
   }
 }
-// Jacobian of the affine Tet4 geometry: J(:,j) = 0.5 (X_{j+1} - X_0)
-__device__ __forceinline__ void tet4_jacobian(const double* Xc, double* J) {
+// Jacobian of the affine Tet4 geometry: J(:,j) = R(0.5) (X_{j+1} - X_0)
+template <class R>
+__device__ __forceinline__ void tet4_jacobian(const R* Xc, R* J) {
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) J[3 * i + j] = -0.5 * Xc[i] + 0.5 * Xc[3 * (j + 1) + i];
+    for (int j = 0; j < 3; ++j) J[3 * i + j] = -R(0.5) * Xc[i] + R(0.5) * Xc[3 * (j + 1) + i];
 }
 
-__device__ __forceinline__ double det3(const double* m) {
+template <class R>
+__device__ __forceinline__ R det3(const R* m) {
   return m[0] * (m[4] * m[8] - m[7] * m[5]) - m[1] * (m[3] * m[8] - m[6] * m[5]) + m[2] * (m[3] * m[7] - m[6] * m[4]);
 }
 // inverse (row-major), returns det; out undefined when det == 0
-__device__ __forceinline__ double inv3(const double* m, double* o) {
-  double d = det3(m);
+template <class R>
+__device__ __forceinline__ R inv3(const R* m, R* o) {
+  R d = det3(m);
   o[0] = (m[4] * m[8] - m[7] * m[5]) / d;
   o[1] = -(m[1] * m[8] - m[7] * m[2]) / d;
   o[2] = (m[1] * m[5] - m[4] * m[2]) / d;
@@ -147,54 +161,57 @@ __device__ __forceinline__ double inv3(const double* m, double* o) {
 // ---- materials (materials.rs) -----------------------------------------------
 // Per quadrature point state.  M1 / M2 are the two matrices the pair
 // contraction needs: SNH: M1 = Cof(F) = J F^-T, StVK: M1 = S, M2 = F F^T.
+template <class R>
 struct QpState {
-  double F[9];
-  double M1[9];
-  double M2[9];
-  double s1, s2, s3, s4;
-  double P[9];
+  R F[9];
+  R M1[9];
+  R M2[9];
+  R s1, s2, s3, s4;
+  R P[9];
 };
 
-__device__ __forceinline__ bool snh_state(const double* F, double mu0, double lam0, QpState& q, bool need_stress) {
-  const double d = 3.0;
-  double mu = (d + 1.0) / d * mu0;
-  double lam = lam0 + (1.0 - 2.0 / (d * (d + 1.0))) * mu0;
-  double alpha = 1.0 + mu / lam * (d / (d + 1.0));
-  double IC = 0.0;
+template <class R>
+__device__ __forceinline__ bool snh_state(const R* F, R mu0, R lam0, QpState<R>& q, bool need_stress) {
+  const R d = R(3.0);
+  R mu = (d + R(1.0)) / d * mu0;
+  R lam = lam0 + (R(1.0) - R(2.0) / (d * (d + R(1.0)))) * mu0;
+  R alpha = R(1.0) + mu / lam * (d / (d + R(1.0)));
+  R IC = R(0.0);
 #pragma unroll
   for (int k = 0; k < 9; ++k) IC += F[k] * F[k];
-  double Fi[9];
-  double J = inv3(F, Fi);
-  if (J == 0.0) return false;
+  R Fi[9];
+  R J = inv3(F, Fi);
+  if (J == R(0.0)) return false;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j) q.M1[3 * i + j] = Fi[3 * j + i] * J;  // dJ/dF = F^-T J
-  double beta = IC + 1.0;
-  q.s1 = mu * (1.0 - 1.0 / beta);
-  q.s2 = mu * 2.0 / (beta * beta);
+  R beta = IC + R(1.0);
+  q.s1 = mu * (R(1.0) - R(1.0) / beta);
+  q.s2 = mu * R(2.0) / (beta * beta);
   q.s3 = lam * (J - alpha);
   q.s4 = lam;
   if (need_stress) {
-    double cf = mu * (1.0 - 1.0 / (IC + 1.0)), cj = lam * (J - alpha);
+    R cf = mu * (R(1.0) - R(1.0) / (IC + R(1.0))), cj = lam * (J - alpha);
 #pragma unroll
     for (int k = 0; k < 9; ++k) q.P[k] = F[k] * cf + q.M1[k] * cj;
   }
   return true;
 }
 
-__device__ __forceinline__ void stvk_state(const double* F, double mu, double lam, QpState& q, bool need_stress) {
-  double E[9];
+template <class R>
+__device__ __forceinline__ void stvk_state(const R* F, R mu, R lam, QpState<R>& q, bool need_stress) {
+  R E[9];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      double s = F[i] * F[j] + F[3 + i] * F[3 + j] + F[6 + i] * F[6 + j];  // (F^T F)(i,j)
-      E[3 * i + j] = (s - (i == j ? 1.0 : 0.0)) * 0.5;
+      R s = F[i] * F[j] + F[3 + i] * F[3 + j] + F[6 + i] * F[6 + j];  // (F^T F)(i,j)
+      E[3 * i + j] = (s - (i == j ? R(1.0) : R(0.0))) * R(0.5);
     }
-  double tr = E[0] + E[4] + E[8];
+  R tr = E[0] + E[4] + E[8];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) q.M1[k] = E[k] * 2.0 * mu + ((k % 4 == 0) ? lam * tr : 0.0);
+  for (int k = 0; k < 9; ++k) q.M1[k] = E[k] * R(2.0) * mu + ((k % 4 == 0) ? lam * tr : R(0.0));
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -210,7 +227,8 @@ __device__ __forceinline__ void stvk_state(const double* F, double mu, double la
   }
 }
 
-__device__ __forceinline__ bool material_state(int kind, const double* F, double mu, double lam, QpState& q,
+template <class R>
+__device__ __forceinline__ bool material_state(int kind, const R* F, R mu, R lam, QpState<R>& q,
                                                bool need_stress) {
 #pragma unroll
   for (int k = 0; k < 9; ++k) q.F[k] = F[k];
@@ -219,7 +237,8 @@ __device__ __forceinline__ bool material_state(int kind, const double* F, double
   return true;
 }
 
-__device__ __forceinline__ void mat3vec(const double* M, const double* a, double* o) {
+template <class R>
+__device__ __forceinline__ void mat3vec(const R* M, const R* a, R* o) {
   o[0] = M[0] * a[0] + M[1] * a[1] + M[2] * a[2];
   o[1] = M[3] * a[0] + M[4] * a[1] + M[5] * a[2];
   o[2] = M[6] * a[0] + M[7] * a[1] + M[8] * a[2];
@@ -229,27 +248,28 @@ __device__ __forceinline__ void mat3vec(const double* M, const double* a, double
 // Per-node vectors: v[0..2] = a, v[3..5] = F a, v[6..8] = M1 a.
 //  SNH : s1 (aI.aJ) I + s2 (F aI)(F aJ)^T + lam (Cof aI)(Cof aJ)^T + s3 eps_ijm (F (aI x aJ))_m
 //  StVK: (aJ . S aI) I + mu (F aJ)(F aI)^T + mu (aI.aJ) F F^T + lam (F aI)(F aJ)^T
-__device__ __forceinline__ void pair_block(int kind, const QpState& q, const double* vI, const double* vJ,
-                                           double* acc) {
-  double dot = vI[0] * vJ[0] + vI[1] * vJ[1] + vI[2] * vJ[2];
+template <class R>
+__device__ __forceinline__ void pair_block(int kind, const QpState<R>& q, const R* vI, const R* vJ,
+                                           R* acc) {
+  R dot = vI[0] * vJ[0] + vI[1] * vJ[1] + vI[2] * vJ[2];
   if (kind == HOEFEM_MAT_SNH) {
-    double cr[3] = {vI[1] * vJ[2] - vI[2] * vJ[1], vI[2] * vJ[0] - vI[0] * vJ[2], vI[0] * vJ[1] - vI[1] * vJ[0]};
-    double w[3];
+    R cr[3] = {vI[1] * vJ[2] - vI[2] * vJ[1], vI[2] * vJ[0] - vI[0] * vJ[2], vI[0] * vJ[1] - vI[1] * vJ[0]};
+    R w[3];
     mat3vec(q.F, cr, w);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = 0; j < 3; ++j) acc[3 * i + j] += q.s2 * vI[3 + i] * vJ[3 + j] + q.s4 * vI[6 + i] * vJ[6 + j];
-    double d1 = q.s1 * dot;
+    R d1 = q.s1 * dot;
     acc[0] += d1; acc[4] += d1; acc[8] += d1;
     // eps_ijm w_m: (0,1)=w2 (0,2)=-w1 (1,0)=-w2 (1,2)=w0 (2,0)=w1 (2,1)=-w0
-    double s3 = q.s3;
+    R s3 = q.s3;
     acc[1] += s3 * w[2]; acc[2] -= s3 * w[1];
     acc[3] -= s3 * w[2]; acc[5] += s3 * w[0];
     acc[6] += s3 * w[1]; acc[7] -= s3 * w[0];
   } else {
-    double d0 = vJ[0] * vI[6] + vJ[1] * vI[7] + vJ[2] * vI[8];  // aJ . S aI
-    double mu = q.s1, lam = q.s4;
+    R d0 = vJ[0] * vI[6] + vJ[1] * vI[7] + vJ[2] * vI[8];  // aJ . S aI
+    R mu = q.s1, lam = q.s4;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -320,7 +340,7 @@ __global__ void __launch_bounds__(TPB) k_forces(const BlockDev b, const int* __r
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int k = 0; k < 3; ++k) F[3 * c + k] = warp_sum(ul[c] * G[k]) + (c == k ? 1.0 : 0.0);
-    QpState st;
+    QpState<double> st;
     if (!material_state(mat.kind, F, mat.mu, mat.lambda, st, true)) { ok = false; break; }
     if (own) {
       double sc = w * fabs(detJ);
@@ -356,7 +376,7 @@ __device__ __forceinline__ void pair_of(int p, int& I, int& J) {
   else { I = c_pairs27[p][0]; J = c_pairs27[p][1]; }
 }
 
-template <int NN, int GROUP>
+template <int NN, int GROUP, class R>
 __global__ void __launch_bounds__(TPB) k_stiffness(const BlockDev b, const int* __restrict__ elems, int count,
                                                    const double* __restrict__ X, const double* __restrict__ u,
                                                    const int* __restrict__ adj_off, double* __restrict__ vals,
@@ -367,20 +387,21 @@ __global__ void __launch_bounds__(TPB) k_stiffness(const BlockDev b, const int* 
   const int grp = threadIdx.x / GROUP, t = threadIdx.x % GROUP;
   const int lane = threadIdx.x & 31;
   const int idx = blockIdx.x * EPC + grp;
-  __shared__ double s_vec[EPC][NN][9];
-  __shared__ double s_corner[EPC][24];
-  __shared__ QpState s_q[EPC];
+  __shared__ R s_vec[EPC][NN][9];
+  __shared__ R s_corner[EPC][24];
+  __shared__ QpState<R> s_q[EPC];
   __shared__ int s_g[EPC][NN];
   __shared__ int s_ok[EPC];
+  __shared__ int s_nq[EPC];
   const bool active = idx < count;
   const int e = active ? elems[idx] : 0;
   const bool nodewarp = (t < 32);
   const bool own = nodewarp && lane < NN && active;
   int g = own ? b.conn[lane * b.ne + e] : 0;
-  double Xl[3] = {0, 0, 0}, ul[3] = {0, 0, 0};
+  R Xl[3] = {0, 0, 0}, ul[3] = {0, 0, 0};
   if (own) {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) { Xl[k] = X[3 * g + k]; ul[k] = u[3 * g + k]; }
+    for (int k = 0; k < 3; ++k) { Xl[k] = (R)X[3 * g + k]; ul[k] = (R)u[3 * g + k]; }
     s_g[grp][lane] = g;
   }
   constexpr int NC = (NN == 10) ? 4 : 8;
@@ -390,53 +411,53 @@ __global__ void __launch_bounds__(TPB) k_stiffness(const BlockDev b, const int* 
   }
   if (t == 0) s_ok[grp] = 1;
   __syncthreads();
-  double J[9], Ji[9], detJ = 0.0;
+  R J[9], Ji[9], detJ = 0;
   if (NN == 10) {
     tet4_jacobian(s_corner[grp], J);
     detJ = inv3(J, Ji);
   }
-  double acc[PPT][9];
+  R acc[PPT][9];
 #pragma unroll
   for (int k = 0; k < PPT; ++k)
 #pragma unroll
-    for (int m = 0; m < 9; ++m) acc[k][m] = 0.0;
+    for (int m = 0; m < 9; ++m) acc[k][m] = 0;
   int q0 = 0, nq = 0;
   if (active) quad_rule(b, e, q0, nq);
   // uniform trip count across the CTA: the max over its elements
-  __shared__ int s_nq[EPC];
   if (t == 0) s_nq[grp] = nq;
   __syncthreads();
   int nq_max = 0;
 #pragma unroll
   for (int k = 0; k < EPC; ++k) nq_max = max(nq_max, s_nq[k]);
+  const R mu = (R)mat.mu, lam = (R)mat.lambda;
   for (int q = 0; q < nq_max; ++q) {
     const bool live = q < nq;
     if (nodewarp && live) {
-      const double xi[3] = {b.qp[3 * (q0 + q)], b.qp[3 * (q0 + q) + 1], b.qp[3 * (q0 + q) + 2]};
-      const double w = b.qw[q0 + q];
+      const R xi[3] = {(R)b.qp[3 * (q0 + q)], (R)b.qp[3 * (q0 + q) + 1], (R)b.qp[3 * (q0 + q) + 2]};
+      const R w = (R)b.qw[q0 + q];
       if (NN == 27) {
         hex8_jacobian(s_corner[grp], xi, J);
         detJ = inv3(J, Ji);
       }
-      double gr[3] = {0, 0, 0}, G[3] = {0, 0, 0};
+      R gr[3] = {0, 0, 0}, G[3] = {0, 0, 0};
       if (lane < NN) {
         if (NN == 10) tet10_grad(lane, xi, gr); else hex27_grad(lane, xi, gr);
 #pragma unroll
         for (int k = 0; k < 3; ++k) G[k] = Ji[k] * gr[0] + Ji[3 + k] * gr[1] + Ji[6 + k] * gr[2];
       }
-      double F[9];
+      R F[9];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) F[3 * c + k] = warp_sum(ul[c] * G[k]) + (c == k ? 1.0 : 0.0);
-      QpState st;
-      bool okq = (detJ != 0.0) && material_state(mat.kind, F, mat.mu, mat.lambda, st, false);
+        for (int k = 0; k < 3; ++k) F[3 * c + k] = warp_sum(ul[c] * G[k]) + (c == k ? R(1) : R(0));
+      QpState<R> st;
+      bool okq = (detJ != R(0)) && material_state(mat.kind, F, mu, lam, st, false);
       if (!okq) {
         if (lane == 0) s_ok[grp] = 0;
       } else if (lane < NN) {
-        double sc = sqrt(w * fabs(detJ));
-        double a[3] = {G[0] * sc, G[1] * sc, G[2] * sc};
-        double* v = s_vec[grp][lane];
+        R sc = sqrt(w * fabs(detJ));
+        R a[3] = {G[0] * sc, G[1] * sc, G[2] * sc};
+        R* v = s_vec[grp][lane];
         v[0] = a[0]; v[1] = a[1]; v[2] = a[2];
         mat3vec(st.F, a, v + 3);
         mat3vec(st.M1, a, v + 6);
@@ -445,7 +466,7 @@ __global__ void __launch_bounds__(TPB) k_stiffness(const BlockDev b, const int* 
     }
     __syncthreads();
     if (live) {
-      const QpState& st = s_q[grp];
+      const QpState<R>& st = s_q[grp];
 #pragma unroll
       for (int k = 0; k < PPT; ++k) {
         int p = t + k * GROUP;
@@ -476,14 +497,14 @@ __global__ void __launch_bounds__(TPB) k_stiffness(const BlockDev b, const int* 
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) vals[bIJ + i * rlI + j] += acc[k][3 * i + j];
+        for (int j = 0; j < 3; ++j) vals[bIJ + i * rlI + j] += (double)acc[k][3 * i + j];
       if (I != Jn) {
         int rlJ = 3 * (adj_off[gJ + 1] - adj_off[gJ]);
         int bJI = em[Jn * NN + I];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
-          for (int j = 0; j < 3; ++j) vals[bJI + j * rlJ + i] += acc[k][3 * i + j];
+          for (int j = 0; j < 3; ++j) vals[bJI + j * rlJ + i] += (double)acc[k][3 * i + j];
       }
     }
   }
@@ -592,16 +613,27 @@ void launch_forces(const Model& m, const MatDev& mat, const double* u, double* f
   HOEFEM_CUDA(cudaGetLastError());
 }
 
-void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s) {
+void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s,
+                      int precision) {
   init_pairs();
   for (const Block* bp : m.blocks) {
     BlockDev bd = bp->dev();
     for_each_color(*bp, [&](const int* elems, int cnt) {
+      const int grid10 = (cnt + TPB / 32 - 1) / (TPB / 32);
       if (bp->kind == HOEFEM_ELEM_TET10) {
-        int grid = (cnt + TPB / 32 - 1) / (TPB / 32);
-        (note_launch(), k_stiffness<10, 32><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p, vals, mat, m.d_err.p));
+        if (precision == PRECISION_FP32)
+          (note_launch(), k_stiffness<10, 32, float><<<grid10, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
+                                                                            vals, mat, m.d_err.p));
+        else
+          (note_launch(), k_stiffness<10, 32, double><<<grid10, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
+                                                                             vals, mat, m.d_err.p));
       } else {
-        (note_launch(), k_stiffness<27, TPB><<<cnt, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p, vals, mat, m.d_err.p));
+        if (precision == PRECISION_FP32)
+          (note_launch(), k_stiffness<27, TPB, float><<<cnt, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
+                                                                          vals, mat, m.d_err.p));
+        else
+          (note_launch(), k_stiffness<27, TPB, double><<<cnt, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
+                                                                           vals, mat, m.d_err.p));
       }
     });
   }

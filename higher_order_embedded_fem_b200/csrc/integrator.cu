@@ -112,6 +112,10 @@ struct Integrator {
   std::unique_ptr<Precond> own;
   double cg_tol = 1e-5;
   i64 cg_max = 500, newton_max = 100;
+  int precision = PRECISION_FP64;  // PRECISION_FP32: mixed (FP32 element stiffness, FP32 operator / Schwarz apply
+                                   // inside FP64 iterative refinement)
+  double inner_tol = 1e-2;
+  DBuf<float> J32;
   double rep_force = 0.0;
   DBuf<unsigned char> bc;
   DBuf<double> M, K, J, gforce, up, vn, w, F, dx, us, vs, f, u, v, partials, scalars;
@@ -119,6 +123,7 @@ struct Integrator {
   double* h_scalar = nullptr;
   CgWork cg;
   hoefem_step_stats stats{};
+  i64 stats_outer = 0;
   cudaEvent_t ev[2] = {nullptr, nullptr};
 
   ~Integrator() {
@@ -221,13 +226,14 @@ struct Integrator {
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
     (note_launch(), k_be_state<<<grid(), TPB, 0, s>>>(n, up.p, vn.p, w.p, dt, bcp, us.p, vs.p));
     K.zero(s);
-    launch_stiffness(*m, mat, us.p, K.p, s);
+    launch_stiffness(*m, mat, us.p, K.p, s, precision);
     // J = gamma M - beta D - alpha K with alpha = -dt^2, gamma = 1, no damping
     jacobian_combination(*m, -(-dt * dt), K.p, 1.0, M.p, bcp, J.p, scalars.p + 4, s);
     HOEFEM_CUDA(cudaEventRecord(ev[1], s));
     check_device_error(*m);
     stats.ms_assemble_stiffness += elapsed();
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
+    P->want_fp32 = (precision == PRECISION_FP32);
     precond_update(*P, J.p, s);
     HOEFEM_CUDA(cudaEventRecord(ev[1], s));
     HOEFEM_CUDA(cudaEventSynchronize(ev[1]));
@@ -236,7 +242,16 @@ struct Integrator {
     (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, F.p, cg.b.p));
     i64 it = 0;
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
-    int st = cg_solve(cg, J.p, P, cg_tol, cg_max, &it, s);
+    int st;
+    if (precision == PRECISION_FP32) {
+      if (J32.n < (size_t)m->nnz) J32.alloc(m->nnz);
+      to_f32(J.p, J32.p, m->nnz, s);
+      i64 outer = 0;
+      st = cg_solve_ir(cg, J.p, J32.p, P, cg_tol, cg_max, inner_tol, &it, &outer, s);
+      stats_outer += outer;
+    } else {
+      st = cg_solve(cg, J.p, P, cg_tol, cg_max, &it, s);
+    }
     HOEFEM_CUDA(cudaEventRecord(ev[1], s));
     HOEFEM_CUDA(cudaEventSynchronize(ev[1]));
     stats.ms_cg += elapsed();
@@ -350,6 +365,10 @@ Integrator* integrator_new(Model* m, const hoefem_material* mat, double density,
   return it.release();
 }
 void integrator_delete(Integrator* it) { delete it; }
+void integrator_set_precision(Integrator* it, int precision, double inner_tol) {
+  it->precision = precision;
+  it->inner_tol = inner_tol;
+}
 void integrator_set_tolerances(Integrator* it, double tol, i64 cg_max, i64 newton_max) {
   it->cg_tol = tol;
   it->cg_max = cg_max;

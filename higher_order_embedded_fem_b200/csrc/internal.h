@@ -141,7 +141,11 @@ struct MatDev {
 
 // ---- element kernels (elements.cu) -----------------------------------------
 void launch_forces(const Model& m, const MatDev& mat, const double* u, double* f, cudaStream_t s);
-void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s);
+enum Precision { PRECISION_FP64 = 0, PRECISION_FP32 = 1 };
+// Element stiffness with the element arithmetic in FP64 or FP32; the CSR
+// values are accumulated in FP64 either way.
+void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s,
+                      int precision = PRECISION_FP64);
 void launch_mass(const Model& m, double density, double* vals, cudaStream_t s);
 
 // ---- sparse / vector kernels (linalg.cu) -----------------------------------

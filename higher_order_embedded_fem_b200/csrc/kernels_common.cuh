@@ -14,16 +14,18 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 }
 
 // Three row sums of node a (warp cooperative; result valid in every lane).
-__device__ __forceinline__ void node_row_dot(const NodeRows& A, const double* __restrict__ vals,
+// Matrix values are FP64 or FP32 (V); products and sums are FP64.
+template <class V>
+__device__ __forceinline__ void node_row_dot(const NodeRows& A, const V* __restrict__ vals,
                                              const double* __restrict__ x, int a, int lane, double& s0, double& s1,
                                              double& s2) {
   s0 = s1 = s2 = 0.0;
   const long long b = A.base[a];
   if (A.diag_only && A.diag_only[a]) {
     if (lane == 0) {
-      s0 = vals[b] * x[3 * a];
-      s1 = vals[b + 1] * x[3 * a + 1];
-      s2 = vals[b + 2] * x[3 * a + 2];
+      s0 = (double)vals[b] * x[3 * a];
+      s1 = (double)vals[b + 1] * x[3 * a + 1];
+      s2 = (double)vals[b + 2] * x[3 * a + 2];
     }
   } else {
     const int o = A.adj_off[a], d = A.adj_off[a + 1] - o;
@@ -31,12 +33,12 @@ __device__ __forceinline__ void node_row_dot(const NodeRows& A, const double* __
     for (int s = lane; s < d; s += 32) {
       const int nb = A.adj[o + s];
       const double x0 = x[3 * nb], x1 = x[3 * nb + 1], x2 = x[3 * nb + 2];
-      const double* r0 = vals + b + 3 * s;
-      s0 += r0[0] * x0 + r0[1] * x1 + r0[2] * x2;
-      const double* r1 = r0 + rl;
-      s1 += r1[0] * x0 + r1[1] * x1 + r1[2] * x2;
-      const double* r2 = r1 + rl;
-      s2 += r2[0] * x0 + r2[1] * x1 + r2[2] * x2;
+      const V* r0 = vals + b + 3 * s;
+      s0 += (double)r0[0] * x0 + (double)r0[1] * x1 + (double)r0[2] * x2;
+      const V* r1 = r0 + rl;
+      s1 += (double)r1[0] * x0 + (double)r1[1] * x1 + (double)r1[2] * x2;
+      const V* r2 = r1 + rl;
+      s2 += (double)r2[0] * x0 + (double)r2[1] * x1 + (double)r2[2] * x2;
     }
   }
   s0 = warp_sum_d(s0);

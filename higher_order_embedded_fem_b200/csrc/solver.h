@@ -25,6 +25,8 @@ struct Precond {
   DBuf<long long> d_base, d_gmap_off;
   DBuf<unsigned char> d_diag_only;
   DBuf<double> vals, staging;
+  DBuf<float> vals32;  // FP32 copy of the Schwarz values (mixed-precision apply)
+  bool want_fp32 = false;
   DBuf<long long> d_stage_off;
   DBuf<int> d_err;
   i64 nnz = 0;
@@ -49,11 +51,14 @@ struct CgWork {
   DBuf<CgState> st;
   DBuf<unsigned> counter;
   CgState* h_st = nullptr;  // pinned
-  cudaGraphExec_t graph = nullptr;
-  const void* graph_key[3] = {nullptr, nullptr, nullptr};
-  int graph_kind = -1;
+  DBuf<double> xo, bo, ro;  // iterative refinement: solution, rhs, FP64 residual
+  struct Graph {
+    const void* key[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaGraphExec_t exec = nullptr;
+    long long kernels = 0;
+  };
+  std::vector<Graph> graphs;  // chunk graphs per (operator, preconditioner, precision)
   int chunk = 8;
-  long long graph_kernels = 0;
   void init(Model* model);
   ~CgWork();
 };
@@ -61,5 +66,9 @@ struct CgWork {
 // Solves A x = b with x = work.x (initial guess) and b = work.b on the model
 // pattern values `vals`.  Returns HOEFEM_OK or a HOEFEM_CG_* status.
 int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 max_iter, i64* iters, cudaStream_t s);
+// FP64 iterative refinement around an FP32-operator / FP32-preconditioner PCG.
+int cg_solve_ir(CgWork& w, const double* A64, const float* A32, const Precond* P, double tol, i64 max_iter,
+                double inner_tol, i64* iters, i64* outer, cudaStream_t s);
+void to_f32(const double* a, float* b, long long n, cudaStream_t s);
 
 }  // namespace hoefem

@@ -99,6 +99,13 @@ class _Model:
                                                    ptr(values)[0], mem))
         return values
 
+    def assemble_stiffness_into_precision(self, values, u, material, mixed):
+        """Stiffness with FP32 element arithmetic when `mixed` (FP64 accumulation)."""
+        mem = _same_space(values, u)
+        check(lib().hoefem_assemble_stiffness_into_precision(self._h, C.byref(material.descriptor()), ptr(u)[0],
+                                                             ptr(values)[0], 1 if mixed else 0, mem))
+        return values
+
     def assemble_stiffness(self, u, material):
         v = np.zeros(self.nnz) if not _capi.is_device_array(u) else u.new_zeros(self.nnz)
         return self.assemble_stiffness_into_par(v, u, material)

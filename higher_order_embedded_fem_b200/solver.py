@@ -159,6 +159,19 @@ class ConjugateGradient:
         self.max_iter = int(n)
         return self
 
+    def solve_with_guess_mixed(self, b, x, inner_tol=1e-2):
+        """FP64 iterative refinement around an FP32-operator PCG."""
+        it = C.c_int64()
+        mem = _same_space(self.values, b, x)
+        st = lib().hoefem_cg_solve_mixed(self.model._h, ptr(self.values)[0],
+                                         self.preconditioner._h if self.preconditioner is not None else None,
+                                         ptr(b)[0], ptr(x)[0], self.criterion.tol, self.max_iter, float(inner_tol),
+                                         C.byref(it), mem)
+        if st in _CG_KIND:
+            raise SolveError(_CG_KIND[st], CgOutput(it.value))
+        check(st)
+        return CgOutput(it.value)
+
     def solve_with_guess(self, b, x):
         it = C.c_int64()
         mem = _same_space(self.values, b, x)
@@ -199,6 +212,11 @@ class NewtonCgIntegrator3d:
 
     def set_tolerances(self, cg_tol=1e-5, cg_max_iter=500, newton_max_iter=100):
         check(lib().hoefem_integrator_set_tolerances(self._h, cg_tol, cg_max_iter, newton_max_iter))
+
+    def set_precision(self, mixed, inner_tol=1e-2):
+        """mixed=True: FP32 element stiffness / operator / Schwarz apply inside
+        FP64 iterative refinement (see hoefem_integrator_set_precision)."""
+        check(lib().hoefem_integrator_set_precision(self._h, 1 if mixed else 0, float(inner_tol)))
 
     def step(self, u, v, t, dt):
         """Advances (u, v) in place by dt; returns the step statistics."""

@@ -139,6 +139,12 @@ int hoefem_assemble_elastic_pseudo_forces_into(hoefem_model m, const hoefem_mate
    model pattern; colored scatter without atomics, one launch per color. */
 int hoefem_assemble_stiffness_into(hoefem_model m, const hoefem_material* mat, const double* u, double* values,
                                    int mem);
+/* hoefem_assemble_stiffness_into with the element arithmetic in the given
+   precision (HOEFEM_PRECISION_MIXED: FP32 kinematics, material tangent and
+   pair contractions; the CSR values are accumulated in FP64).  No counterpart
+   in the reference (its stiffness is FP64). */
+int hoefem_assemble_stiffness_into_precision(hoefem_model m, const hoefem_material* mat, const double* u,
+                                             double* values, int precision, int mem);
 /* ElasticityModel::assemble_mass(density).to_csr (solid/mod.rs:106,
    assembly.rs:624-671): values += M on the model pattern. */
 int hoefem_assemble_mass_into(hoefem_model m, double density, double* values, int mem);
@@ -188,6 +194,13 @@ int hoefem_precond_destroy(hoefem_precond p);
 int hoefem_cg_solve(hoefem_model m, const double* system_values, hoefem_precond p, const double* b, double* x,
                     double tol, int64_t max_iter, int64_t* iterations, int mem);
 
+/* Mixed-precision variant of hoefem_cg_solve: FP64 iterative refinement
+   around a PCG with FP32 operator values (converted from system_values) and,
+   for a Schwarz preconditioner, FP32 preconditioner values.  *iterations is
+   the total number of inner iterations.  No counterpart in the reference. */
+int hoefem_cg_solve_mixed(hoefem_model m, const double* system_values, hoefem_precond p, const double* b, double* x,
+                          double tol, int64_t max_iter, double inner_tol, int64_t* iterations, int mem);
+
 /* ------------------------------------------------------------------------ */
 /* NewtonCgIntegrator3d (simulation_toolbox/src/fem/newton_cg.rs:43-295):
    backward Euler (hamilton2/src/integrators/euler.rs:155-199) solved by
@@ -223,6 +236,17 @@ int hoefem_integrator_create(hoefem_model m, const hoefem_material* mat, double 
    newton_max_iter 100 (newton_cg.rs:282-286,761-773). */
 int hoefem_integrator_set_tolerances(hoefem_integrator it, double cg_tol, int64_t cg_max_iter,
                                      int64_t newton_max_iter);
+/* Arithmetic of the step.  HOEFEM_PRECISION_FP64: the reference's FP64
+   everywhere.  HOEFEM_PRECISION_MIXED: element stiffness arithmetic in FP32
+   (CSR accumulation FP64), Schwarz blocks built in FP64 and applied in FP32,
+   and the Jacobian solve as FP64 iterative refinement (true FP64 residual,
+   stop at ||r|| <= cg_tol ||b||) around an inner PCG with FP32 operator /
+   preconditioner values and FP64 vectors, each inner solve run to the
+   relative tolerance max(inner_tol, what the outer target still needs).
+   Forces, the Newton residual and the line search stay FP64.  No counterpart
+   in the reference (an addition on top of its FP64 path). */
+typedef enum { HOEFEM_PRECISION_FP64 = 0, HOEFEM_PRECISION_MIXED = 1 } hoefem_precision;
+int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double inner_tol);
 /* One time step: u, v (ndof) updated in place. */
 int hoefem_integrator_step(hoefem_integrator it, double* u, double* v, double t, double dt, int mem);
 int hoefem_integrator_stats(hoefem_integrator it, hoefem_step_stats* out);

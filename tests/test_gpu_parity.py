@@ -224,3 +224,31 @@ def test_newton_step_embedded_schwarz_matches_oracle():
     assert st["newton_iterations"] == rs["newton_iters"]
     assert abs(st["total_cg_iterations"] - sum(rs["cg_iters"])) <= max(2, 0.02 * sum(rs["cg_iters"]))
     assert rel(u, ur) < 1e-8 and rel(v, vr) < 1e-8
+
+
+def test_schwarz_indefinite_blocks_take_the_eigen_path():
+    # Negated system matrix: every block is negative definite, the Cholesky fast
+    # path fails and the eigen-decomposition path applies the |lambda| rule.
+    e, m, mat, ref = embedded_setup(6)
+    u = H.scenes.random_normal(3, m.ndof(), 0.01 * e.cell_size)
+    comp = H.SchwarzPreconditionerComponent.from_embedded_model(m, e.volume_fractions, 0.5)
+    ref.set_bc(e.nodes_below(2, 1e-9))
+    ref.set_schwarz(comp.schwarz_connectivity, comp.untreated_nodes)
+    ref.setup()
+    J = -ref.jacobian(ref.stiffness(u), 1e-3)
+    P = comp.build(m)
+    P.update(J)
+    assert rel(P.values(), ref.schwarz_update(J)) < RTOL
+
+
+def test_schwarz_zero_diagonal_is_an_error():
+    e, m, mat, ref = embedded_setup(6)
+    comp = H.SchwarzPreconditionerComponent.from_embedded_model(m, e.volume_fractions, 0.5)
+    P = comp.build(m)
+    with pytest.raises(H.HoefemError) as ei:
+        P.update(np.zeros(m.nnz))
+    assert ei.value.status in ("ZERO_DIAGONAL", "NONFINITE")
+    D = H.DiagonalPreconditioner(m)
+    with pytest.raises(H.HoefemError) as ei:
+        D.update(np.zeros(m.nnz))
+    assert ei.value.status == "ZERO_DIAGONAL"
