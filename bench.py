@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--roofline-reps", type=int, default=20)
+    ap.add_argument("--inner-tol", type=float, default=1e-2, help="mixed variant: inner FP32 PCG tolerance")
+    ap.add_argument("--variants", default="plain,mixed", help="comma list: plain, mixed")
     return ap.parse_args()
 
 
@@ -210,29 +212,48 @@ def run_hoefem(args):
         vd.copy_(v0d)
         return integ.step(ud, vd, 0.0, DT)
 
-    for _ in range(args.warmup):
-        st = step()
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    clocks = Clocks(local)
-    clocks.start()
-    n0 = H._capi.launch_count()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    per = []
-    for _ in range(args.steps):
-        st = step()
-        per.append(st)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    launches = H._capi.launch_count() - n0
-    if world > 1:
-        torch.distributed.barrier()
-    ck = clocks.stop()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    ms = max_over_ranks(ms, world, dev)
+    variants = {}
+    for vname in [v.strip() for v in args.variants.split(",") if v.strip()]:
+        integ.set_precision(vname == "mixed", args.inner_tol)
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        clocks = Clocks(local)
+        clocks.start()
+        n0 = H._capi.launch_count()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        per = []
+        for _ in range(args.steps):
+            per.append(step())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        launches = H._capi.launch_count() - n0
+        if world > 1:
+            torch.distributed.barrier()
+        ck = clocks.stop()
+        ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world, dev)
+        s_ = per[-1]
+        variants[vname] = {
+            "ms_per_step": ms, "cg_iterations": int(s_["total_cg_iterations"]),
+            "newton_iterations": int(s_["newton_iterations"]), "residual_norm": s_["residual_norm"],
+            "phase_ms": {"forces": s_["ms_assemble_forces"], "stiffness": s_["ms_assemble_stiffness"],
+                         "precond_update": s_["ms_precond_update"], "cg": s_["ms_cg"], "total": s_["ms_total"]},
+            "gpu_launches": int(launches), "clocks": ck, "u": ud.cpu().numpy(),
+        }
+    head = "mixed" if "mixed" in variants else list(variants)[0]
+    ms = variants[head]["ms_per_step"]
+    launches = variants[head]["gpu_launches"]
+    ck = variants[head]["clocks"]
+    integ.set_precision(head == "mixed", args.inner_tol)
+    if "mixed" in variants and "plain" in variants:
+        up, um = variants["plain"]["u"], variants["mixed"]["u"]
+        variants["mixed"]["rel_diff_u_vs_plain"] = float(np.abs(um - up).max() / np.abs(up).max())
+    for v in variants.values():
+        v.pop("u")
 
     # end to end through the public API with pinned host buffers
     uh = torch.empty(model.ndof(), dtype=torch.float64, pin_memory=True).numpy()
@@ -266,23 +287,22 @@ def run_hoefem(args):
                "cg_iterations": int(sum(rst["cg_iters"]))}
 
     if rank == 0:
-        s = per[-1]
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
             os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
         line = {
             "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene, replicas per rank)",
-            "variant": "plain_fp64",
+            "variant": {"mixed": "mixed_fp32", "plain": "plain_fp64"}[head],
+            "variants": variants,
             "config": {"workload": "embedded Hex27 hollow cylinder %d^3 (r 0.3-0.4), StVK E=5e5 nu=0.45, one "
                                    "backward-Euler Newton step dt=1e-3, Schwarz-CG to %g" % (args.n, args.cg_tol),
                        "ndof": model.ndof(), "nnz": model.nnz, "elements": model.num_elements,
                        "schwarz_subdomains": len(comp.schwarz_connectivity),
                        "l2": "inputs larger than L2 (CSR values %d MB)" % (model.nnz * 8 // 2 ** 20),
                        "parallelism": "replicas" if world > 1 else "single"},
-            "cg_iterations": int(s["total_cg_iterations"]), "newton_iterations": int(s["newton_iterations"]),
-            "phase_ms": {"forces": s["ms_assemble_forces"], "stiffness": s["ms_assemble_stiffness"],
-                         "precond_update": s["ms_precond_update"], "cg": s["ms_cg"], "total": s["ms_total"]},
+            "cg_iterations": variants[head]["cg_iterations"], "newton_iterations": variants[head]["newton_iterations"],
+            "speedup_vs_plain_fp64": (variants["plain"]["ms_per_step"] / ms) if "plain" in variants else None,
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * 8 * model.ndof(),

@@ -218,6 +218,17 @@ int hoefem_model_set_stream(hoefem_model m, void* stream) {
   API_END
 }
 
+int hoefem_model_autotune(hoefem_model m, int32_t* lanes) {
+  API_BEGIN
+  Model& mm = device_model(m);
+  DBuf<double> v;
+  v.alloc(mm.nnz);
+  v.zero(mm.stream);
+  mm.spmv_lanes = autotune_spmv_lanes(mm.rows(), v.p, mm.stream);
+  if (lanes) *lanes = mm.spmv_lanes;
+  API_END
+}
+
 int hoefem_model_sizes(hoefem_model m, int64_t* ndof, int64_t* nnz, int64_t* num_elements, int64_t* num_blocks) {
   API_BEGIN
   Model& mm = model_of(m);

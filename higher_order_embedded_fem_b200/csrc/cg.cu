@@ -24,24 +24,23 @@
 
 namespace hoefem {
 
-int spmv_grid(int nv);
+int spmv_grid(int nv, int lanes);
 
 namespace {
 
 constexpr int TPB = 256;
 
 // r = b - A x ; partial b.b, r.r
-template <class VA>
+template <int L, class VA>
 __global__ void __launch_bounds__(TPB) k_cg_init(NodeRows A, const VA* __restrict__ vals,
                                                  const double* __restrict__ x, const double* __restrict__ b,
                                                  double* __restrict__ r, double* partials, unsigned* counter,
                                                  CgState* st) {
-  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
   double acc[2] = {0.0, 0.0};
-  for (int a = blockIdx.x * wpb + (threadIdx.x >> 5); a < A.nv; a += gridDim.x * wpb) {
+  for_each_node<L>(A.nv, [&](int a, int sl) {
     double s[3];
-    node_row_dot(A, vals, x, a, lane, s[0], s[1], s[2]);
-    if (lane == 0) {
+    node_row_dot<L>(A, vals, x, a, sl, s[0], s[1], s[2]);
+    if (a >= 0 && sl == 0) {
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
         double bi = b[3 * a + i];
@@ -51,7 +50,7 @@ __global__ void __launch_bounds__(TPB) k_cg_init(NodeRows A, const VA* __restric
         acc[1] += ri * ri;
       }
     }
-  }
+  });
   double tot[2];
   if (grid_reduce_last_k<2>(acc, partials, counter, tot) && threadIdx.x == 0) {
     st->bnorm = sqrt(tot[0]);
@@ -83,24 +82,23 @@ __global__ void __launch_bounds__(TPB) k_cg_prec_vec(int n, int mode, const doub
 }
 
 // z = P r with P a node-row matrix (Schwarz) ; partial z.r.
-template <class VP>
+template <int L, class VP>
 __global__ void __launch_bounds__(TPB) k_cg_prec_spmv(NodeRows P, const VP* __restrict__ pv,
                                                       const double* __restrict__ r, double* __restrict__ z,
                                                       double* partials, unsigned* counter, CgState* st, int init) {
   if (!init && st->done) return;
-  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
   double acc[1] = {0.0};
-  for (int a = blockIdx.x * wpb + (threadIdx.x >> 5); a < P.nv; a += gridDim.x * wpb) {
+  for_each_node<L>(P.nv, [&](int a, int sl) {
     double s[3];
-    node_row_dot(P, pv, r, a, lane, s[0], s[1], s[2]);
-    if (lane == 0) {
+    node_row_dot<L>(P, pv, r, a, sl, s[0], s[1], s[2]);
+    if (a >= 0 && sl == 0) {
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
         z[3 * a + i] = s[i];
         acc[0] += s[i] * r[3 * a + i];
       }
     }
-  }
+  });
   double tot[1];
   if (grid_reduce_last_k<1>(acc, partials, counter, tot) && threadIdx.x == 0) {
     if (init) st->zTr = tot[0];
@@ -129,24 +127,23 @@ __global__ void k_cg_init_check(CgState* st) {
 }
 
 // Ap = A p ; pAp ; checks ; alpha
-template <class VA>
+template <int L, class VA>
 __global__ void __launch_bounds__(TPB) k_cg_Ap(NodeRows A, const VA* __restrict__ vals,
                                                const double* __restrict__ p, double* __restrict__ Ap,
                                                double* partials, unsigned* counter, CgState* st) {
   if (st->done) return;
-  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
   double acc[1] = {0.0};
-  for (int a = blockIdx.x * wpb + (threadIdx.x >> 5); a < A.nv; a += gridDim.x * wpb) {
+  for_each_node<L>(A.nv, [&](int a, int sl) {
     double s[3];
-    node_row_dot(A, vals, p, a, lane, s[0], s[1], s[2]);
-    if (lane == 0) {
+    node_row_dot<L>(A, vals, p, a, sl, s[0], s[1], s[2]);
+    if (a >= 0 && sl == 0) {
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
         Ap[3 * a + i] = s[i];
         acc[0] += p[3 * a + i] * s[i];
       }
     }
-  }
+  });
   double tot[1];
   if (grid_reduce_last_k<1>(acc, partials, counter, tot) && threadIdx.x == 0) {
     double pAp = tot[0];
@@ -253,22 +250,28 @@ const void* prec_key(const Precond* P, bool p32) {
 
 void enqueue_Ap(CgWork& w, Operator A, cudaStream_t s) {
   NodeRows R = w.m->rows();
-  const int sg = spmv_grid(R.nv);
-  if (A.v32)
-    (note_launch(), k_cg_Ap<float><<<sg, TPB, 0, s>>>(R, A.v32, w.p.p, w.Ap.p, w.partials.p, w.counter.p, w.st.p));
-  else
-    (note_launch(), k_cg_Ap<double><<<sg, TPB, 0, s>>>(R, A.v64, w.p.p, w.Ap.p, w.partials.p, w.counter.p, w.st.p));
+  HOEFEM_LANES_DISPATCH(R.lanes, {
+    const int sg = spmv_grid(R.nv, LN);
+    if (A.v32)
+      (note_launch(), k_cg_Ap<LN, float><<<sg, TPB, 0, s>>>(R, A.v32, w.p.p, w.Ap.p, w.partials.p, w.counter.p,
+                                                            w.st.p));
+    else
+      (note_launch(), k_cg_Ap<LN, double><<<sg, TPB, 0, s>>>(R, A.v64, w.p.p, w.Ap.p, w.partials.p, w.counter.p,
+                                                             w.st.p));
+  });
 }
 
 void enqueue_prec_spmv(CgWork& w, const Precond* P, bool p32, int init, cudaStream_t s) {
   NodeRows PR = P->rows();
-  const int g = spmv_grid(PR.nv);
-  if (p32)
-    (note_launch(), k_cg_prec_spmv<float><<<g, TPB, 0, s>>>(PR, P->vals32.p, w.r.p, w.z.p, w.partials.p, w.counter.p,
-                                                            w.st.p, init));
-  else
-    (note_launch(), k_cg_prec_spmv<double><<<g, TPB, 0, s>>>(PR, P->vals.p, w.r.p, w.z.p, w.partials.p, w.counter.p,
-                                                             w.st.p, init));
+  HOEFEM_LANES_DISPATCH(PR.lanes, {
+    const int g = spmv_grid(PR.nv, LN);
+    if (p32)
+      (note_launch(), k_cg_prec_spmv<LN, float><<<g, TPB, 0, s>>>(PR, P->vals32.p, w.r.p, w.z.p, w.partials.p,
+                                                                  w.counter.p, w.st.p, init));
+    else
+      (note_launch(), k_cg_prec_spmv<LN, double><<<g, TPB, 0, s>>>(PR, P->vals.p, w.r.p, w.z.p, w.partials.p,
+                                                                   w.counter.p, w.st.p, init));
+  });
 }
 
 void enqueue_iteration(CgWork& w, Operator A, const Precond* P, bool p32, cudaStream_t s) {
@@ -326,13 +329,16 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   init.tol = tol;
   init.max_iter = max_iter;
   HOEFEM_CUDA(cudaMemcpyAsync(w.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
-  const int sg = spmv_grid(R.nv), vg = vec_grid(n);
-  if (A.v32)
-    (note_launch(), k_cg_init<float><<<sg, TPB, 0, s>>>(R, A.v32, w.x.p, w.b.p, w.r.p, w.partials.p, w.counter.p,
-                                                        w.st.p));
-  else
-    (note_launch(), k_cg_init<double><<<sg, TPB, 0, s>>>(R, A.v64, w.x.p, w.b.p, w.r.p, w.partials.p, w.counter.p,
-                                                         w.st.p));
+  const int vg = vec_grid(n);
+  HOEFEM_LANES_DISPATCH(R.lanes, {
+    const int sg = spmv_grid(R.nv, LN);
+    if (A.v32)
+      (note_launch(), k_cg_init<LN, float><<<sg, TPB, 0, s>>>(R, A.v32, w.x.p, w.b.p, w.r.p, w.partials.p,
+                                                              w.counter.p, w.st.p));
+    else
+      (note_launch(), k_cg_init<LN, double><<<sg, TPB, 0, s>>>(R, A.v64, w.x.p, w.b.p, w.r.p, w.partials.p,
+                                                               w.counter.p, w.st.p));
+  });
   if (kind == PREC_SCHWARZ) {
     enqueue_prec_spmv(w, P, p32, 1, s);
   } else {
@@ -384,15 +390,18 @@ int cg_solve_ir(CgWork& w, const double* A64, const float* A32, const Precond* P
                 double inner_tol, i64* iters, i64* outer, cudaStream_t s) {
   NodeRows R = w.m->rows();
   const int n = (int)w.n;
-  const int sg = spmv_grid(R.nv), vg = vec_grid(n);
+  const int vg = vec_grid(n);
   const bool p32 = P && P->kind == PREC_SCHWARZ && P->vals32.p;
   HOEFEM_CUDA(cudaMemcpyAsync(w.xo.p, w.x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   HOEFEM_CUDA(cudaMemcpyAsync(w.bo.p, w.b.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   auto residual = [&](double* rnorm, double* bnorm) {
     CgState init{};
     HOEFEM_CUDA(cudaMemcpyAsync(w.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
-    (note_launch(), k_cg_init<double><<<sg, TPB, 0, s>>>(R, A64, w.xo.p, w.bo.p, w.ro.p, w.partials.p, w.counter.p,
-                                                         w.st.p));
+    HOEFEM_LANES_DISPATCH(R.lanes, {
+      const int sg = spmv_grid(R.nv, LN);
+      (note_launch(), k_cg_init<LN, double><<<sg, TPB, 0, s>>>(R, A64, w.xo.p, w.bo.p, w.ro.p, w.partials.p,
+                                                               w.counter.p, w.st.p));
+    });
     HOEFEM_CUDA(cudaGetLastError());
     HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
     HOEFEM_CUDA(cudaStreamSynchronize(s));

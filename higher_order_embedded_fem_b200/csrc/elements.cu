@@ -377,11 +377,11 @@ __device__ __forceinline__ void pair_of(int p, int& I, int& J) {
 }
 
 template <int NN, int GROUP, class R>
-__global__ void __launch_bounds__(TPB) k_stiffness(const BlockDev b, const int* __restrict__ elems, int count,
+__global__ void __launch_bounds__(NN == 10 ? TPB : 384, NN == 10 ? 1 : 2) k_stiffness(const BlockDev b, const int* __restrict__ elems, int count,
                                                    const double* __restrict__ X, const double* __restrict__ u,
                                                    const int* __restrict__ adj_off, double* __restrict__ vals,
                                                    MatDev mat, int* err) {
-  constexpr int EPC = TPB / GROUP;                 // elements per CTA
+  constexpr int EPC = (NN == 10 ? TPB : 384) / GROUP;  // elements per CTA
   constexpr int NP = PairTable<NN>::NP;            // node pairs I >= J
   constexpr int PPT = (NP + GROUP - 1) / GROUP;    // pairs per thread
   const int grp = threadIdx.x / GROUP, t = threadIdx.x % GROUP;
@@ -629,10 +629,10 @@ void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double
                                                                              vals, mat, m.d_err.p));
       } else {
         if (precision == PRECISION_FP32)
-          (note_launch(), k_stiffness<27, TPB, float><<<cnt, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
+          (note_launch(), k_stiffness<27, 384, float><<<cnt, 384, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
                                                                           vals, mat, m.d_err.p));
         else
-          (note_launch(), k_stiffness<27, TPB, double><<<cnt, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
+          (note_launch(), k_stiffness<27, 384, double><<<cnt, 384, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
                                                                            vals, mat, m.d_err.p));
       }
     });

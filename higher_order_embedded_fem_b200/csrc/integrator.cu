@@ -22,8 +22,6 @@
 
 namespace hoefem {
 
-int spmv_grid(int nv);
-
 namespace {
 
 constexpr int TPB = 256;
@@ -165,6 +163,7 @@ struct Integrator {
     launch_mass(*m, density, K.p, s);
     jacobian_combination(*m, 0.0, nullptr, 1.0, K.p, bc_nodes.empty() ? nullptr : bc.p, M.p, scalars.p, s);
     check_device_error(*m);
+    m->spmv_lanes = autotune_spmv_lanes(m->rows(), M.p, s);
     // representative force ||M a||, a_i = sqrt(a^2 / 3), a = 10 (fe_model.rs:423-431)
     (note_launch(), k_fill<<<grid(), TPB, 0, s>>>(n, std::sqrt((10.0 * 10.0) / 3.0), us.p));
     spmv_node_rows(m->rows(), M.p, us.p, vs.p, 1.0, 0.0, s);

@@ -84,6 +84,7 @@ struct NodeRows {
   const int* adj = nullptr;         // sorted neighbour nodes
   const int* diag_slot = nullptr;   // slot of a in adj(a) (-1 for diag_only nodes)
   const unsigned char* diag_only = nullptr;  // may be null
+  int lanes = 32;                            // lanes per node in SpMV kernels (32, 16 or 8; autotuned)
 };
 
 // Per-block device data.
@@ -130,6 +131,7 @@ struct Model {
   DBuf<double> d_X;
   DBuf<int> d_adj_off, d_adj, d_diag_slot, d_err;
   DBuf<long long> d_base;
+  int spmv_lanes = 32;
   NodeRows rows() const;
   ~Model();
 };
@@ -152,6 +154,9 @@ void launch_mass(const Model& m, double density, double* vals, cudaStream_t s);
 // y = beta*y + alpha*A x on a node-row matrix.
 void spmv_node_rows(const NodeRows& A, const double* vals, const double* x, double* y, double alpha, double beta,
                     cudaStream_t s);
+// Times the lanes-per-node variants of the node-row SpMV on this structure
+// and returns the fastest (8, 16 or 32); best_ms (optional) gets its time.
+int autotune_spmv_lanes(NodeRows A, const double* vals, cudaStream_t s, float* best_ms = nullptr);
 // Fills out = c_k * K + c_m * M (either may be null) and applies homogeneous
 // Dirichlet rows / columns for the dof mask (may be null).
 void jacobian_combination(const Model& m, double ck, const double* K, double cm, const double* M,

@@ -20,15 +20,14 @@ namespace hoefem {
 
 namespace {
 
+template <int L>
 __global__ void __launch_bounds__(256) k_spmv(NodeRows A, const double* __restrict__ vals,
                                               const double* __restrict__ x, double* __restrict__ y, double alpha,
                                               double beta) {
-  const int lane = threadIdx.x & 31;
-  const int wpb = blockDim.x >> 5;
-  for (int a = blockIdx.x * wpb + (threadIdx.x >> 5); a < A.nv; a += gridDim.x * wpb) {
+  for_each_node<L>(A.nv, [&](int a, int sl) {
     double s0, s1, s2;
-    node_row_dot(A, vals, x, a, lane, s0, s1, s2);
-    if (lane == 0) {
+    node_row_dot<L>(A, vals, x, a, sl, s0, s1, s2);
+    if (a >= 0 && sl == 0) {
       double y0 = (beta == 0.0) ? 0.0 : beta * y[3 * a];
       double y1 = (beta == 0.0) ? 0.0 : beta * y[3 * a + 1];
       double y2 = (beta == 0.0) ? 0.0 : beta * y[3 * a + 2];
@@ -36,7 +35,7 @@ __global__ void __launch_bounds__(256) k_spmv(NodeRows A, const double* __restri
       y[3 * a + 1] = y1 + alpha * s1;
       y[3 * a + 2] = y2 + alpha * s2;
     }
-  }
+  });
 }
 
 // out = ck*K + cm*M (in the reference's order: fill 0, += ck K, += cm M),
@@ -107,15 +106,54 @@ __global__ void k_fill_u64(unsigned long long* p, unsigned long long v) { *p = v
 
 }  // namespace
 
-int spmv_grid(int nv) {
-  int g = (nv + 7) / 8;
-  return g < 148 * 16 ? (g > 0 ? g : 1) : 148 * 16;
+// Node-row kernels run 8 warps per block, 8 blocks per SM: a grid of at most
+// 148 * 8 blocks covers the GPU once and each warp strides over nodes.
+int spmv_grid(int nv, int lanes) {
+  int nodes_per_block = 8 * (32 / lanes);
+  int g = (nv + nodes_per_block - 1) / nodes_per_block;
+  return g < 148 * 8 ? (g > 0 ? g : 1) : 148 * 8;
 }
 
 void spmv_node_rows(const NodeRows& A, const double* vals, const double* x, double* y, double alpha, double beta,
                     cudaStream_t s) {
-  (note_launch(), k_spmv<<<spmv_grid(A.nv), 256, 0, s>>>(A, vals, x, y, alpha, beta));
+  HOEFEM_LANES_DISPATCH(A.lanes,
+                        (note_launch(), k_spmv<LN><<<spmv_grid(A.nv, LN), 256, 0, s>>>(A, vals, x, y, alpha, beta)));
   HOEFEM_CUDA(cudaGetLastError());
+}
+
+// Autotuner for the node-row SpMV: times the 8 / 16 / 32 lanes-per-node
+// variants on this matrix structure (5 launches each after 2 warm-up
+// launches, CUDA events on stream s) and returns the fastest.
+int autotune_spmv_lanes(NodeRows A, const double* vals, cudaStream_t s, float* best_ms) {
+  const int n = 3 * A.nv;
+  double *x = nullptr, *y = nullptr;
+  HOEFEM_CUDA(cudaMallocAsync(&x, sizeof(double) * (n ? n : 1), s));
+  HOEFEM_CUDA(cudaMallocAsync(&y, sizeof(double) * (n ? n : 1), s));
+  HOEFEM_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * (n ? n : 1), s));
+  cudaEvent_t e0, e1;
+  HOEFEM_CUDA(cudaEventCreate(&e0));
+  HOEFEM_CUDA(cudaEventCreate(&e1));
+  int best = 32;
+  float best_t = 1e30f;
+  const int cand[3] = {8, 16, 32};
+  for (int c : cand) {
+    A.lanes = c;
+    for (int k = 0; k < 2; ++k) spmv_node_rows(A, vals, x, y, 1.0, 0.0, s);
+    HOEFEM_CUDA(cudaEventRecord(e0, s));
+    for (int k = 0; k < 5; ++k) spmv_node_rows(A, vals, x, y, 1.0, 0.0, s);
+    HOEFEM_CUDA(cudaEventRecord(e1, s));
+    HOEFEM_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    HOEFEM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best_t) { best_t = ms; best = c; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(x, s);
+  cudaFreeAsync(y, s);
+  HOEFEM_CUDA(cudaStreamSynchronize(s));
+  if (best_ms) *best_ms = best_t / 5.0f;
+  return best;
 }
 
 void jacobian_combination(const Model& m, double ck, const double* K, double cm, const double* M,
@@ -129,7 +167,7 @@ void jacobian_combination(const Model& m, double ck, const double* K, double cm,
     // The scale entry is read before any thread writes: k_dirichlet reads it
     // at entry, and a Dirichlet diagonal entry is overwritten with `scale`
     // itself, so the race is benign (all writers store the same value).
-    (note_launch(), k_dirichlet<<<spmv_grid(A.nv), 256, 0, s>>>(A, bc_dof, out, first));
+    (note_launch(), k_dirichlet<<<spmv_grid(A.nv, 32), 256, 0, s>>>(A, bc_dof, out, first));
   }
   HOEFEM_CUDA(cudaGetLastError());
 }

@@ -43,6 +43,7 @@ NodeRows Model::rows() const {
   r.adj = d_adj.p;
   r.diag_slot = d_diag_slot.p;
   r.diag_only = nullptr;
+  r.lanes = spmv_lanes;
   return r;
 }
 

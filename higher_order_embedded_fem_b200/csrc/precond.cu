@@ -45,6 +45,7 @@ NodeRows Precond::rows() const {
   r.adj = d_adj.p;
   r.diag_slot = d_diag_slot.p;
   r.diag_only = d_diag_only.p;
+  r.lanes = spmv_lanes;
   return r;
 }
 
@@ -74,6 +75,7 @@ __global__ void __launch_bounds__(FACTOR_TPB) k_schwarz_factor(
   double* V = A + m * m;         // m x m
   double* cs = V + m * m;        // m/2 cosines
   double* sn = cs + m / 2;       // m/2 sines
+  double* colk = cs;             // Cholesky: current column (m entries, aliases cs / sn)
   __shared__ int s_g[27];
   __shared__ int s_rl[27];
   __shared__ double s_red[2];
@@ -126,12 +128,18 @@ __global__ void __launch_bounds__(FACTOR_TPB) k_schwarz_factor(
       __syncthreads();
       if (!s_ok) break;
       const double lkk = A[k * m + k];
-      for (int i = k + 1 + threadIdx.x; i < dim; i += blockDim.x) A[i * m + k] /= lkk;
+      // column k below the diagonal, also copied to a contiguous array so the
+      // trailing update reads it without bank conflicts
+      for (int i = k + 1 + threadIdx.x; i < dim; i += blockDim.x) {
+        double l = A[i * m + k] / lkk;
+        A[i * m + k] = l;
+        colk[i] = l;
+      }
       __syncthreads();
       const int rem = dim - k - 1;
       for (int t = threadIdx.x; t < rem * rem; t += blockDim.x) {
         int i = k + 1 + t / rem, j = k + 1 + t % rem;
-        if (j <= i) A[i * m + j] -= A[i * m + k] * A[j * m + k];
+        if (j <= i) A[i * m + j] -= colk[i] * colk[j];
       }
       __syncthreads();
     }
@@ -326,19 +334,19 @@ __global__ void k_mul(int n, const double* __restrict__ d, const double* __restr
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = d[i] * r[i];
 }
 
+template <int L>
 __global__ void k_spmv_plain(NodeRows A, const double* __restrict__ vals, const double* __restrict__ x,
                              double* __restrict__ y) {
-  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-  for (int a = blockIdx.x * wpb + (threadIdx.x >> 5); a < A.nv; a += gridDim.x * wpb) {
+  for_each_node<L>(A.nv, [&](int a, int sl) {
     double s0, s1, s2;
-    node_row_dot(A, vals, x, a, lane, s0, s1, s2);
-    if (lane == 0) { y[3 * a] = s0; y[3 * a + 1] = s1; y[3 * a + 2] = s2; }
-  }
+    node_row_dot<L>(A, vals, x, a, sl, s0, s1, s2);
+    if (a >= 0 && sl == 0) { y[3 * a] = s0; y[3 * a + 1] = s1; y[3 * a + 2] = s2; }
+  });
 }
 
 }  // namespace
 
-int spmv_grid(int nv);
+int spmv_grid(int nv, int lanes);
 
 void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes, i64 nsub, const i64* untreated,
                             i64 nun) {
@@ -448,6 +456,7 @@ void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes
   int m_max = (3 * p.max_nodes + 1) & ~1;
   size_t smem = (size_t)(2 * m_max * m_max + m_max) * sizeof(double);
   HOEFEM_CUDA(cudaFuncSetAttribute(k_schwarz_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  p.spmv_lanes = autotune_spmv_lanes(p.rows(), p.vals.p, st);
 }
 
 static void check_err(DBuf<int>& e, cudaStream_t s) {
@@ -509,7 +518,8 @@ void precond_apply(const Precond& p, const double* r, double* z, cudaStream_t s)
     (note_launch(), k_mul<<<reduce_blocks_for(n), 256, 0, s>>>(n, p.diag.p, r, z));
   } else {
     NodeRows PR = p.rows();
-    (note_launch(), k_spmv_plain<<<spmv_grid(PR.nv), 256, 0, s>>>(PR, p.vals.p, r, z));
+    HOEFEM_LANES_DISPATCH(PR.lanes,
+                          (note_launch(), k_spmv_plain<LN><<<spmv_grid(PR.nv, LN), 256, 0, s>>>(PR, p.vals.p, r, z)));
   }
   HOEFEM_CUDA(cudaGetLastError());
 }

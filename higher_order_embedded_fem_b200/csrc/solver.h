@@ -30,6 +30,7 @@ struct Precond {
   DBuf<long long> d_stage_off;
   DBuf<int> d_err;
   i64 nnz = 0;
+  int spmv_lanes = 32;
   NodeRows rows() const;
 };
 

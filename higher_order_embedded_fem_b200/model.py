@@ -59,6 +59,12 @@ class _Model:
         check(lib().hoefem_model_sizes(self._h, C.byref(nd), C.byref(nz), C.byref(ne), C.byref(nb)))
         self._ndof, self.nnz, self.num_elements = nd.value, nz.value, ne.value
 
+    def autotune(self):
+        """Picks the fastest lanes-per-node SpMV variant for this pattern."""
+        lanes = C.c_int32()
+        check(lib().hoefem_model_autotune(self._h, C.byref(lanes)))
+        return lanes.value
+
     def set_stream(self, stream):
         """Run this model's work on a CUDA stream handle (int), None: own stream."""
         check(lib().hoefem_model_set_stream(self._h, stream))

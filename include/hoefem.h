@@ -121,6 +121,10 @@ int hoefem_model_destroy(hoefem_model m);
    NULL restores the model's own stream.  Calls stay synchronous on return.
    No counterpart in the reference (its path is synchronous host code). */
 int hoefem_model_set_stream(hoefem_model m, void* stream);
+/* Autotunes the lanes-per-node of the node-row SpMV kernels for this
+   model's pattern (8, 16 or 32; the integrator does this at creation) and
+   returns the choice.  No counterpart in the reference. */
+int hoefem_model_autotune(hoefem_model m, int32_t* lanes);
 int hoefem_model_sizes(hoefem_model m, int64_t* ndof, int64_t* nnz, int64_t* num_elements, int64_t* num_blocks);
 /* row_offsets: ndof+1, column_indices: nnz (SparsityPattern, sparse.rs:297-410) */
 int hoefem_model_pattern(hoefem_model m, int64_t* row_offsets, int64_t* column_indices);
