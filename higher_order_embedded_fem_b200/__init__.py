@@ -21,4 +21,5 @@ from .solver import (  # noqa: F401
     SolveError,
     SolveErrorKind,
 )
+from .learned import LearnedCoarseCorrection  # noqa: F401
 from . import scenes  # noqa: F401

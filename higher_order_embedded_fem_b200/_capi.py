@@ -47,7 +47,8 @@ class StepStats(C.Structure):
         ("max_cg_iterations", C.c_int64), ("substeps", C.c_int64), ("last_cg_status", C.c_int32),
         ("residual_norm", C.c_double), ("representative_force", C.c_double), ("ms_assemble_forces", C.c_double),
         ("ms_assemble_stiffness", C.c_double), ("ms_precond_update", C.c_double), ("ms_cg", C.c_double),
-        ("ms_total", C.c_double),
+        ("ms_total", C.c_double), ("learned_accepted", C.c_int64), ("learned_rejected", C.c_int64),
+        ("learned_residual_ratio", C.c_double), ("ms_learned", C.c_double),
     ]
 
     def as_dict(self):
@@ -101,6 +102,18 @@ SIGNATURES = {
     "hoefem_integrator_mass": (C.c_int, [vp, vp]),
     "hoefem_integrator_eval_f": (C.c_int, [vp, vp, vp, vp, C.c_int]),
     "hoefem_integrator_destroy": (C.c_int, [vp]),
+    "hoefem_learned_create": (C.c_int, [vp, vp, i64, C.c_int, C.c_uint64, C.POINTER(vp)]),
+    "hoefem_learned_destroy": (C.c_int, [vp]),
+    "hoefem_learned_num_pairs": (C.c_int, [vp, pi64]),
+    "hoefem_learned_num_params": (C.c_int, [vp, pi64]),
+    "hoefem_learned_add_pair": (C.c_int, [vp, vp, vp, C.c_int]),
+    "hoefem_learned_train": (C.c_int, [vp, i64, C.c_int32, C.c_float, C.c_uint64, vp]),
+    "hoefem_learned_forward_backward": (C.c_int, [vp, vp, vp, C.c_int32, C.POINTER(C.c_float), vp, vp]),
+    "hoefem_learned_infer": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp]),
+    "hoefem_learned_get_weights": (C.c_int, [vp, vp]),
+    "hoefem_learned_set_weights": (C.c_int, [vp, vp]),
+    "hoefem_learned_predict": (C.c_int, [vp, vp, vp, C.c_int]),
+    "hoefem_integrator_set_learned": (C.c_int, [vp, vp, C.c_int]),
     "hoefem_scene_create_tet10_box": (C.c_int, [dbl, i64, i64, i64, i64, C.POINTER(vp)]),
     "hoefem_scene_create_embedded_cylinder": (C.c_int, [i64, dbl, dbl, C.c_int, C.c_int, C.c_uint64, C.POINTER(vp)]),
     "hoefem_scene_info_get": (C.c_int, [vp, C.POINTER(SceneInfo)]),

@@ -12,6 +12,7 @@
 #include "internal.h"
 #include "scene.h"
 #include "solver.h"
+#include "learned.h"
 
 namespace hoefem {
 struct Integrator;
@@ -20,6 +21,7 @@ Integrator* integrator_new(Model* m, const hoefem_material* mat, double density,
 void integrator_delete(Integrator* it);
 void integrator_set_tolerances(Integrator* it, double tol, i64 cg_max, i64 newton_max);
 void integrator_set_precision(Integrator* it, int precision, double inner_tol);
+void integrator_set_learned(Integrator* it, Learned* l, int mode);
 int integrator_step(Integrator* it, double* ud, double* vd, double t, double dt);
 hoefem_step_stats integrator_stats(Integrator* it);
 const double* integrator_mass(Integrator* it);
@@ -50,6 +52,10 @@ struct hoefem_integrator_s {
   Integrator* it = nullptr;
   hoefem_model_s* model = nullptr;
   ~hoefem_integrator_s() { integrator_delete(it); }
+};
+struct hoefem_learned_s {
+  Learned l;
+  hoefem_model_s* model = nullptr;
 };
 struct hoefem_scene_s {
   Scene* s = nullptr;
@@ -603,6 +609,132 @@ int hoefem_integrator_eval_f(hoefem_integrator it, const double* u, const double
 int hoefem_integrator_destroy(hoefem_integrator it) {
   API_BEGIN
   delete it;
+  API_END
+}
+
+// ---- learned coarse correction -----------------------------------------------------
+int hoefem_learned_create(hoefem_model m, const int64_t* bc_nodes, int64_t num_bc, int num_subdomains,
+                          uint64_t seed, hoefem_learned* out) {
+  API_BEGIN
+  Model& mm = device_model(m);
+  HOEFEM_REQUIRE(out && (bc_nodes || num_bc == 0), HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  std::vector<unsigned char> mask(mm.ndof, 0);
+  for (int64_t k = 0; k < num_bc; ++k) {
+    HOEFEM_REQUIRE(bc_nodes[k] >= 0 && bc_nodes[k] < mm.nv, HOEFEM_ERR_INVALID_ARGUMENT, "node out of range");
+    for (int i = 0; i < 3; ++i) mask[3 * bc_nodes[k] + i] = 1;
+  }
+  std::unique_ptr<hoefem_learned_s> h(new hoefem_learned_s());
+  h->model = m;
+  h->l.setup(&mm, mask.data(), num_subdomains, seed);
+  *out = h.release();
+  API_END
+}
+
+int hoefem_learned_destroy(hoefem_learned l) {
+  API_BEGIN
+  delete l;
+  API_END
+}
+
+int hoefem_learned_num_pairs(hoefem_learned l, int64_t* n) {
+  API_BEGIN
+  HOEFEM_REQUIRE(l && n, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  *n = l->l.n_data;
+  API_END
+}
+
+int hoefem_learned_num_params(hoefem_learned l, int64_t* n) {
+  API_BEGIN
+  HOEFEM_REQUIRE(l && n, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  *n = (int64_t)l->l.n_params;
+  API_END
+}
+
+int hoefem_learned_add_pair(hoefem_learned l, const double* r, const double* e, int mem) {
+  API_BEGIN
+  HOEFEM_REQUIRE(l, HOEFEM_ERR_INVALID_ARGUMENT, "null handle");
+  Model& mm = l->model->m;
+  View R(r, mm.ndof, mem, mm.stream, true), E(e, mm.ndof, mem, mm.stream, true);
+  l->l.add_pair(R.d, E.d, mm.stream);
+  sync(mm);
+  API_END
+}
+
+int hoefem_learned_train(hoefem_learned l, int64_t steps, int32_t batch, float lr, uint64_t seed, float* loss_history) {
+  API_BEGIN
+  HOEFEM_REQUIRE(l && steps >= 0 && lr >= 0.f, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  l->l.train(steps, batch, lr, seed, loss_history, l->model->m.stream);
+  API_END
+}
+
+int hoefem_learned_forward_backward(hoefem_learned l, const float* X, const float* T, int32_t rows, float* loss,
+                                    float* grads, float* out) {
+  API_BEGIN
+  HOEFEM_REQUIRE(l && X && T && rows > 0 && rows <= l->l.max_batch, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  Learned& L = l->l;
+  cudaStream_t s = l->model->m.stream;
+  DBuf<float> dX, dT;
+  dX.upload(X, (size_t)rows * Learned::F, s);
+  dT.upload(T, (size_t)rows * Learned::NM, s);
+  float lv = L.train_step(dX.p, dT.p, rows, 0.f, s);
+  if (loss) *loss = lv;
+  if (grads) HOEFEM_CUDA(cudaMemcpyAsync(grads, L.grads.p, sizeof(float) * L.n_params, cudaMemcpyDeviceToHost, s));
+  if (out) HOEFEM_CUDA(cudaMemcpyAsync(out, L.Y3.p, sizeof(float) * rows * Learned::NM, cudaMemcpyDeviceToHost, s));
+  HOEFEM_CUDA(cudaStreamSynchronize(s));
+  API_END
+}
+
+int hoefem_learned_infer(hoefem_learned l, const float* X, int32_t rows, int32_t bf16, float* out) {
+  API_BEGIN
+  HOEFEM_REQUIRE(l && X && out && rows > 0 && rows <= l->l.max_batch, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  Learned& L = l->l;
+  cudaStream_t s = l->model->m.stream;
+  DBuf<float> dX;
+  dX.upload(X, (size_t)rows * Learned::F, s);
+  if (bf16) L.refresh_bf16(s);
+  L.forward(dX.p, rows, bf16 != 0, s);
+  HOEFEM_CUDA(cudaMemcpyAsync(out, L.Y3.p, sizeof(float) * rows * Learned::NM, cudaMemcpyDeviceToHost, s));
+  HOEFEM_CUDA(cudaStreamSynchronize(s));
+  API_END
+}
+
+int hoefem_learned_get_weights(hoefem_learned l, float* w) {
+  API_BEGIN
+  HOEFEM_REQUIRE(l && w, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  cudaStream_t s = l->model->m.stream;
+  HOEFEM_CUDA(cudaMemcpyAsync(w, l->l.params.p, sizeof(float) * l->l.n_params, cudaMemcpyDeviceToHost, s));
+  HOEFEM_CUDA(cudaStreamSynchronize(s));
+  API_END
+}
+
+int hoefem_learned_set_weights(hoefem_learned l, const float* w) {
+  API_BEGIN
+  HOEFEM_REQUIRE(l && w, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  cudaStream_t s = l->model->m.stream;
+  HOEFEM_CUDA(cudaMemcpyAsync(l->l.params.p, w, sizeof(float) * l->l.n_params, cudaMemcpyHostToDevice, s));
+  l->l.refresh_bf16(s);
+  HOEFEM_CUDA(cudaStreamSynchronize(s));
+  l->l.trained = true;
+  API_END
+}
+
+int hoefem_learned_predict(hoefem_learned l, const double* r, double* x0, int mem) {
+  API_BEGIN
+  HOEFEM_REQUIRE(l, HOEFEM_ERR_INVALID_ARGUMENT, "null handle");
+  Model& mm = l->model->m;
+  View R(r, mm.ndof, mem, mm.stream, true), X0(x0, mm.ndof, mem, mm.stream, false);
+  if (l->l.use_bf16) l->l.refresh_bf16(mm.stream);
+  l->l.predict(R.d, X0.d, mm.stream);
+  X0.copy_out();
+  sync(mm);
+  API_END
+}
+
+int hoefem_integrator_set_learned(hoefem_integrator it, hoefem_learned l, int mode) {
+  API_BEGIN
+  HOEFEM_REQUIRE(it && mode >= 0 && mode <= 2, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  HOEFEM_REQUIRE(!l || l->model == it->model, HOEFEM_ERR_INVALID_ARGUMENT, "learned correction of another model");
+  integrator_set_learned(it->it, l ? &l->l : nullptr, mode);
   API_END
 }
 

@@ -369,6 +369,7 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
     g_launch_count.fetch_add(G.kernels, std::memory_order_relaxed);
     HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
     HOEFEM_CUDA(cudaStreamSynchronize(s));
+    if (w.on_chunk && !w.h_st->done) w.on_chunk(s);
     if (w.h_st->done) break;
   }
   *iters = w.h_st->iters;

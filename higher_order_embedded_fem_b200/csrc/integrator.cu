@@ -19,6 +19,7 @@
 #include "internal.h"
 #include "kernels_common.cuh"
 #include "solver.h"
+#include "learned.h"
 
 namespace hoefem {
 
@@ -114,6 +115,11 @@ struct Integrator {
                                    // inside FP64 iterative refinement)
   double inner_tol = 1e-2;
   DBuf<float> J32;
+  Learned* learned = nullptr;
+  int learned_mode = 0;  // 0 off, 1 warm start, 2 collect
+  DBuf<double> x0, r0;
+  std::vector<DBuf<double>*> snaps;  // collected (x_k, r_k) pairs of the current solve
+  double ratio_sum = 0.0;
   double rep_force = 0.0;
   DBuf<unsigned char> bc;
   DBuf<double> M, K, J, gforce, up, vn, w, F, dx, us, vs, f, u, v, partials, scalars;
@@ -239,6 +245,8 @@ struct Integrator {
     stats.ms_precond_update += elapsed();
     HOEFEM_CUDA(cudaMemsetAsync(cg.x.p, 0, sizeof(double) * n, s));
     (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, F.p, cg.b.p));
+    if (learned && learned_mode == 1 && learned->trained) warm_start(s);
+    if (learned && learned_mode == 2) start_collect();
     i64 it = 0;
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
     int st;
@@ -258,10 +266,71 @@ struct Integrator {
     stats.total_cg_iterations += it;
     if (it > stats.max_cg_iterations) stats.max_cg_iterations = it;
     stats.last_cg_status = st;
+    if (learned && learned_mode == 2) finish_collect(st, s);
     (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, cg.x.p, dx.p));
     // MaxIterationsReached and IndefiniteOperator are tolerated (newton_cg.rs:776-797)
     if (st == HOEFEM_OK || st == HOEFEM_CG_MAX_ITERATIONS || st == HOEFEM_CG_INDEFINITE_OPERATOR) return HOEFEM_OK;
     return st;
+  }
+
+  // Learned warm start with the residual guard: x0 from the MLP, kept only
+  // if ||F - J x0|| < ||F||.
+  void warm_start(cudaStream_t s) {
+    const int n = (int)m->ndof;
+    HOEFEM_CUDA(cudaEventRecord(ev[0], s));
+    if (x0.n < (size_t)n) { x0.alloc(n); r0.alloc(n); }
+    learned->predict(F.p, x0.p, s);
+    (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, F.p, r0.p));
+    spmv_node_rows(m->rows(), J.p, x0.p, r0.p, -1.0, 1.0, s);
+    double rr = norm_sq(r0.p), bb = norm_sq(F.p);
+    HOEFEM_CUDA(cudaEventRecord(ev[1], s));
+    HOEFEM_CUDA(cudaEventSynchronize(ev[1]));
+    stats.ms_learned += elapsed();
+    if (rr < bb) {
+      (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, x0.p, cg.x.p));
+      stats.learned_accepted += 1;
+      ratio_sum += std::sqrt(rr / bb);
+      stats.learned_residual_ratio = ratio_sum / stats.learned_accepted;
+    } else {
+      stats.learned_rejected += 1;
+    }
+  }
+
+  // Training-pair collection: snapshot (x_k, r_k) after every CG chunk.
+  void start_collect() {
+    for (auto* b : snaps) delete b;
+    snaps.clear();
+    cg.on_chunk = [this](cudaStream_t st) {
+      if (snaps.size() >= 64) return;
+      const int n = (int)m->ndof;
+      auto* xs = new DBuf<double>();
+      auto* rs = new DBuf<double>();
+      xs->alloc(n);
+      rs->alloc(n);
+      HOEFEM_CUDA(cudaMemcpyAsync(xs->p, cg.x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      HOEFEM_CUDA(cudaMemcpyAsync(rs->p, cg.r.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      snaps.push_back(xs);
+      snaps.push_back(rs);
+    };
+  }
+
+  void finish_collect(int status, cudaStream_t s) {
+    cg.on_chunk = nullptr;
+    const int n = (int)m->ndof;
+    if (status == HOEFEM_OK) {
+      // the right-hand side itself: r = b, e = x*
+      learned->add_pair(cg.b.p, cg.x.p, s);
+      if (x0.n < (size_t)n) { x0.alloc(n); r0.alloc(n); }
+      for (size_t k = 0; k + 1 < snaps.size(); k += 2) {
+        // e_k = x* - x_k
+        (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, cg.x.p, x0.p));
+        (note_launch(), k_axpy_w<<<grid(), TPB, 0, s>>>(n, -1.0, snaps[k]->p, x0.p));
+        learned->add_pair(snaps[k + 1]->p, x0.p, s);
+      }
+    }
+    HOEFEM_CUDA(cudaStreamSynchronize(s));
+    for (auto* b : snaps) delete b;
+    snaps.clear();
   }
 
   int be_step(double dt) {
@@ -307,6 +376,7 @@ struct Integrator {
     cudaStream_t s = m->stream;
     const int n = (int)m->ndof;
     stats = hoefem_step_stats{};
+    ratio_sum = 0.0;
     stats.representative_force = rep_force;
     cudaEvent_t t0, t1;
     HOEFEM_CUDA(cudaEventCreate(&t0));
@@ -364,6 +434,10 @@ Integrator* integrator_new(Model* m, const hoefem_material* mat, double density,
   return it.release();
 }
 void integrator_delete(Integrator* it) { delete it; }
+void integrator_set_learned(Integrator* it, Learned* l, int mode) {
+  it->learned = l;
+  it->learned_mode = l ? mode : 0;
+}
 void integrator_set_precision(Integrator* it, int precision, double inner_tol) {
   it->precision = precision;
   it->inner_tol = inner_tol;

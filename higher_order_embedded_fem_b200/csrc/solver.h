@@ -1,6 +1,8 @@
 // Preconditioner and CG declarations (internal).
 #pragma once
 
+#include <functional>
+
 #include "internal.h"
 
 namespace hoefem {
@@ -60,6 +62,8 @@ struct CgWork {
   };
   std::vector<Graph> graphs;  // chunk graphs per (operator, preconditioner, precision)
   int chunk = 8;
+  // called on the host after every chunk of iterations (solver state synced)
+  std::function<void(cudaStream_t)> on_chunk;
   void init(Model* model);
   ~CgWork();
 };

@@ -213,6 +213,13 @@ class NewtonCgIntegrator3d:
     def set_tolerances(self, cg_tol=1e-5, cg_max_iter=500, newton_max_iter=100):
         check(lib().hoefem_integrator_set_tolerances(self._h, cg_tol, cg_max_iter, newton_max_iter))
 
+    def set_learned(self, learned, mode=1):
+        """mode 1: guarded learned warm start; 2: collect training pairs from
+        this integrator's plain CG solves; 0 / learned=None: off."""
+        self._learned = learned
+        check(lib().hoefem_integrator_set_learned(self._h, learned._h if learned is not None else None,
+                                                  int(mode) if learned is not None else 0))
+
     def set_precision(self, mixed, inner_tol=1e-2):
         """mixed=True: FP32 element stiffness / operator / Schwarz apply inside
         FP64 iterative refinement (see hoefem_integrator_set_precision)."""

@@ -228,6 +228,12 @@ typedef struct {
   double ms_precond_update;
   double ms_cg;
   double ms_total;
+  /* learned coarse correction: warm starts accepted / rejected by the
+     residual guard, and the mean ||b - A x0|| / ||b|| of the accepted ones */
+  int64_t learned_accepted;
+  int64_t learned_rejected;
+  double learned_residual_ratio;
+  double ms_learned;
 } hoefem_step_stats;
 
 /* precond: a preconditioner of this model (ownership stays with the caller),
@@ -260,6 +266,45 @@ int hoefem_integrator_mass(hoefem_integrator it, double* values /* host */);
    with Dirichlet rows zeroed. */
 int hoefem_integrator_eval_f(hoefem_integrator it, const double* u, const double* v, double* f, int mem);
 int hoefem_integrator_destroy(hoefem_integrator it);
+
+/* ------------------------------------------------------------------------ */
+/* Learned coarse correction (no counterpart in the reference: an addition on
+   top of its plain Schwarz-CG).  The nodes are split into num_subdomains
+   coarse subdomains (recursive coordinate bisection, power of two), each with
+   32 orthonormal local polynomial modes; an MLP 64 -> 256 -> 256 -> 32 maps
+   per-subdomain residual features to the coarse coefficients of the converged
+   correction.  Trained with the library's own forward / backward / Adam
+   kernels on (residual, converged correction) pairs that plain Schwarz-CG
+   solves generate; inference in BF16 on the tensor cores.  In an integrator
+   it is a warm start that is kept only if it lowers the residual. */
+typedef struct hoefem_learned_s* hoefem_learned;
+
+int hoefem_learned_create(hoefem_model m, const int64_t* bc_nodes, int64_t num_bc, int num_subdomains,
+                          uint64_t seed, hoefem_learned* out);
+int hoefem_learned_destroy(hoefem_learned l);
+int hoefem_learned_num_pairs(hoefem_learned l, int64_t* num_pairs);
+int hoefem_learned_num_params(hoefem_learned l, int64_t* num_params);
+/* Adds the pairs (features(r), coarse coefficients of e) for one residual r
+   and its correction e (device or host vectors, ndof each). */
+int hoefem_learned_add_pair(hoefem_learned l, const double* r, const double* e, int mem);
+/* steps of Adam on random mini-batches of `batch` pairs (FP32 master weights);
+   loss_history (host, may be NULL) receives the mean squared error per step. */
+int hoefem_learned_train(hoefem_learned l, int64_t steps, int32_t batch, float lr, uint64_t seed,
+                         float* loss_history);
+/* Host buffers: X rows x 64 features, T rows x 32 targets; outputs the MSE
+   loss, the gradient of every parameter (num_params, same layout as the
+   weights) and the network output (rows x 32), with no update. */
+int hoefem_learned_forward_backward(hoefem_learned l, const float* X, const float* T, int32_t rows, float* loss,
+                                    float* grads, float* out);
+/* Inference on host features X (rows x 64, rows % 16 == 0 for bf16). */
+int hoefem_learned_infer(hoefem_learned l, const float* X, int32_t rows, int32_t bf16, float* out);
+int hoefem_learned_get_weights(hoefem_learned l, float* w);
+int hoefem_learned_set_weights(hoefem_learned l, const float* w);
+/* x0 = predicted correction of residual r. */
+int hoefem_learned_predict(hoefem_learned l, const double* r, double* x0, int mem);
+/* mode 0: off, 1: warm start with the guard, 2: collect training pairs from
+   the integrator's plain CG solves (every CG chunk's iterate). */
+int hoefem_integrator_set_learned(hoefem_integrator it, hoefem_learned l, int mode);
 
 /* ------------------------------------------------------------------------ */
 /* Synthetic scenes (input construction; not part of the reference hot path).
