@@ -11,6 +11,7 @@ from ._capi import HoefemError, ELEM_HEX27, ELEM_TET10, LIB_PATH  # noqa: F401
 from .materials import LameParameters, StableNeoHookeanMaterial, StVKMaterial, YoungPoisson  # noqa: F401
 from .model import EmbeddedModel3d, NodalModel3d  # noqa: F401
 from .solver import (  # noqa: F401
+    BatchedNewtonCgIntegrator3d,
     CgOutput,
     ConjugateGradient,
     DiagonalPreconditioner,

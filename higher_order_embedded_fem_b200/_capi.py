@@ -115,6 +115,14 @@ SIGNATURES = {
     "hoefem_learned_predict": (C.c_int, [vp, vp, vp, C.c_int]),
     "hoefem_integrator_set_learned": (C.c_int, [vp, vp, C.c_int]),
     "hoefem_scene_create_tet10_box": (C.c_int, [dbl, i64, i64, i64, i64, C.POINTER(vp)]),
+    "hoefem_scene_create_hex27_box": (C.c_int, [dbl, i64, i64, i64, i64, C.POINTER(vp)]),
+    "hoefem_batch_create": (C.c_int, [vp, C.c_int32, vp, dbl, vp, vp, C.c_int, dbl, C.POINTER(vp)]),
+    "hoefem_batch_destroy": (C.c_int, [vp]),
+    "hoefem_batch_set_stream": (C.c_int, [vp, vp]),
+    "hoefem_batch_set_tolerances": (C.c_int, [vp, dbl, i64, i64]),
+    "hoefem_batch_sizes": (C.c_int, [vp, pi64, pi64, pi64, vp]),
+    "hoefem_batch_step": (C.c_int, [vp, vp, vp, dbl, dbl, C.c_int]),
+    "hoefem_batch_scene_stats": (C.c_int, [vp, C.c_int32, C.POINTER(StepStats), C.POINTER(C.c_int32)]),
     "hoefem_scene_create_embedded_cylinder": (C.c_int, [i64, dbl, dbl, C.c_int, C.c_int, C.c_uint64, C.POINTER(vp)]),
     "hoefem_scene_info_get": (C.c_int, [vp, C.POINTER(SceneInfo)]),
     "hoefem_scene_vertices": (C.c_int, [vp, vp]),

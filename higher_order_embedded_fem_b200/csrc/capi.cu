@@ -26,6 +26,15 @@ int integrator_step(Integrator* it, double* ud, double* vd, double t, double dt)
 hoefem_step_stats integrator_stats(Integrator* it);
 const double* integrator_mass(Integrator* it);
 void integrator_eval_f(Integrator* it, const double* ud, const double* vd, double* f);
+struct Batch;
+Batch* batch_build(const std::vector<const Model*>& scenes, const std::vector<MatDev>& mats, double density,
+                   const i64* bc_off, const i64* bc_nodes, bool gravity_enabled, double gravity);
+void batch_delete(Batch* b);
+Model& batch_model(Batch* b);
+int batch_step(Batch* b, double* u, double* v, double dt);
+void batch_set_tolerances(Batch* b, double tol, i64 cg_max, i64 newton_max);
+const std::vector<int>& batch_node_offsets(Batch* b);
+void batch_scene_stats(Batch* b, int k, hoefem_step_stats* out, int* status);
 void greedy_coloring(const i64* conn, i64 ne, int nn, i64 nv, std::vector<i64>& color_off,
                      std::vector<int>& color_elems);
 }  // namespace hoefem
@@ -60,6 +69,14 @@ struct hoefem_learned_s {
 struct hoefem_scene_s {
   Scene* s = nullptr;
   ~hoefem_scene_s() { delete s; }
+};
+struct hoefem_batch_s {
+  Batch* b = nullptr;
+  cudaStream_t own_stream = nullptr;
+  ~hoefem_batch_s() {
+    if (b && own_stream) batch_model(b).stream = own_stream;
+    batch_delete(b);
+  }
 };
 
 namespace {
@@ -738,6 +755,89 @@ int hoefem_integrator_set_learned(hoefem_integrator it, hoefem_learned l, int mo
   API_END
 }
 
+// ---- batched scenes --------------------------------------------------------
+int hoefem_batch_create(const hoefem_model* models, int32_t num_scenes, const hoefem_material* materials,
+                        double density, const int64_t* bc_offsets, const int64_t* bc_nodes, int gravity_enabled,
+                        double gravity, hoefem_batch* out) {
+  API_BEGIN
+  HOEFEM_REQUIRE(out && models && materials && num_scenes > 0, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  HOEFEM_REQUIRE(!bc_offsets || bc_nodes || bc_offsets[num_scenes] == 0, HOEFEM_ERR_INVALID_ARGUMENT,
+                 "missing Dirichlet nodes");
+  std::vector<const Model*> ms(num_scenes);
+  std::vector<MatDev> mats(num_scenes);
+  for (int k = 0; k < num_scenes; ++k) {
+    ms[k] = &model_of(models[k]);
+    mats[k] = mat_of(materials + k);
+    if (bc_offsets)
+      HOEFEM_REQUIRE(bc_offsets[k + 1] >= bc_offsets[k], HOEFEM_ERR_INVALID_ARGUMENT, "decreasing Dirichlet offsets");
+  }
+  std::unique_ptr<hoefem_batch_s> h(new hoefem_batch_s());
+  h->b = batch_build(ms, mats, density, bc_offsets, bc_nodes, gravity_enabled != 0, gravity);
+  *out = h.release();
+  API_END
+}
+
+int hoefem_batch_destroy(hoefem_batch b) {
+  API_BEGIN
+  delete b;
+  API_END
+}
+
+int hoefem_batch_set_stream(hoefem_batch b, void* stream) {
+  API_BEGIN
+  HOEFEM_REQUIRE(b, HOEFEM_ERR_INVALID_ARGUMENT, "null batch");
+  Model& mm = batch_model(b->b);
+  if (!b->own_stream) b->own_stream = mm.stream;
+  HOEFEM_CUDA(cudaStreamSynchronize(mm.stream));
+  mm.stream = stream ? (cudaStream_t)stream : b->own_stream;
+  API_END
+}
+
+int hoefem_batch_set_tolerances(hoefem_batch b, double cg_tol, int64_t cg_max_iter, int64_t newton_max_iter) {
+  API_BEGIN
+  HOEFEM_REQUIRE(b && cg_tol >= 0.0 && newton_max_iter >= 0, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  batch_set_tolerances(b->b, cg_tol, cg_max_iter, newton_max_iter);
+  API_END
+}
+
+int hoefem_batch_sizes(hoefem_batch b, int64_t* num_scenes, int64_t* ndof, int64_t* nnz, int64_t* dof_offsets) {
+  API_BEGIN
+  HOEFEM_REQUIRE(b, HOEFEM_ERR_INVALID_ARGUMENT, "null batch");
+  Model& mm = batch_model(b->b);
+  const std::vector<int>& no = batch_node_offsets(b->b);
+  if (num_scenes) *num_scenes = (int64_t)no.size() - 1;
+  if (ndof) *ndof = mm.ndof;
+  if (nnz) *nnz = mm.nnz;
+  if (dof_offsets)
+    for (size_t k = 0; k < no.size(); ++k) dof_offsets[k] = 3 * (int64_t)no[k];
+  API_END
+}
+
+int hoefem_batch_step(hoefem_batch b, double* u, double* v, double t, double dt, int mem) {
+  API_BEGIN
+  (void)t;
+  HOEFEM_REQUIRE(b && dt > 0.0, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  Model& mm = batch_model(b->b);
+  View U(u, mm.ndof, mem, mm.stream, true), V(v, mm.ndof, mem, mm.stream, true);
+  int st = batch_step(b->b, U.d, V.d, dt);
+  U.copy_out();
+  V.copy_out();
+  sync(mm);
+  if (st != HOEFEM_OK) return fail(st, "time step failed for at least one scene");
+  API_END
+}
+
+int hoefem_batch_scene_stats(hoefem_batch b, int32_t scene, hoefem_step_stats* out, int32_t* status) {
+  API_BEGIN
+  HOEFEM_REQUIRE(b && out && status, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  HOEFEM_REQUIRE(scene >= 0 && scene < (int)batch_node_offsets(b->b).size() - 1, HOEFEM_ERR_INVALID_ARGUMENT,
+                 "scene out of range");
+  int st = 0;
+  batch_scene_stats(b->b, scene, out, &st);
+  *status = st;
+  API_END
+}
+
 // ---- scenes ---------------------------------------------------------------------
 int hoefem_scene_create_tet10_box(double unit, int64_t ux, int64_t uy, int64_t uz, int64_t cells_per_unit,
                                   hoefem_scene* out) {
@@ -746,6 +846,17 @@ int hoefem_scene_create_tet10_box(double unit, int64_t ux, int64_t uy, int64_t u
                  "bad arguments");
   auto* h = new hoefem_scene_s();
   h->s = scene_tet10_box(unit, ux, uy, uz, cells_per_unit);
+  *out = h;
+  API_END
+}
+
+int hoefem_scene_create_hex27_box(double unit, int64_t ux, int64_t uy, int64_t uz, int64_t cells_per_unit,
+                                  hoefem_scene* out) {
+  API_BEGIN
+  HOEFEM_REQUIRE(out && unit > 0 && ux > 0 && uy > 0 && uz > 0 && cells_per_unit > 0, HOEFEM_ERR_INVALID_ARGUMENT,
+                 "bad arguments");
+  auto* h = new hoefem_scene_s();
+  h->s = scene_hex27_box(unit, ux, uy, uz, cells_per_unit);
   *out = h;
   API_END
 }

@@ -341,7 +341,8 @@ __global__ void __launch_bounds__(TPB) k_forces(const BlockDev b, const int* __r
 #pragma unroll
       for (int k = 0; k < 3; ++k) F[3 * c + k] = warp_sum(ul[c] * G[k]) + (c == k ? 1.0 : 0.0);
     QpState<double> st;
-    if (!material_state(mat.kind, F, mat.mu, mat.lambda, st, true)) { ok = false; break; }
+    const double emu = b.emat ? b.emat[2 * e] : mat.mu, elam = b.emat ? b.emat[2 * e + 1] : mat.lambda;
+    if (!material_state(mat.kind, F, emu, elam, st, true)) { ok = false; break; }
     if (own) {
       double sc = w * fabs(detJ);
 #pragma unroll
@@ -429,7 +430,7 @@ __global__ void __launch_bounds__(NN == 10 ? TPB : 384, NN == 10 ? 1 : 2) k_stif
   int nq_max = 0;
 #pragma unroll
   for (int k = 0; k < EPC; ++k) nq_max = max(nq_max, s_nq[k]);
-  const R mu = (R)mat.mu, lam = (R)mat.lambda;
+  const R mu = (R)(b.emat ? b.emat[2 * e] : mat.mu), lam = (R)(b.emat ? b.emat[2 * e + 1] : mat.lambda);
   for (int q = 0; q < nq_max; ++q) {
     const bool live = q < nq;
     if (nodewarp && live) {

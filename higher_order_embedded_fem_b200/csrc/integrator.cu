@@ -246,7 +246,8 @@ struct Integrator {
     HOEFEM_CUDA(cudaMemsetAsync(cg.x.p, 0, sizeof(double) * n, s));
     (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, F.p, cg.b.p));
     if (learned && learned_mode == 1 && learned->trained) warm_start(s);
-    if (learned && learned_mode == 2) start_collect();
+    const bool collecting = learned && learned_mode == 2 && precision == PRECISION_FP64;
+    if (collecting) start_collect();
     i64 it = 0;
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
     int st;
@@ -266,7 +267,7 @@ struct Integrator {
     stats.total_cg_iterations += it;
     if (it > stats.max_cg_iterations) stats.max_cg_iterations = it;
     stats.last_cg_status = st;
-    if (learned && learned_mode == 2) finish_collect(st, s);
+    if (collecting) finish_collect(st, s);
     (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, cg.x.p, dx.p));
     // MaxIterationsReached and IndefiniteOperator are tolerated (newton_cg.rs:776-797)
     if (st == HOEFEM_OK || st == HOEFEM_CG_MAX_ITERATIONS || st == HOEFEM_CG_INDEFINITE_OPERATOR) return HOEFEM_OK;

@@ -99,6 +99,7 @@ struct BlockDev {
   const double* qw = nullptr;
   const double* qp = nullptr;  // xyz interleaved
   const int* emap = nullptr;   // [e * nn * nn + I * nn + J] = nnz index of (3 gI, 3 gJ)
+  const double* emat = nullptr;  // optional per-element Lame parameters (mu, lambda) pairs
 };
 
 struct Block {
@@ -112,6 +113,8 @@ struct Block {
   std::vector<int> color_elems;  // elements ordered by color
   DBuf<int> d_conn, d_qoff, d_emap, d_color_elems;
   DBuf<double> d_qw, d_qp;
+  std::vector<double> emat;  // optional per-element (mu, lambda)
+  DBuf<double> d_emat;
   BlockDev dev() const;
 };
 

@@ -32,6 +32,7 @@ BlockDev Block::dev() const {
   b.qw = d_qw.p;
   b.qp = d_qp.p;
   b.emap = d_emap.p;
+  b.emat = d_emat.p;
   return b;
 }
 
@@ -218,6 +219,7 @@ void ensure_device(Model& m) {
       std::vector<int> qo(b->qoff.begin(), b->qoff.end());
       b->d_qoff.upload(qo, s);
     }
+    if (!b->emat.empty()) b->d_emat.upload(b->emat, s);
   }
   HOEFEM_CUDA(cudaStreamSynchronize(s));
   m.on_device = true;

@@ -328,6 +328,22 @@ Scene* scene_tet10_box(double unit, int64_t ux, int64_t uy, int64_t uz, int64_t 
   return s;
 }
 
+Scene* scene_hex27_box(double unit, int64_t ux, int64_t uy, int64_t uz, int64_t cpu) {
+  Cells hx = hex_box(unit, ux, uy, uz, cpu);
+  Cells h27 = refine(hx, HOEFEM_ELEM_HEX27);
+  Scene* s = new Scene();
+  s->X = std::move(h27.X);
+  s->cell_size = unit / (double)cpu;
+  SceneBlock b;
+  b.kind = HOEFEM_ELEM_HEX27;
+  b.nn = 27;
+  b.conn = std::move(h27.C);
+  b.uniform = true;
+  hex_quadrature_5(b.qw, b.qp);
+  s->blocks.push_back(std::move(b));
+  return s;
+}
+
 Scene* scene_embedded_cylinder(int64_t n, double r_in, double r_out, int qmin, int qmax, uint64_t seed) {
   Cells hx = hex_box(1.0, 1, 1, 1, n);
   Cells h27 = refine(hx, HOEFEM_ELEM_HEX27);

@@ -44,7 +44,11 @@ class _Model:
             self._h = None
 
     def _add_block(self, kind, connectivity, weights, points, offsets=None):
-        conn = host_i64(connectivity)
+        nn = 10 if kind == _capi.ELEM_TET10 else 27
+        conn = host_i64(connectivity).reshape(-1, nn)
+        if np.ndim(connectivity) == 2 and np.shape(connectivity)[1] != nn:
+            raise ValueError("connectivity has %d nodes per element, element kind needs %d"
+                             % (np.shape(connectivity)[1], nn))
         w = host_f64(weights)
         p = host_f64(points).reshape(-1, 3)
         off = None if offsets is None else host_i64(offsets)

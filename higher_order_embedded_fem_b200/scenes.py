@@ -2,6 +2,7 @@
 
 tet10_box        : box of hexes, each split into 6 Tet10 (Max triangulation),
                    tet_quadrature_strength_5 (14 points)
+hex27_box        : the same box as Hex27 cells, hex_quadrature_strength_5
 embedded_cylinder: Hex27 background grid clipped to a hollow cylinder, interior
                    cells with hex_quadrature_strength_5, interface cells with
                    seeded synthetic quadrature (Q ~ U{q_min..q_max}, weights
@@ -66,6 +67,15 @@ def _read(h):
 def tet10_box(unit=1.0, ux=1, uy=1, uz=1, cells_per_unit=8):
     h = C.c_void_p()
     check(lib().hoefem_scene_create_tet10_box(unit, ux, uy, uz, cells_per_unit, C.byref(h)))
+    try:
+        return _read(h)
+    finally:
+        lib().hoefem_scene_destroy(h)
+
+
+def hex27_box(unit=1.0, ux=1, uy=1, uz=1, cells_per_unit=8):
+    h = C.c_void_p()
+    check(lib().hoefem_scene_create_hex27_box(unit, ux, uy, uz, cells_per_unit, C.byref(h)))
     try:
         return _read(h)
     finally:

@@ -246,3 +246,83 @@ class NewtonCgIntegrator3d:
             f = np.zeros(self.model.ndof()) if not _capi.is_device_array(u) else u.new_zeros(self.model.ndof())
         check(lib().hoefem_integrator_eval_f(self._h, ptr(u)[0], ptr(v)[0], ptr(f)[0], _same_space(u, v, f)))
         return f
+
+
+class BatchedNewtonCgIntegrator3d:
+    """Many independent scenes advanced together: each scene takes the path of
+    NewtonCgIntegrator3d.step with the diagonal preconditioner (its own
+    Dirichlet scale, tolerances, line search and substepping), while all
+    scenes share every kernel launch (see hoefem_batch_create).  `models`:
+    NodalModel3d / EmbeddedModel3d objects; `materials`: one per scene, all of
+    one kind; `dirichlet_nodes`: one node list per scene.  Not in the
+    reference, which steps one model at a time."""
+
+    def __init__(self, models, materials, density, dirichlet_nodes=None, gravity=-9.81, gravity_enabled=True):
+        ns = len(models)
+        if len(materials) != ns:
+            raise ValueError("one material per scene")
+        self.models = list(models)
+        handles = (C.c_void_p * ns)(*[m._h.value if hasattr(m._h, "value") else m._h for m in self.models])
+        descs = (_capi.Material * ns)(*[mat.descriptor() for mat in materials])
+        bc_lists = dirichlet_nodes if dirichlet_nodes is not None else [()] * ns
+        if len(bc_lists) != ns:
+            raise ValueError("one Dirichlet node list per scene")
+        off = np.zeros(ns + 1, dtype=np.int64)
+        flat = []
+        for k, b in enumerate(bc_lists):
+            b = host_i64(b)
+            off[k + 1] = off[k] + b.size
+            flat.append(b)
+        flat = np.concatenate(flat) if off[-1] else np.zeros(1, dtype=np.int64)
+        self._bc = (off, flat)
+        h = C.c_void_p()
+        check(lib().hoefem_batch_create(handles, ns, descs, float(density), off.ctypes.data, flat.ctypes.data,
+                                        1 if gravity_enabled else 0, float(gravity), C.byref(h)))
+        self._h = h
+        self.num_scenes = ns
+        ndof = C.c_int64()
+        nnz = C.c_int64()
+        self.dof_offsets = np.zeros(ns + 1, dtype=np.int64)
+        check(lib().hoefem_batch_sizes(h, None, C.byref(ndof), C.byref(nnz), self.dof_offsets.ctypes.data))
+        self.ndof = ndof.value
+        self.nnz = nnz.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().hoefem_batch_destroy(h)
+            self._h = None
+
+    def set_stream(self, stream):
+        check(lib().hoefem_batch_set_stream(self._h, C.c_void_p(int(stream)) if stream else None))
+
+    def set_tolerances(self, cg_tol=1e-5, cg_max_iter=500, newton_max_iter=100):
+        check(lib().hoefem_batch_set_tolerances(self._h, cg_tol, cg_max_iter, newton_max_iter))
+
+    def split(self, x):
+        """Per-scene views of a concatenated DOF vector."""
+        o = self.dof_offsets
+        return [x[o[k]:o[k + 1]] for k in range(self.num_scenes)]
+
+    def step(self, u, v, t, dt, raise_on_failure=True):
+        """Advances the concatenated (u, v) in place; returns one statistics
+        dict per scene (with its 'status')."""
+        mem = _same_space(u, v)
+        st = lib().hoefem_batch_step(self._h, ptr(u)[0], ptr(v)[0], float(t), float(dt), mem)
+        if st not in (0, 20, 21, 22) and st not in _CG_KIND:
+            check(st)
+        stats = self.stats()
+        if raise_on_failure and st != 0:
+            check(st)
+        return stats
+
+    def stats(self):
+        out = []
+        for k in range(self.num_scenes):
+            s = _capi.StepStats()
+            code = C.c_int32()
+            check(lib().hoefem_batch_scene_stats(self._h, k, C.byref(s), C.byref(code)))
+            d = s.as_dict()
+            d["status"] = code.value
+            out.append(d)
+        return out

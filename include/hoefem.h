@@ -307,6 +307,38 @@ int hoefem_learned_predict(hoefem_learned l, const double* r, double* x0, int me
 int hoefem_integrator_set_learned(hoefem_integrator it, hoefem_learned l, int mode);
 
 /* ------------------------------------------------------------------------ */
+/* Batched steps of many independent scenes (no counterpart in the reference,
+   whose integrator advances one model at a time: an addition for throughput
+   on small scenes).  Each scene takes the path of hoefem_integrator_step with
+   the diagonal preconditioner (newton_cg.rs:131-295): its own Dirichlet
+   scale, representative force, Newton tolerance, CG scalars, line search and
+   substepping.  All scenes share every kernel launch: the scenes' elements
+   are merged per element kind (per-element Lame parameters), colored once
+   (each scene keeps its own greedy coloring) and the CG iterations of all
+   scenes run together in CUDA-graph chunks with per-scene stopping tests.
+   models: num_scenes models (not necessarily finalized; their vertices,
+   blocks and quadrature are copied); materials: one per scene, all of one
+   kind; bc_offsets (num_scenes+1) / bc_nodes: Dirichlet nodes per scene, local
+   node numbers (both NULL for none).  The batch's DOF vector is the scenes'
+   DOF vectors concatenated in order (hoefem_batch_sizes gives the offsets). */
+typedef struct hoefem_batch_s* hoefem_batch;
+
+int hoefem_batch_create(const hoefem_model* models, int32_t num_scenes, const hoefem_material* materials,
+                        double density, const int64_t* bc_offsets, const int64_t* bc_nodes, int gravity_enabled,
+                        double gravity, hoefem_batch* out);
+int hoefem_batch_destroy(hoefem_batch b);
+int hoefem_batch_set_stream(hoefem_batch b, void* stream);
+/* Defaults as hoefem_integrator_set_tolerances: 1e-5, 500, 100. */
+int hoefem_batch_set_tolerances(hoefem_batch b, double cg_tol, int64_t cg_max_iter, int64_t newton_max_iter);
+/* dof_offsets: num_scenes+1 (may be NULL). */
+int hoefem_batch_sizes(hoefem_batch b, int64_t* num_scenes, int64_t* ndof, int64_t* nnz, int64_t* dof_offsets);
+/* One time step of every scene; u, v (total ndof) updated in place for every
+   scene that succeeded.  Returns the status of a failed scene if any failed
+   (the others are still advanced); per-scene status via scene_stats. */
+int hoefem_batch_step(hoefem_batch b, double* u, double* v, double t, double dt, int mem);
+int hoefem_batch_scene_stats(hoefem_batch b, int32_t scene, hoefem_step_stats* out, int32_t* status);
+
+/* ------------------------------------------------------------------------ */
 /* Synthetic scenes (input construction; not part of the reference hot path).
    Restates the reference's procedural meshes and refinements:
    create_rectangular_uniform_hex_mesh (fenris/src/geometry/procedural.rs:
@@ -318,6 +350,10 @@ typedef struct hoefem_scene_s* hoefem_scene;
 /* Box [0, unit*ux] x [0, unit*uy] x [0, unit*uz], cells_per_unit cells per unit,
    each hex split into 6 Tet10; one uniform block with tet_quadrature_strength_5. */
 int hoefem_scene_create_tet10_box(double unit, int64_t ux, int64_t uy, int64_t uz, int64_t cells_per_unit,
+                                  hoefem_scene* out);
+/* The same box as Hex27 elements (no clipping); one uniform block with
+   hex_quadrature_strength_5. */
+int hoefem_scene_create_hex27_box(double unit, int64_t ux, int64_t uy, int64_t uz, int64_t cells_per_unit,
                                   hoefem_scene* out);
 /* Unit-box Hex27 grid (n^3 cells) clipped to the hollow cylinder with axis z
    through (0.5, 0.5), radii [r_inner, r_outer], full height.  Cells with volume

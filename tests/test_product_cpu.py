@@ -63,6 +63,22 @@ def test_tet10_box_non_cubic_matches():
     assert np.array_equal(s.vertices, t.vertices) and np.array_equal(s.blocks[0].connectivity, t.cells)
 
 
+def test_hex27_box_matches_reference_refinement():
+    s = H.scenes.hex27_box(0.5, 2, 1, 3, 2)
+    t = O.hex27_from_hex(O.hex_box(0.5, 2, 1, 3, 2))
+    assert np.array_equal(s.vertices, t.vertices) and np.array_equal(s.blocks[0].connectivity, t.cells)
+    assert s.blocks[0].offsets is None and s.blocks[0].weights.size == 14
+
+
+def test_pattern_and_coloring_bit_exact_hex27_box():
+    s = H.scenes.hex27_box(1.0, 1, 1, 1, 3)
+    b = s.blocks[0]
+    with pytest.raises(ValueError):
+        H.NodalModel3d(s.vertices, b.connectivity, (b.weights, b.points))  # Tet10 by default
+    m = H.NodalModel3d(s.vertices, b.connectivity, (b.weights, b.points), H.ELEM_HEX27)
+    _check_model_vs_oracle(s.blocks, s.vertices, m)
+
+
 def test_embedded_cylinder_matches_reference_refinement_and_keep_cells():
     n = 6
     e = H.scenes.embedded_cylinder(n)
