@@ -49,9 +49,27 @@ def parse():
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--roofline-reps", type=int, default=20)
-    ap.add_argument("--inner-tol", type=float, default=1e-2, help="mixed variant: inner FP32 PCG tolerance")
-    ap.add_argument("--variants", default="plain,mixed", help="comma list: plain, mixed")
+    ap.add_argument("--delta", type=float, default=0.1, help="mixed variant: reliable-update threshold")
+    ap.add_argument("--variants", default="plain,mixed,learned", help="comma list: plain, mixed, learned")
+    ap.add_argument("--train-states", type=int, default=16, help="learned: training initial states (seeded)")
+    ap.add_argument("--train-steps", type=int, default=2000, help="learned: Adam steps")
+    ap.add_argument("--coarse-subdomains", type=int, default=256, help="learned: coarse subdomains")
+    ap.add_argument("--workload", default="cylinder", choices=["cylinder", "batched"],
+                    help="cylinder: embedded Hex27 cylinder Newton step; batched: 64 independent scenes in one batch")
+    ap.add_argument("--scenes", type=int, default=64, help="batched: number of scenes")
+    ap.add_argument("--min-elements", type=float, default=1e3, help="batched: smallest scene (elements)")
+    ap.add_argument("--max-elements", type=float, default=5e4, help="batched: largest scene (elements)")
+    ap.add_argument("--no-sequential", action="store_true", help="batched: skip the one-scene-at-a-time comparison")
     return ap.parse_args()
+
+
+def sway_state(H, e, ndof, amp_x, amp_y, noise_seed):
+    """u = (amp_x z^2, amp_y z^2, 0) + N(0, (0.001 h)^2), v = 0."""
+    X = e.vertices
+    u0 = np.zeros_like(X)
+    u0[:, 0] = amp_x * X[:, 2] ** 2
+    u0[:, 1] = amp_y * X[:, 2] ** 2
+    return u0.reshape(-1) + H.scenes.random_normal(noise_seed, ndof, 0.001 * e.cell_size), np.zeros(ndof)
 
 
 def workload(H, n, seed):
@@ -63,13 +81,36 @@ def workload(H, n, seed):
     bc = e.nodes_below(2, 1e-9)
     comp = H.SchwarzPreconditionerComponent.from_embedded_model(model, e.volume_fractions, 0.5)
     # initial state: smooth sway u = (0.02 z^2, 0.01 z^2, 0) plus seeded noise N(0, (0.001 h)^2), at rest
-    X = e.vertices
-    u0 = np.zeros_like(X)
-    u0[:, 0] = 0.02 * X[:, 2] ** 2
-    u0[:, 1] = 0.01 * X[:, 2] ** 2
-    u0 = u0.reshape(-1) + H.scenes.random_normal(1000 + seed, model.ndof(), 0.001 * e.cell_size)
-    v0 = np.zeros(model.ndof())
+    u0, v0 = sway_state(H, e, model.ndof(), 0.02, 0.01, 1000 + seed)
     return e, model, mat, bc, comp, u0, v0
+
+
+def train_learned(H, e, model, integ, bc, args, dev):
+    """Learned coarse correction trained on (b, x*) pairs of plain FP64
+    Schwarz-CG Jacobian solves from seeded training states (sway amplitudes
+    and noise seeds disjoint from the timed state)."""
+    import torch
+
+    L = H.LearnedCoarseCorrection(model, bc, num_subdomains=args.coarse_subdomains, seed=7)
+    integ.set_precision(False, args.delta)
+    integ.set_learned(L, 2)
+    rng = np.random.default_rng(12345)
+    t0 = time.perf_counter()
+    for k in range(args.train_states):
+        ax, ay = rng.uniform(-0.03, 0.03, size=2)
+        u, v = sway_state(H, e, model.ndof(), ax, ay, 50000 + k)
+        ud, vd = torch.from_numpy(u).to(dev), torch.from_numpy(v).to(dev)
+        integ.step(ud, vd, 0.0, DT)
+    t_collect = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    hist = L.train(args.train_steps, batch=512, lr=1e-3, seed=0)
+    t_train = time.perf_counter() - t0
+    integ.set_learned(None)
+    info = {"rows": int(L.num_pairs()), "coarse_subdomains": args.coarse_subdomains,
+            "train_states": args.train_states, "adam_steps": args.train_steps,
+            "loss_first10": float(np.mean(hist[:10])), "loss_last50": float(np.mean(hist[-50:])),
+            "collect_s": t_collect, "train_s": t_train}
+    return L, info
 
 
 class Clocks:
@@ -213,8 +254,12 @@ def run_hoefem(args):
         return integ.step(ud, vd, 0.0, DT)
 
     variants = {}
+    learned, learned_info = None, None
     for vname in [v.strip() for v in args.variants.split(",") if v.strip()]:
-        integ.set_precision(vname == "mixed", args.inner_tol)
+        if vname == "learned" and learned is None:
+            learned, learned_info = train_learned(H, e, model, integ, bc, args, dev)
+        integ.set_precision(vname in ("mixed", "learned"), args.delta)
+        integ.set_learned(learned if vname == "learned" else None, 1)
         for _ in range(args.warmup):
             step()
         torch.cuda.synchronize()
@@ -244,14 +289,21 @@ def run_hoefem(args):
                          "precond_update": s_["ms_precond_update"], "cg": s_["ms_cg"], "total": s_["ms_total"]},
             "gpu_launches": int(launches), "clocks": ck, "u": ud.cpu().numpy(),
         }
-    head = "mixed" if "mixed" in variants else list(variants)[0]
+        if vname == "learned":
+            variants[vname].update({"learned_accepted": int(s_["learned_accepted"]),
+                                    "learned_rejected": int(s_["learned_rejected"]),
+                                    "learned_residual_ratio": s_["learned_residual_ratio"],
+                                    "ms_learned": s_["ms_learned"], "training": learned_info})
+    head = "learned" if "learned" in variants else ("mixed" if "mixed" in variants else list(variants)[0])
     ms = variants[head]["ms_per_step"]
     launches = variants[head]["gpu_launches"]
     ck = variants[head]["clocks"]
-    integ.set_precision(head == "mixed", args.inner_tol)
-    if "mixed" in variants and "plain" in variants:
-        up, um = variants["plain"]["u"], variants["mixed"]["u"]
-        variants["mixed"]["rel_diff_u_vs_plain"] = float(np.abs(um - up).max() / np.abs(up).max())
+    integ.set_precision(head in ("mixed", "learned"), args.delta)
+    integ.set_learned(learned if head == "learned" else None, 1)
+    for vn in ("mixed", "learned"):
+        if vn in variants and "plain" in variants:
+            up, um = variants["plain"]["u"], variants[vn]["u"]
+            variants[vn]["rel_diff_u_vs_plain"] = float(np.abs(um - up).max() / np.abs(up).max())
     for v in variants.values():
         v.pop("u")
 
@@ -293,7 +345,7 @@ def run_hoefem(args):
             "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene, replicas per rank)",
-            "variant": {"mixed": "mixed_fp32", "plain": "plain_fp64"}[head],
+            "variant": {"mixed": "mixed_fp32", "plain": "plain_fp64", "learned": "learned_mixed"}[head],
             "variants": variants,
             "config": {"workload": "embedded Hex27 hollow cylinder %d^3 (r 0.3-0.4), StVK E=5e5 nu=0.45, one "
                                    "backward-Euler Newton step dt=1e-3, Schwarz-CG to %g" % (args.n, args.cg_tol),
@@ -352,10 +404,143 @@ def spmv_roofline(H, model, integ, mat, ud, stream, reps):
             "algorithmic_bytes": bytes_alg, "peak_source": "measured" if os.path.exists(peaks_path) else "fallback"}
 
 
+def batched_scenes(H, args):
+    """Seeded scene list: element counts log-uniform in [min, max], Tet10 box
+    grids (6 tets per cell) and Hex27 box grids alternating, SNH with E
+    log-uniform in [1e5, 1e7] and nu uniform in [0.3, 0.48], bottom nodes
+    clamped, u0 = small sway + N(0, (0.001 h)^2), v0 = 0."""
+    rng = np.random.default_rng(args.seed)
+    out = []
+    for k in range(args.scenes):
+        target = float(np.exp(rng.uniform(np.log(args.min_elements), np.log(args.max_elements))))
+        tet = (k % 2 == 0)
+        cells = max(1.0, target / 6.0 if tet else target)
+        n = max(1, int(round(cells ** (1.0 / 3.0))))
+        nz = max(1, int(round(cells / (n * n))))
+        h = 1.0 / max(n, nz)
+        young = float(np.exp(rng.uniform(np.log(1e5), np.log(1e7))))
+        nu = float(rng.uniform(0.3, 0.48))
+        if tet:
+            s = H.scenes.tet10_box(h, n, n, nz, 1)
+        else:
+            s = H.scenes.hex27_box(h, n, n, nz, 1)
+        b = s.blocks[0]
+        m = H.NodalModel3d(s.vertices, b.connectivity, (b.weights, b.points), b.kind)
+        mat = H.StableNeoHookeanMaterial(H.YoungPoisson(young, nu))
+        bc = s.nodes_below(2, 1e-9)
+        u0, v0 = sway_state(H, s, m.ndof(), 0.01 * rng.uniform(-1, 1), 0.01 * rng.uniform(-1, 1), 7000 + k)
+        out.append({"scene": s, "model": m, "mat": mat, "bc": bc, "u0": u0, "v0": v0, "kind": "tet10" if tet else "hex27",
+                    "elements": int(m.num_elements), "young": young, "nu": nu})
+    return out
+
+
+def run_batched(args):
+    """Batched solves: all scenes advanced by one backward-Euler Newton-CG step
+    (diagonal preconditioner) in one batch, against the same scenes stepped
+    one at a time by NewtonCgIntegrator3d."""
+    import torch
+
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import higher_order_embedded_fem_b200 as H
+
+    H._capi.check(H._capi.lib().hoefem_set_device(local))
+    t0 = time.perf_counter()
+    sc = batched_scenes(H, args)
+    B = H.BatchedNewtonCgIntegrator3d([x["model"] for x in sc], [x["mat"] for x in sc], 1000.0,
+                                      [x["bc"] for x in sc])
+    setup_s = time.perf_counter() - t0
+    B.set_tolerances(args.cg_tol, args.cg_max_iter, 100)
+    stream = torch.cuda.current_stream(dev)
+    B.set_stream(stream.cuda_stream)
+    u0 = torch.from_numpy(np.concatenate([x["u0"] for x in sc])).to(dev)
+    v0 = torch.from_numpy(np.concatenate([x["v0"] for x in sc])).to(dev)
+    ud, vd = u0.clone(), v0.clone()
+
+    def step():
+        ud.copy_(u0)
+        vd.copy_(v0)
+        return B.step(ud, vd, 0.0, DT)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    n0 = H._capi.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        stats = step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = H._capi.launch_count() - n0
+    ck = clocks.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    # end to end with pinned host buffers
+    uh = torch.empty(B.ndof, dtype=torch.float64, pin_memory=True).numpy()
+    vh = torch.empty(B.ndof, dtype=torch.float64, pin_memory=True).numpy()
+    B.set_stream(None)
+    uh[:] = u0.cpu().numpy()
+    vh[:] = v0.cpu().numpy()
+    B.step(uh, vh, 0.0, DT)
+    t1 = time.perf_counter()
+    for _ in range(args.steps):
+        uh[:] = u0.cpu().numpy()
+        vh[:] = v0.cpu().numpy()
+        B.step(uh, vh, 0.0, DT)
+    e2e_ms = (time.perf_counter() - t1) * 1e3 / args.steps
+    seq_ms = None
+    if not args.no_sequential:
+        # the same scenes one at a time (one integrator alive at a time): the
+        # sum of the per-scene device times of one step each, after a warm-up
+        B.set_stream(stream.cuda_stream)
+        seq_ms = 0.0
+        for x in sc:
+            it = H.NewtonCgIntegrator3d(x["model"], x["mat"], 1000.0, x["bc"])
+            it.set_tolerances(args.cg_tol, args.cg_max_iter, 100)
+            x["model"].set_stream(stream.cuda_stream)
+            a = torch.from_numpy(x["u0"]).to(dev)
+            b = torch.from_numpy(x["v0"]).to(dev)
+            it.step(a.clone(), b.clone(), 0.0, DT)
+            ua, vb = a.clone(), b.clone()
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            it.step(ua, vb, 0.0, DT)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            seq_ms += ev0.elapsed_time(ev1)
+            del it
+    newton = [s["newton_iterations"] for s in stats]
+    cgit = [s["total_cg_iterations"] for s in stats]
+    line = {
+        "metric": "batched Newton step ms (all scenes) on 1 GPU", "value": ms, "unit": "ms", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scenes)",
+        "config": {"workload": "%d scenes, elements log-uniform [%g, %g], Tet10/Hex27 boxes alternating, SNH E "
+                               "log-uniform [1e5, 1e7], nu U[0.3, 0.48], one BE Newton step dt=1e-3, diagonal PCG "
+                               "to %g" % (args.scenes, args.min_elements, args.max_elements, args.cg_tol),
+                   "elements": int(sum(x["elements"] for x in sc)), "ndof": int(B.ndof), "nnz": int(B.nnz),
+                   "l2": "inputs larger than L2 (CSR values %d MB)" % (B.nnz * 8 // 2 ** 20)},
+        "sequential_ms": seq_ms, "speedup_vs_sequential": (seq_ms / ms) if seq_ms else None,
+        "newton_iterations": {"min": int(min(newton)), "max": int(max(newton)), "sum": int(sum(newton))},
+        "cg_iterations": {"min": int(min(cgit)), "max": int(max(cgit)), "sum": int(sum(cgit))},
+        "statuses": sorted({int(s["status"]) for s in stats}),
+        "setup_s": setup_s,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 16 * int(B.ndof),
+                "d2h_bytes_per_step": 16 * int(B.ndof)},
+        "gpu_launches": int(launches), "clocks": ck,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched":
+        run_batched(args)
     else:
         run_hoefem(args)
 

@@ -101,7 +101,7 @@ template <int L>
 __global__ void __launch_bounds__(TPB) k_seg_init(NodeRows A, const double* __restrict__ vals,
                                                   const double* __restrict__ x, const double* __restrict__ b,
                                                   double* __restrict__ r, double* __restrict__ t) {
-  for_each_node<L>(A.nv, [&](int a, int sl) {
+  for_each_node<L>(A, [&](int a, int sl) {
     double s[3];
     node_row_dot<L>(A, vals, x, a, sl, s[0], s[1], s[2]);
     if (a >= 0 && sl == 0) {
@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(TPB) k_seg_init(NodeRows A, const double* __re
       t[A.nv + a] = rr;
     }
   });
+  node_sched_finish(A);
 }
 
 // z = d r, p = z, per node t0 = z.r
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(TPB) k_seg_Ap(NodeRows A, const double* __rest
                                                 const double* __restrict__ p, double* __restrict__ Ap,
                                                 const int* __restrict__ scene_of, const SegCg* __restrict__ st,
                                                 double* __restrict__ t) {
-  for_each_node<L>(A.nv, [&](int a, int sl) {
+  for_each_node<L>(A, [&](int a, int sl) {
     const bool skip = a >= 0 && st[scene_of[a]].done;
     double s[3];
     node_row_dot<L>(A, vals, p, skip ? -1 : a, sl, s[0], s[1], s[2]);
@@ -158,6 +159,7 @@ __global__ void __launch_bounds__(TPB) k_seg_Ap(NodeRows A, const double* __rest
       t[A.nv + a] = 0.0;
     }
   });
+  node_sched_finish(A);
 }
 
 __global__ void k_seg_update(int nv, const int* __restrict__ scene_of, const SegCg* __restrict__ st,
@@ -445,7 +447,7 @@ struct Batch {
     err.zero(s);
     K.zero(s);
     launch_mass(m, density, K.p, s);
-    (note_launch(), k_vcopy<<<vg(), TPB, 0, s>>>((int)m.nnz, K.p, M.p));  // nnz < 2^31
+    HOEFEM_CUDA(cudaMemcpyAsync(M.p, K.p, sizeof(double) * m.nnz, cudaMemcpyDeviceToDevice, s));
     dirichlet(M.p);
     check_device_error(m);
     m.spmv_lanes = autotune_spmv_lanes(m.rows(), M.p, s);

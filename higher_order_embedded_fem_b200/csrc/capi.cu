@@ -20,7 +20,7 @@ Integrator* integrator_new(Model* m, const hoefem_material* mat, double density,
                            int gravity_enabled, double gravity, Precond* P);
 void integrator_delete(Integrator* it);
 void integrator_set_tolerances(Integrator* it, double tol, i64 cg_max, i64 newton_max);
-void integrator_set_precision(Integrator* it, int precision, double inner_tol);
+void integrator_set_precision(Integrator* it, int precision, double delta);
 void integrator_set_learned(Integrator* it, Learned* l, int mode);
 int integrator_step(Integrator* it, double* ud, double* vd, double t, double dt);
 hoefem_step_stats integrator_stats(Integrator* it);
@@ -249,6 +249,15 @@ int hoefem_model_autotune(hoefem_model m, int32_t* lanes) {
   v.zero(mm.stream);
   mm.spmv_lanes = autotune_spmv_lanes(mm.rows(), v.p, mm.stream);
   if (lanes) *lanes = mm.spmv_lanes;
+  API_END
+}
+
+int hoefem_model_set_spmv_variant(hoefem_model m, int32_t variant) {
+  API_BEGIN
+  Model& mm = device_model(m);
+  HOEFEM_REQUIRE(variant == 8 || variant == 16 || variant == 32 || variant == 108 || variant == 116 || variant == 132,
+                 HOEFEM_ERR_INVALID_ARGUMENT, "unknown SpMV variant");
+  mm.spmv_lanes = variant;
   API_END
 }
 
@@ -516,10 +525,10 @@ int hoefem_cg_solve(hoefem_model m, const double* system_values, hoefem_precond 
 }
 
 int hoefem_cg_solve_mixed(hoefem_model m, const double* system_values, hoefem_precond p, const double* b, double* x,
-                          double tol, int64_t max_iter, double inner_tol, int64_t* iterations, int mem) {
+                          double tol, int64_t max_iter, double delta, int64_t* iterations, int mem) {
   API_BEGIN
   Model& mm = device_model(m);
-  HOEFEM_REQUIRE(iterations && inner_tol > 0.0 && inner_tol < 1.0, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  HOEFEM_REQUIRE(iterations && delta > 0.0 && delta < 1.0, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
   HOEFEM_REQUIRE(!p || p->p.m == &mm, HOEFEM_ERR_INVALID_ARGUMENT, "preconditioner of another model");
   if (!m->cg) {
     m->cg.reset(new CgWork());
@@ -538,8 +547,8 @@ int hoefem_cg_solve_mixed(hoefem_model m, const double* system_values, hoefem_pr
   }
   HOEFEM_CUDA(cudaMemcpyAsync(w.b.p, B.d, mm.ndof * sizeof(double), cudaMemcpyDeviceToDevice, mm.stream));
   HOEFEM_CUDA(cudaMemcpyAsync(w.x.p, X.d, mm.ndof * sizeof(double), cudaMemcpyDeviceToDevice, mm.stream));
-  i64 it = 0, outer = 0;
-  int st = cg_solve_ir(w, A.d, A32.p, p ? &p->p : nullptr, tol, max_iter, inner_tol, &it, &outer, mm.stream);
+  i64 it = 0, replacements = 0;
+  int st = cg_solve_reliable(w, A.d, A32.p, p ? &p->p : nullptr, tol, max_iter, delta, &it, &replacements, mm.stream);
   HOEFEM_CUDA(cudaMemcpyAsync(X.d, w.x.p, mm.ndof * sizeof(double), cudaMemcpyDeviceToDevice, mm.stream));
   X.copy_out();
   sync(mm);
@@ -573,12 +582,12 @@ int hoefem_integrator_set_tolerances(hoefem_integrator it, double cg_tol, int64_
   API_END
 }
 
-int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double inner_tol) {
+int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double delta) {
   API_BEGIN
   HOEFEM_REQUIRE(it && (precision == HOEFEM_PRECISION_FP64 || precision == HOEFEM_PRECISION_MIXED) &&
-                     inner_tol > 0.0 && inner_tol < 1.0,
+                     delta > 0.0 && delta < 1.0,
                  HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
-  integrator_set_precision(it->it, precision == HOEFEM_PRECISION_MIXED ? PRECISION_FP32 : PRECISION_FP64, inner_tol);
+  integrator_set_precision(it->it, precision == HOEFEM_PRECISION_MIXED ? PRECISION_FP32 : PRECISION_FP64, delta);
   API_END
 }
 
@@ -749,7 +758,7 @@ int hoefem_learned_predict(hoefem_learned l, const double* r, double* x0, int me
 
 int hoefem_integrator_set_learned(hoefem_integrator it, hoefem_learned l, int mode) {
   API_BEGIN
-  HOEFEM_REQUIRE(it && mode >= 0 && mode <= 2, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  HOEFEM_REQUIRE(it && mode >= 0 && mode <= 3, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
   HOEFEM_REQUIRE(!l || l->model == it->model, HOEFEM_ERR_INVALID_ARGUMENT, "learned correction of another model");
   integrator_set_learned(it->it, l ? &l->l : nullptr, mode);
   API_END

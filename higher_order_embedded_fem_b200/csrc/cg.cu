@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(TPB) k_cg_init(NodeRows A, const VA* __restric
                                                  double* __restrict__ r, double* partials, unsigned* counter,
                                                  CgState* st) {
   double acc[2] = {0.0, 0.0};
-  for_each_node<L>(A.nv, [&](int a, int sl) {
+  for_each_node<L>(A, [&](int a, int sl) {
     double s[3];
     node_row_dot<L>(A, vals, x, a, sl, s[0], s[1], s[2]);
     if (a >= 0 && sl == 0) {
@@ -51,6 +51,7 @@ __global__ void __launch_bounds__(TPB) k_cg_init(NodeRows A, const VA* __restric
       }
     }
   });
+  node_sched_finish(A);
   double tot[2];
   if (grid_reduce_last_k<2>(acc, partials, counter, tot) && threadIdx.x == 0) {
     st->bnorm = sqrt(tot[0]);
@@ -88,7 +89,7 @@ __global__ void __launch_bounds__(TPB) k_cg_prec_spmv(NodeRows P, const VP* __re
                                                       double* partials, unsigned* counter, CgState* st, int init) {
   if (!init && st->done) return;
   double acc[1] = {0.0};
-  for_each_node<L>(P.nv, [&](int a, int sl) {
+  for_each_node<L>(P, [&](int a, int sl) {
     double s[3];
     node_row_dot<L>(P, pv, r, a, sl, s[0], s[1], s[2]);
     if (a >= 0 && sl == 0) {
@@ -99,6 +100,7 @@ __global__ void __launch_bounds__(TPB) k_cg_prec_spmv(NodeRows P, const VP* __re
       }
     }
   });
+  node_sched_finish(P);
   double tot[1];
   if (grid_reduce_last_k<1>(acc, partials, counter, tot) && threadIdx.x == 0) {
     if (init) st->zTr = tot[0];
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(TPB) k_cg_Ap(NodeRows A, const VA* __restrict_
                                                double* partials, unsigned* counter, CgState* st) {
   if (st->done) return;
   double acc[1] = {0.0};
-  for_each_node<L>(A.nv, [&](int a, int sl) {
+  for_each_node<L>(A, [&](int a, int sl) {
     double s[3];
     node_row_dot<L>(A, vals, p, a, sl, s[0], s[1], s[2]);
     if (a >= 0 && sl == 0) {
@@ -144,6 +146,7 @@ __global__ void __launch_bounds__(TPB) k_cg_Ap(NodeRows A, const VA* __restrict_
       }
     }
   });
+  node_sched_finish(A);
   double tot[1];
   if (grid_reduce_last_k<1>(acc, partials, counter, tot) && threadIdx.x == 0) {
     double pAp = tot[0];
@@ -198,6 +201,30 @@ __global__ void __launch_bounds__(TPB) k_cg_p(int n, const double* __restrict__ 
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = z[i] + beta * p[i];
 }
 
+// Residual replacement (reliable update) of the mixed-precision CG: before the
+// true residual overwrites r, keep the recurrence's z.r in pAp.
+__global__ void k_cg_save_ztr(CgState* st) { st->pAp = st->zTr; }
+
+// After r = b - A64 x and z = P r: convergence test on the true residual.
+// `resume`: the recurrence had stopped as converged; if the true residual has
+// not, iterate on with the direction p = z + (z.r / z.r_old) p.
+__global__ void k_cg_reliable(CgState* st, int resume) {
+  if (sqrt(st->rr) <= st->tol * st->bnorm) {
+    st->done = 1;
+    st->status = HOEFEM_OK;
+    return;
+  }
+  if (!resume) return;
+  if (st->max_iter >= 0 && st->iters >= st->max_iter) {
+    st->done = 1;
+    st->status = HOEFEM_CG_MAX_ITERATIONS;
+    return;
+  }
+  st->done = 0;
+  st->status = HOEFEM_OK;
+  st->beta = st->zTr / st->pAp;
+}
+
 int vec_grid(i64 n) { return reduce_blocks_for(n); }
 
 __global__ void k_axpy(int n, double a, const double* __restrict__ x, double* __restrict__ y) {
@@ -215,7 +242,6 @@ void CgWork::init(Model* model) {
   m = model;
   n = model->ndof;
   x.alloc(n); b.alloc(n); r.alloc(n); z.alloc(n); p.alloc(n); Ap.alloc(n);
-  xo.alloc(n); bo.alloc(n); ro.alloc(n);
   partials.alloc(4 * 148 * 16);
   st.alloc(1);
   counter.alloc(1);
@@ -319,8 +345,13 @@ CgWork::Graph& graph_for(CgWork& w, Operator A, const Precond* P, bool p32) {
 }
 
 // PCG on A with preconditioner P: x = w.x (initial guess), b = w.b.
+// With A64 (reliable updates): A holds FP32 values of the same matrix; the
+// initial residual and every residual replacement use the FP64 values A64.
+// A replacement runs at a chunk boundary when the recurrence residual has
+// dropped by `delta` since the last one, and whenever the recurrence reports
+// convergence (which then has to hold for the true residual).
 int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 max_iter, i64* iters,
-            cudaStream_t s) {
+            cudaStream_t s, const double* A64 = nullptr, double delta = 0.0, i64* replacements = nullptr) {
   NodeRows R = w.m->rows();
   const int n = (int)w.n;
   const int kind = P ? P->kind : PREC_NONE;
@@ -330,22 +361,36 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   init.max_iter = max_iter;
   HOEFEM_CUDA(cudaMemcpyAsync(w.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
   const int vg = vec_grid(n);
-  HOEFEM_LANES_DISPATCH(R.lanes, {
-    const int sg = spmv_grid(R.nv, LN);
-    if (A.v32)
-      (note_launch(), k_cg_init<LN, float><<<sg, TPB, 0, s>>>(R, A.v32, w.x.p, w.b.p, w.r.p, w.partials.p,
-                                                              w.counter.p, w.st.p));
-    else
-      (note_launch(), k_cg_init<LN, double><<<sg, TPB, 0, s>>>(R, A.v64, w.x.p, w.b.p, w.r.p, w.partials.p,
+  auto true_residual = [&](const double* vals64) {
+    HOEFEM_LANES_DISPATCH(R.lanes, {
+      const int sg = spmv_grid(R.nv, LN);
+      (note_launch(), k_cg_init<LN, double><<<sg, TPB, 0, s>>>(R, vals64, w.x.p, w.b.p, w.r.p, w.partials.p,
                                                                w.counter.p, w.st.p));
-  });
-  if (kind == PREC_SCHWARZ) {
-    enqueue_prec_spmv(w, P, p32, 1, s);
+    });
+  };
+  auto prec_init = [&]() {
+    if (kind == PREC_SCHWARZ) {
+      enqueue_prec_spmv(w, P, p32, 1, s);
+    } else {
+      (note_launch(), k_cg_prec_vec<<<vg, TPB, 0, s>>>(n, kind == PREC_DIAGONAL ? 1 : 0,
+                                                       kind == PREC_DIAGONAL ? P->diag.p : nullptr, w.r.p, w.z.p,
+                                                       w.partials.p, w.counter.p, w.st.p, 1));
+    }
+  };
+  if (A64) {
+    true_residual(A64);
   } else {
-    (note_launch(), k_cg_prec_vec<<<vg, TPB, 0, s>>>(n, kind == PREC_DIAGONAL ? 1 : 0,
-                                                     kind == PREC_DIAGONAL ? P->diag.p : nullptr, w.r.p, w.z.p,
-                                                     w.partials.p, w.counter.p, w.st.p, 1));
+    HOEFEM_LANES_DISPATCH(R.lanes, {
+      const int sg = spmv_grid(R.nv, LN);
+      if (A.v32)
+        (note_launch(), k_cg_init<LN, float><<<sg, TPB, 0, s>>>(R, A.v32, w.x.p, w.b.p, w.r.p, w.partials.p,
+                                                                w.counter.p, w.st.p));
+      else
+        (note_launch(), k_cg_init<LN, double><<<sg, TPB, 0, s>>>(R, A.v64, w.x.p, w.b.p, w.r.p, w.partials.p,
+                                                                 w.counter.p, w.st.p));
+    });
   }
+  prec_init();
   (note_launch(), k_cg_copy<<<vg, TPB, 0, s>>>(n, w.z.p, w.p.p));
   (note_launch(), k_cg_init_check<<<1, 1, 0, s>>>(w.st.p));
   HOEFEM_CUDA(cudaGetLastError());
@@ -364,14 +409,33 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   // without an iteration limit CG is still bounded: 10 n iterations
   const i64 cap = max_iter >= 0 ? max_iter : 10 * (i64)n;
   const i64 max_chunks = (cap + w.chunk - 1) / w.chunk + 2;
+  double rr_ref = w.h_st->rr;
+  i64 nrep = 0;
   for (i64 c = 0; c < max_chunks; ++c) {
     HOEFEM_CUDA(cudaGraphLaunch(G.exec, s));
     g_launch_count.fetch_add(G.kernels, std::memory_order_relaxed);
     HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
     HOEFEM_CUDA(cudaStreamSynchronize(s));
+    if (A64) {
+      const bool conv = w.h_st->done && w.h_st->status == HOEFEM_OK;
+      const bool trig = !w.h_st->done && w.h_st->rr <= delta * delta * rr_ref;
+      if (conv || trig) {
+        (note_launch(), k_cg_save_ztr<<<1, 1, 0, s>>>(w.st.p));
+        true_residual(A64);
+        prec_init();
+        (note_launch(), k_cg_reliable<<<1, 1, 0, s>>>(w.st.p, conv ? 1 : 0));
+        if (conv) (note_launch(), k_cg_p<<<vg, TPB, 0, s>>>(n, w.z.p, w.p.p, w.st.p));
+        HOEFEM_CUDA(cudaGetLastError());
+        HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+        HOEFEM_CUDA(cudaStreamSynchronize(s));
+        rr_ref = w.h_st->rr;
+        ++nrep;
+      }
+    }
     if (w.on_chunk && !w.h_st->done) w.on_chunk(s);
     if (w.h_st->done) break;
   }
+  if (replacements) *replacements = nrep;
   *iters = w.h_st->iters;
   if (!w.h_st->done) return HOEFEM_CG_MAX_ITERATIONS;
   return w.h_st->status;
@@ -383,62 +447,16 @@ int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 ma
   return run_pcg(w, Operator{vals, nullptr}, P, false, tol, max_iter, iters, s);
 }
 
-// Mixed precision: FP64 iterative refinement around an inner PCG whose
-// operator and preconditioner values are FP32 (vectors, dot products and
-// residual updates stay FP64).  Outer: r = b - A64 x (FP64), stop when
-// ||r|| <= tol ||b||; inner: A32 d = r to a relative tolerance, x += d.
-int cg_solve_ir(CgWork& w, const double* A64, const float* A32, const Precond* P, double tol, i64 max_iter,
-                double inner_tol, i64* iters, i64* outer, cudaStream_t s) {
-  NodeRows R = w.m->rows();
-  const int n = (int)w.n;
-  const int vg = vec_grid(n);
+// Mixed precision: PCG whose operator (and Schwarz preconditioner) values are
+// FP32 while vectors, dot products and residual updates stay FP64, with
+// residual replacement against the FP64 operator (reliable updates,
+// Sleijpen & van der Vorst 1996): the Krylov recurrence is never restarted,
+// and the stopping test ||b - A64 x|| <= tol ||b|| holds for the true FP64
+// residual.
+int cg_solve_reliable(CgWork& w, const double* A64, const float* A32, const Precond* P, double tol, i64 max_iter,
+                      double delta, i64* iters, i64* replacements, cudaStream_t s) {
   const bool p32 = P && P->kind == PREC_SCHWARZ && P->vals32.p;
-  HOEFEM_CUDA(cudaMemcpyAsync(w.xo.p, w.x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-  HOEFEM_CUDA(cudaMemcpyAsync(w.bo.p, w.b.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-  auto residual = [&](double* rnorm, double* bnorm) {
-    CgState init{};
-    HOEFEM_CUDA(cudaMemcpyAsync(w.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
-    HOEFEM_LANES_DISPATCH(R.lanes, {
-      const int sg = spmv_grid(R.nv, LN);
-      (note_launch(), k_cg_init<LN, double><<<sg, TPB, 0, s>>>(R, A64, w.xo.p, w.bo.p, w.ro.p, w.partials.p,
-                                                               w.counter.p, w.st.p));
-    });
-    HOEFEM_CUDA(cudaGetLastError());
-    HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
-    HOEFEM_CUDA(cudaStreamSynchronize(s));
-    *rnorm = std::sqrt(w.h_st->rr);
-    *bnorm = w.h_st->bnorm;
-  };
-  double rn, bn;
-  residual(&rn, &bn);
-  *iters = 0;
-  *outer = 0;
-  int status = HOEFEM_OK;
-  if (bn == 0.0) {
-    HOEFEM_CUDA(cudaMemsetAsync(w.x.p, 0, sizeof(double) * n, s));
-    return HOEFEM_OK;
-  }
-  for (int k = 0; k < 40; ++k) {
-    if (rn <= tol * bn) { status = HOEFEM_OK; break; }
-    const i64 left = max_iter >= 0 ? max_iter - *iters : -1;
-    if (left == 0) { status = HOEFEM_CG_MAX_ITERATIONS; break; }
-    // inner solve A32 d = r, relative tolerance: the larger of inner_tol and
-    // what is still needed to reach the outer target
-    HOEFEM_CUDA(cudaMemcpyAsync(w.b.p, w.ro.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-    HOEFEM_CUDA(cudaMemsetAsync(w.x.p, 0, sizeof(double) * n, s));
-    double tin = std::max(inner_tol, 0.5 * tol * bn / rn);
-    i64 it = 0;
-    int st = run_pcg(w, Operator{nullptr, A32}, P, p32, tin, left, &it, s);
-    *iters += it;
-    *outer += 1;
-    if (it > 0) (note_launch(), k_axpy<<<vg, TPB, 0, s>>>(n, 1.0, w.x.p, w.xo.p));
-    residual(&rn, &bn);
-    if (st != HOEFEM_OK && st != HOEFEM_CG_MAX_ITERATIONS) { status = st; break; }
-    if (st == HOEFEM_CG_MAX_ITERATIONS && rn > tol * bn) { status = st; break; }
-    status = rn <= tol * bn ? HOEFEM_OK : HOEFEM_CG_MAX_ITERATIONS;
-  }
-  HOEFEM_CUDA(cudaMemcpyAsync(w.x.p, w.xo.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-  return status;
+  return run_pcg(w, Operator{nullptr, A32}, P, p32, tol, max_iter, iters, s, A64, delta, replacements);
 }
 
 }  // namespace hoefem

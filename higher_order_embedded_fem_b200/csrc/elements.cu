@@ -244,18 +244,36 @@ __device__ __forceinline__ void mat3vec(const R* M, const R* a, R* o) {
   o[2] = M[6] * a[0] + M[7] * a[1] + M[8] * a[2];
 }
 
+// Per quadrature point data the pair contraction needs (13 values): T = F
+// (SNH, cross term) or F F^T (StVK), and four scalars (SNH: s1, s2, s3 =
+// lam (J - alpha), s4 = lam; StVK: s1 = mu, s4 = lam).
+template <class R>
+struct QpPair {
+  R T[9];
+  R s1, s2, s3, s4;
+};
+
+template <class R>
+__device__ __forceinline__ void qp_pair_from(int kind, const QpState<R>& q, QpPair<R>& o) {
+#pragma unroll
+  for (int k = 0; k < 9; ++k) o.T[k] = (kind == HOEFEM_MAT_SNH) ? q.F[k] : q.M2[k];
+  o.s1 = q.s1;
+  o.s2 = q.s2;
+  o.s3 = q.s3;
+  o.s4 = q.s4;
+}
+
 // Stiffness block of node pair (I row, J column), added into acc (3x3 row-major).
 // Per-node vectors: v[0..2] = a, v[3..5] = F a, v[6..8] = M1 a.
 //  SNH : s1 (aI.aJ) I + s2 (F aI)(F aJ)^T + lam (Cof aI)(Cof aJ)^T + s3 eps_ijm (F (aI x aJ))_m
 //  StVK: (aJ . S aI) I + mu (F aJ)(F aI)^T + mu (aI.aJ) F F^T + lam (F aI)(F aJ)^T
 template <class R>
-__device__ __forceinline__ void pair_block(int kind, const QpState<R>& q, const R* vI, const R* vJ,
-                                           R* acc) {
+__device__ __forceinline__ void pair_block(int kind, const QpPair<R>& q, const R* vI, const R* vJ, R* acc) {
   R dot = vI[0] * vJ[0] + vI[1] * vJ[1] + vI[2] * vJ[2];
   if (kind == HOEFEM_MAT_SNH) {
     R cr[3] = {vI[1] * vJ[2] - vI[2] * vJ[1], vI[2] * vJ[0] - vI[0] * vJ[2], vI[0] * vJ[1] - vI[1] * vJ[0]};
     R w[3];
-    mat3vec(q.F, cr, w);
+    mat3vec(q.T, cr, w);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -274,7 +292,7 @@ __device__ __forceinline__ void pair_block(int kind, const QpState<R>& q, const 
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = 0; j < 3; ++j)
-        acc[3 * i + j] += mu * vJ[3 + i] * vI[3 + j] + mu * dot * q.M2[3 * i + j] + lam * vI[3 + i] * vJ[3 + j];
+        acc[3 * i + j] += mu * vJ[3 + i] * vI[3 + j] + mu * dot * q.T[3 * i + j] + lam * vI[3 + i] * vJ[3 + j];
     acc[0] += d0; acc[4] += d0; acc[8] += d0;
   }
 }
@@ -361,8 +379,97 @@ __global__ void __launch_bounds__(TPB) k_forces(const BlockDev b, const int* __r
 }
 
 // ============================================================================
-// Stiffness + scatter.  GROUP threads own one element; the first warp of the
-// group builds the per-node vectors, all GROUP threads accumulate node pairs.
+// Internal force, Hex27: FW warps per element (one CTA), warp w takes the
+// quadrature points w, w + FW, ...; the per-warp node forces are summed in
+// shared memory in warp order (deterministic) and scattered once.  A color
+// of a few hundred elements then fills the GPU with FW times more warps.
+// ============================================================================
+constexpr int FW = 8;
+
+__global__ void __launch_bounds__(32 * FW, 2) k_forces_hex27(const BlockDev b, const int* __restrict__ elems, int count,
+                                                         const double* __restrict__ X, const double* __restrict__ u,
+                                                         double* __restrict__ f, MatDev mat, int* err) {
+  constexpr int NN = 27;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ double s_corner[24];
+  __shared__ double s_f[FW][NN][3];
+  __shared__ int s_ok;
+  const int e = elems[blockIdx.x];
+  const bool own = lane < NN;
+  const int g = own ? b.conn[lane * b.ne + e] : 0;
+  double ul[3] = {0, 0, 0};
+  if (own) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ul[k] = u[3 * g + k];
+    if (warp == 0 && lane < 8) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) s_corner[3 * lane + k] = X[3 * g + k];
+    }
+  }
+  if (threadIdx.x == 0) s_ok = 1;
+  __syncthreads();
+  int q0, nq;
+  quad_rule(b, e, q0, nq);
+  const double emu = b.emat ? b.emat[2 * e] : mat.mu, elam = b.emat ? b.emat[2 * e + 1] : mat.lambda;
+  double fl[3] = {0, 0, 0};
+  for (int q = warp; q < nq; q += FW) {
+    const double xi[3] = {b.qp[3 * (q0 + q)], b.qp[3 * (q0 + q) + 1], b.qp[3 * (q0 + q) + 2]};
+    const double w = b.qw[q0 + q];
+    double J[9], Ji[9];
+    hex8_jacobian(s_corner, xi, J);
+    const double detJ = inv3(J, Ji);
+    double gr[3] = {0, 0, 0}, G[3] = {0, 0, 0};
+    if (own) {
+      hex27_grad(lane, xi, gr);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) G[k] = Ji[k] * gr[0] + Ji[3 + k] * gr[1] + Ji[6 + k] * gr[2];
+    }
+    double F[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) F[3 * c + k] = warp_sum(ul[c] * G[k]) + (c == k ? 1.0 : 0.0);
+    QpState<double> st;
+    if (detJ == 0.0 || !material_state(mat.kind, F, emu, elam, st, true)) {
+      if (lane == 0) s_ok = 0;
+      break;
+    }
+    if (own) {
+      const double sc = w * fabs(detJ);
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        fl[i] += -(st.P[3 * i] * G[0] + st.P[3 * i + 1] * G[1] + st.P[3 * i + 2] * G[2]) * sc;
+    }
+  }
+  if (own) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) s_f[warp][lane][i] = fl[i];
+  }
+  __syncthreads();
+  if (!s_ok) {
+    if (threadIdx.x == 0) set_error(err, HOEFEM_ERR_SINGULAR);
+    return;
+  }
+  if (threadIdx.x < 3 * NN) {
+    const int I = threadIdx.x / 3, i = threadIdx.x % 3;
+    double acc = 0.0;
+#pragma unroll
+    for (int w = 0; w < FW; ++w) acc += s_f[w][I][i];
+    const int gI = b.conn[I * b.ne + e];
+    f[3 * gI + i] += acc;
+  }
+}
+
+// ============================================================================
+// Stiffness + scatter.  TPE threads (TPE / 32 warps) own one element, EPC
+// elements per CTA.  The quadrature points are processed in tiles of QT:
+//  phase A: warp w of the element takes points w, w + TPE/32, ... of the
+//    tile; its lanes (one per node) build J, grad N, F (warp sums), the
+//    material state and the per-node vectors a, F a, M1 a into shared memory;
+//  phase B: every thread accumulates its node pair(s) over the tile's points
+//    from shared memory, with no barrier between points.
+// Two barriers per tile (one tile for all standard rules), against two per
+// point with a single node-building warp.
 // ============================================================================
 template <int NN>
 struct PairTable {
@@ -377,69 +484,87 @@ __device__ __forceinline__ void pair_of(int p, int& I, int& J) {
   else { I = c_pairs27[p][0]; J = c_pairs27[p][1]; }
 }
 
-template <int NN, int GROUP, class R>
-__global__ void __launch_bounds__(NN == 10 ? TPB : 384, NN == 10 ? 1 : 2) k_stiffness(const BlockDev b, const int* __restrict__ elems, int count,
-                                                   const double* __restrict__ X, const double* __restrict__ u,
-                                                   const int* __restrict__ adj_off, double* __restrict__ vals,
-                                                   MatDev mat, int* err) {
-  constexpr int EPC = (NN == 10 ? TPB : 384) / GROUP;  // elements per CTA
-  constexpr int NP = PairTable<NN>::NP;            // node pairs I >= J
-  constexpr int PPT = (NP + GROUP - 1) / GROUP;    // pairs per thread
-  const int grp = threadIdx.x / GROUP, t = threadIdx.x % GROUP;
-  const int lane = threadIdx.x & 31;
-  const int idx = blockIdx.x * EPC + grp;
-  __shared__ R s_vec[EPC][NN][9];
+template <int NN>
+struct StiffCfg {
+  static constexpr int TPE = NN == 10 ? 64 : 384;  // threads per element
+  static constexpr int EPC = NN == 10 ? 4 : 1;     // elements per CTA
+  static constexpr int QT = NN == 10 ? 14 : 27;    // quadrature points per tile
+  static constexpr int TPB = TPE * EPC;
+};
+
+template <int NN, class R>
+constexpr size_t stiffness_smem() {
+  using C = StiffCfg<NN>;
+  return sizeof(R) * (size_t)C::EPC * C::QT * NN * 9 + sizeof(QpPair<R>) * (size_t)C::EPC * C::QT;
+}
+
+template <int NN, class R>
+__global__ void __launch_bounds__(StiffCfg<NN>::TPB, 2) k_stiffness(const BlockDev b, const int* __restrict__ elems,
+                                                                    int count, const double* __restrict__ X,
+                                                                    const double* __restrict__ u,
+                                                                    const int* __restrict__ adj_off,
+                                                                    const long long* __restrict__ base,
+                                                                    double* __restrict__ vals, MatDev mat, int* err) {
+  using C = StiffCfg<NN>;
+  constexpr int TPE = C::TPE, EPC = C::EPC, QT = C::QT, WPE = TPE / 32;
+  constexpr int NP = PairTable<NN>::NP;
+  constexpr int PPT = (NP + TPE - 1) / TPE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R(*s_vec)[QT][NN][9] = reinterpret_cast<R(*)[QT][NN][9]>(smem_raw);
+  QpPair<R>(*s_qp)[QT] =
+      reinterpret_cast<QpPair<R>(*)[QT]>(smem_raw + sizeof(R) * (size_t)EPC * QT * NN * 9);
   __shared__ R s_corner[EPC][24];
-  __shared__ QpState<R> s_q[EPC];
   __shared__ int s_g[EPC][NN];
   __shared__ int s_ok[EPC];
   __shared__ int s_nq[EPC];
+  const int grp = threadIdx.x / TPE, t = threadIdx.x % TPE;
+  const int lane = threadIdx.x & 31, wl = t >> 5;
+  const int idx = blockIdx.x * EPC + grp;
   const bool active = idx < count;
   const int e = active ? elems[idx] : 0;
-  const bool nodewarp = (t < 32);
-  const bool own = nodewarp && lane < NN && active;
-  int g = own ? b.conn[lane * b.ne + e] : 0;
-  R Xl[3] = {0, 0, 0}, ul[3] = {0, 0, 0};
-  if (own) {
+  if (active && t < NN) {
+    const int g = b.conn[t * b.ne + e];
+    s_g[grp][t] = g;
+    constexpr int NC = (NN == 10) ? 4 : 8;
+    if (t < NC) {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) { Xl[k] = (R)X[3 * g + k]; ul[k] = (R)u[3 * g + k]; }
-    s_g[grp][lane] = g;
+      for (int k = 0; k < 3; ++k) s_corner[grp][3 * t + k] = (R)X[3 * g + k];
+    }
   }
-  constexpr int NC = (NN == 10) ? 4 : 8;
-  if (own && lane < NC) {
-#pragma unroll
-    for (int k = 0; k < 3; ++k) s_corner[grp][3 * lane + k] = Xl[k];
+  int q0 = 0, nq = 0;
+  if (active) quad_rule(b, e, q0, nq);
+  if (t == 0) {
+    s_ok[grp] = 1;
+    s_nq[grp] = nq;
   }
-  if (t == 0) s_ok[grp] = 1;
   __syncthreads();
-  R J[9], Ji[9], detJ = 0;
-  if (NN == 10) {
-    tet4_jacobian(s_corner[grp], J);
-    detJ = inv3(J, Ji);
+  int nq_max = 0;
+#pragma unroll
+  for (int k = 0; k < EPC; ++k) nq_max = max(nq_max, s_nq[k]);
+  const R mu = (R)(b.emat ? b.emat[2 * e] : mat.mu), lam = (R)(b.emat ? b.emat[2 * e + 1] : mat.lambda);
+  // the lane's node data, kept in registers across tiles
+  const bool own = active && lane < NN;
+  R ul[3] = {0, 0, 0};
+  if (own) {
+    const int g = s_g[grp][lane];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ul[k] = (R)u[3 * g + k];
   }
   R acc[PPT][9];
 #pragma unroll
   for (int k = 0; k < PPT; ++k)
 #pragma unroll
     for (int m = 0; m < 9; ++m) acc[k][m] = 0;
-  int q0 = 0, nq = 0;
-  if (active) quad_rule(b, e, q0, nq);
-  // uniform trip count across the CTA: the max over its elements
-  if (t == 0) s_nq[grp] = nq;
-  __syncthreads();
-  int nq_max = 0;
-#pragma unroll
-  for (int k = 0; k < EPC; ++k) nq_max = max(nq_max, s_nq[k]);
-  const R mu = (R)(b.emat ? b.emat[2 * e] : mat.mu), lam = (R)(b.emat ? b.emat[2 * e + 1] : mat.lambda);
-  for (int q = 0; q < nq_max; ++q) {
-    const bool live = q < nq;
-    if (nodewarp && live) {
-      const R xi[3] = {(R)b.qp[3 * (q0 + q)], (R)b.qp[3 * (q0 + q) + 1], (R)b.qp[3 * (q0 + q) + 2]};
-      const R w = (R)b.qw[q0 + q];
-      if (NN == 27) {
-        hex8_jacobian(s_corner[grp], xi, J);
-        detJ = inv3(J, Ji);
-      }
+  for (int qt = 0; qt < nq_max; qt += QT) {
+    // ---- phase A: per-point data of this tile ----
+    for (int ql = wl; ql < QT && qt + ql < nq; ql += WPE) {
+      const int q = q0 + qt + ql;
+      const R xi[3] = {(R)b.qp[3 * q], (R)b.qp[3 * q + 1], (R)b.qp[3 * q + 2]};
+      const R w = (R)b.qw[q];
+      R J[9], Ji[9];
+      if (NN == 10) tet4_jacobian(s_corner[grp], J);
+      else hex8_jacobian(s_corner[grp], xi, J);
+      const R detJ = inv3(J, Ji);
       R gr[3] = {0, 0, 0}, G[3] = {0, 0, 0};
       if (lane < NN) {
         if (NN == 10) tet10_grad(lane, xi, gr); else hex27_grad(lane, xi, gr);
@@ -452,30 +577,31 @@ __global__ void __launch_bounds__(NN == 10 ? TPB : 384, NN == 10 ? 1 : 2) k_stif
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[3 * c + k] = warp_sum(ul[c] * G[k]) + (c == k ? R(1) : R(0));
       QpState<R> st;
-      bool okq = (detJ != R(0)) && material_state(mat.kind, F, mu, lam, st, false);
+      const bool okq = (detJ != R(0)) && material_state(mat.kind, F, mu, lam, st, false);
       if (!okq) {
         if (lane == 0) s_ok[grp] = 0;
-      } else if (lane < NN) {
-        R sc = sqrt(w * fabs(detJ));
-        R a[3] = {G[0] * sc, G[1] * sc, G[2] * sc};
-        R* v = s_vec[grp][lane];
-        v[0] = a[0]; v[1] = a[1]; v[2] = a[2];
-        mat3vec(st.F, a, v + 3);
-        mat3vec(st.M1, a, v + 6);
+      } else {
+        if (lane < NN) {
+          const R sc = sqrt(w * fabs(detJ));
+          const R a[3] = {G[0] * sc, G[1] * sc, G[2] * sc};
+          R* v = s_vec[grp][ql][lane];
+          v[0] = a[0]; v[1] = a[1]; v[2] = a[2];
+          mat3vec(st.F, a, v + 3);
+          mat3vec(st.M1, a, v + 6);
+        }
+        if (lane == 0) qp_pair_from(mat.kind, st, s_qp[grp][ql]);
       }
-      if (lane == 0) s_q[grp] = st;
     }
     __syncthreads();
-    if (live) {
-      const QpState<R>& st = s_q[grp];
+    // ---- phase B: node pairs over the tile's points ----
+    const int nql = min(QT, nq - qt);
 #pragma unroll
-      for (int k = 0; k < PPT; ++k) {
-        int p = t + k * GROUP;
-        if (p < NP) {
-          int I, Jn;
-          pair_of<NN>(p, I, Jn);
-          pair_block(mat.kind, st, s_vec[grp][I], s_vec[grp][Jn], acc[k]);
-        }
+    for (int k = 0; k < PPT; ++k) {
+      const int p = t + k * TPE;
+      if (p < NP && active) {
+        int I, Jn;
+        pair_of<NN>(p, I, Jn);
+        for (int ql = 0; ql < nql; ++ql) pair_block(mat.kind, s_qp[grp][ql], s_vec[grp][ql][I], s_vec[grp][ql][Jn], acc[k]);
       }
     }
     __syncthreads();
@@ -488,20 +614,20 @@ __global__ void __launch_bounds__(NN == 10 ? TPB : 384, NN == 10 ? 1 : 2) k_stif
   const int* em = b.emap + (size_t)e * NN * NN;
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
-    int p = t + k * GROUP;
+    int p = t + k * TPE;
     if (p < NP) {
       int I, Jn;
       pair_of<NN>(p, I, Jn);
       int gI = s_g[grp][I], gJ = s_g[grp][Jn];
       int rlI = 3 * (adj_off[gI + 1] - adj_off[gI]);
-      int bIJ = em[I * NN + Jn];
+      long long bIJ = base[gI] + em[I * NN + Jn];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) vals[bIJ + i * rlI + j] += (double)acc[k][3 * i + j];
       if (I != Jn) {
         int rlJ = 3 * (adj_off[gJ + 1] - adj_off[gJ]);
-        int bJI = em[Jn * NN + I];
+        long long bJI = base[gJ] + em[Jn * NN + I];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -518,7 +644,8 @@ __global__ void __launch_bounds__(NN == 10 ? TPB : 384, NN == 10 ? 1 : 2) k_stif
 template <int NN>
 __global__ void __launch_bounds__(TPB) k_mass(const BlockDev b, const int* __restrict__ elems, int count,
                                               const double* __restrict__ X, const int* __restrict__ adj_off,
-                                              double* __restrict__ vals, double density, int* err) {
+                                              const long long* __restrict__ nbase, double* __restrict__ vals,
+                                              double density, int* err) {
   constexpr int NE = NN * NN;
   constexpr int EPT = (NE + 31) / 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -565,7 +692,7 @@ __global__ void __launch_bounds__(TPB) k_mass(const BlockDev b, const int* __res
       int I = p / NN, Jn = p % NN;
       int gI = s_g[warp][I];
       int rl = 3 * (adj_off[gI + 1] - adj_off[gI]);
-      int base = em[p];
+      long long base = nbase[gI] + em[p];
 #pragma unroll
       for (int c = 0; c < 3; ++c) vals[base + c * rl + c] += acc[k];
     }
@@ -608,35 +735,44 @@ void launch_forces(const Model& m, const MatDev& mat, const double* u, double* f
       if (bp->kind == HOEFEM_ELEM_TET10)
         (note_launch(), k_forces<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p));
       else
-        (note_launch(), k_forces<27><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p));
+        (note_launch(), k_forces_hex27<<<cnt, 32 * FW, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p));
     });
   }
   HOEFEM_CUDA(cudaGetLastError());
+}
+
+template <int NN, class R>
+void launch_stiffness_kind(const Model& m, const Block& blk, const MatDev& mat, const double* u, double* vals,
+                           cudaStream_t s) {
+  using C = StiffCfg<NN>;
+  constexpr size_t smem = stiffness_smem<NN, R>();
+  static bool attr_set[64] = {};
+  int dev = 0;
+  HOEFEM_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    HOEFEM_CUDA(cudaFuncSetAttribute(k_stiffness<NN, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set[dev] = true;
+  }
+  BlockDev bd = blk.dev();
+  for_each_color(blk, [&](const int* elems, int cnt) {
+    const int grid = (cnt + C::EPC - 1) / C::EPC;
+    (note_launch(), k_stiffness<NN, R><<<grid, C::TPB, smem, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
+                                                                   m.d_base.p, vals, mat, m.d_err.p));
+  });
 }
 
 void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s,
                       int precision) {
   init_pairs();
   for (const Block* bp : m.blocks) {
-    BlockDev bd = bp->dev();
-    for_each_color(*bp, [&](const int* elems, int cnt) {
-      const int grid10 = (cnt + TPB / 32 - 1) / (TPB / 32);
-      if (bp->kind == HOEFEM_ELEM_TET10) {
-        if (precision == PRECISION_FP32)
-          (note_launch(), k_stiffness<10, 32, float><<<grid10, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
-                                                                            vals, mat, m.d_err.p));
-        else
-          (note_launch(), k_stiffness<10, 32, double><<<grid10, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
-                                                                             vals, mat, m.d_err.p));
-      } else {
-        if (precision == PRECISION_FP32)
-          (note_launch(), k_stiffness<27, 384, float><<<cnt, 384, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
-                                                                          vals, mat, m.d_err.p));
-        else
-          (note_launch(), k_stiffness<27, 384, double><<<cnt, 384, 0, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
-                                                                           vals, mat, m.d_err.p));
-      }
-    });
+    const bool f32 = precision == PRECISION_FP32;
+    if (bp->kind == HOEFEM_ELEM_TET10) {
+      if (f32) launch_stiffness_kind<10, float>(m, *bp, mat, u, vals, s);
+      else launch_stiffness_kind<10, double>(m, *bp, mat, u, vals, s);
+    } else {
+      if (f32) launch_stiffness_kind<27, float>(m, *bp, mat, u, vals, s);
+      else launch_stiffness_kind<27, double>(m, *bp, mat, u, vals, s);
+    }
   }
   HOEFEM_CUDA(cudaGetLastError());
 }
@@ -647,9 +783,11 @@ void launch_mass(const Model& m, double density, double* vals, cudaStream_t s) {
     for_each_color(*bp, [&](const int* elems, int cnt) {
       int grid = (cnt + TPB / 32 - 1) / (TPB / 32);
       if (bp->kind == HOEFEM_ELEM_TET10)
-        (note_launch(), k_mass<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, m.d_adj_off.p, vals, density, m.d_err.p));
+        (note_launch(), k_mass<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, m.d_adj_off.p, m.d_base.p, vals, density,
+                                                         m.d_err.p));
       else
-        (note_launch(), k_mass<27><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, m.d_adj_off.p, vals, density, m.d_err.p));
+        (note_launch(), k_mass<27><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, m.d_adj_off.p, m.d_base.p, vals, density,
+                                                         m.d_err.p));
     });
   }
   HOEFEM_CUDA(cudaGetLastError());

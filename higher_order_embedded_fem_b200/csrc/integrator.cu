@@ -70,6 +70,15 @@ __global__ void k_axpy_w(int n, double da, const double* __restrict__ dx, double
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) w[i] = da * dx[i] + 1.0 * w[i];
 }
 
+// y = a y + b  (in place on y)
+__global__ void k_axpby(int n, double a, double* __restrict__ y, const double* __restrict__ b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a * y[i] + b[i];
+}
+
+__global__ void k_scale(int n, double a, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] *= a;
+}
+
 __global__ void k_neg(int n, double* __restrict__ x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] *= -1.0;
 }
@@ -113,10 +122,10 @@ struct Integrator {
   i64 cg_max = 500, newton_max = 100;
   int precision = PRECISION_FP64;  // PRECISION_FP32: mixed (FP32 element stiffness, FP32 operator / Schwarz apply
                                    // inside FP64 iterative refinement)
-  double inner_tol = 1e-2;
+  double delta = 0.1;  // reliable-update threshold of the mixed CG
   DBuf<float> J32;
   Learned* learned = nullptr;
-  int learned_mode = 0;  // 0 off, 1 warm start, 2 collect
+  int learned_mode = 0;  // 0 off, 1 warm start, 2 collect (b, x*), 3 collect (b, x*) and CG iterates
   DBuf<double> x0, r0;
   std::vector<DBuf<double>*> snaps;  // collected (x_k, r_k) pairs of the current solve
   double ratio_sum = 0.0;
@@ -127,7 +136,7 @@ struct Integrator {
   double* h_scalar = nullptr;
   CgWork cg;
   hoefem_step_stats stats{};
-  i64 stats_outer = 0;
+  i64 stats_replacements = 0;
   cudaEvent_t ev[2] = {nullptr, nullptr};
 
   ~Integrator() {
@@ -138,8 +147,10 @@ struct Integrator {
 
   int grid() const { return reduce_blocks_for(m->ndof); }
 
-  double norm_sq(const double* a) {
-    dot_device(a, a, m->ndof, scalars.p, partials.p, counter.p, m->stream);
+  double norm_sq(const double* a) { return dot(a, a); }
+
+  double dot(const double* a, const double* b) {
+    dot_device(a, b, m->ndof, scalars.p, partials.p, counter.p, m->stream);
     HOEFEM_CUDA(cudaMemcpyAsync(h_scalar, scalars.p, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
     HOEFEM_CUDA(cudaStreamSynchronize(m->stream));
     return *h_scalar;
@@ -246,17 +257,17 @@ struct Integrator {
     HOEFEM_CUDA(cudaMemsetAsync(cg.x.p, 0, sizeof(double) * n, s));
     (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, F.p, cg.b.p));
     if (learned && learned_mode == 1 && learned->trained) warm_start(s);
-    const bool collecting = learned && learned_mode == 2 && precision == PRECISION_FP64;
-    if (collecting) start_collect();
+    const bool collecting = learned && learned_mode >= 2 && precision == PRECISION_FP64;
+    if (collecting && learned_mode == 3) start_collect();
     i64 it = 0;
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
     int st;
     if (precision == PRECISION_FP32) {
       if (J32.n < (size_t)m->nnz) J32.alloc(m->nnz);
       to_f32(J.p, J32.p, m->nnz, s);
-      i64 outer = 0;
-      st = cg_solve_ir(cg, J.p, J32.p, P, cg_tol, cg_max, inner_tol, &it, &outer, s);
-      stats_outer += outer;
+      i64 reps = 0;
+      st = cg_solve_reliable(cg, J.p, J32.p, P, cg_tol, cg_max, delta, &it, &reps, s);
+      stats_replacements += reps;
     } else {
       st = cg_solve(cg, J.p, P, cg_tol, cg_max, &it, s);
     }
@@ -274,20 +285,28 @@ struct Integrator {
     return st;
   }
 
-  // Learned warm start with the residual guard: x0 from the MLP, kept only
-  // if ||F - J x0|| < ||F||.
+  // Learned warm start with the residual guard: the MLP's correction d,
+  // scaled by the energy-optimal alpha = d.F / d.J d (the minimiser of the
+  // J-norm error along d), kept only if ||F - alpha J d|| < ||F||.
   void warm_start(cudaStream_t s) {
     const int n = (int)m->ndof;
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
     if (x0.n < (size_t)n) { x0.alloc(n); r0.alloc(n); }
     learned->predict(F.p, x0.p, s);
-    (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, F.p, r0.p));
-    spmv_node_rows(m->rows(), J.p, x0.p, r0.p, -1.0, 1.0, s);
-    double rr = norm_sq(r0.p), bb = norm_sq(F.p);
+    spmv_node_rows(m->rows(), J.p, x0.p, r0.p, 1.0, 0.0, s);
+    const double dJd = dot(x0.p, r0.p), db = dot(x0.p, F.p), bb = norm_sq(F.p);
+    double rr = bb;
+    const double alpha = (dJd > 0.0 && db > 0.0) ? db / dJd : 0.0;
+    if (alpha > 0.0) {
+      // r0 = F - alpha J d, x0 = alpha d
+      (note_launch(), k_axpby<<<grid(), TPB, 0, s>>>(n, -alpha, r0.p, F.p));
+      (note_launch(), k_scale<<<grid(), TPB, 0, s>>>(n, alpha, x0.p));
+      rr = norm_sq(r0.p);
+    }
     HOEFEM_CUDA(cudaEventRecord(ev[1], s));
     HOEFEM_CUDA(cudaEventSynchronize(ev[1]));
     stats.ms_learned += elapsed();
-    if (rr < bb) {
+    if (alpha > 0.0 && rr < bb) {
       (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, x0.p, cg.x.p));
       stats.learned_accepted += 1;
       ratio_sum += std::sqrt(rr / bb);
@@ -439,9 +458,9 @@ void integrator_set_learned(Integrator* it, Learned* l, int mode) {
   it->learned = l;
   it->learned_mode = l ? mode : 0;
 }
-void integrator_set_precision(Integrator* it, int precision, double inner_tol) {
+void integrator_set_precision(Integrator* it, int precision, double delta) {
   it->precision = precision;
-  it->inner_tol = inner_tol;
+  it->delta = delta;
 }
 void integrator_set_tolerances(Integrator* it, double tol, i64 cg_max, i64 newton_max) {
   it->cg_tol = tol;

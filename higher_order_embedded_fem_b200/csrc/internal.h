@@ -84,7 +84,8 @@ struct NodeRows {
   const int* adj = nullptr;         // sorted neighbour nodes
   const int* diag_slot = nullptr;   // slot of a in adj(a) (-1 for diag_only nodes)
   const unsigned char* diag_only = nullptr;  // may be null
-  int lanes = 32;                            // lanes per node in SpMV kernels (32, 16 or 8; autotuned)
+  int lanes = 32;  // SpMV variant: lanes per node (8, 16, 32), +100 for column streaming; autotuned
+  unsigned* sched = nullptr;  // 2 words: node work counter, finished-block counter (dynamic scheduling)
 };
 
 // Per-block device data.
@@ -98,7 +99,7 @@ struct BlockDev {
   const int* qoff = nullptr;   // ne + 1 (non-uniform)
   const double* qw = nullptr;
   const double* qp = nullptr;  // xyz interleaved
-  const int* emap = nullptr;   // [e * nn * nn + I * nn + J] = nnz index of (3 gI, 3 gJ)
+  const int* emap = nullptr;   // [e * nn * nn + I * nn + J] = nnz index of (3 gI, 3 gJ) - base[gI]
   const double* emat = nullptr;  // optional per-element Lame parameters (mu, lambda) pairs
 };
 
@@ -133,6 +134,7 @@ struct Model {
   // device
   DBuf<double> d_X;
   DBuf<int> d_adj_off, d_adj, d_diag_slot, d_err;
+  DBuf<unsigned> d_sched;  // SpMV dynamic-scheduling counters (zero between launches)
   DBuf<long long> d_base;
   int spmv_lanes = 32;
   NodeRows rows() const;

@@ -13,14 +13,28 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   return v;
 }
 
-// Three row sums of node a computed by a group of L lanes (L = 32, 16 or 8;
-// sub-lane sl in [0, L)); a < 0 gives zeros.  All 32 lanes of the warp must
-// call it (the group reduction uses xor shuffles inside aligned L-lane groups).
+// SpMV variant code L: lanes per node = L % 100 (8, 16 or 32); L >= 100
+// selects the column-streaming traversal.
+template <int L>
+struct LaneCfg {
+  static constexpr int lanes = L % 100;
+  static constexpr bool stream = L >= 100;
+};
+
+// Three row sums of node a computed by a group of LaneCfg<L>::lanes lanes
+// (sub-lane sl in [0, lanes)); a < 0 gives zeros.  All 32 lanes of the warp
+// must call it (the group reduction uses xor shuffles inside aligned groups).
 // Matrix values are FP64 or FP32 (V); products and sums are FP64.
+// Neighbour-major traversal (L < 100): a lane takes whole neighbours (its
+// 3 x 3 block in the node's three rows).  Column-streaming traversal
+// (L >= 100): a lane takes scalar columns c = sl, sl + lanes, ... of the
+// node's rows, so consecutive lanes read consecutive values of each row
+// (fully coalesced) and share one x gather across the three rows.
 template <int L, class V>
 __device__ __forceinline__ void node_row_dot(const NodeRows& A, const V* __restrict__ vals,
                                              const double* __restrict__ x, int a, int sl, double& s0, double& s1,
                                              double& s2) {
+  constexpr int LNS = LaneCfg<L>::lanes;
   s0 = s1 = s2 = 0.0;
   if (a >= 0) {
     const long long b = A.base[a];
@@ -30,10 +44,23 @@ __device__ __forceinline__ void node_row_dot(const NodeRows& A, const V* __restr
         s1 = (double)vals[b + 1] * x[3 * a + 1];
         s2 = (double)vals[b + 2] * x[3 * a + 2];
       }
+    } else if constexpr (LaneCfg<L>::stream) {
+      const int o = A.adj_off[a], d = A.adj_off[a + 1] - o;
+      const int rl = 3 * d;
+      const V* r0 = vals + b;
+#pragma unroll 4
+      for (int c = sl; c < rl; c += LNS) {
+        const int s = c / 3, j = c - 3 * s;
+        const double xv = x[3 * A.adj[o + s] + j];
+        s0 += (double)r0[c] * xv;
+        s1 += (double)r0[rl + c] * xv;
+        s2 += (double)r0[2 * rl + c] * xv;
+      }
     } else {
       const int o = A.adj_off[a], d = A.adj_off[a + 1] - o;
       const long long rl = 3LL * d;
-      for (int s = sl; s < d; s += L) {
+#pragma unroll 2
+      for (int s = sl; s < d; s += LNS) {
         const int nb = A.adj[o + s];
         const double x0 = x[3 * nb], x1 = x[3 * nb + 1], x2 = x[3 * nb + 2];
         const V* r0 = vals + b + 3 * s;
@@ -46,24 +73,62 @@ __device__ __forceinline__ void node_row_dot(const NodeRows& A, const V* __restr
     }
   }
 #pragma unroll
-  for (int off = L / 2; off > 0; off >>= 1) {
+  for (int off = LNS / 2; off > 0; off >>= 1) {
     s0 += __shfl_xor_sync(0xffffffffu, s0, off);
     s1 += __shfl_xor_sync(0xffffffffu, s1, off);
     s2 += __shfl_xor_sync(0xffffffffu, s2, off);
   }
 }
 
-// Iterates the nodes of a node-row matrix with L lanes per node:
-// body(a, sl) is called by every lane, with a = -1 for lanes whose group has
-// no node in this round (they must still take part in the reductions).
+// Iterates the nodes of a node-row matrix with LaneCfg<L>::lanes lanes per
+// node: body(a, sl) is called by every lane, with a = -1 for lanes whose group
+// has no node (they must still take part in the reductions).  With
+// A.sched, warps take chunks of NF consecutive nodes from a global work
+// counter until the nodes run out (dynamic load balance: node degrees vary
+// and a fixed grid-stride split leaves a tail); node_sched_finish resets the
+// counters in the last block.  Without A.sched: a grid-stride loop.
 template <int L, class F>
-__device__ __forceinline__ void for_each_node(int nv, F&& body) {
-  constexpr int G = 32 / L;
+__device__ __forceinline__ void for_each_node(const NodeRows& A, F&& body) {
+  constexpr int LNS = LaneCfg<L>::lanes;
+  constexpr int G = 32 / LNS;
+  constexpr int NF = G >= 4 ? 16 : 8;
   const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-  const int grp = lane / L, sl = lane % L;
-  for (int a0 = (blockIdx.x * wpb + (threadIdx.x >> 5)) * G; a0 < nv; a0 += gridDim.x * wpb * G) {
-    const int a = a0 + grp;
-    body(a < nv ? a : -1, sl);
+  const int grp = lane / LNS, sl = lane % LNS;
+  const int nv = A.nv;
+  if (A.sched == nullptr) {
+    for (int a0 = (blockIdx.x * wpb + (threadIdx.x >> 5)) * G; a0 < nv; a0 += gridDim.x * wpb * G) {
+      const int a = a0 + grp;
+      body(a < nv ? a : -1, sl);
+    }
+    return;
+  }
+  for (;;) {
+    unsigned start = 0;
+    if (lane == 0) start = atomicAdd(A.sched, (unsigned)NF);
+    start = __shfl_sync(0xffffffffu, start, 0);
+    if (start >= (unsigned)nv) break;
+    const int end = min((int)start + NF, nv);
+#pragma unroll 1
+    for (int a0 = (int)start; a0 < (int)start + NF; a0 += G) {
+      const int a = a0 + grp;
+      body(a < end ? a : -1, sl);
+    }
+  }
+}
+
+// End of a dynamically scheduled node loop: every thread of the block must
+// call it; the last block to arrive resets the counters for the next launch.
+__device__ __forceinline__ void node_sched_finish(const NodeRows& A) {
+  if (A.sched == nullptr) return;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned t = atomicAdd(A.sched + 1, 1u);
+    if (t == gridDim.x - 1) {
+      A.sched[0] = 0u;
+      A.sched[1] = 0u;
+      __threadfence();
+    }
   }
 }
 
@@ -75,6 +140,15 @@ __device__ __forceinline__ void for_each_node(int nv, F&& body) {
       KERNEL_CALL;                                \
     } else if ((lanes) == 16) {                   \
       constexpr int LN = 16;                      \
+      KERNEL_CALL;                                \
+    } else if ((lanes) == 108) {                  \
+      constexpr int LN = 108;                     \
+      KERNEL_CALL;                                \
+    } else if ((lanes) == 116) {                  \
+      constexpr int LN = 116;                     \
+      KERNEL_CALL;                                \
+    } else if ((lanes) == 132) {                  \
+      constexpr int LN = 132;                     \
       KERNEL_CALL;                                \
     } else {                                      \
       constexpr int LN = 32;                      \

@@ -10,10 +10,12 @@
 //  * features of subdomain s (F = 64): the NM local projections Phi_s^T r_s,
 //    the NG = 29 projections of r on global polynomial modes, and the
 //    subdomain centroid; projections are divided by ||r||;
-//  * MLP F -> 256 -> 256 -> NM (ReLU), trained on (features(r_k), Phi_s^T e_k
-//    / ||r_k||) pairs taken from the iterates of plain Schwarz-CG solves
-//    (e_k = x* - x_k with x* the converged solution), FP32 master weights,
-//    hand-written forward / backward / Adam kernels;
+//  * MLP F -> 256 -> 256 -> NM (ReLU), trained on (features(r), Phi_s^T e /
+//    ||r||) pairs from plain Schwarz-CG solves: the right-hand side b with
+//    the converged solution x* (the pair a warm start is asked for), and
+//    optionally the iterates (r_k, e_k = x* - x_k); features and targets are
+//    standardised per column with the training set's statistics; FP32 master
+//    weights, hand-written forward / backward / Adam kernels;
 //  * inference: BF16 weights and activations on the tensor cores (mma.sync
 //    m16n8k16, FP32 accumulation), x0 = ||r|| sum_s Phi_s c_s.
 // The integrator uses x0 as the initial guess of a Jacobian solve only if it
@@ -344,6 +346,32 @@ __global__ void k_gather_rows(int rows, int width, const long long* __restrict__
   dst[i] = src[idx[r] * width + c];
 }
 
+// dst = (src[idx] - mean) / std, row by row
+__global__ void k_gather_rows_std(int rows, int width, const long long* __restrict__ idx,
+                                  const float* __restrict__ src, const float* __restrict__ mean,
+                                  const float* __restrict__ sd, float* __restrict__ dst) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * width) return;
+  int r = i / width, c = i % width;
+  dst[i] = (src[idx[r] * width + c] - mean[c]) / sd[c];
+}
+
+__global__ void k_standardise(int rows, int width, const float* __restrict__ mean, const float* __restrict__ sd,
+                              float* __restrict__ x) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * width) return;
+  int c = i % width;
+  x[i] = (x[i] - mean[c]) / sd[c];
+}
+
+__global__ void k_unstandardise(int rows, int width, const float* __restrict__ mean, const float* __restrict__ sd,
+                                float* __restrict__ y) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * width) return;
+  int c = i % width;
+  y[i] = mean[c] + sd[c] * y[i];
+}
+
 void gemm(int M, int N, int K, const float* A, int lda, int ta, const float* B, int ldb, int tb, float* C, int ldc,
           const float* bias, int relu, cudaStream_t s) {
   dim3 grid((N + 63) / 64, (M + 63) / 64);
@@ -460,6 +488,13 @@ void Learned::setup(Model* model, const unsigned char* bc_mask, int num_sub, uin
     b->zero(s);
   }
   params_bf16.alloc((size_t)F * H + (size_t)H * H + (size_t)H * NM);
+  {
+    std::vector<float> zf(F, 0.f), of(F, 1.f), zt(NM, 0.f), ot(NM, 1.f);
+    x_mean.upload(zf, s);
+    x_std.upload(of, s);
+    t_mean.upload(zt, s);
+    t_std.upload(ot, s);
+  }
   max_batch = std::max(S, 1024);
   for (auto* b : {&X, &dY1}) b->alloc((size_t)max_batch * std::max(F, H));
   for (auto* b : {&Y1, &Y2, &dY2}) b->alloc((size_t)max_batch * H);
@@ -611,6 +646,36 @@ float Learned::train_step(const float* Xb, const float* Tb, int rows, float lr, 
 void Learned::train(long long steps, int batch, float lr, uint64_t seed, float* loss_hist, cudaStream_t s) {
   HOEFEM_REQUIRE(n_data > 0, HOEFEM_ERR_INVALID_ARGUMENT, "no training pairs collected");
   HOEFEM_REQUIRE(batch > 0 && batch <= max_batch, HOEFEM_ERR_INVALID_ARGUMENT, "bad batch size");
+  // column statistics of the training set (FP64 sums on the host)
+  {
+    std::vector<float> hx((size_t)n_data * F), ht((size_t)n_data * NM);
+    HOEFEM_CUDA(cudaMemcpyAsync(hx.data(), data_X.p, sizeof(float) * hx.size(), cudaMemcpyDeviceToHost, s));
+    HOEFEM_CUDA(cudaMemcpyAsync(ht.data(), data_T.p, sizeof(float) * ht.size(), cudaMemcpyDeviceToHost, s));
+    HOEFEM_CUDA(cudaStreamSynchronize(s));
+    auto stats = [&](const std::vector<float>& d, int w, DBuf<float>& mean, DBuf<float>& sd) {
+      std::vector<double> s1(w, 0.0), s2(w, 0.0);
+      for (long long r = 0; r < n_data; ++r)
+        for (int c = 0; c < w; ++c) {
+          double v = d[(size_t)r * w + c];
+          s1[c] += v;
+          s2[c] += v * v;
+        }
+      std::vector<float> mu(w), sg(w);
+      double smax = 0.0;
+      std::vector<double> sdv(w);
+      for (int c = 0; c < w; ++c) {
+        double mc = s1[c] / n_data;
+        sdv[c] = std::sqrt(std::max(s2[c] / n_data - mc * mc, 0.0));
+        smax = std::max(smax, sdv[c]);
+        mu[c] = (float)mc;
+      }
+      for (int c = 0; c < w; ++c) sg[c] = (float)std::max({sdv[c], 1e-6 * smax, 1e-30});
+      mean.upload(mu, s);
+      sd.upload(sg, s);
+    };
+    stats(hx, F, x_mean, x_std);
+    stats(ht, NM, t_mean, t_std);
+  }
   std::mt19937_64 rng(seed);
   std::uniform_int_distribution<long long> pick(0, n_data - 1);
   std::vector<long long> idx(batch);
@@ -619,8 +684,10 @@ void Learned::train(long long steps, int batch, float lr, uint64_t seed, float* 
   for (long long k = 0; k < steps; ++k) {
     for (auto& v : idx) v = pick(rng);
     HOEFEM_CUDA(cudaMemcpyAsync(d_idx.p, idx.data(), sizeof(long long) * batch, cudaMemcpyHostToDevice, s));
-    (note_launch(), k_gather_rows<<<(batch * F + 255) / 256, 256, 0, s>>>(batch, F, d_idx.p, data_X.p, X.p));
-    (note_launch(), k_gather_rows<<<(batch * NM + 255) / 256, 256, 0, s>>>(batch, NM, d_idx.p, data_T.p, T.p));
+    (note_launch(), k_gather_rows_std<<<(batch * F + 255) / 256, 256, 0, s>>>(batch, F, d_idx.p, data_X.p, x_mean.p,
+                                                                              x_std.p, X.p));
+    (note_launch(), k_gather_rows_std<<<(batch * NM + 255) / 256, 256, 0, s>>>(batch, NM, d_idx.p, data_T.p,
+                                                                               t_mean.p, t_std.p, T.p));
     float l = train_step(X.p, T.p, batch, lr, s);
     if (loss_hist) loss_hist[k] = l;
   }
@@ -635,7 +702,9 @@ void Learned::predict(const double* r, double* x0, cudaStream_t s) {
     HOEFEM_CUDA(cudaMemsetAsync(x0, 0, sizeof(double) * m->ndof, s));
     return;
   }
+  (note_launch(), k_standardise<<<(S * F + 255) / 256, 256, 0, s>>>(S, F, x_mean.p, x_std.p, X.p));
   forward(X.p, S, use_bf16 != 0, s);
+  (note_launch(), k_unstandardise<<<(S * NM + 255) / 256, 256, 0, s>>>(S, NM, t_mean.p, t_std.p, Y3.p));
   HOEFEM_CUDA(cudaMemsetAsync(x0, 0, sizeof(double) * m->ndof, s));
   apply(Y3.p, rn, x0, s);
 }

@@ -27,6 +27,10 @@ struct Learned {
   // MLP (FP32 master weights, Adam moments); layout: W1 F x H, b1 H, W2 H x H, b2 H, W3 H x NM, b3 NM
   size_t n_params = 0;
   DBuf<float> params, grads, adam_m, adam_v;
+  // per-column standardisation of features and targets (statistics of the
+  // training set at the last train() call); the network works on standardised
+  // values, predictions are mapped back with t_mean + t_std * y
+  DBuf<float> x_mean, x_std, t_mean, t_std;
   DBuf<uint16_t> params_bf16;   // BF16 copies of W1, W2, W3 for tensor-core inference
   int adam_t = 0;
   // activations (batch up to max_batch rows)

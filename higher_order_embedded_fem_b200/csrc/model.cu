@@ -45,6 +45,7 @@ NodeRows Model::rows() const {
   r.diag_slot = d_diag_slot.p;
   r.diag_only = nullptr;
   r.lanes = spmv_lanes;
+  r.sched = d_sched.p;
   return r;
 }
 
@@ -139,7 +140,7 @@ static void build_emap(const Block& blk, const std::vector<int>& adj_off, const 
       for (int J = 0; J < nn; ++J) {
         const int* it = std::lower_bound(b0, b1, (int)c[J]);
         HOEFEM_REQUIRE(it != b1 && *it == (int)c[J], HOEFEM_ERR_PATTERN, "element node missing from pattern");
-        emap[(size_t)e * nn * nn + I * nn + J] = (int)(base[a] + 3 * (it - b0));
+        emap[(size_t)e * nn * nn + I * nn + J] = (int)(3 * (it - b0));
       }
     }
   }
@@ -179,7 +180,7 @@ void finalize_model(Model& m) {
   }
   m.ndof = 3 * m.nv;
   m.nnz = m.base[m.nv];
-  HOEFEM_REQUIRE(m.nnz < (i64)2147483647, HOEFEM_ERR_INVALID_ARGUMENT, "pattern exceeds 2^31 non-zeros");
+  HOEFEM_REQUIRE(3 * m.nv < (i64)2147483647, HOEFEM_ERR_INVALID_ARGUMENT, "more than 2^31 DOFs");
 
   for (Block* b : m.blocks) greedy_coloring(b->conn.data(), b->ne, b->nn, m.nv, b->color_off, b->color_elems);
   m.finalized = true;
@@ -203,6 +204,8 @@ void ensure_device(Model& m) {
   m.d_diag_slot.upload(m.diag_slot, s);
   m.d_base.upload(m.base, s);
   m.d_err.alloc(1);
+  m.d_sched.alloc(2);
+  m.d_sched.zero(s);
   m.d_err.zero(s);
   for (Block* b : m.blocks) {
     std::vector<int> soa((size_t)b->ne * b->nn);

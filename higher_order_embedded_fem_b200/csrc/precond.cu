@@ -7,13 +7,18 @@
 // 134-216,250-342, newton_cg.rs:297-370).
 //
 // Schwarz update on the device, in three steps:
-//  1. k_schwarz_factor: one CTA per subdomain gathers its 3n x 3n principal
-//     block of the system matrix (element-to-nnz map, no searches), runs a
-//     parallel cyclic Jacobi eigensolver in shared memory (round-robin
-//     ordering: m/2 disjoint rotations per round, rows then columns), applies
-//     the reference's spectrum rule (1/|lambda|, floor 1e-12 max|lambda|) and
-//     writes the recomposed block V f(L) V^T to a staging buffer.  All
-//     subdomains are factored in one launch.
+//  1. k_schwarz_gj: one CTA per subdomain gathers its 3n x 3n principal block
+//     of the system matrix (element-to-nnz map, no searches) into registers
+//     (16 x 16 threads, each a T x T tile) and inverts it by Gauss-Jordan
+//     elimination without pivoting.  For a symmetric block every pivot is
+//     positive exactly when the block is positive definite; with
+//     ||A||_F ||A^-1||_F <= 1e12 (so lambda_min >= 1e-12 lambda_max) the
+//     reference's spectrum rule is the plain inverse, which is written to a
+//     staging buffer.  Blocks that fail either test are listed for
+//     k_schwarz_factor: a parallel cyclic Jacobi eigensolver in shared memory
+//     (round-robin ordering: m/2 disjoint rotations per round, rows then
+//     columns) that applies the spectrum rule (1/|lambda|, floor
+//     1e-12 max|lambda|) and writes the recomposed block V f(L) V^T.
 //  2. k_schwarz_scatter: per subdomain color (greedy coloring of the subdomain
 //     node lists, as the reference), the staged blocks are added into the
 //     preconditioner's own CSR values, so every entry receives its
@@ -46,6 +51,7 @@ NodeRows Precond::rows() const {
   r.diag_slot = d_diag_slot.p;
   r.diag_only = d_diag_only.p;
   r.lanes = spmv_lanes;
+  r.sched = d_sched.p;
   return r;
 }
 
@@ -62,12 +68,142 @@ __device__ __forceinline__ void jacobi_cs(double app, double aqq, double apq, do
   s = t * c;
 }
 
-__global__ void __launch_bounds__(FACTOR_TPB) k_schwarz_factor(
-    int nsub, const int* __restrict__ sub_off, const int* __restrict__ sub_nodes, const long long* __restrict__ gmap_off,
-    const int* __restrict__ gmap, const int* __restrict__ adj_off, const double* __restrict__ J,
-    const long long* __restrict__ stage_off, double* __restrict__ stage, int* err) {
-  extern __shared__ double smem[];
+// Gauss-Jordan inversion of one SPD principal block per CTA, matrix in
+// registers: thread (ty, tx) owns rows ty + 16 ii and columns tx + 16 jj
+// (ii, jj < T), padding (index >= dim) is the identity.  Step k broadcasts
+// pivot row and column through shared memory (double-buffered: one barrier
+// per step).  Blocks with a non-positive pivot or a failed condition
+// certificate go to the fallback list.
+template <int T>
+__global__ void __launch_bounds__(256, 2) k_schwarz_gj(
+    int nsub, const int* __restrict__ sub_off, const int* __restrict__ sub_nodes,
+    const long long* __restrict__ gmap_off, const int* __restrict__ gmap, const int* __restrict__ adj_off, const long long* __restrict__ jbase,
+    const double* __restrict__ J, const long long* __restrict__ stage_off, double* __restrict__ stage,
+    int* __restrict__ fallback) {
+  constexpr int M = 16 * T;
+  __shared__ double s_row[2][M], s_col[2][M];
+  __shared__ int s_g[27], s_rl[27];
+  __shared__ long long s_jb[27];
+  __shared__ double s_red;
   const int sidx = blockIdx.x;
+  const int n = sub_off[sidx + 1] - sub_off[sidx];
+  const int dim = 3 * n;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int* nodes = sub_nodes + sub_off[sidx];
+  if (threadIdx.x < n) {
+    int g = nodes[threadIdx.x];
+    s_g[threadIdx.x] = g;
+    s_rl[threadIdx.x] = 3 * (adj_off[g + 1] - adj_off[g]);
+    s_jb[threadIdx.x] = jbase[g];
+  }
+  __syncthreads();
+  const int* gm = gmap + gmap_off[sidx];
+  double a[T][T];
+  double fa = 0.0;
+#pragma unroll
+  for (int ii = 0; ii < T; ++ii) {
+    const int r = ty + 16 * ii;
+#pragma unroll
+    for (int jj = 0; jj < T; ++jj) {
+      const int c = tx + 16 * jj;
+      double v = (r == c) ? 1.0 : 0.0;
+      if (r < dim && c < dim) {
+        const int I = r / 3, i = r - 3 * I, Jn = c / 3, j = c - 3 * Jn;
+        v = J[s_jb[I] + gm[I * n + Jn] + i * s_rl[I] + j];
+        fa += v * v;
+      }
+      a[ii][jj] = v;
+    }
+  }
+  double v1[1] = {fa};
+  block_sum<1>(v1);
+  if (threadIdx.x == 0) s_red = sqrt(v1[0]);
+  bool ok = true;
+  for (int k = 0; k < dim; ++k) {
+    const int buf = k & 1;
+    const int kq = k >> 4, kr = k & 15;
+    if (ty == kr) {
+#pragma unroll
+      for (int ii = 0; ii < T; ++ii)
+        if (ii == kq) {
+#pragma unroll
+          for (int jj = 0; jj < T; ++jj) s_row[buf][tx + 16 * jj] = a[ii][jj];
+        }
+    }
+    if (tx == kr) {
+#pragma unroll
+      for (int jj = 0; jj < T; ++jj)
+        if (jj == kq) {
+#pragma unroll
+          for (int ii = 0; ii < T; ++ii) s_col[buf][ty + 16 * ii] = a[ii][jj];
+        }
+    }
+    __syncthreads();
+    const double piv = s_row[buf][k];
+    if (!(piv > 0.0) || !isfinite(piv)) {
+      ok = false;
+      break;
+    }
+    const double inv = 1.0 / piv;
+    double rj[T], ci[T];
+#pragma unroll
+    for (int jj = 0; jj < T; ++jj) rj[jj] = s_row[buf][tx + 16 * jj] * inv;
+#pragma unroll
+    for (int ii = 0; ii < T; ++ii) ci[ii] = s_col[buf][ty + 16 * ii];
+#pragma unroll
+    for (int ii = 0; ii < T; ++ii) {
+      const bool rowk = (ii == kq) && (ty == kr);
+#pragma unroll
+      for (int jj = 0; jj < T; ++jj) {
+        const bool colk = (jj == kq) && (tx == kr);
+        double v = a[ii][jj] - ci[ii] * rj[jj];
+        if (rowk) v = colk ? inv : rj[jj];
+        else if (colk) v = -ci[ii] * inv;
+        a[ii][jj] = v;
+      }
+    }
+  }
+  double fi = 0.0;
+  if (ok) {
+#pragma unroll
+    for (int ii = 0; ii < T; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < T; ++jj) {
+        const int r = ty + 16 * ii, c = tx + 16 * jj;
+        if (r < dim && c < dim) fi += a[ii][jj] * a[ii][jj];
+      }
+  }
+  double v2[1] = {fi};
+  block_sum<1>(v2);  // uniform: `ok` is the same in every thread
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    const double cond = s_red * sqrt(v2[0]);
+    s_ok = ok && (cond <= 1e12) && isfinite(cond);
+    if (!s_ok) {
+      const int slot = atomicAdd(fallback, 1);
+      fallback[1 + slot] = sidx;
+    }
+  }
+  __syncthreads();
+  if (!s_ok) return;
+  double* out = stage + stage_off[sidx];
+#pragma unroll
+  for (int ii = 0; ii < T; ++ii)
+#pragma unroll
+    for (int jj = 0; jj < T; ++jj) {
+      const int r = ty + 16 * ii, c = tx + 16 * jj;
+      if (r < dim && c < dim) out[r * dim + c] = a[ii][jj];
+    }
+}
+
+// Eigen path for the blocks listed by k_schwarz_gj (count in fallback[0]).
+__global__ void __launch_bounds__(FACTOR_TPB) k_schwarz_factor(
+    const int* __restrict__ fallback, const int* __restrict__ sub_off, const int* __restrict__ sub_nodes,
+    const long long* __restrict__ gmap_off, const int* __restrict__ gmap, const int* __restrict__ adj_off, const long long* __restrict__ jbase,
+    const double* __restrict__ J, const long long* __restrict__ stage_off, double* __restrict__ stage, int* err) {
+  if ((int)blockIdx.x >= fallback[0]) return;
+  extern __shared__ double smem[];
+  const int sidx = fallback[1 + blockIdx.x];
   const int n = sub_off[sidx + 1] - sub_off[sidx];
   const int dim = 3 * n;
   const int m = (dim + 1) & ~1;  // even, padded with a dummy index
@@ -75,111 +211,32 @@ __global__ void __launch_bounds__(FACTOR_TPB) k_schwarz_factor(
   double* V = A + m * m;         // m x m
   double* cs = V + m * m;        // m/2 cosines
   double* sn = cs + m / 2;       // m/2 sines
-  double* colk = cs;             // Cholesky: current column (m entries, aliases cs / sn)
   __shared__ int s_g[27];
   __shared__ int s_rl[27];
+  __shared__ long long s_jb[27];
   __shared__ double s_red[2];
   const int* nodes = sub_nodes + sub_off[sidx];
   for (int I = threadIdx.x; I < n; I += blockDim.x) {
     int g = nodes[I];
     s_g[I] = g;
     s_rl[I] = 3 * (adj_off[g + 1] - adj_off[g]);
+    s_jb[I] = jbase[g];
   }
   __syncthreads();
   // gather the principal block
   const int* gm = gmap + gmap_off[sidx];
-  auto gather = [&]() {
-    for (int k = threadIdx.x; k < m * m; k += blockDim.x) {
-      int r = k / m, c = k % m;
-      double v = 0.0;
-      if (r < dim && c < dim) {
-        int I = r / 3, i = r % 3, Jn = c / 3, j = c % 3;
-        v = J[gm[I * n + Jn] + i * s_rl[I] + j];
-      }
-      A[k] = v;
-      V[k] = (r == c) ? 1.0 : 0.0;
+  for (int k = threadIdx.x; k < m * m; k += blockDim.x) {
+    int r = k / m, c = k % m;
+    double v = 0.0;
+    if (r < dim && c < dim) {
+      int I = r / 3, i = r % 3, Jn = c / 3, j = c % 3;
+      v = J[s_jb[I] + gm[I * n + Jn] + i * s_rl[I] + j];
     }
-    __syncthreads();
-  };
-  gather();
-  double* out = stage + stage_off[sidx];
-
-  // ---- fast path --------------------------------------------------------------
-  // For a symmetric positive definite block with lambda_min >= 1e-12 lambda_max
-  // the spectrum rule below is the identity on the eigenvalues' reciprocals,
-  // i.e. the block's inverse.  lambda_max <= ||A||_F and lambda_min >=
-  // 1 / ||A^-1||_F, so ||A||_F ||A^-1||_F <= 1e12 certifies that case; the
-  // inverse then comes from a Cholesky factorisation (1/20 of the Jacobi work).
-  // Any failed pivot or a failed certificate falls through to Jacobi.
-  __shared__ int s_ok;
-  {
-    double fa = 0.0;
-    for (int k = threadIdx.x; k < m * m; k += blockDim.x) fa += A[k] * A[k];
-    double v1[1] = {fa};
-    block_sum<1>(v1);
-    if (threadIdx.x == 0) { s_red[0] = sqrt(v1[0]); s_ok = 1; }
-    __syncthreads();
-    for (int k = 0; k < dim; ++k) {
-      if (threadIdx.x == 0) {
-        double d = A[k * m + k];
-        if (!(d > 0.0) || !isfinite(d)) s_ok = 0;
-        else A[k * m + k] = sqrt(d);
-      }
-      __syncthreads();
-      if (!s_ok) break;
-      const double lkk = A[k * m + k];
-      // column k below the diagonal, also copied to a contiguous array so the
-      // trailing update reads it without bank conflicts
-      for (int i = k + 1 + threadIdx.x; i < dim; i += blockDim.x) {
-        double l = A[i * m + k] / lkk;
-        A[i * m + k] = l;
-        colk[i] = l;
-      }
-      __syncthreads();
-      const int rem = dim - k - 1;
-      for (int t = threadIdx.x; t < rem * rem; t += blockDim.x) {
-        int i = k + 1 + t / rem, j = k + 1 + t % rem;
-        if (j <= i) A[i * m + j] -= colk[i] * colk[j];
-      }
-      __syncthreads();
-    }
-    if (s_ok) {
-      // column j of A^-1: L y = e_j, then L^T x = y (in V)
-      for (int j = threadIdx.x; j < dim; j += blockDim.x) {
-        for (int i = 0; i < dim; ++i) {
-          double sacc = (i == j) ? 1.0 : 0.0;
-          for (int k = j; k < i; ++k) sacc -= A[i * m + k] * V[k * m + j];
-          V[i * m + j] = (i < j) ? 0.0 : sacc / A[i * m + i];
-        }
-        for (int i = dim - 1; i >= 0; --i) {
-          double sacc = V[i * m + j];
-          for (int k = i + 1; k < dim; ++k) sacc -= A[k * m + i] * V[k * m + j];
-          V[i * m + j] = sacc / A[i * m + i];
-        }
-      }
-      __syncthreads();
-      double fi = 0.0;
-      for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) {
-        double x = V[(k / dim) * m + k % dim];
-        fi += x * x;
-      }
-      double v2[1] = {fi};
-      block_sum<1>(v2);
-      if (threadIdx.x == 0) {
-        double cond = s_red[0] * sqrt(v2[0]);
-        if (!(cond <= 1e12) || !isfinite(cond)) s_ok = 0;
-      }
-      __syncthreads();
-      if (s_ok) {
-        for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) {
-          int i = k / dim, j = k % dim;
-          out[k] = 0.5 * (V[i * m + j] + V[j * m + i]);
-        }
-        return;
-      }
-    }
-    gather();
+    A[k] = v;
+    V[k] = (r == c) ? 1.0 : 0.0;
   }
+  __syncthreads();
+  double* out = stage + stage_off[sidx];
 
   // ---- general path: cyclic Jacobi eigen-decomposition -------------------------
   const int half = m / 2;
@@ -289,12 +346,14 @@ __global__ void __launch_bounds__(256) k_schwarz_scatter(const int* __restrict__
   const int* nodes = sub_nodes + sub_off[sidx];
   const int* sm = smap + gmap_off[sidx];
   const double* blk = stage + stage_off[sidx];
+  // symmetric part of the staged block (the Gauss-Jordan inverse is symmetric
+  // only up to rounding; the eigen path's recomposition is symmetric exactly)
   for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) {
     int r = k / dim, c = k % dim;
     int I = r / 3, i = r % 3, Jn = c / 3, j = c % 3;
     int g = nodes[I];
     int rl = 3 * (padj_off[g + 1] - padj_off[g]);
-    pv[sm[I * n + Jn] + i * rl + j] += blk[k];
+    pv[sm[I * n + Jn] + i * rl + j] += 0.5 * (blk[k] + blk[c * dim + r]);
   }
 }
 
@@ -337,11 +396,12 @@ __global__ void k_mul(int n, const double* __restrict__ d, const double* __restr
 template <int L>
 __global__ void k_spmv_plain(NodeRows A, const double* __restrict__ vals, const double* __restrict__ x,
                              double* __restrict__ y) {
-  for_each_node<L>(A.nv, [&](int a, int sl) {
+  for_each_node<L>(A, [&](int a, int sl) {
     double s0, s1, s2;
     node_row_dot<L>(A, vals, x, a, sl, s0, s1, s2);
     if (a >= 0 && sl == 0) { y[3 * a] = s0; y[3 * a + 1] = s1; y[3 * a + 2] = s2; }
   });
+  node_sched_finish(A);
 }
 
 }  // namespace
@@ -394,6 +454,7 @@ void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes
     if (it != e0 && *it == a) p.diag_slot[a] = (int)(it - b0);
   }
   p.nnz = p.base[m.nv];
+  HOEFEM_REQUIRE(p.nnz < (i64)2147483647, HOEFEM_ERR_INVALID_ARGUMENT, "Schwarz pattern exceeds 2^31 non-zeros");
   // gather map (system pattern) and scatter map (preconditioner pattern)
   std::vector<long long> gmap_off(nsub + 1, 0), stage_off(nsub + 1, 0);
   for (i64 s = 0; s < nsub; ++s) {
@@ -412,7 +473,7 @@ void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes
         const int* m1 = m.adj.data() + m.adj_off[a + 1];
         const int* it = std::lower_bound(m0, m1, (int)b);
         HOEFEM_REQUIRE(it != m1 && *it == b, HOEFEM_ERR_PATTERN, "subdomain block not in the system pattern");
-        gmap[gmap_off[s] + I * n + J] = (int)(m.base[a] + 3 * (it - m0));
+        gmap[gmap_off[s] + I * n + J] = (int)(3 * (it - m0));
         const int* p0 = p.adj.data() + p.adj_off[a];
         const int* p1 = p.adj.data() + p.adj_off[a + 1];
         const int* jt = std::lower_bound(p0, p1, (int)b);
@@ -451,6 +512,9 @@ void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes
   p.vals.zero(st);
   p.staging.alloc(stage_off[nsub]);
   p.d_err.alloc(1);
+  p.d_fallback.alloc(1 + nsub);
+  p.d_sched.alloc(2);
+  p.d_sched.zero(st);
   p.d_err.zero(st);
   HOEFEM_CUDA(cudaStreamSynchronize(st));
   int m_max = (3 * p.max_nodes + 1) & ~1;
@@ -484,11 +548,23 @@ void precond_update(Precond& p, const double* J, cudaStream_t s) {
   }
   p.vals.zero(s);
   if (p.nsub > 0) {
-    int m_max = (3 * p.max_nodes + 1) & ~1;
+    HOEFEM_CUDA(cudaMemsetAsync(p.d_fallback.p, 0, sizeof(int), s));
+    const int dmax = 3 * p.max_nodes;
+#define HOEFEM_GJ(TT)                                                                                               \
+  (note_launch(), k_schwarz_gj<TT><<<(int)p.nsub, 256, 0, s>>>((int)p.nsub, p.d_sub_off.p, p.d_sub_nodes.p,         \
+                                                               p.d_gmap_off.p, p.d_gmap.p, m.d_adj_off.p, m.d_base.p, J,\
+                                                               p.d_stage_off.p, p.staging.p, p.d_fallback.p))
+    if (dmax <= 32) HOEFEM_GJ(2);
+    else if (dmax <= 48) HOEFEM_GJ(3);
+    else if (dmax <= 64) HOEFEM_GJ(4);
+    else HOEFEM_GJ(6);
+#undef HOEFEM_GJ
+    int m_max = (dmax + 1) & ~1;
     size_t smem = (size_t)(2 * m_max * m_max + m_max) * sizeof(double);
-    (note_launch(), k_schwarz_factor<<<(int)p.nsub, FACTOR_TPB, smem, s>>>((int)p.nsub, p.d_sub_off.p, p.d_sub_nodes.p,
-                                                           p.d_gmap_off.p, p.d_gmap.p, m.d_adj_off.p, J,
-                                                           p.d_stage_off.p, p.staging.p, p.d_err.p));
+    (note_launch(), k_schwarz_factor<<<(int)p.nsub, FACTOR_TPB, smem, s>>>(p.d_fallback.p, p.d_sub_off.p,
+                                                                           p.d_sub_nodes.p, p.d_gmap_off.p, p.d_gmap.p,
+                                                                           m.d_adj_off.p, m.d_base.p, J, p.d_stage_off.p,
+                                                                           p.staging.p, p.d_err.p));
     HOEFEM_CUDA(cudaGetLastError());
     const int nc = (int)p.color_off.size() - 1;
     for (int c = 0; c < nc; ++c) {

@@ -31,6 +31,8 @@ struct Precond {
   bool want_fp32 = false;
   DBuf<long long> d_stage_off;
   DBuf<int> d_err;
+  DBuf<int> d_fallback;
+  DBuf<unsigned> d_sched;  // SpMV dynamic-scheduling counters of the Schwarz pattern  // [0]: count, [1..]: subdomains for the eigen path
   i64 nnz = 0;
   int spmv_lanes = 32;
   NodeRows rows() const;
@@ -54,7 +56,6 @@ struct CgWork {
   DBuf<CgState> st;
   DBuf<unsigned> counter;
   CgState* h_st = nullptr;  // pinned
-  DBuf<double> xo, bo, ro;  // iterative refinement: solution, rhs, FP64 residual
   struct Graph {
     const void* key[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaGraphExec_t exec = nullptr;
@@ -72,8 +73,8 @@ struct CgWork {
 // pattern values `vals`.  Returns HOEFEM_OK or a HOEFEM_CG_* status.
 int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 max_iter, i64* iters, cudaStream_t s);
 // FP64 iterative refinement around an FP32-operator / FP32-preconditioner PCG.
-int cg_solve_ir(CgWork& w, const double* A64, const float* A32, const Precond* P, double tol, i64 max_iter,
-                double inner_tol, i64* iters, i64* outer, cudaStream_t s);
+int cg_solve_reliable(CgWork& w, const double* A64, const float* A32, const Precond* P, double tol, i64 max_iter,
+                      double delta, i64* iters, i64* replacements, cudaStream_t s);
 void to_f32(const double* a, float* b, long long n, cudaStream_t s);
 
 }  // namespace hoefem

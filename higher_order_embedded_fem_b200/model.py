@@ -69,6 +69,10 @@ class _Model:
         check(lib().hoefem_model_autotune(self._h, C.byref(lanes)))
         return lanes.value
 
+    def set_spmv_variant(self, variant):
+        """8 / 16 / 32 lanes per node, +100 for the column-streaming traversal."""
+        check(lib().hoefem_model_set_spmv_variant(self._h, int(variant)))
+
     def set_stream(self, stream):
         """Run this model's work on a CUDA stream handle (int), None: own stream."""
         check(lib().hoefem_model_set_stream(self._h, stream))

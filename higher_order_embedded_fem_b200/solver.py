@@ -159,13 +159,15 @@ class ConjugateGradient:
         self.max_iter = int(n)
         return self
 
-    def solve_with_guess_mixed(self, b, x, inner_tol=1e-2):
-        """FP64 iterative refinement around an FP32-operator PCG."""
+    def solve_with_guess_mixed(self, b, x, delta=0.1):
+        """PCG with FP32 operator / preconditioner values and FP64 vectors;
+        the residual is replaced by the true FP64 residual whenever it has
+        dropped by `delta` (reliable updates) and before stopping."""
         it = C.c_int64()
         mem = _same_space(self.values, b, x)
         st = lib().hoefem_cg_solve_mixed(self.model._h, ptr(self.values)[0],
                                          self.preconditioner._h if self.preconditioner is not None else None,
-                                         ptr(b)[0], ptr(x)[0], self.criterion.tol, self.max_iter, float(inner_tol),
+                                         ptr(b)[0], ptr(x)[0], self.criterion.tol, self.max_iter, float(delta),
                                          C.byref(it), mem)
         if st in _CG_KIND:
             raise SolveError(_CG_KIND[st], CgOutput(it.value))
@@ -214,16 +216,18 @@ class NewtonCgIntegrator3d:
         check(lib().hoefem_integrator_set_tolerances(self._h, cg_tol, cg_max_iter, newton_max_iter))
 
     def set_learned(self, learned, mode=1):
-        """mode 1: guarded learned warm start; 2: collect training pairs from
-        this integrator's plain CG solves; 0 / learned=None: off."""
+        """mode 1: guarded learned warm start; 2: collect (b, x*) training pairs
+        from this integrator's plain FP64 CG solves; 3: as 2 plus the CG
+        iterates (r_k, x* - x_k); 0 / learned=None: off."""
         self._learned = learned
         check(lib().hoefem_integrator_set_learned(self._h, learned._h if learned is not None else None,
                                                   int(mode) if learned is not None else 0))
 
-    def set_precision(self, mixed, inner_tol=1e-2):
-        """mixed=True: FP32 element stiffness / operator / Schwarz apply inside
-        FP64 iterative refinement (see hoefem_integrator_set_precision)."""
-        check(lib().hoefem_integrator_set_precision(self._h, 1 if mixed else 0, float(inner_tol)))
+    def set_precision(self, mixed, delta=0.1):
+        """mixed=True: FP32 element stiffness, FP32 operator / Schwarz apply in
+        a reliable-update PCG with FP64 vectors (see
+        hoefem_integrator_set_precision)."""
+        check(lib().hoefem_integrator_set_precision(self._h, 1 if mixed else 0, float(delta)))
 
     def step(self, u, v, t, dt):
         """Advances (u, v) in place by dt; returns the step statistics."""

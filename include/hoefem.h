@@ -125,6 +125,10 @@ int hoefem_model_set_stream(hoefem_model m, void* stream);
    model's pattern (8, 16 or 32; the integrator does this at creation) and
    returns the choice.  No counterpart in the reference. */
 int hoefem_model_autotune(hoefem_model m, int32_t* lanes);
+/* Selects the SpMV variant explicitly: lanes per node 8, 16 or 32
+   (neighbour-major), or 108, 116, 132 (the same lane counts, column-streaming
+   traversal).  hoefem_model_autotune picks the fastest of these. */
+int hoefem_model_set_spmv_variant(hoefem_model m, int32_t variant);
 int hoefem_model_sizes(hoefem_model m, int64_t* ndof, int64_t* nnz, int64_t* num_elements, int64_t* num_blocks);
 /* row_offsets: ndof+1, column_indices: nnz (SparsityPattern, sparse.rs:297-410) */
 int hoefem_model_pattern(hoefem_model m, int64_t* row_offsets, int64_t* column_indices);
@@ -161,6 +165,7 @@ int hoefem_apply_dirichlet_bc_csr(hoefem_model m, const int64_t* nodes, int64_t 
 int hoefem_jacobian_combination(hoefem_model m, double c_stiffness, const double* stiffness_values, double c_mass,
                                 const double* mass_values, const int64_t* bc_nodes, int64_t num_bc, double* out,
                                 int mem);
+
 /* spmv_csr (fenris/src/sparse.rs:1164-1199) / LinearOperator::apply for the
    model pattern (cg.rs:15-17): y = beta*y + alpha*A x. */
 int hoefem_spmv(hoefem_model m, double beta, double* y, double alpha, const double* values, const double* x, int mem);
@@ -198,12 +203,15 @@ int hoefem_precond_destroy(hoefem_precond p);
 int hoefem_cg_solve(hoefem_model m, const double* system_values, hoefem_precond p, const double* b, double* x,
                     double tol, int64_t max_iter, int64_t* iterations, int mem);
 
-/* Mixed-precision variant of hoefem_cg_solve: FP64 iterative refinement
-   around a PCG with FP32 operator values (converted from system_values) and,
-   for a Schwarz preconditioner, FP32 preconditioner values.  *iterations is
-   the total number of inner iterations.  No counterpart in the reference. */
+/* Mixed-precision variant of hoefem_cg_solve: PCG with FP32 operator values
+   (converted from system_values) and, for a Schwarz preconditioner, FP32
+   preconditioner values; vectors, dot products and residual updates FP64.
+   The recurrence residual is replaced by the true FP64 residual b - A x
+   (reliable update) whenever it has dropped by the factor `delta` (0 < delta
+   < 1, e.g. 0.1) since the last replacement, and before the solve stops, so
+   ||b - A x|| <= tol ||b|| holds in FP64.  No counterpart in the reference. */
 int hoefem_cg_solve_mixed(hoefem_model m, const double* system_values, hoefem_precond p, const double* b, double* x,
-                          double tol, int64_t max_iter, double inner_tol, int64_t* iterations, int mem);
+                          double tol, int64_t max_iter, double delta, int64_t* iterations, int mem);
 
 /* ------------------------------------------------------------------------ */
 /* NewtonCgIntegrator3d (simulation_toolbox/src/fem/newton_cg.rs:43-295):
@@ -249,14 +257,13 @@ int hoefem_integrator_set_tolerances(hoefem_integrator it, double cg_tol, int64_
 /* Arithmetic of the step.  HOEFEM_PRECISION_FP64: the reference's FP64
    everywhere.  HOEFEM_PRECISION_MIXED: element stiffness arithmetic in FP32
    (CSR accumulation FP64), Schwarz blocks built in FP64 and applied in FP32,
-   and the Jacobian solve as FP64 iterative refinement (true FP64 residual,
-   stop at ||r|| <= cg_tol ||b||) around an inner PCG with FP32 operator /
-   preconditioner values and FP64 vectors, each inner solve run to the
-   relative tolerance max(inner_tol, what the outer target still needs).
-   Forces, the Newton residual and the line search stay FP64.  No counterpart
-   in the reference (an addition on top of its FP64 path). */
+   and the Jacobian solve as hoefem_cg_solve_mixed (FP32 operator /
+   preconditioner values, FP64 vectors, reliable updates with threshold
+   `delta`, stop at ||b - A x|| <= cg_tol ||b|| in FP64).  Forces, the Newton
+   residual and the line search stay FP64.  No counterpart in the reference
+   (an addition on top of its FP64 path). */
 typedef enum { HOEFEM_PRECISION_FP64 = 0, HOEFEM_PRECISION_MIXED = 1 } hoefem_precision;
-int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double inner_tol);
+int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double delta);
 /* One time step: u, v (ndof) updated in place. */
 int hoefem_integrator_step(hoefem_integrator it, double* u, double* v, double t, double dt, int mem);
 int hoefem_integrator_stats(hoefem_integrator it, hoefem_step_stats* out);
@@ -303,7 +310,8 @@ int hoefem_learned_set_weights(hoefem_learned l, const float* w);
 /* x0 = predicted correction of residual r. */
 int hoefem_learned_predict(hoefem_learned l, const double* r, double* x0, int mem);
 /* mode 0: off, 1: warm start with the guard, 2: collect training pairs from
-   the integrator's plain CG solves (every CG chunk's iterate). */
+   the integrator's plain FP64 CG solves (right-hand side b with the converged
+   solution), 3: as 2 plus every CG chunk's iterate (r_k, x* - x_k). */
 int hoefem_integrator_set_learned(hoefem_integrator it, hoefem_learned l, int mode);
 
 /* ------------------------------------------------------------------------ */

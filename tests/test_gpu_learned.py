@@ -49,7 +49,7 @@ def _integrator(e, m, mat, comp, mixed=False):
     P = comp.build(m)
     it = H.NewtonCgIntegrator3d(m, mat, 1000.0, e.nodes_below(2, 1e-9), preconditioner=P)
     it.set_tolerances(1e-6, 500, 100)
-    it.set_precision(mixed, 1e-2)
+    it.set_precision(mixed, 0.1)
     it._P = P
     return it
 

@@ -45,7 +45,7 @@ def test_mixed_cg_reaches_fp64_tolerance():
     x = np.zeros(m.ndof())
     out = (H.ConjugateGradient(m).with_operator(J).with_preconditioner(P)
            .with_stopping_criterion(H.RelativeResidualCriterion(1e-6)).with_max_iter(2000)
-           .solve_with_guess_mixed(b, x, 1e-2))
+           .solve_with_guess_mixed(b, x, 0.1))
     y = m.spmv(np.zeros(m.ndof()), J, x)
     assert np.linalg.norm(y - b) <= 1e-6 * np.linalg.norm(b)
     x64 = np.zeros(m.ndof())
@@ -63,7 +63,7 @@ def test_mixed_newton_step_matches_oracle():
     P = comp.build(m)
     integ = H.NewtonCgIntegrator3d(m, mat, 1000.0, bc, preconditioner=P)
     integ.set_tolerances(1e-6, 500, 100)
-    integ.set_precision(True, 1e-2)
+    integ.set_precision(True, 0.1)
     ref.set_bc(bc)
     ref.set_gravity(True)
     ref.set_schwarz(comp.schwarz_connectivity, comp.untreated_nodes)

@@ -116,6 +116,33 @@ def test_spmv_jacobian_dirichlet():
     assert np.array_equal(Kb, Kr)
 
 
+@pytest.mark.parametrize("variant", [8, 16, 32, 108, 116, 132])
+def test_spmv_variants_agree(variant):
+    # every SpMV traversal (also the ones inside CG) sums the same products
+    e, m, mat, ref = embedded_setup(6)
+    u = H.scenes.random_normal(1, m.ndof(), 0.01 * e.cell_size)
+    K = ref.stiffness(u)
+    x = H.scenes.random_normal(9, m.ndof(), 1.0)
+    ro, ci = m.pattern()
+    dense_y = np.array([np.dot(K[ro[r]:ro[r + 1]], x[ci[ro[r]:ro[r + 1]]]) for r in range(m.ndof())])
+    m.set_spmv_variant(variant)
+    assert rel(m.spmv(np.zeros(m.ndof()), K, x), dense_y) < 1e-13
+    bc = e.nodes_below(2, 1e-9)
+    ref.set_bc(bc)
+    ref.setup()
+    J = ref.jacobian(ref.stiffness(np.zeros(m.ndof())), 1e-3)  # SPD at rest
+    P = H.DiagonalPreconditioner(m)
+    P.update(J)
+    b = H.scenes.random_normal(6, m.ndof(), 1.0)
+    b[np.repeat(3 * bc, 3) + np.tile(np.arange(3), bc.size)] = 0.0
+    xs = np.zeros(m.ndof())
+    out = (H.ConjugateGradient(m).with_operator(J).with_preconditioner(P)
+           .with_stopping_criterion(H.RelativeResidualCriterion(1e-8)).with_max_iter(5000).solve_with_guess(b, xs))
+    st, xr, itr = ref.cg(J, b, 1e-8, 5000)
+    assert st == 0 and abs(out.num_iterations - itr) <= 1
+    assert rel(xs, xr) < 1e-6
+
+
 def test_diagonal_preconditioner_and_cg():
     s, m, mat, ref = tet10_setup(6)
     u = H.scenes.random_normal(1, m.ndof(), 0.01 * s.cell_size)
