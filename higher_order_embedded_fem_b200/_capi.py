@@ -84,6 +84,7 @@ SIGNATURES = {
     "hoefem_assemble_mass_into": (C.c_int, [vp, dbl, vp, C.c_int]),
     "hoefem_apply_dirichlet_bc_csr": (C.c_int, [vp, vp, i64, vp, C.c_int]),
     "hoefem_jacobian_combination": (C.c_int, [vp, dbl, vp, dbl, vp, vp, i64, vp, C.c_int]),
+    "hoefem_jacobian_combination_noalloc": (C.c_int, [vp, dbl, vp, dbl, vp, vp, i64, vp]),
     "hoefem_spmv": (C.c_int, [vp, dbl, vp, dbl, vp, vp, C.c_int]),
     "hoefem_precond_create_diagonal": (C.c_int, [vp, C.POINTER(vp)]),
     "hoefem_precond_create_schwarz": (C.c_int, [vp, vp, vp, i64, vp, i64, C.POINTER(vp)]),

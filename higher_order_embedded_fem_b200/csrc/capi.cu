@@ -26,6 +26,8 @@ int integrator_step(Integrator* it, double* ud, double* vd, double t, double dt)
 hoefem_step_stats integrator_stats(Integrator* it);
 const double* integrator_mass(Integrator* it);
 void integrator_eval_f(Integrator* it, const double* ud, const double* vd, double* f);
+void jacobian_combination_noalloc(Model& m, double ck, const double* K, double cm, const double* M,
+                                  const long long* bc_nodes, long long num_bc, double* out);
 struct Batch;
 Batch* batch_build(const std::vector<const Model*>& scenes, const std::vector<MatDev>& mats, double density,
                    const i64* bc_off, const i64* bc_nodes, bool gravity_enabled, double gravity);
@@ -397,6 +399,16 @@ int hoefem_jacobian_combination(hoefem_model m, double c_stiffness, const double
                        num_bc > 0 ? mask.p : nullptr, O.d, scratch.p, mm.stream);
   O.copy_out();
   sync(mm);
+  API_END
+}
+
+int hoefem_jacobian_combination_noalloc(hoefem_model m, double c_stiffness, const double* stiffness_values,
+                                        double c_mass, const double* mass_values, const int64_t* bc_nodes,
+                                        int64_t num_bc, double* out) {
+  API_BEGIN
+  Model& mm = model_of(m);
+  jacobian_combination_noalloc(mm, c_stiffness, stiffness_values, c_mass, mass_values,
+                               reinterpret_cast<const long long*>(bc_nodes), num_bc, out);
   API_END
 }
 

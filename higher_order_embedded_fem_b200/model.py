@@ -148,6 +148,20 @@ class _Model:
                                                 ptr(out)[0], mem))
         return out
 
+    def jacobian_combination_noalloc(self, out, c_stiffness, stiffness, c_mass, mass, bc_nodes=()):
+        """jacobian_combination on device tensors with no device allocation
+        (scratch preallocated in the library; see
+        hoefem_jacobian_combination_noalloc for the limits)."""
+        for a in (out, stiffness, mass):
+            if a is not None and not _capi.is_device_array(a):
+                raise ValueError("device tensors only")
+        bc = host_i64(bc_nodes)
+        check(lib().hoefem_jacobian_combination_noalloc(self._h, float(c_stiffness), ptr(stiffness)[0],
+                                                        float(c_mass), ptr(mass)[0],
+                                                        bc.ctypes.data if bc.size else None, bc.size,
+                                                        ptr(out)[0]))
+        return out
+
     def spmv(self, y, values, x, alpha=1.0, beta=0.0):
         """y = beta y + alpha A x (spmv_csr, sparse.rs:1164-1199)."""
         mem = _same_space(y, values, x)

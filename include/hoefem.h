@@ -165,7 +165,25 @@ int hoefem_apply_dirichlet_bc_csr(hoefem_model m, const int64_t* nodes, int64_t 
 int hoefem_jacobian_combination(hoefem_model m, double c_stiffness, const double* stiffness_values, double c_mass,
                                 const double* mass_values, const int64_t* bc_nodes, int64_t num_bc, double* out,
                                 int mem);
-
+/* hoefem_jacobian_combination without any device allocation.  No counterpart
+   in the reference: for callers that cannot allocate device memory while
+   they step (a host that reserves its device memory budget up front, or a
+   real-time loop that must not wait on the allocator).  stiffness_values /
+   mass_values (either may be NULL) and out are device pointers on the
+   current device (nnz each); bc_nodes is a host array.  Scratch (the
+   Dirichlet DOF mask, the node list and the diagonal-scale word) is a fixed
+   array inside the library, one per device, sized for at most 4,194,304 DOFs
+   and 262,144 Dirichlet nodes; larger inputs return
+   HOEFEM_ERR_INVALID_ARGUMENT.  The mask is cleared on every call.  The
+   model must already be resident on the device (any compute entry point
+   puts it there).  The first call on each device looks up the scratch
+   address (cudaGetSymbolAddress) and should come before any stream capture.
+   All calls on one device share the one scratch: calls that overlap in time
+   (other threads or streams) race and must be serialised by the caller.
+   Synchronous on return, like every entry point. */
+int hoefem_jacobian_combination_noalloc(hoefem_model m, double c_stiffness, const double* stiffness_values,
+                                        double c_mass, const double* mass_values, const int64_t* bc_nodes,
+                                        int64_t num_bc, double* out);
 /* spmv_csr (fenris/src/sparse.rs:1164-1199) / LinearOperator::apply for the
    model pattern (cg.rs:15-17): y = beta*y + alpha*A x. */
 int hoefem_spmv(hoefem_model m, double beta, double* y, double alpha, const double* values, const double* x, int mem);
