@@ -81,6 +81,9 @@ SIGNATURES = {
     "hoefem_assemble_elastic_pseudo_forces_into": (C.c_int, [vp, C.POINTER(Material), vp, vp, C.c_int]),
     "hoefem_assemble_stiffness_into": (C.c_int, [vp, C.POINTER(Material), vp, vp, C.c_int]),
     "hoefem_assemble_stiffness_into_precision": (C.c_int, [vp, C.POINTER(Material), vp, vp, C.c_int, C.c_int]),
+    "hoefem_assemble_projected_stiffness_into": (C.c_int, [vp, C.POINTER(Material), vp, vp, C.c_int]),
+    "hoefem_jacobian_combination_damped": (C.c_int, [vp, dbl, vp, dbl, vp, dbl, vp, vp, i64, vp, C.c_int]),
+    "hoefem_integrator_set_damping": (C.c_int, [vp, C.c_int, dbl, C.c_int, dbl]),
     "hoefem_assemble_mass_into": (C.c_int, [vp, dbl, vp, C.c_int]),
     "hoefem_apply_dirichlet_bc_csr": (C.c_int, [vp, vp, i64, vp, C.c_int]),
     "hoefem_jacobian_combination": (C.c_int, [vp, dbl, vp, dbl, vp, vp, i64, vp, C.c_int]),
@@ -90,6 +93,7 @@ SIGNATURES = {
     "hoefem_precond_create_schwarz": (C.c_int, [vp, vp, vp, i64, vp, i64, C.POINTER(vp)]),
     "hoefem_precond_update": (C.c_int, [vp, vp, C.c_int]),
     "hoefem_precond_apply": (C.c_int, [vp, vp, vp, C.c_int]),
+    "hoefem_precond_set_spmv_variant": (C.c_int, [vp, C.c_int32]),
     "hoefem_precond_nnz": (C.c_int, [vp, pi64]),
     "hoefem_precond_pattern": (C.c_int, [vp, vp, vp]),
     "hoefem_precond_values": (C.c_int, [vp, vp]),

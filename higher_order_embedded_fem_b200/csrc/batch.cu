@@ -390,6 +390,7 @@ struct Batch {
   // device
   DBuf<int> d_node_off, d_scene_of;
   DBuf<unsigned char> d_bc, d_ok, d_active;
+  DBuf<unsigned char> emask;  // scenes whose elements the force / stiffness kernels evaluate
   DBuf<double> M, K, J, gforce, up, vn, w, F, dx, us, vs, f, u, v, diag, x, b, r, z, p, Ap, t, scale, coef, nrm;
   DBuf<unsigned long long> first;
   DBuf<SegCg> st;
@@ -460,10 +461,16 @@ struct Batch {
     HOEFEM_CUDA(cudaStreamSynchronize(s));
   }
 
-  // F(w) for all scenes; returns per-scene ||F||^2
-  void eval_F(double dt, std::vector<double>& fsq) {
+  void set_emask(const std::vector<unsigned char>& mask) {
+    HOEFEM_CUDA(cudaMemcpyAsync(emask.p, mask.data(), nscene, cudaMemcpyHostToDevice, m.stream));
+  }
+
+  // F(w) for the scenes in `mask` (other scenes' entries are not meaningful);
+  // returns per-scene ||F||^2
+  void eval_F(double dt, const std::vector<unsigned char>& mask, std::vector<double>& fsq) {
     cudaStream_t s = m.stream;
     const int n = (int)m.ndof;
+    set_emask(mask);
     (note_launch(), k_seg_state<<<vg(), TPB, 0, s>>>(n, d_scene_of.p, up.p, vn.p, w.p, dt, d_bc.p, us.p, vs.p));
     (note_launch(), k_vcopy<<<vg(), TPB, 0, s>>>(n, gforce.p, f.p));
     launch_forces(m, MatDev{mat_kind, 0.0, 0.0}, us.p, f.p, s);
@@ -535,7 +542,7 @@ struct Batch {
     (note_launch(), k_be_init2<<<vg(), TPB, 0, s>>>(n, u.p, v.p, dt, up.p, vn.p, w.p));
     std::vector<double> fsq, tol(nscene);
     for (int k = 0; k < nscene; ++k) tol[k] = dt * (1e-5 * rep[k]);
-    eval_F(dt, fsq);
+    eval_F(dt, part, fsq);
     std::vector<unsigned char> active(nscene);
     std::vector<i64> iter(nscene, 0);
     for (int k = 0; k < nscene; ++k)
@@ -554,6 +561,7 @@ struct Batch {
       // J = dt^2 K + M with the per-scene Dirichlet scale, diagonal preconditioner
       (note_launch(), k_seg_state<<<vg(), TPB, 0, s>>>(n, d_scene_of.p, up.p, vn.p, w.p, dt, d_bc.p, us.p, vs.p));
       K.zero(s);
+      set_emask(active);
       launch_stiffness(m, MatDev{mat_kind, 0.0, 0.0}, us.p, K.p, s);
       (note_launch(), k_combine2<<<148 * 8, TPB, 0, s>>>(m.nnz, -(-dt * dt), K.p, M.p, J.p));
       dirichlet(J.p);
@@ -608,7 +616,7 @@ struct Batch {
         HOEFEM_CUDA(cudaMemcpyAsync(coef.p, da.data(), sizeof(double) * nscene, cudaMemcpyHostToDevice, s));
         (note_launch(), k_seg_axpy<<<vg(), TPB, 0, s>>>(n, d_scene_of.p, coef.p, dx.p, w.p));
         std::vector<double> nf;
-        eval_F(dt, nf);
+        eval_F(dt, ls, nf);
         for (int k = 0; k < nscene; ++k) {
           if (!ls[k]) continue;
           fsq[k] = nf[k];
@@ -792,6 +800,7 @@ Batch* batch_build(const std::vector<const Model*>& scenes, const std::vector<Ma
         for (i64 e = 0; e < b->ne; ++e) {
           mb->emat.push_back(mats[k].mu);
           mb->emat.push_back(mats[k].lambda);
+          mb->escene.push_back(k);
           if (!uniform) {
             const i64 q0 = b->uniform ? 0 : b->qoff[e];
             const i64 q1 = b->uniform ? (i64)b->qw.size() : b->qoff[e + 1];
@@ -817,6 +826,8 @@ Batch* batch_build(const std::vector<const Model*>& scenes, const std::vector<Ma
   finalize_model(m);
   ensure_device(m);
   B->setup();
+  B->emask.alloc(ns);
+  for (Block* b : m.blocks) b->scene_active = B->emask.p;
   return B.release();
 }
 

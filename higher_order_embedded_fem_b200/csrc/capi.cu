@@ -20,6 +20,8 @@ Integrator* integrator_new(Model* m, const hoefem_material* mat, double density,
                            int gravity_enabled, double gravity, Precond* P);
 void integrator_delete(Integrator* it);
 void integrator_set_tolerances(Integrator* it, double tol, i64 cg_max, i64 newton_max);
+void integrator_set_damping(Integrator* it, bool has_mass, double mass_coeff, bool has_stiffness,
+                            double stiffness_coeff);
 void integrator_set_precision(Integrator* it, int precision, double delta);
 void integrator_set_learned(Integrator* it, Learned* l, int mode);
 int integrator_step(Integrator* it, double* ud, double* vd, double t, double dt);
@@ -260,6 +262,8 @@ int hoefem_model_set_spmv_variant(hoefem_model m, int32_t variant) {
   HOEFEM_REQUIRE(variant == 8 || variant == 16 || variant == 32 || variant == 108 || variant == 116 || variant == 132,
                  HOEFEM_ERR_INVALID_ARGUMENT, "unknown SpMV variant");
   mm.spmv_lanes = variant;
+  mm.spmv_lanes32 = variant;
+  mm.spmv_pinned = true;
   API_END
 }
 
@@ -345,6 +349,19 @@ int hoefem_assemble_stiffness_into_precision(hoefem_model m, const hoefem_materi
   API_END
 }
 
+int hoefem_assemble_projected_stiffness_into(hoefem_model m, const hoefem_material* mat, const double* u,
+                                             double* values, int mem) {
+  API_BEGIN
+  Model& mm = device_model(m);
+  MatDev md = mat_of(mat);
+  View U(u, mm.ndof, mem, mm.stream, true), V(values, mm.nnz, mem, mm.stream, true);
+  launch_stiffness_projected(mm, md, U.d, V.d, mm.stream);
+  V.copy_out();
+  sync(mm);
+  check_device_error(mm);
+  API_END
+}
+
 int hoefem_assemble_mass_into(hoefem_model m, double density, double* values, int mem) {
   API_BEGIN
   Model& mm = device_model(m);
@@ -397,6 +414,28 @@ int hoefem_jacobian_combination(hoefem_model m, double c_stiffness, const double
   View O(out, mm.nnz, mem, mm.stream, false);
   jacobian_combination(mm, c_stiffness, stiffness_values ? K.d : nullptr, c_mass, mass_values ? M.d : nullptr,
                        num_bc > 0 ? mask.p : nullptr, O.d, scratch.p, mm.stream);
+  O.copy_out();
+  sync(mm);
+  API_END
+}
+
+int hoefem_jacobian_combination_damped(hoefem_model m, double c_stiffness, const double* stiffness_values,
+                                       double c_damping, const double* damping_values, double c_mass,
+                                       const double* mass_values, const int64_t* bc_nodes, int64_t num_bc,
+                                       double* out, int mem) {
+  API_BEGIN
+  Model& mm = device_model(m);
+  DBuf<unsigned char> mask;
+  if (num_bc > 0) bc_mask(mm, bc_nodes, num_bc, mask);
+  DBuf<double> scratch;
+  scratch.alloc(1);
+  View K(stiffness_values, stiffness_values ? mm.nnz : 0, mem, mm.stream, true);
+  View D(damping_values, damping_values ? mm.nnz : 0, mem, mm.stream, true);
+  View M(mass_values, mass_values ? mm.nnz : 0, mem, mm.stream, true);
+  View O(out, mm.nnz, mem, mm.stream, false);
+  jacobian_combination(mm, c_stiffness, stiffness_values ? K.d : nullptr, c_mass, mass_values ? M.d : nullptr,
+                       num_bc > 0 ? mask.p : nullptr, O.d, scratch.p, mm.stream, c_damping,
+                       damping_values ? D.d : nullptr);
   O.copy_out();
   sync(mm);
   API_END
@@ -469,6 +508,17 @@ int hoefem_precond_apply(hoefem_precond p, const double* r, double* z, int mem) 
   precond_apply(p->p, R.d, Z.d, mm.stream);
   Z.copy_out();
   sync(mm);
+  API_END
+}
+
+int hoefem_precond_set_spmv_variant(hoefem_precond p, int32_t variant) {
+  API_BEGIN
+  HOEFEM_REQUIRE(p && p->p.kind == PREC_SCHWARZ, HOEFEM_ERR_INVALID_ARGUMENT, "not a Schwarz preconditioner");
+  HOEFEM_REQUIRE(variant == 8 || variant == 16 || variant == 32 || variant == 108 || variant == 116 || variant == 132,
+                 HOEFEM_ERR_INVALID_ARGUMENT, "unknown SpMV variant");
+  p->p.spmv_lanes = variant;
+  p->p.spmv_lanes32 = variant;
+  p->p.spmv_pinned = true;
   API_END
 }
 
@@ -613,6 +663,14 @@ int hoefem_integrator_step(hoefem_integrator it, double* u, double* v, double t,
   V.copy_out();
   sync(mm);
   if (st != HOEFEM_OK) return fail(st, "time step failed");
+  API_END
+}
+
+int hoefem_integrator_set_damping(hoefem_integrator it, int has_mass, double mass_coeff, int has_stiffness,
+                                  double stiffness_coeff) {
+  API_BEGIN
+  HOEFEM_REQUIRE(it, HOEFEM_ERR_INVALID_ARGUMENT, "null integrator");
+  integrator_set_damping(it->it, has_mass != 0, mass_coeff, has_stiffness != 0, stiffness_coeff);
   API_END
 }
 

@@ -10,8 +10,11 @@
 // `chunk` iterations and reads the state once per chunk, so a solve costs one
 // host round trip per chunk instead of per iteration, and the result (x,
 // iteration count, status) is the one the sequential loop would produce.
-// All reductions are deterministic (fixed grid, block partials summed in
-// block order by the last block).
+// All reductions are deterministic: the node-row kernels fetch chunks of
+// nodes dynamically but sum each chunk in a fixed order and the chunks in
+// index order; the vector kernels use a fixed grid and sum block partials in
+// block order.  The SpMV variants of the operator and of the Schwarz apply
+// are chosen online per value precision by timing the first chunks.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -34,10 +37,8 @@ constexpr int TPB = 256;
 template <int L, class VA>
 __global__ void __launch_bounds__(TPB) k_cg_init(NodeRows A, const VA* __restrict__ vals,
                                                  const double* __restrict__ x, const double* __restrict__ b,
-                                                 double* __restrict__ r, double* partials, unsigned* counter,
-                                                 CgState* st) {
-  double acc[2] = {0.0, 0.0};
-  for_each_node<L>(A, [&](int a, int sl) {
+                                                 double* __restrict__ r, double* part, CgState* st) {
+  for_each_node_reduce<L, 2>(A, part, [&](int a, int sl, double (&acc)[2]) {
     double s[3];
     node_row_dot<L>(A, vals, x, a, sl, s[0], s[1], s[2]);
     if (a >= 0 && sl == 0) {
@@ -51,9 +52,8 @@ __global__ void __launch_bounds__(TPB) k_cg_init(NodeRows A, const VA* __restric
       }
     }
   });
-  node_sched_finish(A);
-  double tot[2];
-  if (grid_reduce_last_k<2>(acc, partials, counter, tot) && threadIdx.x == 0) {
+  double extra[2] = {0.0, 0.0}, tot[2];
+  if (node_reduce_finish<L, 2>(A, part, extra, tot) && threadIdx.x == 0) {
     st->bnorm = sqrt(tot[0]);
     st->rr = tot[1];
   }
@@ -86,10 +86,9 @@ __global__ void __launch_bounds__(TPB) k_cg_prec_vec(int n, int mode, const doub
 template <int L, class VP>
 __global__ void __launch_bounds__(TPB) k_cg_prec_spmv(NodeRows P, const VP* __restrict__ pv,
                                                       const double* __restrict__ r, double* __restrict__ z,
-                                                      double* partials, unsigned* counter, CgState* st, int init) {
+                                                      double* part, CgState* st, int init) {
   if (!init && st->done) return;
-  double acc[1] = {0.0};
-  for_each_node<L>(P, [&](int a, int sl) {
+  for_each_node_reduce<L, 1>(P, part, [&](int a, int sl, double (&acc)[1]) {
     double s[3];
     node_row_dot<L>(P, pv, r, a, sl, s[0], s[1], s[2]);
     if (a >= 0 && sl == 0) {
@@ -100,9 +99,13 @@ __global__ void __launch_bounds__(TPB) k_cg_prec_spmv(NodeRows P, const VP* __re
       }
     }
   });
-  node_sched_finish(P);
-  double tot[1];
-  if (grid_reduce_last_k<1>(acc, partials, counter, tot) && threadIdx.x == 0) {
+  // untreated (diagonal-only) nodes, elementwise
+  double extra[1] = {0.0}, tot[1];
+  for_each_diag_dof(P, pv, r, [&](int dof, double v) {
+    z[dof] = v;
+    extra[0] += v * r[dof];
+  });
+  if (node_reduce_finish<L, 1>(P, part, extra, tot) && threadIdx.x == 0) {
     if (init) st->zTr = tot[0];
     else {
       st->beta = tot[0] / st->zTr;
@@ -131,11 +134,10 @@ __global__ void k_cg_init_check(CgState* st) {
 // Ap = A p ; pAp ; checks ; alpha
 template <int L, class VA>
 __global__ void __launch_bounds__(TPB) k_cg_Ap(NodeRows A, const VA* __restrict__ vals,
-                                               const double* __restrict__ p, double* __restrict__ Ap,
-                                               double* partials, unsigned* counter, CgState* st) {
+                                               const double* __restrict__ p, double* __restrict__ Ap, double* part,
+                                               CgState* st) {
   if (st->done) return;
-  double acc[1] = {0.0};
-  for_each_node<L>(A, [&](int a, int sl) {
+  for_each_node_reduce<L, 1>(A, part, [&](int a, int sl, double (&acc)[1]) {
     double s[3];
     node_row_dot<L>(A, vals, p, a, sl, s[0], s[1], s[2]);
     if (a >= 0 && sl == 0) {
@@ -146,9 +148,8 @@ __global__ void __launch_bounds__(TPB) k_cg_Ap(NodeRows A, const VA* __restrict_
       }
     }
   });
-  node_sched_finish(A);
-  double tot[1];
-  if (grid_reduce_last_k<1>(acc, partials, counter, tot) && threadIdx.x == 0) {
+  double extra[1] = {0.0}, tot[1];
+  if (node_reduce_finish<L, 1>(A, part, extra, tot) && threadIdx.x == 0) {
     double pAp = tot[0];
     st->pAp = pAp;
     if (pAp <= 0.0) { st->done = 1; st->status = HOEFEM_CG_INDEFINITE_OPERATOR; }
@@ -242,7 +243,8 @@ void CgWork::init(Model* model) {
   m = model;
   n = model->ndof;
   x.alloc(n); b.alloc(n); r.alloc(n); z.alloc(n); p.alloc(n); Ap.alloc(n);
-  partials.alloc(4 * 148 * 16);
+  // node-chunk partials (<= nv / 8 chunks) + block partials, K <= 2 values
+  partials.alloc(std::max<size_t>(4 * 148 * 16, 2 * ((size_t)model->nv / 8 + 2) + 2 * 4096));
   st.alloc(1);
   counter.alloc(1);
   HOEFEM_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), model->stream));
@@ -253,6 +255,10 @@ CgWork::~CgWork() {
   for (auto& g : graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   if (h_st) cudaFreeHost(h_st);
+  for (auto& t : tuning) {
+    if (t.e0) cudaEventDestroy(t.e0);
+    if (t.e1) cudaEventDestroy(t.e1);
+  }
 }
 
 void to_f32(const double* a, float* b, long long n, cudaStream_t s) {
@@ -274,29 +280,33 @@ const void* prec_key(const Precond* P, bool p32) {
   return (const void*)P->diag.p;
 }
 
+int lanes_for(const Model& m, bool f32) { return f32 && m.spmv_lanes32 ? m.spmv_lanes32 : m.spmv_lanes; }
+int lanes_for(const Precond& p, bool f32) { return f32 && p.spmv_lanes32 ? p.spmv_lanes32 : p.spmv_lanes; }
+
 void enqueue_Ap(CgWork& w, Operator A, cudaStream_t s) {
   NodeRows R = w.m->rows();
+  R.lanes = lanes_for(*w.m, A.v32 != nullptr);
+  HOEFEM_REQUIRE(R.sched, HOEFEM_ERR_INVALID_ARGUMENT, "node-row matrix without scheduling counters");
   HOEFEM_LANES_DISPATCH(R.lanes, {
-    const int sg = spmv_grid(R.nv, LN);
+    const int sg = spmv_grid(R.count(), LN);
     if (A.v32)
-      (note_launch(), k_cg_Ap<LN, float><<<sg, TPB, 0, s>>>(R, A.v32, w.p.p, w.Ap.p, w.partials.p, w.counter.p,
-                                                            w.st.p));
+      (note_launch(), k_cg_Ap<LN, float><<<sg, TPB, 0, s>>>(R, A.v32, w.p.p, w.Ap.p, w.partials.p, w.st.p));
     else
-      (note_launch(), k_cg_Ap<LN, double><<<sg, TPB, 0, s>>>(R, A.v64, w.p.p, w.Ap.p, w.partials.p, w.counter.p,
-                                                             w.st.p));
+      (note_launch(), k_cg_Ap<LN, double><<<sg, TPB, 0, s>>>(R, A.v64, w.p.p, w.Ap.p, w.partials.p, w.st.p));
   });
 }
 
 void enqueue_prec_spmv(CgWork& w, const Precond* P, bool p32, int init, cudaStream_t s) {
   NodeRows PR = P->rows();
+  PR.lanes = lanes_for(*P, p32);
   HOEFEM_LANES_DISPATCH(PR.lanes, {
     const int g = spmv_grid(PR.nv, LN);
     if (p32)
       (note_launch(), k_cg_prec_spmv<LN, float><<<g, TPB, 0, s>>>(PR, P->vals32.p, w.r.p, w.z.p, w.partials.p,
-                                                                  w.counter.p, w.st.p, init));
+                                                                  w.st.p, init));
     else
       (note_launch(), k_cg_prec_spmv<LN, double><<<g, TPB, 0, s>>>(PR, P->vals.p, w.r.p, w.z.p, w.partials.p,
-                                                                   w.counter.p, w.st.p, init));
+                                                                   w.st.p, init));
   });
 }
 
@@ -318,8 +328,11 @@ void enqueue_iteration(CgWork& w, Operator A, const Precond* P, bool p32, cudaSt
 }
 
 CgWork::Graph& graph_for(CgWork& w, Operator A, const Precond* P, bool p32) {
+  // the key also holds the SpMV variants the graph was captured with
+  const intptr_t variants = (intptr_t)lanes_for(*w.m, A.v32 != nullptr) * 1024 +
+                            (P && P->kind == PREC_SCHWARZ ? lanes_for(*P, p32) : 0);
   const void* key[4] = {A.v32 ? (const void*)A.v32 : (const void*)A.v64, (const void*)P, prec_key(P, p32),
-                        (const void*)(intptr_t)((P ? P->kind : 0) * 2 + (p32 ? 1 : 0))};
+                        (const void*)(intptr_t)(((P ? P->kind : 0) * 2 + (p32 ? 1 : 0)) + 8 * variants)};
   for (auto& g : w.graphs)
     if (g.exec && std::equal(key, key + 4, g.key)) return g;
   if (w.graphs.size() >= 4) {
@@ -361,11 +374,13 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   init.max_iter = max_iter;
   HOEFEM_CUDA(cudaMemcpyAsync(w.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
   const int vg = vec_grid(n);
+  HOEFEM_REQUIRE(R.sched, HOEFEM_ERR_INVALID_ARGUMENT, "node-row matrix without scheduling counters");
   auto true_residual = [&](const double* vals64) {
+    R.lanes = lanes_for(*w.m, false);
     HOEFEM_LANES_DISPATCH(R.lanes, {
       const int sg = spmv_grid(R.nv, LN);
       (note_launch(), k_cg_init<LN, double><<<sg, TPB, 0, s>>>(R, vals64, w.x.p, w.b.p, w.r.p, w.partials.p,
-                                                               w.counter.p, w.st.p));
+                                                               w.st.p));
     });
   };
   auto prec_init = [&]() {
@@ -380,14 +395,15 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   if (A64) {
     true_residual(A64);
   } else {
+    R.lanes = lanes_for(*w.m, A.v32 != nullptr);
     HOEFEM_LANES_DISPATCH(R.lanes, {
       const int sg = spmv_grid(R.nv, LN);
       if (A.v32)
         (note_launch(), k_cg_init<LN, float><<<sg, TPB, 0, s>>>(R, A.v32, w.x.p, w.b.p, w.r.p, w.partials.p,
-                                                                w.counter.p, w.st.p));
+                                                                w.st.p));
       else
         (note_launch(), k_cg_init<LN, double><<<sg, TPB, 0, s>>>(R, A.v64, w.x.p, w.b.p, w.r.p, w.partials.p,
-                                                                 w.counter.p, w.st.p));
+                                                                 w.st.p));
     });
   }
   prec_init();
@@ -405,17 +421,56 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
     *iters = w.h_st->iters;
     return w.h_st->status;
   }
-  CgWork::Graph& G = graph_for(w, A, P, p32);
+  // online SpMV variant choice: candidate pairs (operator lanes, Schwarz lanes)
+  const bool f32 = A.v32 != nullptr;
+  const bool schwarz = P && P->kind == PREC_SCHWARZ;
+  static const int cand_lanes[4] = {8, 16, 32, 132};
+  const int ncand = schwarz ? 16 : 4;
+  CgWork::Tuning& tu = w.tuning[f32 ? 1 : 0];
+  if (!w.online_tuning || w.m->spmv_pinned || (schwarz && P->spmv_pinned)) tu.done = true;
+  if (!tu.done && !tu.e0) {
+    HOEFEM_CUDA(cudaEventCreate(&tu.e0));
+    HOEFEM_CUDA(cudaEventCreate(&tu.e1));
+  }
+  auto set_candidate = [&](int c) {
+    const int lj = cand_lanes[c % 4], lp = cand_lanes[c / 4];
+    if (f32) w.m->spmv_lanes32 = lj;
+    else w.m->spmv_lanes = lj;
+    if (schwarz) {
+      Precond* Pm = const_cast<Precond*>(P);
+      if (p32) Pm->spmv_lanes32 = lp;
+      else Pm->spmv_lanes = lp;
+    }
+  };
   // without an iteration limit CG is still bounded: 10 n iterations
   const i64 cap = max_iter >= 0 ? max_iter : 10 * (i64)n;
   const i64 max_chunks = (cap + w.chunk - 1) / w.chunk + 2;
   double rr_ref = w.h_st->rr;
   i64 nrep = 0;
   for (i64 c = 0; c < max_chunks; ++c) {
+    const i64 it0 = w.h_st->iters;
+    const bool timing = !tu.done;
+    if (timing) set_candidate(tu.next);
+    CgWork::Graph& G = graph_for(w, A, P, p32);
+    if (timing) HOEFEM_CUDA(cudaEventRecord(tu.e0, s));
     HOEFEM_CUDA(cudaGraphLaunch(G.exec, s));
     g_launch_count.fetch_add(G.kernels, std::memory_order_relaxed);
+    if (timing) HOEFEM_CUDA(cudaEventRecord(tu.e1, s));
     HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
     HOEFEM_CUDA(cudaStreamSynchronize(s));
+    if (timing) {
+      // a chunk that ran all its iterations is a valid sample of candidate tu.next
+      if (w.h_st->iters - it0 == w.chunk) {
+        float ms = 0.f;
+        HOEFEM_CUDA(cudaEventElapsedTime(&ms, tu.e0, tu.e1));
+        if (ms < tu.best_ms) {
+          tu.best_ms = ms;
+          tu.best = tu.next;
+        }
+        if (++tu.next == ncand) tu.done = true;
+      }
+      set_candidate(tu.done ? tu.best : tu.next);
+    }
     if (A64) {
       const bool conv = w.h_st->done && w.h_st->status == HOEFEM_OK;
       const bool trig = !w.h_st->done && w.h_st->rr <= delta * delta * rr_ref;

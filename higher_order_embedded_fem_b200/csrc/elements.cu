@@ -315,6 +315,7 @@ __global__ void __launch_bounds__(TPB) k_forces(const BlockDev b, const int* __r
   __shared__ double s_corner[TPB / 32][24];
   if (idx >= count) return;
   const int e = elems[idx];
+  if (b.scene_active && !b.scene_active[b.escene[e]]) return;
   const bool own = lane < NN;
   int g = own ? b.conn[lane * b.ne + e] : 0;
   double Xl[3] = {0, 0, 0}, ul[3] = {0, 0, 0};
@@ -395,6 +396,7 @@ __global__ void __launch_bounds__(32 * FW, 2) k_forces_hex27(const BlockDev b, c
   __shared__ double s_f[FW][NN][3];
   __shared__ int s_ok;
   const int e = elems[blockIdx.x];
+  if (b.scene_active && !b.scene_active[b.escene[e]]) return;  // uniform over the CTA
   const bool own = lane < NN;
   const int g = own ? b.conn[lane * b.ne + e] : 0;
   double ul[3] = {0, 0, 0};
@@ -504,7 +506,8 @@ __global__ void __launch_bounds__(StiffCfg<NN>::TPB, 2) k_stiffness(const BlockD
                                                                     const double* __restrict__ u,
                                                                     const int* __restrict__ adj_off,
                                                                     const long long* __restrict__ base,
-                                                                    double* __restrict__ vals, MatDev mat, int* err) {
+                                                                    double* __restrict__ vals, MatDev mat, int* err,
+                                                                    double* __restrict__ stage) {
   using C = StiffCfg<NN>;
   constexpr int TPE = C::TPE, EPC = C::EPC, QT = C::QT, WPE = TPE / 32;
   constexpr int NP = PairTable<NN>::NP;
@@ -520,8 +523,8 @@ __global__ void __launch_bounds__(StiffCfg<NN>::TPB, 2) k_stiffness(const BlockD
   const int grp = threadIdx.x / TPE, t = threadIdx.x % TPE;
   const int lane = threadIdx.x & 31, wl = t >> 5;
   const int idx = blockIdx.x * EPC + grp;
-  const bool active = idx < count;
-  const int e = active ? elems[idx] : 0;
+  const int e = idx < count ? elems[idx] : 0;
+  const bool active = idx < count && (!b.scene_active || b.scene_active[b.escene[e]]);
   if (active && t < NN) {
     const int g = b.conn[t * b.ne + e];
     s_g[grp][t] = g;
@@ -609,6 +612,27 @@ __global__ void __launch_bounds__(StiffCfg<NN>::TPB, 2) k_stiffness(const BlockD
   if (!active) return;
   if (!s_ok[grp]) {
     if (t == 0) set_error(err, HOEFEM_ERR_SINGULAR);
+    return;
+  }
+  if (stage) {
+    // dense element matrix (row-major 3NN x 3NN) instead of the scatter
+    constexpr int D = 3 * NN;
+    double* ke = stage + (size_t)e * D * D;
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      int p = t + k * TPE;
+      if (p < NP) {
+        int I, Jn;
+        pair_of<NN>(p, I, Jn);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            ke[(3 * I + i) * D + 3 * Jn + j] = (double)acc[k][3 * i + j];
+            if (I != Jn) ke[(3 * Jn + j) * D + 3 * I + i] = (double)acc[k][3 * i + j];
+          }
+      }
+    }
     return;
   }
   const int* em = b.emap + (size_t)e * NN * NN;
@@ -743,7 +767,7 @@ void launch_forces(const Model& m, const MatDev& mat, const double* u, double* f
 
 template <int NN, class R>
 void launch_stiffness_kind(const Model& m, const Block& blk, const MatDev& mat, const double* u, double* vals,
-                           cudaStream_t s) {
+                           cudaStream_t s, double* stage = nullptr) {
   using C = StiffCfg<NN>;
   constexpr size_t smem = stiffness_smem<NN, R>();
   static bool attr_set[64] = {};
@@ -754,11 +778,30 @@ void launch_stiffness_kind(const Model& m, const Block& blk, const MatDev& mat, 
     attr_set[dev] = true;
   }
   BlockDev bd = blk.dev();
+  if (stage) {
+    // all elements at once (no scatter, no coloring needed)
+    const int cnt = (int)blk.ne;
+    if (cnt > 0)
+      (note_launch(), k_stiffness<NN, R><<<(cnt + C::EPC - 1) / C::EPC, C::TPB, smem, s>>>(
+                          bd, blk.d_color_elems.p, cnt, m.d_X.p, u, m.d_adj_off.p, m.d_base.p, vals, mat, m.d_err.p,
+                          stage));
+    return;
+  }
   for_each_color(blk, [&](const int* elems, int cnt) {
     const int grid = (cnt + C::EPC - 1) / C::EPC;
     (note_launch(), k_stiffness<NN, R><<<grid, C::TPB, smem, s>>>(bd, elems, cnt, m.d_X.p, u, m.d_adj_off.p,
-                                                                   m.d_base.p, vals, mat, m.d_err.p));
+                                                                   m.d_base.p, vals, mat, m.d_err.p, nullptr));
   });
+}
+
+// Dense FP64 element matrices of one block into stage (element e at
+// e * (3 nn)^2), no scatter.
+void launch_stiffness_staged(const Model& m, const Block& blk, const MatDev& mat, const double* u, double* stage,
+                             cudaStream_t s) {
+  init_pairs();
+  if (blk.kind == HOEFEM_ELEM_TET10) launch_stiffness_kind<10, double>(m, blk, mat, u, nullptr, s, stage);
+  else launch_stiffness_kind<27, double>(m, blk, mat, u, nullptr, s, stage);
+  HOEFEM_CUDA(cudaGetLastError());
 }
 
 void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s,

@@ -130,6 +130,11 @@ struct Integrator {
   std::vector<DBuf<double>*> snaps;  // collected (x_k, r_k) pairs of the current solve
   double ratio_sum = 0.0;
   double rep_force = 0.0;
+  // damping D = gamma M + alpha K_proj(u) from the (sub)step's initial state
+  // (compute_damping_matrix_into, system_assembly.rs:145-193)
+  bool has_mass_damping = false, has_stiffness_damping = false, has_damping = false;
+  double mass_damping = 0.0, stiffness_damping = 0.0;
+  DBuf<double> D;
   DBuf<unsigned char> bc;
   DBuf<double> M, K, J, gforce, up, vn, w, F, dx, us, vs, f, u, v, partials, scalars;
   DBuf<unsigned> counter;
@@ -180,7 +185,7 @@ struct Integrator {
     launch_mass(*m, density, K.p, s);
     jacobian_combination(*m, 0.0, nullptr, 1.0, K.p, bc_nodes.empty() ? nullptr : bc.p, M.p, scalars.p, s);
     check_device_error(*m);
-    m->spmv_lanes = autotune_spmv_lanes(m->rows(), M.p, s);
+    if (!m->spmv_pinned) m->spmv_lanes = autotune_spmv_lanes(m->rows(), M.p, s);
     // representative force ||M a||, a_i = sqrt(a^2 / 3), a = 10 (fe_model.rs:423-431)
     (note_launch(), k_fill<<<grid(), TPB, 0, s>>>(n, std::sqrt((10.0 * 10.0) / 3.0), us.p));
     spmv_node_rows(m->rows(), M.p, us.p, vs.p, 1.0, 0.0, s);
@@ -213,6 +218,7 @@ struct Integrator {
     if (!bc_nodes.empty()) (note_launch(), k_bc_uv<<<grid(), TPB, 0, s>>>(n, bc.p, us.p, vs.p));
     (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, gforce.p, out));
     launch_forces(*m, mat, us.p, out, s);
+    if (has_damping) spmv_node_rows(m->rows(), D.p, vs.p, out, -1.0, 1.0, s);  // f += -D v
     if (!bc_nodes.empty()) (note_launch(), k_zero_bc<<<grid(), TPB, 0, s>>>(n, bc.p, out));
     check_device_error(*m);
   }
@@ -226,6 +232,7 @@ struct Integrator {
     (note_launch(), k_be_state<<<grid(), TPB, 0, s>>>(n, up.p, vn.p, w.p, dt, bcp, us.p, vs.p));
     (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, gforce.p, f.p));
     launch_forces(*m, mat, us.p, f.p, s);
+    if (has_damping) spmv_node_rows(m->rows(), D.p, vs.p, f.p, -1.0, 1.0, s);  // f += -D v
     HOEFEM_CUDA(cudaEventRecord(ev[1], s));
     (note_launch(), k_F<<<grid(), TPB, 0, s>>>(n, f.p, bcp, dt, F.p));
     spmv_node_rows(m->rows(), M.p, w.p, F.p, 1.0, 1.0, s);
@@ -243,8 +250,9 @@ struct Integrator {
     (note_launch(), k_be_state<<<grid(), TPB, 0, s>>>(n, up.p, vn.p, w.p, dt, bcp, us.p, vs.p));
     K.zero(s);
     launch_stiffness(*m, mat, us.p, K.p, s, precision);
-    // J = gamma M - beta D - alpha K with alpha = -dt^2, gamma = 1, no damping
-    jacobian_combination(*m, -(-dt * dt), K.p, 1.0, M.p, bcp, J.p, scalars.p + 4, s);
+    // J = gamma M - beta D - alpha K with alpha = -dt^2, beta = -dt, gamma = 1
+    jacobian_combination(*m, -(-dt * dt), K.p, 1.0, M.p, bcp, J.p, scalars.p + 4, s, -(-dt),
+                         has_damping ? D.p : nullptr);
     HOEFEM_CUDA(cudaEventRecord(ev[1], s));
     check_device_error(*m);
     stats.ms_assemble_stiffness += elapsed();
@@ -353,9 +361,27 @@ struct Integrator {
     snaps.clear();
   }
 
+  // Damping matrix of the (sub)step starting at state u (no boundary
+  // conditions on D; the stiffness part is assembled with element-wise PSD
+  // projection, then D = 0 + alpha K_proj + gamma M).
+  void compute_damping() {
+    has_damping = has_mass_damping || has_stiffness_damping;
+    if (!has_damping) return;
+    cudaStream_t s = m->stream;
+    if (D.n < (size_t)m->nnz) D.alloc(m->nnz);
+    if (has_stiffness_damping) {
+      K.zero(s);
+      launch_stiffness_projected(*m, mat, u.p, K.p, s);
+      check_device_error(*m);
+    }
+    jacobian_combination(*m, stiffness_damping, has_stiffness_damping ? K.p : nullptr, mass_damping,
+                         has_mass_damping ? M.p : nullptr, nullptr, D.p, scalars.p + 4, s);
+  }
+
   int be_step(double dt) {
     cudaStream_t s = m->stream;
     const int n = (int)m->ndof;
+    compute_damping();
     (note_launch(), k_be_init<<<grid(), TPB, 0, s>>>(n, u.p, v.p, dt, up.p, vn.p, w.p));
     const double tol = dt * (1e-5 * rep_force);
     double fsq = eval_F(dt);
@@ -462,6 +488,14 @@ void integrator_set_precision(Integrator* it, int precision, double delta) {
   it->precision = precision;
   it->delta = delta;
 }
+void integrator_set_damping(Integrator* it, bool has_mass, double mass_coeff, bool has_stiffness,
+                            double stiffness_coeff) {
+  it->has_mass_damping = has_mass;
+  it->mass_damping = mass_coeff;
+  it->has_stiffness_damping = has_stiffness;
+  it->stiffness_damping = stiffness_coeff;
+}
+
 void integrator_set_tolerances(Integrator* it, double tol, i64 cg_max, i64 newton_max) {
   it->cg_tol = tol;
   it->cg_max = cg_max;

@@ -86,6 +86,13 @@ struct NodeRows {
   const unsigned char* diag_only = nullptr;  // may be null
   int lanes = 32;  // SpMV variant: lanes per node (8, 16, 32), +100 for column streaming; autotuned
   unsigned* sched = nullptr;  // 2 words: node work counter, finished-block counter (dynamic scheduling)
+  // optional: the row-node kernels visit only `nodes` (nnodes entries), and
+  // the diagonal-only nodes `dnodes` (ndnodes) are applied elementwise
+  const int* nodes = nullptr;
+  int nnodes = 0;
+  const int* dnodes = nullptr;
+  int ndnodes = 0;
+  __host__ __device__ int count() const { return nodes ? nnodes : nv; }
 };
 
 // Per-block device data.
@@ -101,6 +108,10 @@ struct BlockDev {
   const double* qp = nullptr;  // xyz interleaved
   const int* emap = nullptr;   // [e * nn * nn + I * nn + J] = nnz index of (3 gI, 3 gJ) - base[gI]
   const double* emat = nullptr;  // optional per-element Lame parameters (mu, lambda) pairs
+  // optional (batched scenes): element -> scene and a per-scene flag; elements
+  // of scenes whose flag is 0 are skipped by the force / stiffness kernels
+  const int* escene = nullptr;
+  const unsigned char* scene_active = nullptr;
 };
 
 struct Block {
@@ -116,6 +127,9 @@ struct Block {
   DBuf<double> d_qw, d_qp;
   std::vector<double> emat;  // optional per-element (mu, lambda)
   DBuf<double> d_emat;
+  std::vector<int> escene;   // optional element -> scene (batched scenes)
+  DBuf<int> d_escene;
+  const unsigned char* scene_active = nullptr;  // non-owning device mask, per scene
   BlockDev dev() const;
 };
 
@@ -135,8 +149,11 @@ struct Model {
   DBuf<double> d_X;
   DBuf<int> d_adj_off, d_adj, d_diag_slot, d_err;
   DBuf<unsigned> d_sched;  // SpMV dynamic-scheduling counters (zero between launches)
+  DBuf<double> d_stage;    // dense element matrices (projected stiffness), allocated on first use
   DBuf<long long> d_base;
-  int spmv_lanes = 32;
+  int spmv_lanes = 32;    // SpMV variant for FP64 values (autotuned)
+  int spmv_lanes32 = 0;   // SpMV variant for FP32 values (0: as spmv_lanes)
+  bool spmv_pinned = false;  // set explicitly by the caller: no autotuning
   NodeRows rows() const;
   ~Model();
 };
@@ -154,6 +171,9 @@ enum Precision { PRECISION_FP64 = 0, PRECISION_FP32 = 1 };
 void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s,
                       int precision = PRECISION_FP64);
 void launch_mass(const Model& m, double density, double* vals, cudaStream_t s);
+// Stiffness with every element matrix projected onto PSD (negative eigenvalues
+// set to zero) before the colored scatter; adds into vals.
+void launch_stiffness_projected(Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s);
 
 // ---- sparse / vector kernels (linalg.cu) -----------------------------------
 // y = beta*y + alpha*A x on a node-row matrix.
@@ -162,10 +182,12 @@ void spmv_node_rows(const NodeRows& A, const double* vals, const double* x, doub
 // Times the lanes-per-node variants of the node-row SpMV on this structure
 // and returns the fastest (8, 16 or 32); best_ms (optional) gets its time.
 int autotune_spmv_lanes(NodeRows A, const double* vals, cudaStream_t s, float* best_ms = nullptr);
-// Fills out = c_k * K + c_m * M (either may be null) and applies homogeneous
-// Dirichlet rows / columns for the dof mask (may be null).
+// Fills out = c_k * K + c_d * D + c_m * M (any may be null; summed in that
+// order) and applies homogeneous Dirichlet rows / columns for the dof mask
+// (may be null).
 void jacobian_combination(const Model& m, double ck, const double* K, double cm, const double* M,
-                          const unsigned char* bc_dof, double* out, double* d_scratch, cudaStream_t s);
+                          const unsigned char* bc_dof, double* out, double* d_scratch, cudaStream_t s,
+                          double cd = 0.0, const double* D = nullptr);
 // Deterministic reductions: result written to *out (device).
 void dot_device(const double* a, const double* b, i64 n, double* out, double* partials, unsigned* counter,
                 cudaStream_t s);

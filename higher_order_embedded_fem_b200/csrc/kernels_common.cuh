@@ -94,14 +94,17 @@ __device__ __forceinline__ void for_each_node(const NodeRows& A, F&& body) {
   constexpr int NF = G >= 4 ? 16 : 8;
   const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
   const int grp = lane / LNS, sl = lane % LNS;
-  const int nv = A.nv;
+  const int nv = A.count();
+  const int* __restrict__ list = A.nodes;
   if (A.sched == nullptr) {
     for (int a0 = (blockIdx.x * wpb + (threadIdx.x >> 5)) * G; a0 < nv; a0 += gridDim.x * wpb * G) {
-      const int a = a0 + grp;
-      body(a < nv ? a : -1, sl);
+      const int i = a0 + grp;
+      body(i < nv ? (list ? list[i] : i) : -1, sl);
     }
     return;
   }
+  // (claiming the next chunk before processing the current one measured
+  // slower: the chunk is claimed when the warp is free)
   for (;;) {
     unsigned start = 0;
     if (lane == 0) start = atomicAdd(A.sched, (unsigned)NF);
@@ -110,9 +113,21 @@ __device__ __forceinline__ void for_each_node(const NodeRows& A, F&& body) {
     const int end = min((int)start + NF, nv);
 #pragma unroll 1
     for (int a0 = (int)start; a0 < (int)start + NF; a0 += G) {
-      const int a = a0 + grp;
-      body(a < end ? a : -1, sl);
+      const int i = a0 + grp;
+      body(i < end ? (list ? list[i] : i) : -1, sl);
     }
+  }
+}
+
+// The diagonal-only nodes of A (A.dnodes): body(dof, A_dd * x_dof) for each
+// of their DOFs, grid-stride over all threads.
+template <class V, class F>
+__device__ __forceinline__ void for_each_diag_dof(const NodeRows& A, const V* __restrict__ vals,
+                                                  const double* __restrict__ x, F&& body) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * A.ndnodes; t += gridDim.x * blockDim.x) {
+    const int a = A.dnodes[t / 3], i = t - 3 * (t / 3);
+    const int dof = 3 * a + i;
+    body(dof, (double)vals[A.base[a] + i] * x[dof]);
   }
 }
 
@@ -219,6 +234,93 @@ __device__ __forceinline__ bool grid_reduce_last(double v, double* partials, uns
   bool last = grid_reduce_last_k<1>(a, partials, counter, t);
   tot = t[0];
   return last;
+}
+
+// Nodes per dynamically fetched chunk for lane configuration L.
+template <int L>
+struct NodeChunk {
+  static constexpr int G = 32 / LaneCfg<L>::lanes;
+  static constexpr int NF = G >= 4 ? 16 : 8;
+};
+__host__ __device__ inline int node_chunk_count(int count, int nf) { return (count + nf - 1) / nf; }
+
+// Dynamically scheduled node loop with a deterministic reduction of K values:
+// body(a, sl, acc) adds its contribution into acc (any lane); each fetched
+// chunk of NF consecutive nodes is summed by its warp in a fixed order and
+// stored at part[k * C + chunk] (C chunks), whichever warp took it.
+// node_reduce_finish sums the chunks in index order.  Requires A.sched.
+template <int L, int K, class F>
+__device__ __forceinline__ void for_each_node_reduce(const NodeRows& A, double* __restrict__ part, F&& body) {
+  constexpr int LNS = LaneCfg<L>::lanes;
+  constexpr int G = NodeChunk<L>::G, NF = NodeChunk<L>::NF;
+  const int lane = threadIdx.x & 31;
+  const int grp = lane / LNS, sl = lane % LNS;
+  const int count = A.count();
+  const int C = node_chunk_count(count, NF);
+  const int* __restrict__ list = A.nodes;
+  for (;;) {
+    unsigned start = 0;
+    if (lane == 0) start = atomicAdd(A.sched, (unsigned)NF);
+    start = __shfl_sync(0xffffffffu, start, 0);
+    if (start >= (unsigned)count) break;
+    const int end = min((int)start + NF, count);
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+#pragma unroll 1
+    for (int a0 = (int)start; a0 < (int)start + NF; a0 += G) {
+      const int i = a0 + grp;
+      body(i < end ? (list ? list[i] : i) : -1, sl, acc);
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const double v = warp_sum_d(acc[k]);
+      if (lane == 0) part[(size_t)k * C + start / NF] = v;
+    }
+  }
+}
+
+// Finishes a kernel that used for_each_node_reduce<L, K>: `extra` holds each
+// thread's share of a statically scheduled part of the same sums (may be 0);
+// it is block-summed into part[K * C + k * gridDim.x + block].  The last block
+// to arrive resets the scheduling counters and returns true with tot = the
+// chunk sums (index order) plus the block sums (block order) in thread 0.
+// Every thread of every block must call it.
+template <int L, int K>
+__device__ __forceinline__ bool node_reduce_finish(const NodeRows& A, double* __restrict__ part,
+                                                   double (&extra)[K], double (&tot)[K]) {
+  __shared__ bool s_last;
+  const int C = node_chunk_count(A.count(), NodeChunk<L>::NF);
+  block_sum<K>(extra);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) part[(size_t)K * C + (size_t)k * gridDim.x + blockIdx.x] = extra[k];
+    __threadfence();
+    const unsigned t = atomicAdd(A.sched + 1, 1u);
+    s_last = (t == gridDim.x - 1);
+    if (s_last) {
+      A.sched[0] = 0u;
+      A.sched[1] = 0u;
+    }
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0.0;
+  for (int c = threadIdx.x; c < C; c += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] += __ldcg(part + (size_t)k * C + c);
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] += __ldcg(part + (size_t)K * C + (size_t)k * gridDim.x + b);
+  block_sum<K>(acc);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) tot[k] = acc[k];
+  }
+  return true;
 }
 
 }  // namespace hoefem

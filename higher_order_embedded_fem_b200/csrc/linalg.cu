@@ -39,17 +39,23 @@ __global__ void __launch_bounds__(256) k_spmv(NodeRows A, const double* __restri
     }
   });
   node_sched_finish(A);
+  for_each_diag_dof(A, vals, x, [&](int dof, double v) {
+    y[dof] = ((beta == 0.0) ? 0.0 : beta * y[dof]) + alpha * v;
+  });
 }
 
-// out = ck*K + cm*M (in the reference's order: fill 0, += ck K, += cm M),
-// then Dirichlet rows / columns; diagonal of Dirichlet rows = |first non-zero
-// diagonal| (found by the first pass, see k_first_nonzero_diag).
-__global__ void __launch_bounds__(256) k_combine(NodeRows A, double ck, const double* __restrict__ K, double cm,
+// out = ck*K + cd*D + cm*M (in the reference's order: fill 0, += ck K,
+// += cd D, += cm M), then Dirichlet rows / columns; diagonal of Dirichlet rows
+// = |first non-zero diagonal| (found by the first pass, see
+// k_first_nonzero_diag).
+__global__ void __launch_bounds__(256) k_combine(NodeRows A, double ck, const double* __restrict__ K, double cd,
+                                                 const double* __restrict__ D, double cm,
                                                  const double* __restrict__ M, double* __restrict__ out) {
   const long long nnz = A.base[A.nv];
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nnz; k += (long long)gridDim.x * blockDim.x) {
     double v = 0.0;
     if (K) v += ck * K[k];
+    if (D) v += cd * D[k];
     if (M) v += cm * M[k];
     out[k] = v;
   }
@@ -175,9 +181,10 @@ int autotune_spmv_lanes(NodeRows A, const double* vals, cudaStream_t s, float* b
 }
 
 void jacobian_combination(const Model& m, double ck, const double* K, double cm, const double* M,
-                          const unsigned char* bc_dof, double* out, double* d_scratch, cudaStream_t s) {
+                          const unsigned char* bc_dof, double* out, double* d_scratch, cudaStream_t s, double cd,
+                          const double* D) {
   NodeRows A = m.rows();
-  (note_launch(), k_combine<<<148 * 8, 256, 0, s>>>(A, ck, K, cm, M, out));
+  (note_launch(), k_combine<<<148 * 8, 256, 0, s>>>(A, ck, K, cd, D, cm, M, out));
   if (bc_dof) {
     unsigned long long* first = reinterpret_cast<unsigned long long*>(d_scratch);
     (note_launch(), k_fill_u64<<<1, 1, 0, s>>>(first, ~0ull));

@@ -33,6 +33,8 @@ BlockDev Block::dev() const {
   b.qp = d_qp.p;
   b.emap = d_emap.p;
   b.emat = d_emat.p;
+  b.escene = d_escene.p;
+  b.scene_active = d_escene.p ? scene_active : nullptr;
   return b;
 }
 
@@ -223,6 +225,7 @@ void ensure_device(Model& m) {
       b->d_qoff.upload(qo, s);
     }
     if (!b->emat.empty()) b->d_emat.upload(b->emat, s);
+    if (!b->escene.empty()) b->d_escene.upload(b->escene, s);
   }
   HOEFEM_CUDA(cudaStreamSynchronize(s));
   m.on_device = true;

@@ -33,6 +33,7 @@
 
 #include "internal.h"
 #include "kernels_common.cuh"
+#include "jacobi.cuh"
 #include "solver.h"
 
 namespace hoefem {
@@ -52,6 +53,10 @@ NodeRows Precond::rows() const {
   r.diag_only = d_diag_only.p;
   r.lanes = spmv_lanes;
   r.sched = d_sched.p;
+  r.nodes = d_tnodes.p;
+  r.nnodes = (int)tnodes_count;
+  r.dnodes = d_untreated.p;
+  r.ndnodes = (int)untreated.size();
   return r;
 }
 
@@ -59,14 +64,6 @@ namespace {
 
 constexpr int FACTOR_TPB = 256;
 
-// Jacobi rotation parameters zeroing A[p][q] (same formulas as the oracle).
-__device__ __forceinline__ void jacobi_cs(double app, double aqq, double apq, double& c, double& s) {
-  if (apq == 0.0) { c = 1.0; s = 0.0; return; }
-  double theta = (aqq - app) / (2.0 * apq);
-  double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-  c = 1.0 / sqrt(t * t + 1.0);
-  s = t * c;
-}
 
 // Gauss-Jordan inversion of one SPD principal block per CTA, matrix in
 // registers: thread (ty, tx) owns rows ty + 16 ii and columns tx + 16 jj
@@ -239,67 +236,7 @@ __global__ void __launch_bounds__(FACTOR_TPB) k_schwarz_factor(
   double* out = stage + stage_off[sidx];
 
   // ---- general path: cyclic Jacobi eigen-decomposition -------------------------
-  const int half = m / 2;
-  for (int sweep = 0; sweep < 40; ++sweep) {
-    // convergence test on the off-diagonal mass
-    double off = 0.0, tot = 0.0;
-    for (int k = threadIdx.x; k < m * m; k += blockDim.x) {
-      double x = A[k] * A[k];
-      tot += x;
-      if (k / m != k % m) off += x;
-    }
-    double vv[2] = {off, tot};
-    block_sum<2>(vv);
-    if (threadIdx.x == 0) { s_red[0] = vv[0]; s_red[1] = vv[1]; }
-    __syncthreads();
-    if (s_red[0] == 0.0 || s_red[0] <= 1e-32 * s_red[1]) break;
-    for (int round = 0; round < m - 1; ++round) {
-      for (int k = threadIdx.x; k < half; k += blockDim.x) {
-        int p, q;
-        if (k == 0) { p = round; q = m - 1; }
-        else { p = (round + k) % (m - 1); q = (round - k + (m - 1)) % (m - 1); }
-        if (p > q) { int t = p; p = q; q = t; }
-        double c = 1.0, s = 0.0;
-        if (q < dim) jacobi_cs(A[p * m + p], A[q * m + q], A[p * m + q], c, s);
-        cs[k] = c;
-        sn[k] = s;
-      }
-      __syncthreads();
-      // rows p, q of A
-      for (int it = threadIdx.x; it < half * m; it += blockDim.x) {
-        int k = it / m, j = it % m;
-        double s = sn[k];
-        if (s == 0.0) continue;
-        int p, q;
-        if (k == 0) { p = round; q = m - 1; }
-        else { p = (round + k) % (m - 1); q = (round - k + (m - 1)) % (m - 1); }
-        if (p > q) { int t = p; p = q; q = t; }
-        double c = cs[k];
-        double a = A[p * m + j], b = A[q * m + j];
-        A[p * m + j] = c * a - s * b;
-        A[q * m + j] = s * a + c * b;
-      }
-      __syncthreads();
-      // columns p, q of A and V
-      for (int it = threadIdx.x; it < half * m; it += blockDim.x) {
-        int k = it % half, i = it / half;
-        double s = sn[k];
-        if (s == 0.0) continue;
-        int p, q;
-        if (k == 0) { p = round; q = m - 1; }
-        else { p = (round + k) % (m - 1); q = (round - k + (m - 1)) % (m - 1); }
-        if (p > q) { int t = p; p = q; q = t; }
-        double c = cs[k];
-        double a = A[i * m + p], b = A[i * m + q];
-        A[i * m + p] = c * a - s * b;
-        A[i * m + q] = s * a + c * b;
-        double va = V[i * m + p], vb = V[i * m + q];
-        V[i * m + p] = c * va - s * vb;
-        V[i * m + q] = s * va + c * vb;
-      }
-      __syncthreads();
-    }
-  }
+  jacobi_eigen_block(A, V, cs, sn, m, dim, s_red);
   // spectrum rule of invert_element_block: f = 1/|l| if |l| >= 1e-12 max|l| else 1/(1e-12 max|l|)
   double amax = 0.0;
   for (int k = threadIdx.x; k < dim; k += blockDim.x) amax = fmax(amax, fabs(A[k * m + k]));
@@ -402,6 +339,7 @@ __global__ void k_spmv_plain(NodeRows A, const double* __restrict__ vals, const 
     if (a >= 0 && sl == 0) { y[3 * a] = s0; y[3 * a + 1] = s1; y[3 * a + 2] = s2; }
   });
   node_sched_finish(A);
+  for_each_diag_dof(A, vals, x, [&](int dof, double v) { y[dof] = v; });
 }
 
 }  // namespace
@@ -498,6 +436,13 @@ void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes
   p.d_sub_off.upload(so, st);
   p.d_sub_nodes.upload(sn, st);
   p.d_untreated.upload(un, st);
+  // rows with subdomain entries (or none at all) are visited by the row
+  // kernels; the untreated nodes are applied elementwise
+  std::vector<int> tn;
+  for (i64 a = 0; a < m.nv; ++a)
+    if (!p.diag_only[a]) tn.push_back((int)a);
+  p.tnodes_count = (i64)tn.size();
+  if (!tn.empty()) p.d_tnodes.upload(tn, st);
   p.d_gmap_off.upload(gmap_off, st);
   p.d_gmap.upload(gmap, st);
   p.d_smap.upload(smap, st);

@@ -34,7 +34,11 @@ struct Precond {
   DBuf<int> d_fallback;
   DBuf<unsigned> d_sched;  // SpMV dynamic-scheduling counters of the Schwarz pattern  // [0]: count, [1..]: subdomains for the eigen path
   i64 nnz = 0;
-  int spmv_lanes = 32;
+  int spmv_lanes = 32;   // SpMV variant of the Schwarz apply, FP64 values
+  int spmv_lanes32 = 0;  // FP32 values (0: as spmv_lanes)
+  bool spmv_pinned = false;  // set explicitly by the caller: no autotuning
+  DBuf<int> d_tnodes;      // nodes with subdomain rows (the rest are untreated, diagonal only)
+  i64 tnodes_count = 0;
   NodeRows rows() const;
 };
 
@@ -61,7 +65,19 @@ struct CgWork {
     cudaGraphExec_t exec = nullptr;
     long long kernels = 0;
   };
-  std::vector<Graph> graphs;  // chunk graphs per (operator, preconditioner, precision)
+  std::vector<Graph> graphs;  // chunk graphs per (operator, preconditioner, precision, SpMV variants)
+  // Online choice of the SpMV variants (operator x Schwarz apply) per value
+  // precision: the first chunks of the first solves run one candidate pair
+  // each and are timed; the fastest pair is kept.
+  struct Tuning {
+    int next = 0;  // candidate index to measure next
+    bool done = false;
+    float best_ms = 1e30f;
+    int best = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+  };
+  Tuning tuning[2];  // [0] FP64 values, [1] FP32 values
+  bool online_tuning = true;
   int chunk = 8;
   // called on the host after every chunk of iterations (solver state synced)
   std::function<void(cudaStream_t)> on_chunk;

@@ -140,6 +140,25 @@ class _Model:
                                                   ptr(values)[0], mem))
         return values
 
+    def assemble_projected_stiffness_into_par(self, values, u, material):
+        """values += K(u) with every element matrix projected onto PSD
+        (DefaultSemidefiniteProjection, assembly.rs:549-564)."""
+        mem = _same_space(values, u)
+        check(lib().hoefem_assemble_projected_stiffness_into(self._h, C.byref(material.descriptor()), ptr(u)[0],
+                                                             ptr(values)[0], mem))
+        return values
+
+    def jacobian_combination_damped(self, out, c_stiffness, stiffness, c_damping, damping, c_mass, mass,
+                                    bc_nodes=()):
+        """out = c_k K + c_d D + c_m M (summed in that order), then Dirichlet."""
+        bc = host_i64(bc_nodes)
+        mem = _same_space(out, stiffness, damping, mass)
+        check(lib().hoefem_jacobian_combination_damped(self._h, float(c_stiffness), ptr(stiffness)[0],
+                                                       float(c_damping), ptr(damping)[0], float(c_mass),
+                                                       ptr(mass)[0], bc.ctypes.data if bc.size else None, bc.size,
+                                                       ptr(out)[0], mem))
+        return out
+
     def jacobian_combination(self, out, c_stiffness, stiffness, c_mass, mass, bc_nodes=()):
         bc = host_i64(bc_nodes)
         mem = _same_space(out, stiffness, mass)

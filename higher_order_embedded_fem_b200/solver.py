@@ -71,6 +71,10 @@ class SchwarzPreconditioner(DiagonalPreconditioner):
         self._h = h
         self.num_subdomains = len(subs)
 
+    def set_spmv_variant(self, variant):
+        """8 / 16 / 32 lanes per node, +100 for the column-streaming traversal."""
+        check(lib().hoefem_precond_set_spmv_variant(self._h, int(variant)))
+
     def pattern(self):
         nnz = C.c_int64()
         check(lib().hoefem_precond_nnz(self._h, C.byref(nnz)))
@@ -214,6 +218,13 @@ class NewtonCgIntegrator3d:
 
     def set_tolerances(self, cg_tol=1e-5, cg_max_iter=500, newton_max_iter=100):
         check(lib().hoefem_integrator_set_tolerances(self._h, cg_tol, cg_max_iter, newton_max_iter))
+
+    def set_damping(self, mass=None, stiffness=None):
+        """Rayleigh damping D = mass M + stiffness K_proj(u) per (sub)step;
+        None = no such term (the reference's Option::None)."""
+        check(lib().hoefem_integrator_set_damping(self._h, 0 if mass is None else 1, 0.0 if mass is None else mass,
+                                                  0 if stiffness is None else 1,
+                                                  0.0 if stiffness is None else stiffness))
 
     def set_learned(self, learned, mode=1):
         """mode 1: guarded learned warm start; 2: collect (b, x*) training pairs

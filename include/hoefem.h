@@ -127,7 +127,10 @@ int hoefem_model_set_stream(hoefem_model m, void* stream);
 int hoefem_model_autotune(hoefem_model m, int32_t* lanes);
 /* Selects the SpMV variant explicitly: lanes per node 8, 16 or 32
    (neighbour-major), or 108, 116, 132 (the same lane counts, column-streaming
-   traversal).  hoefem_model_autotune picks the fastest of these. */
+   traversal), for FP64 and FP32 values, and turns the automatic choice off.
+   Otherwise hoefem_model_autotune / integrator set-up time the variants on
+   the SpMV alone, and the first CG solves time candidate pairs (operator,
+   Schwarz apply) chunk by chunk per value precision and keep the fastest. */
 int hoefem_model_set_spmv_variant(hoefem_model m, int32_t variant);
 int hoefem_model_sizes(hoefem_model m, int64_t* ndof, int64_t* nnz, int64_t* num_elements, int64_t* num_blocks);
 /* row_offsets: ndof+1, column_indices: nnz (SparsityPattern, sparse.rs:297-410) */
@@ -155,6 +158,13 @@ int hoefem_assemble_stiffness_into_precision(hoefem_model m, const hoefem_materi
                                              double* values, int precision, int mem);
 /* ElasticityModel::assemble_mass(density).to_csr (solid/mod.rs:106,
    assembly.rs:624-671): values += M on the model pattern. */
+/* assemble_transformed_stiffness_into_par with DefaultSemidefiniteProjection
+   (fenris/src/assembly.rs:549-564; compute_stiffness_matrix_into with
+   projected = true, simulation_toolbox/src/fem/system_assembly.rs:107-142):
+   every element matrix is eigen-decomposed and its negative eigenvalues set
+   to zero before the colored scatter.  Adds into values. */
+int hoefem_assemble_projected_stiffness_into(hoefem_model m, const hoefem_material* mat, const double* u,
+                                             double* values, int mem);
 int hoefem_assemble_mass_into(hoefem_model m, double density, double* values, int mem);
 /* apply_homogeneous_dirichlet_bc_csr (fenris/src/assembly.rs:799-869) on
    values of the model pattern; nodes are host indices. */
@@ -184,6 +194,13 @@ int hoefem_jacobian_combination(hoefem_model m, double c_stiffness, const double
 int hoefem_jacobian_combination_noalloc(hoefem_model m, double c_stiffness, const double* stiffness_values,
                                         double c_mass, const double* mass_values, const int64_t* bc_nodes,
                                         int64_t num_bc, double* out);
+/* compute_jacobian_combination_into with a damping matrix
+   (system_assembly.rs:196-235): out = c_stiffness K + c_damping D + c_mass M
+   (summed in that order; any array may be NULL), then Dirichlet as above. */
+int hoefem_jacobian_combination_damped(hoefem_model m, double c_stiffness, const double* stiffness_values,
+                                       double c_damping, const double* damping_values, double c_mass,
+                                       const double* mass_values, const int64_t* bc_nodes, int64_t num_bc,
+                                       double* out, int mem);
 /* spmv_csr (fenris/src/sparse.rs:1164-1199) / LinearOperator::apply for the
    model pattern (cg.rs:15-17): y = beta*y + alpha*A x. */
 int hoefem_spmv(hoefem_model m, double beta, double* y, double alpha, const double* values, const double* x, int mem);
@@ -208,6 +225,10 @@ int hoefem_precond_update(hoefem_precond p, const double* system_values, int mem
 int hoefem_precond_apply(hoefem_precond p, const double* r, double* z, int mem);
 /* Schwarz pattern / values for inspection (nnz first, then the arrays). */
 int hoefem_precond_nnz(hoefem_precond p, int64_t* nnz);
+/* SpMV variant of the Schwarz apply (as hoefem_model_set_spmv_variant);
+   chosen by the autotuner at creation and by the CG's online choice
+   otherwise. */
+int hoefem_precond_set_spmv_variant(hoefem_precond p, int32_t variant);
 int hoefem_precond_pattern(hoefem_precond p, int64_t* row_offsets, int64_t* column_indices);
 int hoefem_precond_values(hoefem_precond p, double* values /* host */);
 int hoefem_precond_destroy(hoefem_precond p);
@@ -272,6 +293,14 @@ int hoefem_integrator_create(hoefem_model m, const hoefem_material* mat, double 
    newton_max_iter 100 (newton_cg.rs:282-286,761-773). */
 int hoefem_integrator_set_tolerances(hoefem_integrator it, double cg_tol, int64_t cg_max_iter,
                                      int64_t newton_max_iter);
+/* Rayleigh damping of the material (MaterialComponent mass / stiffness
+   damping coefficients, newton_cg.rs:90-100): at the start of every
+   (sub)step D = mass_coeff M + stiffness_coeff K_proj(u) with the element-wise
+   PSD-projected stiffness (compute_damping_matrix_into,
+   system_assembly.rs:145-193); f gains -D v and the Jacobian dt D.  has_* = 0
+   is the reference's None.  Default: no damping. */
+int hoefem_integrator_set_damping(hoefem_integrator it, int has_mass, double mass_coeff, int has_stiffness,
+                                  double stiffness_coeff);
 /* Arithmetic of the step.  HOEFEM_PRECISION_FP64: the reference's FP64
    everywhere.  HOEFEM_PRECISION_MIXED: element stiffness arithmetic in FP32
    (CSR accumulation FP64), Schwarz blocks built in FP64 and applied in FP32,

@@ -885,6 +885,54 @@ static void invert_block(int n, std::vector<double>& A, std::vector<double>& out
     }
 }
 
+// DefaultSemidefiniteProjection (fenris/src/assembly.rs:549-564): symmetric
+// eigen-decomposition, negative eigenvalues set to zero, recomposed.
+static void psd_project(int n, double* Ke) {
+  std::vector<double> A(Ke, Ke + n * n), V, lam;
+  jacobi_eigen(n, A, V, lam);
+  for (double& l : lam) l = std::max(0.0, l);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < n; ++k) s += V[i * n + k] * lam[k] * V[j * n + k];
+      Ke[i * n + j] = s;
+    }
+}
+
+// assemble_transformed_stiffness_into_par with DefaultSemidefiniteProjection
+// (system_assembly.rs:107-142 with projected = true): every element matrix is
+// projected before the colored scatter.  Adds into v.
+static bool assemble_stiffness_projected(const Model& m, const Material& mat, const double* u, double* v) {
+  bool ok = true;
+  for (const Block& b : m.blocks) {
+    const int n = element_nodes(b.kind);
+    for (const auto& color : b.colors) {
+#pragma omp parallel for schedule(dynamic, 4)
+      for (i64 ci = 0; ci < (i64)color.size(); ++ci) {
+        i64 e = color[ci];
+        double Xe[27 * 3], ue[3 * 27];
+        std::vector<double> Ke(9 * n * n);
+        gather_element(m, b, e, u, Xe, ue);
+        if (!element_stiffness(b.kind, Xe, ue, b.quad.rule(e), mat, Ke.data())) {
+#pragma omp atomic write
+          ok = false;
+          continue;
+        }
+        psd_project(3 * n, Ke.data());
+        const auto& c = b.conn[e];
+        int perm[27];
+        std::iota(perm, perm + n, 0);
+        std::sort(perm, perm + n, [&](int a, int bb) { return c[a] < c[bb]; });
+        for (int I = 0; I < n; ++I)
+          for (int i = 0; i < 3; ++i)
+            add_element_row(m.pattern, v, 3 * c[I] + i, c.data(), perm, n, 3, Ke.data() + (3 * I + i) * 3 * n);
+      }
+      if (!ok) return false;
+    }
+  }
+  return ok;
+}
+
 struct Schwarz {
   std::vector<std::vector<i64>> subdomains;  // node lists
   std::vector<i64> untreated;                // sorted node indices
@@ -1040,6 +1088,12 @@ struct Scene {
   i64 cg_max_iter = 500;
   i64 newton_max_iter = 100;
   double newton_tol_factor = 1e-5;
+  // damping D = gamma M + alpha K_proj(u), recomputed at the start of every
+  // (sub)step (compute_damping_matrix_into, system_assembly.rs:145-193)
+  bool has_mass_damping = false, has_stiffness_damping = false;
+  double mass_damping = 0.0, stiffness_damping = 0.0;
+  bool has_damping = false;
+  std::vector<double> damping;
   // statistics of the last step
   std::vector<i64> cg_iters;
   std::vector<int> cg_status;
@@ -1081,14 +1135,33 @@ static void scene_setup(Scene& s) {
   }
 }
 
-// NewtonCgDynamicSystem::eval_f (newton_cg.rs:441-478), no damping.
+// NewtonCgDynamicSystem::eval_f (newton_cg.rs:441-478):
+//   f = M g + f_int(u) - D v, Dirichlet rows zeroed.
 static bool eval_f(Scene& s, const double* u_in, const double* v_in, double* f) {
   const i64 n = s.model.pattern.nrows;
   std::vector<double> u(u_in, u_in + n), v(v_in, v_in + n);
   std::copy(s.g_force.begin(), s.g_force.end(), f);
   apply_bc_unknowns(s, u.data(), v.data());
   if (!assemble_forces(s.model, s.mat, u.data(), f)) return false;
+  if (s.has_damping) spmv(1.0, f, -1.0, s.model.pattern, s.damping.data(), v.data());
   for (i64 i = 0; i < n; ++i) if (s.bc_dof[i]) f[i] = 0.0;
+  return true;
+}
+
+// compute_damping_matrix_into (system_assembly.rs:145-193): K projected at u
+// (no boundary conditions applied to u or D), then D = 0 + alpha K + gamma M
+// in the order of compute_jacobian_combination_into (stiffness, then mass).
+static bool compute_damping(Scene& s, const double* u) {
+  s.has_damping = s.has_mass_damping || s.has_stiffness_damping;
+  if (!s.has_damping) return true;
+  const Pattern& p = s.model.pattern;
+  std::vector<double> K(p.col_indices.size(), 0.0);
+  if (s.has_stiffness_damping && !assemble_stiffness_projected(s.model, s.mat, u, K.data())) return false;
+  s.damping.assign(p.col_indices.size(), 0.0);
+  if (s.has_stiffness_damping)
+    for (size_t k = 0; k < K.size(); ++k) s.damping[k] += s.stiffness_damping * K[k];
+  if (s.has_mass_damping)
+    for (size_t k = 0; k < K.size(); ++k) s.damping[k] += s.mass_damping * s.mass[k];
   return true;
 }
 
@@ -1115,10 +1188,15 @@ static int solve_jacobian(Scene& s, const std::vector<double>& up, const std::ve
   apply_bc_unknowns(s, u.data(), v.data());
   std::vector<double> K(p.col_indices.size(), 0.0);
   if (!assemble_stiffness(s.model, s.mat, u.data(), K.data())) return STEP_ASSEMBLY_ERROR;
-  // J = gamma M - beta D - alpha K with alpha = -dt^2, gamma = 1 (no damping)
+  // J = gamma M - beta D - alpha K with alpha = -dt^2, beta = -dt, gamma = 1
+  // (euler.rs:136), accumulated in the order stiffness, damping, mass
   std::vector<double> J(p.col_indices.size(), 0.0);
   double ck = -(-dt * dt);
   for (size_t k = 0; k < J.size(); ++k) J[k] += ck * K[k];
+  if (s.has_damping) {
+    double cd = -(-dt);
+    for (size_t k = 0; k < J.size(); ++k) J[k] += cd * s.damping[k];
+  }
   for (size_t k = 0; k < J.size(); ++k) J[k] += 1.0 * s.mass[k];
   dirichlet_csr(p, J.data(), s.bc_nodes.data(), (i64)s.bc_nodes.size(), 3);
   LinOp A = [&](double* y, const double* x) { spmv(0.0, y, 1.0, p, J.data(), x); return true; };
@@ -1210,7 +1288,9 @@ static int integrate(Scene& s, double* u, double* v, double t, double dt) {
     bool failed = false;
     for (i64 k = 0; k < num; ++k) {
       double st = t + (double)k * sdt;
-      int r = backward_euler_step(s, us.data(), vs.data(), st, sdt);
+      // integrate_model: damping from the substep's initial state, then the step
+      int r = compute_damping(s, us.data()) ? backward_euler_step(s, us.data(), vs.data(), st, sdt)
+                                            : STEP_ASSEMBLY_ERROR;
       if (r == STEP_OK) apply_bc_unknowns(s, us.data(), vs.data());
       else { failed = true; break; }
     }
@@ -1745,6 +1825,24 @@ void oracle_scene_set_gravity(void* sp, int enabled, double g) {
   auto* s = (Scene*)sp;
   s->gravity_enabled = enabled != 0;
   s->gravity = g;
+}
+void oracle_scene_set_damping(void* sp, int has_mass, double mass_coeff, int has_stiffness, double stiffness_coeff) {
+  auto* s = (Scene*)sp;
+  s->has_mass_damping = has_mass != 0;
+  s->mass_damping = mass_coeff;
+  s->has_stiffness_damping = has_stiffness != 0;
+  s->stiffness_damping = stiffness_coeff;
+}
+// Damping matrix at state u (after set_damping and setup); returns 0 on success.
+int oracle_scene_damping(void* sp, const double* u, double* out) {
+  auto* s = (Scene*)sp;
+  if (!compute_damping(*s, u)) return 1;
+  if (s->has_damping) std::copy(s->damping.begin(), s->damping.end(), out);
+  return 0;
+}
+int oracle_scene_assemble_stiffness_projected(void* sp, const double* u, double* v) {
+  auto* s = (Scene*)sp;
+  return assemble_stiffness_projected(s->model, s->mat, u, v) ? 0 : 1;
 }
 void oracle_scene_set_solver(void* sp, double cg_tol, int64_t cg_max_iter, int64_t newton_max_iter) {
   auto* s = (Scene*)sp;

@@ -80,6 +80,9 @@ def lib():
             "oracle_scene_set_bc": (None, [vp, i64p, C.c_int64]),
             "oracle_scene_set_gravity": (None, [vp, C.c_int, C.c_double]),
             "oracle_scene_set_solver": (None, [vp, C.c_double, C.c_int64, C.c_int64]),
+            "oracle_scene_set_damping": (None, [vp, C.c_int, C.c_double, C.c_int, C.c_double]),
+            "oracle_scene_damping": (C.c_int, [vp, f64p, f64p]),
+            "oracle_scene_assemble_stiffness_projected": (C.c_int, [vp, f64p, f64p]),
             "oracle_scene_set_schwarz": (None, [vp, i64p, i64p, C.c_int64, i64p, C.c_int64]),
             "oracle_scene_setup": (C.c_int, [vp]),
             "oracle_scene_mass": (None, [vp, f64p]),
@@ -397,6 +400,26 @@ class Scene:
         if lib().oracle_scene_schwarz_update(self._h, f64(jv), pv):
             raise ArithmeticError("schwarz update failed")
         return pv
+
+    def stiffness_projected(self, u):
+        """Stiffness with every element matrix projected onto PSD (eigenvalues
+        clamped at zero) before the scatter."""
+        v = np.zeros(self.nnz)
+        if lib().oracle_scene_assemble_stiffness_projected(self._h, f64(u), v):
+            raise ArithmeticError("stiffness assembly failed")
+        return v
+
+    def set_damping(self, mass=None, stiffness=None):
+        """D = mass * M + stiffness * K_proj(u) at the start of every (sub)step;
+        None = term absent (Option::None in the reference)."""
+        lib().oracle_scene_set_damping(self._h, 0 if mass is None else 1, 0.0 if mass is None else float(mass),
+                                       0 if stiffness is None else 1, 0.0 if stiffness is None else float(stiffness))
+
+    def damping(self, u):
+        d = np.zeros(self.nnz)
+        if lib().oracle_scene_damping(self._h, f64(u), d):
+            raise ArithmeticError("damping assembly failed")
+        return d
 
     def jacobian(self, K, dt):
         J = np.zeros(self.nnz)
