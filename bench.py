@@ -321,6 +321,9 @@ def run_hoefem(args):
                                     "learned_rejected": int(s_["learned_rejected"]),
                                     "learned_residual_ratio": s_["learned_residual_ratio"],
                                     "ms_learned": s_["ms_learned"], "training": learned_info})
+    op64, op32 = model.spmv_variants()
+    pr64, pr32 = P.spmv_variants()
+    spmv_variants = {"operator_fp64": op64, "operator_fp32": op32, "schwarz_fp64": pr64, "schwarz_fp32": pr32}
     head = "learned" if "learned" in variants else ("mixed" if "mixed" in variants else list(variants)[0])
     ms = variants[head]["ms_per_step"]
     launches = variants[head]["gpu_launches"]
@@ -382,6 +385,7 @@ def run_hoefem(args):
             "cg_iterations": variants[head]["cg_iterations"], "newton_iterations": variants[head]["newton_iterations"],
             "speedup_vs_plain_fp64": (variants["plain"]["ms_per_step"] / ms) if "plain" in variants else None,
             "roofline": roof,
+            "spmv_variants": spmv_variants,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * 8 * model.ndof(),
                     "d2h_bytes_per_step": 2 * 8 * model.ndof()},

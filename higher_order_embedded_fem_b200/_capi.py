@@ -94,6 +94,8 @@ SIGNATURES = {
     "hoefem_precond_update": (C.c_int, [vp, vp, C.c_int]),
     "hoefem_precond_apply": (C.c_int, [vp, vp, vp, C.c_int]),
     "hoefem_precond_set_spmv_variant": (C.c_int, [vp, C.c_int32]),
+    "hoefem_precond_get_spmv_variants": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "hoefem_model_get_spmv_variants": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "hoefem_precond_nnz": (C.c_int, [vp, pi64]),
     "hoefem_precond_pattern": (C.c_int, [vp, vp, vp]),
     "hoefem_precond_values": (C.c_int, [vp, vp]),

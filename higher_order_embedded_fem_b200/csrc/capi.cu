@@ -267,6 +267,14 @@ int hoefem_model_set_spmv_variant(hoefem_model m, int32_t variant) {
   API_END
 }
 
+int hoefem_model_get_spmv_variants(hoefem_model m, int32_t* fp64_values, int32_t* fp32_values) {
+  API_BEGIN
+  Model& mm = model_of(m);
+  if (fp64_values) *fp64_values = mm.spmv_lanes;
+  if (fp32_values) *fp32_values = mm.spmv_lanes32 ? mm.spmv_lanes32 : mm.spmv_lanes;
+  API_END
+}
+
 int hoefem_model_sizes(hoefem_model m, int64_t* ndof, int64_t* nnz, int64_t* num_elements, int64_t* num_blocks) {
   API_BEGIN
   Model& mm = model_of(m);
@@ -519,6 +527,14 @@ int hoefem_precond_set_spmv_variant(hoefem_precond p, int32_t variant) {
   p->p.spmv_lanes = variant;
   p->p.spmv_lanes32 = variant;
   p->p.spmv_pinned = true;
+  API_END
+}
+
+int hoefem_precond_get_spmv_variants(hoefem_precond p, int32_t* fp64_values, int32_t* fp32_values) {
+  API_BEGIN
+  HOEFEM_REQUIRE(p, HOEFEM_ERR_INVALID_ARGUMENT, "null preconditioner");
+  if (fp64_values) *fp64_values = p->p.spmv_lanes;
+  if (fp32_values) *fp32_values = p->p.spmv_lanes32 ? p->p.spmv_lanes32 : p->p.spmv_lanes;
   API_END
 }
 

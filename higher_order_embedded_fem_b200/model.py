@@ -69,6 +69,12 @@ class _Model:
         check(lib().hoefem_model_autotune(self._h, C.byref(lanes)))
         return lanes.value
 
+    def spmv_variants(self):
+        """(FP64-value variant, FP32-value variant) in use."""
+        a, b = C.c_int32(), C.c_int32()
+        check(lib().hoefem_model_get_spmv_variants(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def set_spmv_variant(self, variant):
         """8 / 16 / 32 lanes per node, +100 for the column-streaming traversal."""
         check(lib().hoefem_model_set_spmv_variant(self._h, int(variant)))

@@ -75,6 +75,12 @@ class SchwarzPreconditioner(DiagonalPreconditioner):
         """8 / 16 / 32 lanes per node, +100 for the column-streaming traversal."""
         check(lib().hoefem_precond_set_spmv_variant(self._h, int(variant)))
 
+    def spmv_variants(self):
+        """(FP64-value variant, FP32-value variant) in use."""
+        a, b = C.c_int32(), C.c_int32()
+        check(lib().hoefem_precond_get_spmv_variants(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def pattern(self):
         nnz = C.c_int64()
         check(lib().hoefem_precond_nnz(self._h, C.byref(nnz)))

@@ -132,6 +132,8 @@ int hoefem_model_autotune(hoefem_model m, int32_t* lanes);
    the SpMV alone, and the first CG solves time candidate pairs (operator,
    Schwarz apply) chunk by chunk per value precision and keep the fastest. */
 int hoefem_model_set_spmv_variant(hoefem_model m, int32_t variant);
+/* The SpMV variants in use for FP64 and FP32 operator values. */
+int hoefem_model_get_spmv_variants(hoefem_model m, int32_t* fp64_values, int32_t* fp32_values);
 int hoefem_model_sizes(hoefem_model m, int64_t* ndof, int64_t* nnz, int64_t* num_elements, int64_t* num_blocks);
 /* row_offsets: ndof+1, column_indices: nnz (SparsityPattern, sparse.rs:297-410) */
 int hoefem_model_pattern(hoefem_model m, int64_t* row_offsets, int64_t* column_indices);
@@ -229,6 +231,7 @@ int hoefem_precond_nnz(hoefem_precond p, int64_t* nnz);
    chosen by the autotuner at creation and by the CG's online choice
    otherwise. */
 int hoefem_precond_set_spmv_variant(hoefem_precond p, int32_t variant);
+int hoefem_precond_get_spmv_variants(hoefem_precond p, int32_t* fp64_values, int32_t* fp32_values);
 int hoefem_precond_pattern(hoefem_precond p, int64_t* row_offsets, int64_t* column_indices);
 int hoefem_precond_values(hoefem_precond p, double* values /* host */);
 int hoefem_precond_destroy(hoefem_precond p);
