@@ -55,8 +55,9 @@ def parse():
     ap.add_argument("--train-states", type=int, default=16, help="learned: training initial states (seeded)")
     ap.add_argument("--train-steps", type=int, default=2000, help="learned: Adam steps")
     ap.add_argument("--coarse-subdomains", type=int, default=256, help="learned: coarse subdomains")
-    ap.add_argument("--workload", default="cylinder", choices=["cylinder", "batched"],
-                    help="cylinder: embedded Hex27 cylinder Newton step; batched: 64 independent scenes in one batch")
+    ap.add_argument("--workload", default="cylinder", choices=["cylinder", "batched", "tet10"],
+                    help="cylinder: embedded Hex27 cylinder Newton step; batched: 64 independent scenes in one "
+                         "batch; tet10: 201,600-element Tet10 box, plain vs mixed precision")
     ap.add_argument("--scenes", type=int, default=64, help="batched: number of scenes")
     ap.add_argument("--min-elements", type=float, default=1e3, help="batched: smallest scene (elements)")
     ap.add_argument("--max-elements", type=float, default=5e4, help="batched: largest scene (elements)")
@@ -590,12 +591,86 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+def run_tet10(args):
+    """Mixed precision at scale: Tet10 box 40 x 40 x 21 cells of h = 0.025
+    (201,600 elements, 6 Tet10 per hex), SNH E = 1e6 nu = 0.4, bottom
+    clamped, u0 ~ N(0, (0.02 h)^2), v0 = 0; one backward-Euler Newton step
+    (diagonal PCG, the reference's choice without a Schwarz component) in
+    FP64 and in the mixed form; element stiffness / force errors against the
+    FP64 oracle at u0."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    import higher_order_embedded_fem_b200 as H
+
+    s = H.scenes.tet10_box(0.025, 40, 40, 21, 1)
+    b = s.blocks[0]
+    model = H.NodalModel3d(s.vertices, b.connectivity, (b.weights, b.points))
+    mat = H.StableNeoHookeanMaterial(H.YoungPoisson(1e6, 0.4))
+    bc = s.nodes_below(2, 1e-9)
+    u0 = H.scenes.random_normal(args.seed, model.ndof(), 0.02 * 0.025)
+    v0 = np.zeros(model.ndof())
+    stream = torch.cuda.current_stream(dev)
+    model.set_stream(stream.cuda_stream)
+    integ = H.NewtonCgIntegrator3d(model, mat, 1000.0, bc)
+    integ.set_tolerances(args.cg_tol, args.cg_max_iter, 100)
+    u0d, v0d = torch.from_numpy(u0).to(dev), torch.from_numpy(v0).to(dev)
+    out = {}
+    for vname in ("plain", "mixed"):
+        integ.set_precision(vname == "mixed", args.delta)
+        for _ in range(args.warmup):
+            integ.step(u0d.clone(), v0d.clone(), 0.0, DT)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ud, vd = u0d.clone(), v0d.clone()
+            st = integ.step(ud, vd, 0.0, DT)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        out[vname] = {"ms_per_step": ev0.elapsed_time(ev1) / args.steps, "cg_iterations": int(st["total_cg_iterations"]),
+                      "newton_iterations": int(st["newton_iterations"]),
+                      "phase_ms": {"forces": st["ms_assemble_forces"], "stiffness": st["ms_assemble_stiffness"],
+                                   "cg": st["ms_cg"], "total": st["ms_total"]},
+                      "u": ud.cpu().numpy()}
+    up, um = out["plain"].pop("u"), out["mixed"].pop("u")
+    out["mixed"]["rel_diff_u_vs_plain"] = float(np.abs(um - up).max() / np.abs(up).max())
+    # element arithmetic errors at u0 against the FP64 oracle (host arrays)
+    K64 = model.assemble_stiffness_into_par(np.zeros(model.nnz), u0, mat)
+    K32 = model.assemble_stiffness_into_precision(np.zeros(model.nnz), u0, mat, True)
+    f64 = model.assemble_elastic_pseudo_forces_into_par(np.zeros(model.ndof()), u0, mat)
+    errs = {"stiffness_fp32_vs_fp64_gpu": float(np.abs(K32 - K64).max() / np.abs(K64).max())}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        ref = O.Scene(s.vertices)
+        ref.add_block(O.ELEM_TET10, b.connectivity, b.weights, b.points)
+        ref.finalize_pattern()
+        ref.set_material(O.MAT_SNH, mat.lame.mu, mat.lame.lam, 1000.0)
+        Kr = ref.stiffness(u0)
+        fr = ref.forces(u0)
+        errs.update({"stiffness_fp64_vs_oracle": float(np.abs(K64 - Kr).max() / np.abs(Kr).max()),
+                     "stiffness_fp32_vs_oracle": float(np.abs(K32 - Kr).max() / np.abs(Kr).max()),
+                     "forces_fp64_vs_oracle": float(np.abs(f64 - fr).max() / np.abs(fr).max())})
+    line = {"metric": "Newton-step ms, plain FP64 vs mixed, Tet10 box 201,600 elements, 1 GPU",
+            "value": out["mixed"]["ms_per_step"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "dtype": "f64/f32", "data": "synthetic (seeded)",
+            "config": {"workload": "Tet10 box 40x40x21 cells h=0.025 x6 tets, SNH E=1e6 nu=0.4, u0 ~ N(0,(0.02h)^2), "
+                                   "one BE Newton step dt=1e-3, diagonal PCG to %g" % args.cg_tol,
+                       "elements": int(model.num_elements), "ndof": int(model.ndof()), "nnz": int(model.nnz)},
+            "variants": out, "speedup_mixed_vs_plain": out["plain"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+            "errors": errs}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "tet10":
+        run_tet10(args)
     elif args.roofline_only:
         run_roofline_only(args)
     else:
