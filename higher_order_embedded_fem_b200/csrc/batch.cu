@@ -45,28 +45,76 @@ struct SegCg {
   int status;
 };
 
-// ---- per-scene segmented sums: one block per scene over nodes [lo, hi) ---------
+// ---- node chunks --------------------------------------------------------------
+// Every scene's node range is split into chunks of at most CHN nodes; chunk c
+// covers nodes [clo[c], clo[c + 1]) of scene cscene[c] and scene s owns chunks
+// [cs_off[s], cs_off[s + 1]).  The CG kernels run one CTA per chunk: a CTA
+// whose scene has finished returns at once, so an iteration costs what the
+// active scenes need (no node scan, no shared work counter), and each CTA
+// writes its chunk's partial sums cpart[k * nch + c].  The per-scene sums add
+// a scene's chunk partials in chunk order: deterministic, and independent of
+// the other scenes.
+constexpr int CHN = 256;
+
+struct Chunks {
+  const int* lo;     // nch + 1
+  const int* scene;  // nch
+  const int* cs_off;  // nscene + 1
+  int n;
+};
+
+// The chunk's nodes with LaneCfg<L>::lanes lanes per node: body(a, sl), a = -1
+// for lanes without a node (all lanes of a warp take part).
+template <int L, class F>
+__device__ __forceinline__ void for_chunk_nodes(int lo, int hi, F&& body) {
+  constexpr int LNS = LaneCfg<L>::lanes;
+  constexpr int G = 32 / LNS;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int grp = lane / LNS, sl = lane % LNS;
+  for (int a0 = lo + w * G; a0 < hi; a0 += nw * G) {
+    const int a = a0 + grp;
+    body(a < hi ? a : -1, sl);
+  }
+}
+
 template <int K>
-__device__ __forceinline__ void seg_sum(const double* __restrict__ t, int nv, int lo, int hi, double (&out)[K]) {
+__device__ __forceinline__ void chunk_store(double (&acc)[K], double* __restrict__ cpart, int nch) {
+  block_sum<K>(acc);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) cpart[(size_t)k * nch + blockIdx.x] = acc[k];
+}
+
+// per-scene sums of the chunk partials (block per scene, fixed order)
+template <int K>
+__device__ __forceinline__ void scene_sum(const Chunks ch, const double* __restrict__ cpart, int s,
+                                          double (&out)[K]) {
   double acc[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) acc[k] = 0.0;
-  for (int a = lo + threadIdx.x; a < hi; a += blockDim.x)
+  for (int c = ch.cs_off[s] + threadIdx.x; c < ch.cs_off[s + 1]; c += blockDim.x)
 #pragma unroll
-    for (int k = 0; k < K; ++k) acc[k] += t[(size_t)k * nv + a];
+    for (int k = 0; k < K; ++k) acc[k] += cpart[(size_t)k * ch.n + c];
   block_sum<K>(acc);
 #pragma unroll
   for (int k = 0; k < K; ++k) out[k] = acc[k];
 }
 
-// mode 0: init (b.b, r.r) ; 1: zTr init ; 2: pAp -> alpha ; 3: (r.r, z.r) -> convergence, beta
-__global__ void k_seg_finalize(int mode, int nv, const int* __restrict__ node_off, const double* __restrict__ t,
-                               SegCg* st, double tol, long long max_iter) {
+// mode 0: init (b.b, r.r) ; 1: zTr init ; 2: pAp -> alpha ; 3: (r.r, z.r) -> convergence, beta.
+// Scenes already finished (or masked out) keep their state.
+__global__ void k_seg_finalize(int mode, const Chunks ch, const double* __restrict__ cpart, SegCg* st, double tol,
+                               long long max_iter) {
   const int s = blockIdx.x;
   SegCg& c = st[s];
-  if (mode >= 2 && c.done) return;
+  if (c.done) {
+    if (mode == 1 && threadIdx.x == 0) {
+      c.iters = 0;
+      c.status = HOEFEM_OK;
+    }
+    return;
+  }
   double v[2];
-  seg_sum<2>(t, nv, node_off[s], node_off[s + 1], v);
+  scene_sum<2>(ch, cpart, s, v);
   if (threadIdx.x != 0) return;
   if (mode == 0) {
     c.bnorm = sqrt(v[0]);
@@ -75,7 +123,6 @@ __global__ void k_seg_finalize(int mode, int nv, const int* __restrict__ node_of
     c.zTr = v[0];
     c.iters = 0;
     c.status = HOEFEM_OK;
-    if (c.done) return;  // masked scene
     if (c.bnorm == 0.0) { c.done = 2; return; }
     if (sqrt(c.rr) <= tol * c.bnorm) { c.done = 1; return; }
     if (max_iter >= 0 && c.iters >= max_iter) { c.done = 1; c.status = HOEFEM_CG_MAX_ITERATIONS; }
@@ -96,119 +143,116 @@ __global__ void k_seg_finalize(int mode, int nv, const int* __restrict__ node_of
   }
 }
 
-// r = b - A x, per node t0 = b.b, t1 = r.r
+// r = b - A x ; chunk partials b.b, r.r
 template <int L>
 __global__ void __launch_bounds__(TPB) k_seg_init(NodeRows A, const double* __restrict__ vals,
                                                   const double* __restrict__ x, const double* __restrict__ b,
-                                                  double* __restrict__ r, double* __restrict__ t) {
-  for_each_node<L>(A, [&](int a, int sl) {
+                                                  double* __restrict__ r, const Chunks ch, const SegCg* __restrict__ st,
+                                                  double* __restrict__ cpart) {
+  const int c = blockIdx.x;
+  if (st[ch.scene[c]].done) return;
+  double acc[2] = {0.0, 0.0};
+  for_chunk_nodes<L>(ch.lo[c], ch.lo[c + 1], [&](int a, int sl) {
     double s[3];
     node_row_dot<L>(A, vals, x, a, sl, s[0], s[1], s[2]);
     if (a >= 0 && sl == 0) {
-      double bb = 0, rr = 0;
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
         double bi = b[3 * a + i], ri = bi - s[i];
         r[3 * a + i] = ri;
-        bb += bi * bi;
-        rr += ri * ri;
+        acc[0] += bi * bi;
+        acc[1] += ri * ri;
       }
-      t[a] = bb;
-      t[A.nv + a] = rr;
     }
   });
-  node_sched_finish(A);
+  chunk_store<2>(acc, cpart, ch.n);
 }
 
-// z = d r, p = z, per node t0 = z.r
-__global__ void k_seg_prec0(int nv, const double* __restrict__ d, const double* __restrict__ r, double* __restrict__ z,
-                            double* __restrict__ p, double* __restrict__ t) {
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nv; a += gridDim.x * blockDim.x) {
-    double acc = 0;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      double zi = d[3 * a + i] * r[3 * a + i];
-      z[3 * a + i] = zi;
-      p[3 * a + i] = zi;
-      acc += zi * r[3 * a + i];
-    }
-    t[a] = acc;
-    t[nv + a] = 0.0;
+// z = d r, p = z ; chunk partials z.r
+__global__ void __launch_bounds__(TPB) k_seg_prec0(const Chunks ch, const SegCg* __restrict__ st,
+                                                   const double* __restrict__ d, const double* __restrict__ r,
+                                                   double* __restrict__ z, double* __restrict__ p,
+                                                   double* __restrict__ cpart) {
+  const int c = blockIdx.x;
+  if (st[ch.scene[c]].done) return;
+  double acc[2] = {0.0, 0.0};
+  for (int k = 3 * ch.lo[c] + threadIdx.x; k < 3 * ch.lo[c + 1]; k += blockDim.x) {
+    double zi = d[k] * r[k];
+    z[k] = zi;
+    p[k] = zi;
+    acc[0] += zi * r[k];
   }
+  chunk_store<2>(acc, cpart, ch.n);
 }
 
+// Ap = A p ; chunk partials p.Ap
 template <int L>
 __global__ void __launch_bounds__(TPB) k_seg_Ap(NodeRows A, const double* __restrict__ vals,
-                                                const double* __restrict__ p, double* __restrict__ Ap,
-                                                const int* __restrict__ scene_of, const SegCg* __restrict__ st,
-                                                double* __restrict__ t) {
-  for_each_node<L>(A, [&](int a, int sl) {
-    const bool skip = a >= 0 && st[scene_of[a]].done;
+                                                const double* __restrict__ p, double* __restrict__ Ap, const Chunks ch,
+                                                const SegCg* __restrict__ st, double* __restrict__ cpart) {
+  const int c = blockIdx.x;
+  if (st[ch.scene[c]].done) return;
+  double acc[2] = {0.0, 0.0};
+  for_chunk_nodes<L>(ch.lo[c], ch.lo[c + 1], [&](int a, int sl) {
     double s[3];
-    node_row_dot<L>(A, vals, p, skip ? -1 : a, sl, s[0], s[1], s[2]);
+    node_row_dot<L>(A, vals, p, a, sl, s[0], s[1], s[2]);
     if (a >= 0 && sl == 0) {
-      double acc = 0;
-      if (!skip) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          Ap[3 * a + i] = s[i];
-          acc += p[3 * a + i] * s[i];
-        }
-      }
-      t[a] = acc;
-      t[A.nv + a] = 0.0;
-    }
-  });
-  node_sched_finish(A);
-}
-
-__global__ void k_seg_update(int nv, const int* __restrict__ scene_of, const SegCg* __restrict__ st,
-                             const double* __restrict__ d, double* __restrict__ x, double* __restrict__ r,
-                             const double* __restrict__ p, const double* __restrict__ Ap, double* __restrict__ z,
-                             double* __restrict__ t) {
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nv; a += gridDim.x * blockDim.x) {
-    const SegCg& c = st[scene_of[a]];
-    double rr = 0, zr = 0;
-    if (!c.done) {
-      const double al = c.alpha;
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
-        const int k = 3 * a + i;
-        x[k] = x[k] + al * p[k];
-        double ri = r[k] - al * Ap[k];
-        r[k] = ri;
-        double zi = d[k] * ri;
-        z[k] = zi;
-        rr += ri * ri;
-        zr += zi * ri;
+        Ap[3 * a + i] = s[i];
+        acc[0] += p[3 * a + i] * s[i];
       }
     }
-    t[a] = rr;
-    t[nv + a] = zr;
-  }
+  });
+  chunk_store<2>(acc, cpart, ch.n);
 }
 
-__global__ void k_seg_p(int nv, const int* __restrict__ scene_of, const SegCg* __restrict__ st,
-                        const double* __restrict__ z, double* __restrict__ p) {
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nv; a += gridDim.x * blockDim.x) {
-    const SegCg& c = st[scene_of[a]];
-    if (c.done) continue;
-    const double be = c.beta;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) p[3 * a + i] = z[3 * a + i] + be * p[3 * a + i];
+// x += alpha p ; r -= alpha Ap ; z = d r ; chunk partials r.r, z.r
+__global__ void __launch_bounds__(TPB) k_seg_update(const Chunks ch, const SegCg* __restrict__ st,
+                                                    const double* __restrict__ d, double* __restrict__ x,
+                                                    double* __restrict__ r, const double* __restrict__ p,
+                                                    const double* __restrict__ Ap, double* __restrict__ z,
+                                                    double* __restrict__ cpart) {
+  const int c = blockIdx.x;
+  const SegCg& sc = st[ch.scene[c]];
+  if (sc.done) return;
+  const double al = sc.alpha;
+  double acc[2] = {0.0, 0.0};
+  for (int k = 3 * ch.lo[c] + threadIdx.x; k < 3 * ch.lo[c + 1]; k += blockDim.x) {
+    x[k] = x[k] + al * p[k];
+    double ri = r[k] - al * Ap[k];
+    r[k] = ri;
+    double zi = d[k] * ri;
+    z[k] = zi;
+    acc[0] += ri * ri;
+    acc[1] += zi * ri;
   }
+  chunk_store<2>(acc, cpart, ch.n);
 }
 
-// per-scene sum of squares of a vector into out[s]
-__global__ void k_seg_norm2(int nv, const int* __restrict__ node_off, const double* __restrict__ v,
-                            double* __restrict__ out) {
-  const int s = blockIdx.x;
+// p = z + beta p
+__global__ void __launch_bounds__(TPB) k_seg_p(const Chunks ch, const SegCg* __restrict__ st,
+                                               const double* __restrict__ z, double* __restrict__ p) {
+  const int c = blockIdx.x;
+  const SegCg& sc = st[ch.scene[c]];
+  if (sc.done) return;
+  const double be = sc.beta;
+  for (int k = 3 * ch.lo[c] + threadIdx.x; k < 3 * ch.lo[c + 1]; k += blockDim.x) p[k] = z[k] + be * p[k];
+}
+
+// per-scene sum of squares of a vector into out[s]: chunk partials, then scenes
+__global__ void __launch_bounds__(TPB) k_chunk_norm2(const Chunks ch, const double* __restrict__ v,
+                                                     double* __restrict__ cpart) {
+  const int c = blockIdx.x;
   double acc[1] = {0.0};
-  for (int a = node_off[s] + threadIdx.x; a < node_off[s + 1]; a += blockDim.x)
-#pragma unroll
-    for (int i = 0; i < 3; ++i) acc[0] += v[3 * a + i] * v[3 * a + i];
-  block_sum<1>(acc);
-  if (threadIdx.x == 0) out[s] = acc[0];
+  for (int k = 3 * ch.lo[c] + threadIdx.x; k < 3 * ch.lo[c + 1]; k += blockDim.x) acc[0] += v[k] * v[k];
+  chunk_store<1>(acc, cpart, ch.n);
+}
+
+__global__ void k_seg_norm2(const Chunks ch, const double* __restrict__ cpart, double* __restrict__ out) {
+  double v[1];
+  scene_sum<1>(ch, cpart, blockIdx.x, v);
+  if (threadIdx.x == 0) out[blockIdx.x] = v[0];
 }
 
 // Dirichlet with a per-scene diagonal scale (first non-zero diagonal of the scene)
@@ -389,9 +433,11 @@ struct Batch {
   int chunk = 8;
   // device
   DBuf<int> d_node_off, d_scene_of;
+  DBuf<int> d_clo, d_cscene, d_cs_off;  // node chunks (see Chunks)
+  int nch = 0;
   DBuf<unsigned char> d_bc, d_ok, d_active;
   DBuf<unsigned char> emask;  // scenes whose elements the force / stiffness kernels evaluate
-  DBuf<double> M, K, J, gforce, up, vn, w, F, dx, us, vs, f, u, v, diag, x, b, r, z, p, Ap, t, scale, coef, nrm;
+  DBuf<double> M, K, J, gforce, up, vn, w, F, dx, us, vs, f, u, v, diag, x, b, r, z, p, Ap, cpart, scale, coef, nrm;
   DBuf<unsigned long long> first;
   DBuf<SegCg> st;
   DBuf<int> err;
@@ -409,10 +455,12 @@ struct Batch {
   }
 
   int vg() const { return reduce_blocks_for(m.ndof); }
+  Chunks chunks() const { return Chunks{d_clo.p, d_cscene.p, d_cs_off.p, nch}; }
 
   void seg_norm2(const double* vec, std::vector<double>& out) {
     cudaStream_t s = m.stream;
-    (note_launch(), k_seg_norm2<<<nscene, 256, 0, s>>>((int)m.nv, d_node_off.p, vec, nrm.p));
+    (note_launch(), k_chunk_norm2<<<nch, TPB, 0, s>>>(chunks(), vec, cpart.p));
+    (note_launch(), k_seg_norm2<<<nscene, TPB, 0, s>>>(chunks(), cpart.p, nrm.p));
     out.resize(nscene);
     HOEFEM_CUDA(cudaMemcpyAsync(out.data(), nrm.p, sizeof(double) * nscene, cudaMemcpyDeviceToHost, s));
     HOEFEM_CUDA(cudaStreamSynchronize(s));
@@ -434,11 +482,27 @@ struct Batch {
     const int n = (int)m.ndof;
     d_node_off.upload(node_off, s);
     d_scene_of.upload(scene_of, s);
+    {
+      std::vector<int> clo, cscene, cs_off(1, 0);
+      for (int k = 0; k < nscene; ++k) {
+        for (int a = node_off[k]; a < node_off[k + 1]; a += CHN) {
+          clo.push_back(a);
+          cscene.push_back(k);
+        }
+        cs_off.push_back((int)clo.size());
+      }
+      nch = (int)clo.size();
+      clo.push_back((int)m.nv);
+      HOEFEM_REQUIRE(nch > 0, HOEFEM_ERR_INVALID_ARGUMENT, "batch without nodes");
+      d_clo.upload(clo, s);
+      d_cscene.upload(cscene, s);
+      d_cs_off.upload(cs_off, s);
+    }
     d_bc.upload(bc_host, s);
     for (auto* bf : {&M, &K, &J}) bf->alloc(m.nnz);
     for (auto* bf : {&gforce, &up, &vn, &w, &F, &dx, &us, &vs, &f, &u, &v, &diag, &x, &b, &r, &z, &p, &Ap})
       bf->alloc(n);
-    t.alloc(2 * (size_t)m.nv);
+    cpart.alloc(2 * (size_t)nch);
     for (auto* bf : {&scale, &coef, &nrm}) bf->alloc(nscene);
     first.alloc(nscene);
     st.alloc(nscene);
@@ -482,29 +546,28 @@ struct Batch {
 
   void enqueue_iter(cudaStream_t s) {
     NodeRows A = m.rows();
-    const int nv = (int)m.nv;
-    HOEFEM_LANES_DISPATCH(A.lanes, (note_launch(), k_seg_Ap<LN><<<spmv_grid(nv, LN), TPB, 0, s>>>(
-                                                       A, J.p, p.p, Ap.p, d_scene_of.p, st.p, t.p)));
-    (note_launch(), k_seg_finalize<<<nscene, 256, 0, s>>>(2, nv, d_node_off.p, t.p, st.p, cg_tol, cg_max));
-    (note_launch(), k_seg_update<<<reduce_blocks_for(nv), TPB, 0, s>>>(nv, d_scene_of.p, st.p, diag.p, x.p, r.p, p.p,
-                                                                       Ap.p, z.p, t.p));
-    (note_launch(), k_seg_finalize<<<nscene, 256, 0, s>>>(3, nv, d_node_off.p, t.p, st.p, cg_tol, cg_max));
-    (note_launch(), k_seg_p<<<reduce_blocks_for(nv), TPB, 0, s>>>(nv, d_scene_of.p, st.p, z.p, p.p));
+    const Chunks ch = chunks();
+    HOEFEM_LANES_DISPATCH(A.lanes, (note_launch(), k_seg_Ap<LN><<<nch, TPB, 0, s>>>(A, J.p, p.p, Ap.p, ch, st.p,
+                                                                                   cpart.p)));
+    (note_launch(), k_seg_finalize<<<nscene, TPB, 0, s>>>(2, ch, cpart.p, st.p, cg_tol, cg_max));
+    (note_launch(), k_seg_update<<<nch, TPB, 0, s>>>(ch, st.p, diag.p, x.p, r.p, p.p, Ap.p, z.p, cpart.p));
+    (note_launch(), k_seg_finalize<<<nscene, TPB, 0, s>>>(3, ch, cpart.p, st.p, cg_tol, cg_max));
+    (note_launch(), k_seg_p<<<nch, TPB, 0, s>>>(ch, st.p, z.p, p.p));
   }
 
   // batched PCG with the diagonal preconditioner on J for the active scenes
   void cg(const std::vector<unsigned char>& active) {
     cudaStream_t s = m.stream;
     NodeRows A = m.rows();
-    const int nv = (int)m.nv;
     HOEFEM_CUDA(cudaMemcpyAsync(d_active.p, active.data(), nscene, cudaMemcpyHostToDevice, s));
     (note_launch(), k_seg_mask_done<<<(nscene + 127) / 128, 128, 0, s>>>(nscene, d_active.p, st.p));
     HOEFEM_CUDA(cudaMemsetAsync(x.p, 0, sizeof(double) * m.ndof, s));
-    HOEFEM_LANES_DISPATCH(A.lanes, (note_launch(), k_seg_init<LN><<<spmv_grid(nv, LN), TPB, 0, s>>>(
-                                                       A, J.p, x.p, b.p, r.p, t.p)));
-    (note_launch(), k_seg_finalize<<<nscene, 256, 0, s>>>(0, nv, d_node_off.p, t.p, st.p, cg_tol, cg_max));
-    (note_launch(), k_seg_prec0<<<reduce_blocks_for(nv), TPB, 0, s>>>(nv, diag.p, r.p, z.p, p.p, t.p));
-    (note_launch(), k_seg_finalize<<<nscene, 256, 0, s>>>(1, nv, d_node_off.p, t.p, st.p, cg_tol, cg_max));
+    const Chunks ch = chunks();
+    HOEFEM_LANES_DISPATCH(A.lanes, (note_launch(), k_seg_init<LN><<<nch, TPB, 0, s>>>(A, J.p, x.p, b.p, r.p, ch,
+                                                                                     st.p, cpart.p)));
+    (note_launch(), k_seg_finalize<<<nscene, TPB, 0, s>>>(0, ch, cpart.p, st.p, cg_tol, cg_max));
+    (note_launch(), k_seg_prec0<<<nch, TPB, 0, s>>>(ch, st.p, diag.p, r.p, z.p, p.p, cpart.p));
+    (note_launch(), k_seg_finalize<<<nscene, TPB, 0, s>>>(1, ch, cpart.p, st.p, cg_tol, cg_max));
     HOEFEM_CUDA(cudaGetLastError());
     if (!graph) {
       cudaStream_t cs;
