@@ -55,9 +55,10 @@ def parse():
     ap.add_argument("--train-states", type=int, default=16, help="learned: training initial states (seeded)")
     ap.add_argument("--train-steps", type=int, default=2000, help="learned: Adam steps")
     ap.add_argument("--coarse-subdomains", type=int, default=256, help="learned: coarse subdomains")
-    ap.add_argument("--workload", default="cylinder", choices=["cylinder", "batched", "tet10"],
+    ap.add_argument("--workload", default="cylinder", choices=["cylinder", "batched", "tet10", "embed"],
                     help="cylinder: embedded Hex27 cylinder Newton step; batched: 64 independent scenes in one "
-                         "batch; tet10: 201,600-element Tet10 box, plain vs mixed precision")
+                         "batch; tet10: 201,600-element Tet10 box, plain vs mixed precision; embed: embedded "
+                         "quadrature construction (classification, cut-cell rules, simplification)")
     ap.add_argument("--scenes", type=int, default=64, help="batched: number of scenes")
     ap.add_argument("--min-elements", type=float, default=1e3, help="batched: smallest scene (elements)")
     ap.add_argument("--max-elements", type=float, default=5e4, help="batched: largest scene (elements)")
@@ -663,6 +664,61 @@ def run_tet10(args):
     print(json.dumps(line), flush=True)
 
 
+def run_embed(args):
+    """Embedded quadrature construction for the benchmark's background grid:
+    Hex27 24^3 on [0, 1]^3, hollow-cylinder Tet4 mesh (r 0.3-0.4, 3 x 144 x 72
+    cells x 6 = 186,624 tets); embed_mesh_3d, the cut-cell rules of
+    tet_quadrature_strength_3, simplified to strength 3.  Each stage timed
+    through the public API with host arrays (device work + copies), the
+    oracle on all host cores on the same input."""
+    import higher_order_embedded_fem_b200 as H
+
+    bg = H.scenes.hex27_box(1.0, 1, 1, 1, 24)
+    V, conn = bg.vertices, bg.blocks[0].connectivity
+    X, T = H.scenes.hollow_cylinder_tets(0.3, 0.4, 1.0, 3, 144, 72)
+    tq = H.tet_quadrature_strength(3)
+    H.embed_mesh_3d(V, conn, X[T[0]], np.array([[0, 1, 2, 3]]))  # context / module load outside the timing
+    runs = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        emb = H.embed_mesh_3d(V, conn, X, T)
+        t1 = time.perf_counter()
+        o, w, p = H.embedding.compute_interface_quadrature_rules(emb, tq)
+        t2 = time.perf_counter()
+        oo, ow, op = H.embedding.simplify_rules(o, w, p, 3)
+        t3 = time.perf_counter()
+        if it >= args.warmup:
+            runs.append((t1 - t0, t2 - t1, t3 - t2))
+    g = np.median(np.array(runs), axis=0) * 1e3
+    line = {"metric": "embedded quadrature construction ms (classify + cut-cell rules + simplify), 1 GPU",
+            "value": float(g.sum()), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": False, "dtype": "f64", "data": "synthetic (procedural hollow cylinder)",
+            "config": {"workload": "Hex27 24^3 background, hollow-cylinder Tet4 mesh 186,624 tets, tet rule strength 3, "
+                                   "simplified to strength 3", "background_cells": int(len(conn)), "tets": int(len(T)),
+                       "interface_cells": int(len(emb.interface_cells)), "interior_cells": int(len(emb.interior_cells)),
+                       "cut_points": int(len(w)), "simplified_points": int(len(ow))},
+            "stages_ms": {"embed_mesh_3d": float(g[0]), "interface_quadrature": float(g[1]), "simplify": float(g[2])},
+            "e2e": {"value": float(g.sum()), "unit": "ms", "h2d_bytes_per_step": int(V.nbytes + conn.nbytes + X.nbytes +
+                                                                                 T.nbytes + w.nbytes + p.nbytes),
+                    "d2h_bytes_per_step": int(w.nbytes + p.nbytes + ow.nbytes + op.nbytes)}}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        t0 = time.perf_counter()
+        ref = O.Embedding(V, conn, X, T)
+        t1 = time.perf_counter()
+        ro, rw, rp = ref.interface_quadratures(*tq)
+        t2 = time.perf_counter()
+        O.simplify_quadratures(ro, rw, rp, 3)
+        t3 = time.perf_counter()
+        line["cpu_baseline"] = {"value": (t3 - t0) * 1e3, "unit": "ms", "cores": O.num_threads(), "kind": "port",
+                                "sample": "the full workload once",
+                                "stages_ms": {"embed_mesh_3d": (t1 - t0) * 1e3, "interface_quadrature": (t2 - t1) * 1e3,
+                                              "simplify": (t3 - t2) * 1e3}}
+        line["classification_equal"] = bool(np.array_equal(ref.cell_class, emb.cell_class))
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -671,6 +727,8 @@ def main():
         run_batched(args)
     elif args.workload == "tet10":
         run_tet10(args)
+    elif args.workload == "embed":
+        run_embed(args)
     elif args.roofline_only:
         run_roofline_only(args)
     else:

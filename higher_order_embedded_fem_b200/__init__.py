@@ -23,4 +23,13 @@ from .solver import (  # noqa: F401
     SolveErrorKind,
 )
 from .learned import LearnedCoarseCorrection  # noqa: F401
+from .embedding import (  # noqa: F401
+    EmbedOptions,
+    EmbeddedQuadrature,
+    StabilizationOptions,
+    embed_mesh_3d,
+    embed_quadrature_3d,
+    simplify_quadrature,
+    tet_quadrature_strength,
+)
 from . import scenes  # noqa: F401

@@ -139,6 +139,13 @@ SIGNATURES = {
     "hoefem_scene_nodes_below": (C.c_int, [vp, C.c_int, dbl, vp, pi64]),
     "hoefem_scene_destroy": (C.c_int, [vp]),
     "hoefem_random_normal": (C.c_int, [C.c_uint64, i64, dbl, vp]),
+    "hoefem_tet_quadrature": (C.c_int, [C.c_int, vp, vp, vp]),
+    "hoefem_embed_mesh_3d": (C.c_int, [vp, i64, vp, i64, C.c_int, vp, i64, vp, i64, dbl, dbl, vp]),
+    "hoefem_embedding_cells": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+    "hoefem_embedding_quadrature": (C.c_int, [vp, vp, vp, i64, dbl, vp, vp, i64, vp]),
+    "hoefem_embedding_copy_quadrature": (C.c_int, [vp, vp, vp, vp]),
+    "hoefem_embedding_destroy": (C.c_int, [vp]),
+    "hoefem_quadrature_simplify": (C.c_int, [i64, vp, vp, vp, C.c_int, vp, vp, vp]),
 }
 
 _lib = None

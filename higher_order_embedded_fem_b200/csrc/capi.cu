@@ -156,6 +156,19 @@ void sync(Model& m) { HOEFEM_CUDA(cudaStreamSynchronize(m.stream)); }
 
 }  // namespace
 
+namespace hoefem {
+struct Embedding;
+Embedding* embedding_create(const double* bgX, i64 nbv, const i64* bg_conn, i64 nbc, int npc, const double* eX,
+                            i64 nev, const i64* tets, i64 nt, double lower, double upper);
+void embedding_destroy(Embedding* e);
+void embedding_cells(const Embedding& e, i64* ne, i64* ni, i64* nf, int* cls, double* cut);
+i64 embedding_quadrature(Embedding& e, const double* tw, const double* tp, i64 nq, double stab_factor,
+                         const double* sw, const double* sp, i64 ns);
+void embedding_copy_quadrature(const Embedding& e, i64* off, double* w, double* p);
+void quadrature_simplify(i64 nrules, const i64* off, const double* w, const double* p, int strength, i64* out_off,
+                         double* out_w, double* out_p);
+}  // namespace hoefem
+
 extern "C" {
 
 const char* hoefem_last_error(void) { return g_error.c_str(); }
@@ -1034,6 +1047,74 @@ int hoefem_random_normal(uint64_t seed, int64_t n, double sigma, double* out) {
   API_BEGIN
   HOEFEM_REQUIRE(out || n == 0, HOEFEM_ERR_INVALID_ARGUMENT, "null output");
   random_normal(seed, n, sigma, out);
+  API_END
+}
+
+int hoefem_tet_quadrature(int strength, double* weights, double* points, int64_t* num_points) {
+  API_BEGIN
+  std::vector<double> w, p;
+  HOEFEM_REQUIRE(tet_quadrature(strength, w, p), HOEFEM_ERR_INVALID_ARGUMENT, "tet rule strength must be 1, 2, 3 or 5");
+  if (num_points) *num_points = (int64_t)w.size();
+  if (weights) std::copy(w.begin(), w.end(), weights);
+  if (points) std::copy(p.begin(), p.end(), points);
+  API_END
+}
+
+int hoefem_embed_mesh_3d(const double* bg_vertices, int64_t num_bg_vertices, const int64_t* bg_connectivity,
+                         int64_t num_bg_cells, int bg_nodes_per_cell, const double* emb_vertices,
+                         int64_t num_emb_vertices, const int64_t* emb_tets, int64_t num_emb_tets,
+                         double lower_volume_threshold, double upper_volume_threshold, hoefem_embedding* out) {
+  API_BEGIN
+  HOEFEM_REQUIRE(out && bg_vertices && bg_connectivity && (emb_vertices || num_emb_vertices == 0) &&
+                     (emb_tets || num_emb_tets == 0),
+                 HOEFEM_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  *out = (hoefem_embedding)embedding_create(bg_vertices, num_bg_vertices, (const i64*)bg_connectivity, num_bg_cells,
+                                            bg_nodes_per_cell, emb_vertices, num_emb_vertices, (const i64*)emb_tets,
+                                            num_emb_tets, lower_volume_threshold, upper_volume_threshold);
+  API_END
+}
+
+int hoefem_embedding_cells(hoefem_embedding e, int64_t* num_exterior, int64_t* num_interior, int64_t* num_interface,
+                           int32_t* cell_class, double* cut_volume) {
+  API_BEGIN
+  HOEFEM_REQUIRE(e, HOEFEM_ERR_INVALID_ARGUMENT, "null embedding");
+  embedding_cells(*(const Embedding*)e, (i64*)num_exterior, (i64*)num_interior, (i64*)num_interface, cell_class,
+                  cut_volume);
+  API_END
+}
+
+int hoefem_embedding_quadrature(hoefem_embedding e, const double* tet_weights, const double* tet_points,
+                                int64_t tet_num_points, double stab_factor, const double* stab_weights,
+                                const double* stab_points, int64_t stab_num_points, int64_t* total_points) {
+  API_BEGIN
+  HOEFEM_REQUIRE(e && total_points, HOEFEM_ERR_INVALID_ARGUMENT, "null argument");
+  *total_points = embedding_quadrature(*(Embedding*)e, tet_weights, tet_points, tet_num_points, stab_factor,
+                                       stab_weights, stab_points, stab_num_points);
+  API_END
+}
+
+int hoefem_embedding_copy_quadrature(hoefem_embedding e, int64_t* offsets, double* weights, double* points) {
+  API_BEGIN
+  HOEFEM_REQUIRE(e && offsets && weights && points, HOEFEM_ERR_INVALID_ARGUMENT, "null argument");
+  embedding_copy_quadrature(*(const Embedding*)e, (i64*)offsets, weights, points);
+  API_END
+}
+
+int hoefem_embedding_destroy(hoefem_embedding e) {
+  API_BEGIN
+  embedding_destroy((Embedding*)e);
+  API_END
+}
+
+int hoefem_quadrature_simplify(int64_t num_rules, const int64_t* offsets, const double* weights,
+                               const double* points, int strength, int64_t* out_offsets, double* out_weights,
+                               double* out_points) {
+  API_BEGIN
+  HOEFEM_REQUIRE(offsets && out_offsets && (num_rules == 0 || (weights && points && out_weights && out_points)),
+                 HOEFEM_ERR_INVALID_ARGUMENT, "null argument");
+  quadrature_simplify(num_rules, (const i64*)offsets, weights, points, strength, (i64*)out_offsets, out_weights,
+                      out_points);
   API_END
 }
 

@@ -51,6 +51,43 @@ static const double HEX5_P[14][3] = {{-H5A, 0, 0},      {0, 0, H5A},      {0, H5
                                      {-H5B, H5B, -H5B}, {-H5B, -H5B, -H5B}, {-H5B, -H5B, H5B}, {H5B, H5B, -H5B},
                                      {H5B, H5B, H5B},   {H5B, -H5B, H5B}};
 
+// tet_quadrature_strength_1 / _2 / _3 (quadrature.rs:570-696): 1, 4 and 8
+// points on the same simplex (embedded cut-cell quadrature).
+static const double T2A = -0.72360679774997896964091736687312762354, T2B = 0.17082039324993690892275210061938287063;
+static const double T3A = -0.34367339496723662642072827083693243093, T3B = -0.9689798150982901207378151874892027072;
+static const double T3C = -0.78390550020314279176487322158837338344, T3D = 0.35171650060942837529461966476512015033;
+static const double T3W1 = 0.18162379004944980942342872025562069427, T3W2 = 0.15170954328388352390990461307771263906;
+static const double TET1_P[1][3] = {{-0.5, -0.5, -0.5}};
+static const double TET2_P[4][3] = {{T2A, T2A, T2B}, {T2A, T2B, T2A}, {T2B, T2A, T2A}, {T2A, T2A, T2A}};
+static const double TET3_W[8] = {T3W1, T3W1, T3W1, T3W1, T3W2, T3W2, T3W2, T3W2};
+static const double TET3_P[8][3] = {{T3A, T3A, T3B}, {T3A, T3B, T3A}, {T3B, T3A, T3A}, {T3A, T3A, T3A},
+                                    {T3C, T3C, T3D}, {T3C, T3D, T3C}, {T3D, T3C, T3C}, {T3C, T3C, T3C}};
+
+// Tet rule of the given strength (1, 2, 3, 5); false for other strengths.
+bool tet_quadrature(int strength, std::vector<double>& w, std::vector<double>& p) {
+  p.clear();
+  switch (strength) {
+    case 1:
+      w.assign(1, 4.0 / 3.0);
+      p.assign(&TET1_P[0][0], &TET1_P[0][0] + 3);
+      return true;
+    case 2:
+      w.assign(4, 0.33333333333333333333333333333333333333);
+      for (auto& x : TET2_P) p.insert(p.end(), x, x + 3);
+      return true;
+    case 3:
+      w.assign(TET3_W, TET3_W + 8);
+      for (auto& x : TET3_P) p.insert(p.end(), x, x + 3);
+      return true;
+    case 5:
+      w.assign(TET5_W, TET5_W + 14);
+      for (auto& x : TET5_P) p.insert(p.end(), x, x + 3);
+      return true;
+    default:
+      return false;
+  }
+}
+
 void tet_quadrature_5(std::vector<double>& w, std::vector<double>& p) {
   w.assign(TET5_W, TET5_W + 14);
   p.clear();

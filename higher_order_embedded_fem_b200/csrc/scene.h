@@ -28,5 +28,7 @@ Scene* scene_hex27_box(double unit, int64_t ux, int64_t uy, int64_t uz, int64_t 
 Scene* scene_embedded_cylinder(int64_t n, double r_in, double r_out, int qmin, int qmax, uint64_t seed);
 void scene_volume_fractions(const Scene& s, double* out);
 void random_normal(uint64_t seed, int64_t n, double sigma, double* out);
+bool tet_quadrature(int strength, std::vector<double>& w, std::vector<double>& p);
+void hex_quadrature_5(std::vector<double>& w, std::vector<double>& p);
 
 }  // namespace hoefem

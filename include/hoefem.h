@@ -446,6 +446,49 @@ int hoefem_scene_destroy(hoefem_scene s);
 /* Seeded N(0, sigma^2) samples (splitmix64 + Box-Muller), identical on all hosts. */
 int hoefem_random_normal(uint64_t seed, int64_t n, double sigma, double* out);
 
+/* tet_quadrature_strength_{1,2,3,5} (fenris/src/quadrature.rs:570-781) on the
+   [-1,1]^3 corner simplex: query the count with weights == NULL. */
+int hoefem_tet_quadrature(int strength, double* weights, double* points, int64_t* num_points);
+
+/* ---- embedded quadrature construction (host arrays; computed on the device) ----
+   embed_mesh_3d_with_opts (fenris/src/embedding/embedding3d.rs:57-196): every
+   background cell (Hex8 or Hex27 connectivity, the first 8 nodes its corners,
+   planar faces) is intersected with the embedded Tet4 mesh and classified by
+   the intersection volume V against its own volume Vc: exterior if
+   V < lower Vc, interface if V < upper Vc, interior otherwise (EmbedOptions
+   defaults 1e-4 / 0.999).  Errors: HOEFEM_ERR_INVALID_ARGUMENT (indices out of
+   range, degenerate input), HOEFEM_ERR_NO_DEVICE. */
+typedef struct hoefem_embedding_s* hoefem_embedding;
+int hoefem_embed_mesh_3d(const double* bg_vertices, int64_t num_bg_vertices, const int64_t* bg_connectivity,
+                         int64_t num_bg_cells, int bg_nodes_per_cell, const double* emb_vertices,
+                         int64_t num_emb_vertices, const int64_t* emb_tets, int64_t num_emb_tets,
+                         double lower_volume_threshold, double upper_volume_threshold, hoefem_embedding* out);
+/* Cell counts; cell_class (0 exterior, 1 interior, 2 interface) and the
+   intersection volume per background cell (either may be NULL). */
+int hoefem_embedding_cells(hoefem_embedding e, int64_t* num_exterior, int64_t* num_interior, int64_t* num_interface,
+                           int32_t* cell_class, double* cut_volume);
+/* compute_interface_quadrature_rules / compute_element_embedded_quadrature
+   (embedding3d.rs:233-289,355-397): the tet rule on every tetrahedron of each
+   interface cell's cut polyhedron, mapped to the background element's
+   reference coordinates (w |det J_tet| / |det J_bg|), plus optional
+   stabilization (stab_factor x the stabilization rule, StabilizationOptions).
+   Interface cells in cell order; returns the total point count. */
+int hoefem_embedding_quadrature(hoefem_embedding e, const double* tet_weights, const double* tet_points,
+                                int64_t tet_num_points, double stab_factor, const double* stab_weights,
+                                const double* stab_points, int64_t stab_num_points, int64_t* total_points);
+/* The rules of the last hoefem_embedding_quadrature: offsets (num_interface + 1),
+   weights (total), points (total x 3). */
+int hoefem_embedding_copy_quadrature(hoefem_embedding e, int64_t* offsets, double* weights, double* points);
+int hoefem_embedding_destroy(hoefem_embedding e);
+/* simplify_quadrature / optimize_quadrature
+   (fenris/src/embedding/quadrature_reduction.rs:107-260): every rule with more
+   points than the number r of Chebyshev moments up to `strength` (0..5) is
+   reduced to at most r of its points with non-negative weights and the same
+   moments.  Outputs use the offsets layout and fit in input-sized buffers. */
+int hoefem_quadrature_simplify(int64_t num_rules, const int64_t* offsets, const double* weights,
+                               const double* points, int strength, int64_t* out_offsets, double* out_weights,
+                               double* out_points);
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,6 +100,15 @@ def lib():
             "oracle_scene_last_substeps": (C.c_int64, [vp]),
             "oracle_scene_last_residual": (C.c_double, [vp]),
             "oracle_scene_destroy": (None, [vp]),
+            "oracle_embed_last_error": (C.c_char_p, []),
+            "oracle_embed_create": (vp, [f64p, C.c_int64, i64p, C.c_int64, C.c_int, f64p, C.c_int64, i64p, C.c_int64,
+                                         C.c_double, C.c_double]),
+            "oracle_embed_destroy": (None, [vp]),
+            "oracle_embed_cells": (None, [vp, i32p, vp]),
+            "oracle_embed_quadrature": (C.c_int64, [vp, f64p, f64p, C.c_int, C.c_double, vp, vp, C.c_int]),
+            "oracle_embed_copy_quadrature": (None, [vp, i64p, f64p, f64p]),
+            "oracle_quadrature_simplify": (C.c_int, [C.c_int64, i64p, f64p, f64p, C.c_int, i64p, f64p, f64p]),
+            "oracle_moment_matrix": (C.c_int, [f64p, C.c_int, C.c_int, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -450,3 +459,79 @@ class Scene:
                      cg_iters=its[:ncg].tolist(), cg_status=sts[:ncg].tolist(),
                      substeps=L.oracle_scene_last_substeps(self._h), residual=L.oracle_scene_last_residual(self._h))
         return u, v, stats
+
+
+# ---- embedded quadrature construction (embed_oracle.cpp) --------------------
+class Embedding:
+    """embed_mesh_3d + embed_quadrature_3d restated on the CPU
+    (fenris/src/embedding/embedding3d.rs:57-289).  Background cells: Hex8 or
+    Hex27 connectivity (the first 8 nodes are the corners); embedded mesh:
+    Tet4."""
+
+    def __init__(self, bg_vertices, bg_connectivity, emb_vertices, emb_tets, lower=1e-4, upper=0.999):
+        L = lib()
+        self._bgv = f64(bg_vertices)
+        self._conn = i64(bg_connectivity)
+        self._ev = f64(emb_vertices)
+        self._et = i64(emb_tets)
+        nbc, npc = self._conn.shape
+        h = L.oracle_embed_create(self._bgv, self._bgv.shape[0], self._conn, nbc, npc, self._ev,
+                                  self._ev.shape[0], self._et, self._et.shape[0], lower, upper)
+        if not h:
+            raise RuntimeError(L.oracle_embed_last_error().decode())
+        self._h = h
+        self.num_cells = nbc
+        cls = np.zeros(nbc, dtype=np.int32)
+        vol = np.zeros(nbc)
+        L.oracle_embed_cells(h, cls, vol.ctypes.data)
+        self.cell_class = cls
+        self.cut_volume = vol
+        self.exterior_cells = np.nonzero(cls == 0)[0]
+        self.interior_cells = np.nonzero(cls == 1)[0]
+        self.interface_cells = np.nonzero(cls == 2)[0]
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().oracle_embed_destroy(self._h)
+            self._h = None
+
+    def interface_quadratures(self, tet_weights, tet_points, stabilization=None):
+        """(offsets, weights, points) of the interface cells' rules, in
+        interface-cell order; stabilization = (factor, weights, points)."""
+        L = lib()
+        tw, tp = f64(tet_weights), f64(tet_points)
+        if stabilization is None:
+            fac, sw, sp, ns = 0.0, None, None, 0
+        else:
+            fac = float(stabilization[0])
+            sw, sp = f64(stabilization[1]), f64(stabilization[2])
+            ns = sw.shape[0]
+        total = L.oracle_embed_quadrature(self._h, tw, tp, tw.shape[0], fac,
+                                          sw.ctypes.data if ns else None, sp.ctypes.data if ns else None, ns)
+        if total < 0:
+            raise RuntimeError(L.oracle_embed_last_error().decode())
+        off = np.zeros(len(self.interface_cells) + 1, dtype=np.int64)
+        w = np.zeros(total)
+        p = np.zeros((total, 3))
+        L.oracle_embed_copy_quadrature(self._h, off, w, p)
+        return off, w, p
+
+
+def simplify_quadratures(offsets, weights, points, strength):
+    """Moment-preserving reduction of every rule (Caratheodory elimination
+    standing in for the reference's LP basic feasible point)."""
+    off, w, p = i64(offsets), f64(weights), f64(points)
+    oo = np.zeros_like(off)
+    ow = np.zeros_like(w)
+    op = np.zeros_like(p)
+    lib().oracle_quadrature_simplify(len(off) - 1, off, w, p, int(strength), oo, ow, op)
+    n = int(oo[-1])
+    return oo, ow[:n].copy(), op[:n].copy()
+
+
+def moment_matrix(points, strength):
+    p = f64(points)
+    r = lib().oracle_moment_matrix(p, p.shape[0], int(strength), None)
+    P = np.zeros((r, p.shape[0]))
+    lib().oracle_moment_matrix(p, p.shape[0], int(strength), P.ctypes.data)
+    return P

@@ -15,7 +15,7 @@ Sources read (paths inside the reference project):
   fenris/tests/unit_tests/cg.rs         solve_arbitrary / solve_arbitrary_preconditioned
   simulation_toolbox/src/fem/newton_cg.rs  build_block_preconditioner (827-876)
   hamilton2/tests/unit_tests/newton.rs  newton_converges_in_single_iteration_for_linear_system
-  fenris/src/quadrature.rs              tet_quadrature_strength_5, hex_quadrature_strength_5
+  fenris/src/quadrature.rs              tet_quadrature_strength_{1,2,3,5}, hex_quadrature_strength_5
 """
 import json
 import os
@@ -27,6 +27,22 @@ FLOAT = r"-?\d+(?:\.\d*)?(?:[eE][-+]?\d+)?"
 
 def floats(s):
     return [float(x) for x in re.findall(FLOAT, s)]
+
+
+def float_items(s):
+    """The comma-separated items of a vec![...] body (brackets excluded),
+    each a literal or a quotient of two literals (e.g. `(4.0 / 3.0)`)."""
+    out = []
+    for item in s.split(","):
+        item = item.strip().strip("()").strip()
+        if not item:
+            continue
+        if "/" in item:
+            num, den = item.split("/")
+            out.append(float(num) / float(den))
+        else:
+            out.append(float(item))
+    return out
 
 
 def ints(s):
@@ -176,14 +192,15 @@ def newton_linear(ref):
 def quadrature(ref):
     text = open(os.path.join(ref, "fenris/src/quadrature.rs")).read()
     out = {}
-    for name in ["tet_quadrature_strength_5", "hex_quadrature_strength_5"]:
+    for name in ["tet_quadrature_strength_1", "tet_quadrature_strength_2", "tet_quadrature_strength_3",
+                 "tet_quadrature_strength_5", "hex_quadrature_strength_5"]:
         body = strip_comments(body_of(text, "pub fn " + name))
         groups = {}
         for key in ["w", "x", "y", "z"]:
             m = re.search(r"let " + key + r"(?::\s*Vec<T>)?\s*=\s*vec!\[", body)
             start = m.end() - 1
             grp = bracket_groups(body[start - 4:], "vec![")[0]
-            groups[key] = floats(grp)
+            groups[key] = float_items(grp)
         out[name] = dict(weights=groups["w"], points=[list(p) for p in zip(groups["x"], groups["y"], groups["z"])])
     return out
 
