@@ -22,18 +22,19 @@
 // thread: the tet is clipped by the six half-spaces in registers / local
 // memory, the result split into tetrahedra, and their volumes summed in pair
 // order.  Vertex labels, which pick the triangulation's apex and fan origins,
-// follow the reference's first-appearance rule over the pair's own faces; the
-// reference applies it over the whole region, so the two triangulations of a
-// cut polyhedron may differ while every integral of a polynomial up to the
-// rule's strength agrees.
+// follow the reference's first-appearance rule over the pair's own faces (the
+// tet's faces in Tet4 face order, its vertices initially in ascending global
+// index); the reference applies it over the whole region, with faces shared
+// between cells, so the two triangulations of a cut polyhedron may differ
+// while every integral of a polynomial up to the rule's strength agrees.
 //
 // Simplification.  The reference finds a basic feasible point of
 // {w >= 0 : P w = P w0} with the OR-Tools GLOP solver (P: Chebyshev tensor
-// moments up to the strength on the points' bounding box).  Here one CTA per
-// rule runs Caratheodory elimination: while more than r points carry weight,
-// the null vector of r + 1 of their moment columns (Gaussian elimination with
-// partial pivoting in shared memory) moves the weights until one reaches zero.
-// Every moment is kept and at most r points remain.
+// moments up to the strength on the points' bounding box).  Here Caratheodory
+// elimination does it: while more than r points carry weight, the null vector
+// of r + 1 of their moment columns moves the weights until one reaches zero.
+// Every moment is kept and at most r points remain (see k_simplify for the
+// parallel form).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -544,7 +545,15 @@ __global__ void k_embed_stab(long long ncell, const long long* __restrict__ soff
 }
 
 // ---- simplification ------------------------------------------------------------
-constexpr int SIMP_TPB = 256;
+// Any subset of a rule's points can be reduced on its own: keeping the subset's
+// moments keeps the rule's.  So one CTA per rule reduces groups of 2r
+// consecutive points to at most r points each (one warp per group), then
+// merges neighbouring groups pairwise (2r -> r) until one group is left.  A
+// reduction step takes the first r + 1 points of a group's list, computes a
+// null vector of their r x (r + 1) moment block (Gaussian elimination with
+// partial pivoting in the warp's shared memory; the block is evaluated from
+// the points on the fly), moves the weights along it until one reaches zero,
+// and drops that point.
 constexpr int SIMP_RMAX = 56;  // strength 5
 
 __device__ __forceinline__ double cheb(double x, int n) {
@@ -571,20 +580,148 @@ __device__ double block_reduce_max(double v, double* sh) {
 }
 __device__ double block_reduce_min(double v, double* sh) { return -block_reduce_max(-v, sh); }
 
-// One CTA per rule.  wk: the rule's weights (modified in place), P: r x n
-// scratch, keep / nkeep: the indices kept, in index order.
-__global__ void __launch_bounds__(SIMP_TPB) k_simplify(const long long* __restrict__ off,
-                                                       const double* __restrict__ p, double* __restrict__ wk,
-                                                       double* __restrict__ Pbuf, int strength, int r,
-                                                       int* __restrict__ keep, int* __restrict__ nkeep, int* err) {
-  __shared__ double sh[32];
-  __shared__ double A[SIMP_RMAX * (SIMP_RMAX + 1)];
-  __shared__ double z[SIMP_RMAX + 1];
-  __shared__ int win[SIMP_RMAX + 1];
-  __shared__ int piv[SIMP_RMAX + 1];
-  __shared__ int s_nwin, s_next, s_npiv, s_row, s_pr, s_skip;
-  __shared__ double s_f[SIMP_RMAX];
-  __shared__ double al[3], be[3];
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+// (value, index) reductions: the largest (smallest) value, ties to the smaller index
+__device__ __forceinline__ void warp_argmax(double& v, int& i) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
+  }
+}
+__device__ __forceinline__ void warp_argmin(double& v, int& i) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    if (ov < v || (ov == v && oi < i)) { v = ov; i = oi; }
+  }
+}
+
+struct SimpCta {
+  unsigned char mono[SIMP_RMAX][3];  // (a, b, c) of every moment row
+  double al[3], be[3];               // Chebyshev scaling of the rule's bounding box
+  double sh[32];
+};
+
+// Reduces the warp's list L (nL sorted point indices with positive weight) to
+// at most r points; returns the new length.  A: r x (r + 1), z, pv: m entries.
+__device__ int warp_reduce_list(const SimpCta& C, int r, int strength, const double* __restrict__ pp,
+                                double* __restrict__ w, int* L, int nL, double* A, double* z, int* pv, int* err) {
+  const int lane = threadIdx.x & 31;
+  const int m = r + 1;
+  while (nL > r) {
+    // moment block of the first m points, element by element
+    for (int t = lane; t < r * m; t += 32) {
+      const int i = t / m, j = t - i * m;
+      const double* x = pp + 3 * (size_t)L[j];
+      A[t] = __dmul_rn(__dmul_rn(cheb(C.al[0] * x[0] + C.be[0], C.mono[i][0]), cheb(C.al[1] * x[1] + C.be[1], C.mono[i][1])),
+                       cheb(C.al[2] * x[2] + C.be[2], C.mono[i][2]));
+    }
+    __syncwarp();
+    double amax = 0.0;
+    for (int t = lane; t < r * m; t += 32) amax = fmax(amax, fabs(A[t]));
+    const double eps = 1e-13 * warp_max(amax);
+    int row = 0, npiv = 0;
+    unsigned long long pivmask = 0ull;
+    for (int c = 0; c < m && row < r; ++c) {
+      double best = -1.0;
+      int bi = r;
+      for (int i = row + lane; i < r; i += 32) {
+        const double v = fabs(A[i * m + c]);
+        if (v > best) { best = v; bi = i; }
+      }
+      warp_argmax(best, bi);
+      if (!(best > eps)) continue;
+      if (bi != row)
+        for (int j = lane; j < m; j += 32) {
+          const double t = A[row * m + j];
+          A[row * m + j] = A[bi * m + j];
+          A[bi * m + j] = t;
+        }
+      __syncwarp();
+      // row factors (into z, free until the back substitution), then the
+      // update element by element over all lanes
+      for (int i = row + 1 + lane; i < r; i += 32) z[i] = A[i * m + c] / A[row * m + c];
+      __syncwarp();
+      const int nrow = r - row - 1, ncol = m - c;
+      for (int t = lane; t < nrow * ncol; t += 32) {
+        const int i = row + 1 + t / ncol, j = c + t % ncol;
+        A[i * m + j] = __dsub_rn(A[i * m + j], __dmul_rn(z[i], A[row * m + j]));
+      }
+      __syncwarp();
+      if (lane == 0) pv[npiv] = c;
+      ++npiv;
+      pivmask |= 1ull << c;
+      ++row;
+    }
+    __syncwarp();
+    const unsigned long long freemask = ~pivmask & ((m == 64) ? ~0ull : ((1ull << m) - 1ull));
+    if (freemask == 0ull) {  // (cannot happen with m = r + 1 columns)
+      if (lane == 0) atomicOr(err, ERR_DEGENERATE);
+      return nL;
+    }
+    const int fc = 63 - __clzll((long long)freemask);
+    for (int j = lane; j < m; j += 32) z[j] = (j == fc) ? 1.0 : 0.0;
+    __syncwarp();
+    for (int k = npiv - 1; k >= 0; --k) {
+      const int c = pv[k];
+      double s = 0.0;
+      for (int j = c + 1 + lane; j < m; j += 32) s = __dadd_rn(s, __dmul_rn(A[k * m + j], z[j]));
+      s = warp_sum(s);
+      if (lane == 0) z[c] = -s / A[k * m + c];
+      __syncwarp();
+    }
+    // direction: flipped when no component is positive
+    bool pos = false;
+    for (int j = lane; j < m; j += 32) pos = pos || z[j] > 0.0;
+    const bool flip = !__any_sync(0xffffffffu, pos);
+    double tmin = INFINITY;
+    int arg = m;
+    for (int j = lane; j < m; j += 32) {
+      const double zj = flip ? -z[j] : z[j];
+      if (zj > 0.0) {
+        const double q = w[L[j]] / zj;
+        if (q < tmin) { tmin = q; arg = j; }
+      }
+    }
+    warp_argmin(tmin, arg);
+    for (int j = lane; j < m; j += 32) {
+      const double zj = flip ? -z[j] : z[j];
+      const double v = __dsub_rn(w[L[j]], __dmul_rn(tmin, zj));
+      w[L[j]] = (j == arg || v < 0.0) ? 0.0 : v;
+    }
+    __syncwarp();
+    // drop the points whose weight reached zero (order kept)
+    int out = 0;
+    for (int base = 0; base < nL; base += 32) {
+      const int j = base + lane;
+      const int idx = j < nL ? L[j] : -1;
+      const bool keep = j < nL && w[idx] > 0.0;
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      __syncwarp();
+      if (keep) L[out + __popc(bal & ((1u << lane) - 1u))] = idx;
+      out += __popc(bal);
+      __syncwarp();
+    }
+    nL = out;
+  }
+  return nL;
+}
+
+// One CTA per rule (warps = blockDim.x / 32).  grp: per-rule scratch of n
+// ints (group lists, stride 2r), gcnt: group lengths (n entries per rule).
+__global__ void __launch_bounds__(256, 4) k_simplify(const long long* __restrict__ off, const double* __restrict__ p, double* __restrict__ wk,
+                           int strength, int r, int* __restrict__ grp, int* __restrict__ gcnt,
+                           int* __restrict__ keep, int* __restrict__ nkeep, int* err) {
+  extern __shared__ double smem[];
+  __shared__ SimpCta C;
   const long long o = off[blockIdx.x];
   const int n = (int)(off[blockIdx.x + 1] - o);
   const double* pp = p + 3 * o;
@@ -595,146 +732,98 @@ __global__ void __launch_bounds__(SIMP_TPB) k_simplify(const long long* __restri
     if (threadIdx.x == 0) nkeep[blockIdx.x] = n;
     return;
   }
-  double* P = Pbuf + (size_t)r * o;
-  // bounding box -> Chebyshev scaling
+  if (threadIdx.x == 0) {
+    int row = 0;
+    for (int a = 0; a <= strength; ++a)
+      for (int b = 0; b <= strength; ++b)
+        for (int c = 0; c <= strength; ++c)
+          if (a + b + c <= strength && row < SIMP_RMAX) {
+            C.mono[row][0] = (unsigned char)a;
+            C.mono[row][1] = (unsigned char)b;
+            C.mono[row][2] = (unsigned char)c;
+            ++row;
+          }
+  }
   for (int d = 0; d < 3; ++d) {
     double lo = INFINITY, hi = -INFINITY;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       lo = fmin(lo, pp[3 * i + d]);
       hi = fmax(hi, pp[3 * i + d]);
     }
-    lo = block_reduce_min(lo, sh);
-    hi = block_reduce_max(hi, sh);
+    lo = block_reduce_min(lo, C.sh);
+    hi = block_reduce_max(hi, C.sh);
     if (threadIdx.x == 0) {
       const double c = (lo + hi) / 2.0, l = (hi - lo) / 2.0;
-      al[d] = l != 0.0 ? 1.0 / l : 0.0;
-      be[d] = 1.0 - al[d] * (c + l);
+      C.al[d] = l != 0.0 ? 1.0 / l : 0.0;
+      C.be[d] = 1.0 - C.al[d] * (c + l);
     }
   }
   __syncthreads();
-  // moment matrix rows in (a, b, c) lexicographic order, a + b + c <= strength
-  {
-    int row = 0;
-    for (int a = 0; a <= strength; ++a)
-      for (int b = 0; b <= strength; ++b)
-        for (int c = 0; c <= strength; ++c) {
-          if (a + b + c > strength) continue;
-          for (int i = threadIdx.x; i < n; i += blockDim.x)
-            P[(size_t)row * n + i] = __dmul_rn(__dmul_rn(cheb(al[0] * pp[3 * i] + be[0], a),
-                                                         cheb(al[1] * pp[3 * i + 1] + be[1], b)),
-                                               cheb(al[2] * pp[3 * i + 2] + be[2], c));
-          ++row;
-        }
-  }
-  // window: the first r + 1 points with positive weight
-  if (threadIdx.x == 0) {
-    int m = 0, i = 0;
-    for (; i < n && m < r + 1; ++i)
-      if (w[i] > 0.0) win[m++] = i;
-    s_nwin = m;
-    s_next = i;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int m = r + 1, G = 2 * r;
+  // per-warp shared memory: A (r x m), z (m), L (2r ints), pv (m ints)
+  const size_t per = (size_t)r * m + m + (size_t)(G + m + 1) / 2 + 1;
+  double* A = smem + per * wid;
+  double* z = A + (size_t)r * m;
+  int* L = (int*)(z + m);
+  int* pv = L + G;
+  int* glist = grp + o;
+  int* gc = gcnt + o;
+  const int ng = (n + G - 1) / G;
+  // level 0: groups of G consecutive points
+  for (int g = wid; g < ng; g += nw) {
+    const int lo = g * G, hi = min(lo + G, n);
+    int nL = 0;
+    for (int base = lo; base < hi; base += 32) {
+      const int i = base + lane;
+      const bool pos = i < hi && w[i] > 0.0;
+      const unsigned bal = __ballot_sync(0xffffffffu, pos);
+      if (pos) L[nL + __popc(bal & ((1u << lane) - 1u))] = i;
+      nL += __popc(bal);
+    }
+    __syncwarp();
+    nL = warp_reduce_list(C, r, strength, pp, w, L, nL, A, z, pv, err);
+    for (int j = lane; j < nL; j += 32) glist[(size_t)g * G + j] = L[j];
+    if (lane == 0) gc[g] = nL;
+    __syncwarp();
   }
   __syncthreads();
-  const int m = r + 1;
-  for (int guard = 0; guard < n + 8; ++guard) {
-    if (s_nwin <= r) break;  // (uniform: shared, read after a barrier)
-    // A = P(:, win)
-    for (int t = threadIdx.x; t < r * m; t += blockDim.x) {
-      const int i = t / m, j = t - i * m;
-      A[t] = P[(size_t)i * n + win[j]];
-    }
-    __syncthreads();
-    double amax = 0.0;
-    for (int t = threadIdx.x; t < r * m; t += blockDim.x) amax = fmax(amax, fabs(A[t]));
-    const double eps = 1e-13 * block_reduce_max(amax, sh);
-    if (threadIdx.x == 0) { s_row = 0; s_npiv = 0; }
-    __syncthreads();
-    for (int c = 0; c < m; ++c) {
-      // (every thread is done with the previous column's shared state)
-      __syncthreads();
-      const int row = s_row;
-      if (row >= r) break;
-      if (threadIdx.x == 0) {
-        int pr = row;
-        for (int i = row + 1; i < r; ++i)
-          if (fabs(A[i * m + c]) > fabs(A[pr * m + c])) pr = i;
-        s_pr = pr;
-        s_skip = fabs(A[pr * m + c]) <= eps;
-      }
-      __syncthreads();
-      const int pr = s_pr;
-      if (s_skip) continue;
-      if (pr != row)
-        for (int j = threadIdx.x; j < m; j += blockDim.x) {
-          const double t = A[row * m + j];
-          A[row * m + j] = A[pr * m + j];
-          A[pr * m + j] = t;
+  // pairwise merges
+  for (int s = 1; s < ng; s *= 2) {
+    for (int g = 2 * s * wid; g < ng; g += 2 * s * nw) {
+      int nL = gc[g];
+      for (int j = lane; j < nL; j += 32) L[j] = glist[(size_t)g * G + j];
+      if (g + s < ng) {
+        const int n2 = gc[g + s];
+        if (nL + n2 > G) {  // (a reduction left more than r points: cannot happen)
+          if (lane == 0) atomicOr(err, ERR_DEGENERATE);
+          continue;
         }
-      __syncthreads();
-      for (int i = row + 1 + threadIdx.x; i < r; i += blockDim.x) s_f[i] = A[i * m + c] / A[row * m + c];
-      __syncthreads();
-      const int nrow = r - row - 1, ncol = m - c;
-      for (int t = threadIdx.x; t < nrow * ncol; t += blockDim.x) {
-        const int i = row + 1 + t / ncol, j = c + t % ncol;
-        A[i * m + j] = __dsub_rn(A[i * m + j], __dmul_rn(s_f[i], A[row * m + j]));
+        for (int j = lane; j < n2; j += 32) L[nL + j] = glist[(size_t)(g + s) * G + j];
+        nL += n2;
       }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        piv[s_npiv++] = c;
-        s_row = row + 1;
-      }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      // null vector: the last free column set to 1, back substitution
-      bool is_piv[SIMP_RMAX + 1];
-      for (int j = 0; j < m; ++j) is_piv[j] = false;
-      for (int k = 0; k < s_npiv; ++k) is_piv[piv[k]] = true;
-      int fc = m - 1;
-      while (fc >= 0 && is_piv[fc]) --fc;
-      for (int j = 0; j < m; ++j) z[j] = 0.0;
-      if (fc < 0) {
-        atomicOr(err, ERR_DEGENERATE);
-        s_nwin = 0;
-      } else {
-        z[fc] = 1.0;
-        for (int k = s_npiv - 1; k >= 0; --k) {
-          const int c = piv[k];
-          double s = 0.0;
-          for (int j = c + 1; j < m; ++j) s = __dadd_rn(s, __dmul_rn(A[k * m + j], z[j]));
-          z[c] = -s / A[k * m + c];
-        }
-        bool pos = false;
-        for (int j = 0; j < m; ++j) pos = pos || z[j] > 0.0;
-        if (!pos)
-          for (int j = 0; j < m; ++j) z[j] = -z[j];
-        int arg = -1;
-        double t = INFINITY;
-        for (int j = 0; j < m; ++j)
-          if (z[j] > 0.0 && w[win[j]] / z[j] < t) {
-            t = w[win[j]] / z[j];
-            arg = j;
-          }
-        int nw = 0;
-        for (int j = 0; j < m; ++j) {
-          const double v = __dsub_rn(w[win[j]], __dmul_rn(t, z[j]));
-          const double nv = (j == arg || v < 0.0) ? 0.0 : v;
-          w[win[j]] = nv;
-          if (nv > 0.0) win[nw++] = win[j];
-        }
-        int i = s_next;
-        for (; i < n && nw < m; ++i)
-          if (w[i] > 0.0) win[nw++] = i;
-        s_next = i;
-        s_nwin = nw;
-      }
+      __syncwarp();
+      nL = warp_reduce_list(C, r, strength, pp, w, L, nL, A, z, pv, err);
+      for (int j = lane; j < nL; j += 32) glist[(size_t)g * G + j] = L[j];
+      if (lane == 0) gc[g] = nL;
+      __syncwarp();
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    if (s_nwin > r) atomicOr(err, ERR_DEGENERATE);
-    for (int j = 0; j < s_nwin; ++j) kp[j] = win[j];
-    nkeep[blockIdx.x] = s_nwin;
+  for (int j = threadIdx.x; j < gc[0]; j += blockDim.x) kp[j] = glist[j];
+  if (threadIdx.x == 0) nkeep[blockIdx.x] = gc[0];
+}
+
+// The kept points of every rule, compacted to the output offsets.
+__global__ void k_simplify_gather(const long long* __restrict__ off, const long long* __restrict__ outoff,
+                                  const int* __restrict__ keep, const double* __restrict__ w,
+                                  const double* __restrict__ p, double* __restrict__ ow, double* __restrict__ op) {
+  const long long o = off[blockIdx.x], q = outoff[blockIdx.x];
+  const int nk = (int)(outoff[blockIdx.x + 1] - q);
+  for (int j = threadIdx.x; j < nk; j += blockDim.x) {
+    const long long i = o + keep[o + j];
+    ow[q + j] = w[i];
+    for (int d = 0; d < 3; ++d) op[3 * (q + j) + d] = p[3 * i + d];
   }
 }
 
@@ -752,9 +841,10 @@ struct Embedding {
   DBuf<double> d_corners, d_eX;
   DBuf<int> d_tet_faces, d_pcell, d_ptet;
   std::vector<int> ntet;
-  // last quadrature
+  // last quadrature (device resident until copied out)
   std::vector<i64> q_off;
-  std::vector<double> q_w, q_p;
+  DBuf<double> q_w, q_p;
+  i64 q_total = 0;
   ~Embedding() {
     if (stream) cudaStreamDestroy(stream);
   }
@@ -804,36 +894,28 @@ Embedding* embedding_create(const double* bgX, i64 nbv, const i64* bg_conn, i64 
       }
     }
   }
-  // embedded poly mesh faces: deduplicated by vertex set, first-occurrence
-  // vertex order; Tet4 face order (0,2,1), (0,1,3), (1,2,3), (0,3,2)
+  // every tet's faces in Tet4 face order (0,2,1), (0,1,3), (1,2,3), (0,3,2);
+  // bounding boxes
   static const int TF[4][3] = {{0, 2, 1}, {0, 1, 3}, {1, 2, 3}, {0, 3, 2}};
   std::vector<int> tet_faces((size_t)12 * std::max<i64>(nt, 1));
   std::vector<double> tbox((size_t)6 * std::max<i64>(nt, 1));
-  std::map<std::array<i64, 3>, std::array<int, 3>> first;
   for (i64 t = 0; t < nt; ++t) {
+    const i64* v = tets + 4 * t;
+    for (int i = 0; i < 4; ++i) {
+      HOEFEM_REQUIRE(v[i] >= 0 && v[i] < nev, HOEFEM_ERR_INVALID_ARGUMENT, "tet connectivity out of range");
+      for (int j = 0; j < i; ++j)
+        HOEFEM_REQUIRE(v[i] != v[j], HOEFEM_ERR_INVALID_ARGUMENT, "tet with repeated vertices");
+    }
+    for (int f = 0; f < 4; ++f)
+      for (int i = 0; i < 3; ++i) tet_faces[12 * t + 3 * f + i] = (int)v[TF[f][i]];
     double* b = &tbox[6 * t];
-    for (int k = 0; k < 3; ++k) { b[k] = INFINITY; b[3 + k] = -INFINITY; }
-    for (int f = 0; f < 4; ++f) {
-      std::array<i64, 3> v{tets[4 * t + TF[f][0]], tets[4 * t + TF[f][1]], tets[4 * t + TF[f][2]]};
-      for (i64 x : v) HOEFEM_REQUIRE(x >= 0 && x < nev, HOEFEM_ERR_INVALID_ARGUMENT, "tet connectivity out of range");
-      std::array<i64, 3> key = v;
-      std::sort(key.begin(), key.end());
-      HOEFEM_REQUIRE(key[0] != key[1] && key[1] != key[2], HOEFEM_ERR_INVALID_ARGUMENT, "tet with repeated vertices");
-      auto it = first.find(key);
-      std::array<int, 3> o;
-      if (it == first.end()) {
-        o = {(int)v[0], (int)v[1], (int)v[2]};
-        first.emplace(key, o);
-      } else {
-        o = it->second;
-      }
-      for (int i = 0; i < 3; ++i) {
-        tet_faces[12 * t + 3 * f + i] = o[i];
-        for (int k = 0; k < 3; ++k) {
-          const double x = eX[3 * o[i] + k];
-          b[k] = std::min(b[k], x);
-          b[3 + k] = std::max(b[3 + k], x);
-        }
+    for (int k = 0; k < 3; ++k) {
+      b[k] = INFINITY;
+      b[3 + k] = -INFINITY;
+      for (int i = 0; i < 4; ++i) {
+        const double x = eX[3 * v[i] + k];
+        b[k] = std::min(b[k], x);
+        b[3 + k] = std::max(b[3 + k], x);
       }
     }
   }
@@ -933,7 +1015,9 @@ i64 embedding_quadrature(Embedding& e, const double* tw, const double* tp, i64 n
   }
   const i64 ncell = (i64)e.q_off.size() - 1;
   DBuf<long long> d_list, d_qoff, d_soff;
-  DBuf<double> d_tw, d_tp, d_sw, d_sp, d_w, d_p;
+  DBuf<double> d_tw, d_tp, d_sw, d_sp;
+  DBuf<double>& d_w = e.q_w;
+  DBuf<double>& d_p = e.q_p;
   DBuf<int> d_err;
   d_list.upload(list, s);
   d_qoff.upload(qoff, s);
@@ -958,20 +1042,20 @@ i64 embedding_quadrature(Embedding& e, const double* tw, const double* tp, i64 n
                                                                                       stab_factor, d_sw.p, d_sp.p,
                                                                                       d_w.p, d_p.p));
   HOEFEM_CUDA(cudaGetLastError());
-  e.q_w.resize(total);
-  e.q_p.resize(3 * total);
-  if (total) {
-    HOEFEM_CUDA(cudaMemcpyAsync(e.q_w.data(), d_w.p, sizeof(double) * total, cudaMemcpyDeviceToHost, s));
-    HOEFEM_CUDA(cudaMemcpyAsync(e.q_p.data(), d_p.p, sizeof(double) * 3 * total, cudaMemcpyDeviceToHost, s));
-  }
   check_err(d_err, s);
+  e.q_total = total;
   return total;
 }
 
 void embedding_copy_quadrature(const Embedding& e, i64* off, double* w, double* p) {
+  HOEFEM_REQUIRE(!e.q_off.empty(), HOEFEM_ERR_INVALID_ARGUMENT, "no interface quadrature has been built");
+  HOEFEM_CUDA(cudaSetDevice(e.device));
   std::copy(e.q_off.begin(), e.q_off.end(), off);
-  std::copy(e.q_w.begin(), e.q_w.end(), w);
-  std::copy(e.q_p.begin(), e.q_p.end(), p);
+  if (e.q_total) {
+    HOEFEM_CUDA(cudaMemcpyAsync(w, e.q_w.p, sizeof(double) * e.q_total, cudaMemcpyDeviceToHost, e.stream));
+    HOEFEM_CUDA(cudaMemcpyAsync(p, e.q_p.p, sizeof(double) * 3 * e.q_total, cudaMemcpyDeviceToHost, e.stream));
+  }
+  HOEFEM_CUDA(cudaStreamSynchronize(e.stream));
 }
 
 int polynomial_space_dim(int strength) {
@@ -1002,37 +1086,46 @@ void quadrature_simplify(i64 nrules, const i64* off, const double* w, const doub
   } guard{s};
   std::vector<long long> offl(off, off + nrules + 1);
   DBuf<long long> d_off;
-  DBuf<double> d_p, d_w, d_P;
-  DBuf<int> d_keep, d_nkeep, d_err;
+  DBuf<double> d_p, d_w;
+  DBuf<int> d_keep, d_nkeep, d_err, d_grp, d_gcnt;
   d_off.upload(offl, s);
   d_p.upload(p, 3 * total, s);
   d_w.upload(w, total, s);
-  d_P.alloc((size_t)r * std::max<i64>(total, 1));
   d_keep.alloc(total);
   d_nkeep.alloc(nrules);
+  d_grp.alloc(total);
+  d_gcnt.alloc(total);
   d_err.alloc(1);
   d_err.zero(s);
-  (note_launch(), k_simplify<<<(unsigned)nrules, SIMP_TPB, 0, s>>>(d_off.p, d_p.p, d_w.p, d_P.p, strength, r,
-                                                                    d_keep.p, d_nkeep.p, d_err.p));
+  // warps per CTA from the per-warp shared memory (A, z, list, pivots)
+  const int m = r + 1, G = 2 * r;
+  const size_t per = (size_t)r * m + m + (size_t)(G + m + 1) / 2 + 1;
+  const int nw = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024) / (per * sizeof(double))));
+  const size_t smem = (size_t)nw * per * sizeof(double);
+  HOEFEM_CUDA(cudaFuncSetAttribute(k_simplify, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  (note_launch(), k_simplify<<<(unsigned)nrules, 32 * nw, smem, s>>>(d_off.p, d_p.p, d_w.p, strength, r, d_grp.p,
+                                                                      d_gcnt.p, d_keep.p, d_nkeep.p, d_err.p));
   HOEFEM_CUDA(cudaGetLastError());
-  std::vector<double> wn(total);
-  std::vector<int> keep(total), nkeep(nrules);
-  if (total) {
-    HOEFEM_CUDA(cudaMemcpyAsync(wn.data(), d_w.p, sizeof(double) * total, cudaMemcpyDeviceToHost, s));
-    HOEFEM_CUDA(cudaMemcpyAsync(keep.data(), d_keep.p, sizeof(int) * total, cudaMemcpyDeviceToHost, s));
-  }
+  std::vector<int> nkeep(nrules);
   HOEFEM_CUDA(cudaMemcpyAsync(nkeep.data(), d_nkeep.p, sizeof(int) * nrules, cudaMemcpyDeviceToHost, s));
   check_err(d_err, s);
-  for (i64 k = 0; k < nrules; ++k) {
-    i64 o = out_off[k];
-    for (int j = 0; j < nkeep[k]; ++j) {
-      const i64 i = off[k] + keep[off[k] + j];
-      out_w[o] = wn[i];
-      for (int d = 0; d < 3; ++d) out_p[3 * o + d] = p[3 * i + d];
-      ++o;
-    }
-    out_off[k + 1] = o;
+  std::vector<long long> oo(nrules + 1, 0);
+  for (i64 k = 0; k < nrules; ++k) oo[k + 1] = oo[k] + nkeep[k];
+  const i64 kept = oo[nrules];
+  DBuf<long long> d_oo;
+  DBuf<double> d_ow, d_op;
+  d_oo.upload(oo, s);
+  d_ow.alloc(kept);
+  d_op.alloc(3 * kept);
+  (note_launch(), k_simplify_gather<<<(unsigned)nrules, 128, 0, s>>>(d_off.p, d_oo.p, d_keep.p, d_w.p, d_p.p, d_ow.p,
+                                                                      d_op.p));
+  HOEFEM_CUDA(cudaGetLastError());
+  if (kept) {
+    HOEFEM_CUDA(cudaMemcpyAsync(out_w, d_ow.p, sizeof(double) * kept, cudaMemcpyDeviceToHost, s));
+    HOEFEM_CUDA(cudaMemcpyAsync(out_p, d_op.p, sizeof(double) * 3 * kept, cudaMemcpyDeviceToHost, s));
   }
+  HOEFEM_CUDA(cudaStreamSynchronize(s));
+  for (i64 k = 0; k <= nrules; ++k) out_off[k] = oo[k];
 }
 
 }  // namespace hoefem

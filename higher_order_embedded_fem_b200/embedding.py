@@ -103,8 +103,8 @@ def compute_interface_quadrature_rules(embedding, tet_quadrature, stabilization=
     check(lib().hoefem_embedding_quadrature(embedding._h, tw.ctypes.data, tp.ctypes.data, tw.shape[0], fac, swp, spp,
                                             ns, C.byref(total)))
     off = np.zeros(len(embedding.interface_cells) + 1, dtype=np.int64)
-    w = np.zeros(total.value)
-    p = np.zeros((total.value, 3))
+    w = np.empty(total.value)
+    p = np.empty((total.value, 3))
     check(lib().hoefem_embedding_copy_quadrature(embedding._h, off.ctypes.data, w.ctypes.data, p.ctypes.data))
     return off, w, p
 
@@ -116,8 +116,8 @@ def simplify_rules(offsets, weights, points, strength):
     w = _capi.host_f64(weights)
     p = _capi.host_f64(points).reshape(-1, 3)
     oo = np.zeros_like(off)
-    ow = np.zeros_like(w)
-    op = np.zeros_like(p)
+    ow = np.empty_like(w)
+    op = np.empty_like(p)
     check(lib().hoefem_quadrature_simplify(len(off) - 1, off.ctypes.data, w.ctypes.data, p.ctypes.data, int(strength),
                                            oo.ctypes.data, ow.ctypes.data, op.ctypes.data))
     n = int(oo[-1])
