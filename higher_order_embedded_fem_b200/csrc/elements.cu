@@ -380,6 +380,93 @@ __global__ void __launch_bounds__(TPB) k_forces(const BlockDev b, const int* __r
 }
 
 // ============================================================================
+// Internal force, Tet10 (affine geometry, uniform rule of <= 32 points): warp
+// per element, lane q evaluates quadrature point q (F from all 10 nodes, the
+// stress once) and writes its contribution to every node into shared memory;
+// the node lanes then add the points' contributions in point order, as the
+// sequential loop of the reference does.
+// ============================================================================
+constexpr int T10_FSTRIDE = 31;  // doubles per point row (30 used; odd stride)
+
+__global__ void __launch_bounds__(TPB) k_forces_tet10(const BlockDev b, const int* __restrict__ elems, int count,
+                                                      const double* __restrict__ X, const double* __restrict__ u,
+                                                      double* __restrict__ f, MatDev mat, int* err) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int idx = blockIdx.x * (TPB / 32) + warp;
+  __shared__ double s_corner[TPB / 32][12];
+  __shared__ double s_u[TPB / 32][30];
+  __shared__ double s_f[TPB / 32][32 * T10_FSTRIDE];
+  if (idx >= count) return;
+  const int e = elems[idx];
+  if (b.scene_active && !b.scene_active[b.escene[e]]) return;
+  int g = 0;
+  if (lane < 10) {
+    g = b.conn[lane * b.ne + e];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double x = X[3 * g + k];
+      s_u[warp][3 * lane + k] = u[3 * g + k];
+      if (lane < 4) s_corner[warp][3 * lane + k] = x;
+    }
+  }
+  __syncwarp();
+  double J[9], Ji[9];
+  tet4_jacobian(s_corner[warp], J);
+  const double detJ = inv3(J, Ji);
+  const int nq = b.nq;
+  bool ok = detJ != 0.0;
+  if (ok && lane < nq) {
+    const double xi[3] = {b.qp[3 * lane], b.qp[3 * lane + 1], b.qp[3 * lane + 2]};
+    double F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int I = 0; I < 10; ++I) {
+      double gr[3], G[3];
+      tet10_grad(I, xi, gr);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) G[k] = Ji[k] * gr[0] + Ji[3 + k] * gr[1] + Ji[6 + k] * gr[2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[3 * c + k] += s_u[warp][3 * I + c] * G[k];
+    }
+    F[0] += 1.0;
+    F[4] += 1.0;
+    F[8] += 1.0;
+    QpState<double> st;
+    const double emu = b.emat ? b.emat[2 * e] : mat.mu, elam = b.emat ? b.emat[2 * e + 1] : mat.lambda;
+    ok = material_state(mat.kind, F, emu, elam, st, true);
+    if (ok) {
+      const double sc = b.qw[lane] * fabs(detJ);
+      double* out = s_f[warp] + lane * T10_FSTRIDE;
+#pragma unroll
+      for (int I = 0; I < 10; ++I) {
+        double gr[3], G[3];
+        tet10_grad(I, xi, gr);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) G[k] = Ji[k] * gr[0] + Ji[3 + k] * gr[1] + Ji[6 + k] * gr[2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+          out[3 * I + i] = -(st.P[3 * i] * G[0] + st.P[3 * i + 1] * G[1] + st.P[3 * i + 2] * G[2]) * sc;
+      }
+    }
+  }
+  ok = __all_sync(0xffffffffu, ok);
+  __syncwarp();
+  if (!ok) {
+    if (lane == 0) set_error(err, HOEFEM_ERR_SINGULAR);
+    return;
+  }
+  if (lane < 10) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      double acc = 0.0;
+      for (int q = 0; q < nq; ++q) acc += s_f[warp][q * T10_FSTRIDE + 3 * lane + i];
+      f[3 * g + i] += acc;
+    }
+  }
+}
+
+// ============================================================================
 // Internal force, Hex27: FW warps per element (one CTA), warp w takes the
 // quadrature points w, w + FW, ...; the per-warp node forces are summed in
 // shared memory in warp order (deterministic) and scattered once.  A color
@@ -517,6 +604,7 @@ __global__ void __launch_bounds__(StiffCfg<NN>::TPB, 2) k_stiffness(const BlockD
   QpPair<R>(*s_qp)[QT] =
       reinterpret_cast<QpPair<R>(*)[QT]>(smem_raw + sizeof(R) * (size_t)EPC * QT * NN * 9);
   __shared__ R s_corner[EPC][24];
+  __shared__ R s_u[EPC][NN == 10 ? 30 : 1];  // Tet10: node displacements for the point lanes
   __shared__ int s_g[EPC][NN];
   __shared__ int s_ok[EPC];
   __shared__ int s_nq[EPC];
@@ -552,7 +640,13 @@ __global__ void __launch_bounds__(StiffCfg<NN>::TPB, 2) k_stiffness(const BlockD
     const int g = s_g[grp][lane];
 #pragma unroll
     for (int k = 0; k < 3; ++k) ul[k] = (R)u[3 * g + k];
+    if constexpr (NN == 10) {
+      if (wl == 0)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s_u[grp][3 * lane + k] = ul[k];
+    }
   }
+  if constexpr (NN == 10) __syncthreads();
   R acc[PPT][9];
 #pragma unroll
   for (int k = 0; k < PPT; ++k)
@@ -560,6 +654,54 @@ __global__ void __launch_bounds__(StiffCfg<NN>::TPB, 2) k_stiffness(const BlockD
     for (int m = 0; m < 9; ++m) acc[k][m] = 0;
   for (int qt = 0; qt < nq_max; qt += QT) {
     // ---- phase A: per-point data of this tile ----
+    if constexpr (NN == 10) {
+      // affine geometry: lane ql of the element's first warp takes point ql
+      // (the material state once per point, F from all 10 nodes)
+      const int ql = lane;
+      if (wl == 0 && ql < QT && qt + ql < nq) {
+        const int q = q0 + qt + ql;
+        const R xi[3] = {(R)b.qp[3 * q], (R)b.qp[3 * q + 1], (R)b.qp[3 * q + 2]};
+        const R w = (R)b.qw[q];
+        R J[9], Ji[9];
+        tet4_jacobian(s_corner[grp], J);
+        const R detJ = inv3(J, Ji);
+        R F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int I = 0; I < 10; ++I) {
+          R gr[3], G[3];
+          tet10_grad(I, xi, gr);
+#pragma unroll
+          for (int k = 0; k < 3; ++k) G[k] = Ji[k] * gr[0] + Ji[3 + k] * gr[1] + Ji[6 + k] * gr[2];
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) F[3 * c + k] += s_u[grp][3 * I + c] * G[k];
+        }
+        F[0] += R(1);
+        F[4] += R(1);
+        F[8] += R(1);
+        QpState<R> st;
+        const bool okq = (detJ != R(0)) && material_state(mat.kind, F, mu, lam, st, false);
+        if (!okq) {
+          s_ok[grp] = 0;
+        } else {
+          const R sc = sqrt(w * fabs(detJ));
+#pragma unroll
+          for (int I = 0; I < 10; ++I) {
+            R gr[3];
+            tet10_grad(I, xi, gr);
+            const R a[3] = {(Ji[0] * gr[0] + Ji[3] * gr[1] + Ji[6] * gr[2]) * sc,
+                            (Ji[1] * gr[0] + Ji[4] * gr[1] + Ji[7] * gr[2]) * sc,
+                            (Ji[2] * gr[0] + Ji[5] * gr[1] + Ji[8] * gr[2]) * sc};
+            R* v = s_vec[grp][ql][I];
+            v[0] = a[0]; v[1] = a[1]; v[2] = a[2];
+            mat3vec(st.F, a, v + 3);
+            mat3vec(st.M1, a, v + 6);
+          }
+          qp_pair_from(mat.kind, st, s_qp[grp][ql]);
+        }
+      }
+    } else
     for (int ql = wl; ql < QT && qt + ql < nq; ql += WPE) {
       const int q = q0 + qt + ql;
       const R xi[3] = {(R)b.qp[3 * q], (R)b.qp[3 * q + 1], (R)b.qp[3 * q + 2]};
@@ -756,7 +898,9 @@ void launch_forces(const Model& m, const MatDev& mat, const double* u, double* f
     BlockDev bd = bp->dev();
     for_each_color(*bp, [&](const int* elems, int cnt) {
       int grid = (cnt + TPB / 32 - 1) / (TPB / 32);
-      if (bp->kind == HOEFEM_ELEM_TET10)
+      if (bp->kind == HOEFEM_ELEM_TET10 && bd.uniform && bd.nq <= 32)
+        (note_launch(), k_forces_tet10<<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p));
+      else if (bp->kind == HOEFEM_ELEM_TET10)
         (note_launch(), k_forces<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p));
       else
         (note_launch(), k_forces_hex27<<<cnt, 32 * FW, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p));
