@@ -259,7 +259,7 @@ def run_hoefem(args):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     import higher_order_embedded_fem_b200 as H
