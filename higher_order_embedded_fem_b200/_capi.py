@@ -140,6 +140,7 @@ SIGNATURES = {
     "hoefem_scene_destroy": (C.c_int, [vp]),
     "hoefem_random_normal": (C.c_int, [C.c_uint64, i64, dbl, vp]),
     "hoefem_tet_quadrature": (C.c_int, [C.c_int, vp, vp, vp]),
+    "hoefem_precond_set_block_apply": (C.c_int, [vp, C.c_int32]),
     "hoefem_embed_mesh_3d": (C.c_int, [vp, i64, vp, i64, C.c_int, vp, i64, vp, i64, dbl, dbl, vp]),
     "hoefem_embedding_cells": (C.c_int, [vp, vp, vp, vp, vp, vp]),
     "hoefem_embedding_quadrature": (C.c_int, [vp, vp, vp, i64, dbl, vp, vp, i64, vp]),

@@ -543,6 +543,15 @@ int hoefem_precond_set_spmv_variant(hoefem_precond p, int32_t variant) {
   API_END
 }
 
+int hoefem_precond_set_block_apply(hoefem_precond p, int32_t on) {
+  API_BEGIN
+  HOEFEM_REQUIRE(p && p->p.kind == PREC_SCHWARZ, HOEFEM_ERR_INVALID_ARGUMENT, "not a Schwarz preconditioner");
+  HOEFEM_REQUIRE(!on || 3 * p->p.max_nodes <= 96, HOEFEM_ERR_INVALID_ARGUMENT,
+                 "block apply supports subdomains of at most 32 nodes");
+  p->p.block_apply = on != 0;
+  API_END
+}
+
 int hoefem_precond_get_spmv_variants(hoefem_precond p, int32_t* fp64_values, int32_t* fp32_values) {
   API_BEGIN
   HOEFEM_REQUIRE(p, HOEFEM_ERR_INVALID_ARGUMENT, "null preconditioner");
@@ -633,8 +642,7 @@ int hoefem_cg_solve_mixed(hoefem_model m, const double* system_values, hoefem_pr
   to_f32(A.d, A32.p, mm.nnz, mm.stream);
   if (p && p->p.kind == PREC_SCHWARZ && p->p.ready && (!p->p.vals32.p || !p->p.want_fp32)) {
     p->p.want_fp32 = true;
-    p->p.vals32.alloc(p->p.nnz);
-    to_f32(p->p.vals.p, p->p.vals32.p, p->p.nnz, mm.stream);
+    precond_to_fp32(p->p, mm.stream);
   }
   HOEFEM_CUDA(cudaMemcpyAsync(w.b.p, B.d, mm.ndof * sizeof(double), cudaMemcpyDeviceToDevice, mm.stream));
   HOEFEM_CUDA(cudaMemcpyAsync(w.x.p, X.d, mm.ndof * sizeof(double), cudaMemcpyDeviceToDevice, mm.stream));

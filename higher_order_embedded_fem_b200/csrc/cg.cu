@@ -114,6 +114,71 @@ __global__ void __launch_bounds__(TPB) k_cg_prec_spmv(NodeRows P, const VP* __re
   }
 }
 
+// Schwarz apply as dense block products: y_s = B_s r_s for every subdomain s
+// (B_s the symmetric part of the inverted block, row-major dim x dim).  B_s is
+// symmetric, so thread j accumulates column j over the rows: every row is
+// read by consecutive threads (coalesced) and no reduction is needed.
+constexpr int SCHWARZ_BLOCK_TPB = 96;  // >= 3 x 27 rows of a Hex27 subdomain
+
+template <class VB>
+__global__ void __launch_bounds__(SCHWARZ_BLOCK_TPB) k_cg_schwarz_blocks(const int* __restrict__ sub_off,
+                                                                         const int* __restrict__ sub_nodes,
+                                                                         const long long* __restrict__ stage_off,
+                                                                         const VB* __restrict__ B,
+                                                                         const double* __restrict__ r,
+                                                                         double* __restrict__ y, const CgState* st,
+                                                                         int init) {
+  if (!init && st->done) return;
+  __shared__ double rs[SCHWARZ_BLOCK_TPB];
+  const int s = blockIdx.x;
+  const int o = sub_off[s];
+  const int dim = 3 * (sub_off[s + 1] - o);
+  const int j = threadIdx.x;
+  if (j < dim) rs[j] = r[3 * sub_nodes[o + j / 3] + j % 3];
+  __syncthreads();
+  if (j >= dim) return;
+  const VB* Bs = B + stage_off[s];
+  double acc = 0.0;
+#pragma unroll 9
+  for (int i = 0; i < dim; ++i) acc += (double)Bs[(size_t)i * dim + j] * rs[i];
+  y[3 * o + j] = acc;
+}
+
+// z = P r from the block products (each node: its subdomains' entries in
+// subdomain order; untreated nodes: their diagonal value times r) ; z.r ;
+// when `init` the last block stores zTr, otherwise it forms beta.
+template <class VP>
+__global__ void __launch_bounds__(TPB) k_cg_schwarz_gather(int n, const int* __restrict__ pair_off,
+                                                           const int* __restrict__ pair_y,
+                                                           const double* __restrict__ y,
+                                                           const unsigned char* __restrict__ diag_only,
+                                                           const long long* __restrict__ pbase,
+                                                           const VP* __restrict__ pv, const double* __restrict__ r,
+                                                           double* __restrict__ z, double* partials, unsigned* counter,
+                                                           CgState* st, int init) {
+  if (!init && st->done) return;
+  double acc[1] = {0.0};
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int a = t / 3, i = t - 3 * a;
+    double v = 0.0;
+    if (diag_only[a]) {
+      v = (double)pv[pbase[a] + i] * r[t];
+    } else {
+      for (int q = pair_off[a]; q < pair_off[a + 1]; ++q) v += y[pair_y[q] + i];
+    }
+    z[t] = v;
+    acc[0] += v * r[t];
+  }
+  double tot[1];
+  if (grid_reduce_last_k<1>(acc, partials, counter, tot) && threadIdx.x == 0) {
+    if (init) st->zTr = tot[0];
+    else {
+      st->beta = tot[0] / st->zTr;
+      st->zTr = tot[0];
+    }
+  }
+}
+
 __global__ void k_cg_copy(int n, const double* __restrict__ a, double* __restrict__ b) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
@@ -297,6 +362,30 @@ void enqueue_Ap(CgWork& w, Operator A, cudaStream_t s) {
 }
 
 void enqueue_prec_spmv(CgWork& w, const Precond* P, bool p32, int init, cudaStream_t s) {
+  if (P->block_apply) {
+    const int n = (int)w.n;
+    HOEFEM_REQUIRE(!p32 || P->nsub == 0 || P->bsym32.p, HOEFEM_ERR_INVALID_ARGUMENT,
+                   "FP32 Schwarz blocks missing (update the preconditioner for FP32)");
+    if (P->nsub > 0) {
+      if (p32)
+        (note_launch(), k_cg_schwarz_blocks<float><<<(int)P->nsub, SCHWARZ_BLOCK_TPB, 0, s>>>(
+                            P->d_sub_off.p, P->d_sub_nodes.p, P->d_stage_off.p, P->bsym32.p, w.r.p, P->ysub.p, w.st.p,
+                            init));
+      else
+        (note_launch(), k_cg_schwarz_blocks<double><<<(int)P->nsub, SCHWARZ_BLOCK_TPB, 0, s>>>(
+                            P->d_sub_off.p, P->d_sub_nodes.p, P->d_stage_off.p, P->bsym.p, w.r.p, P->ysub.p, w.st.p,
+                            init));
+    }
+    if (p32)
+      (note_launch(), k_cg_schwarz_gather<float><<<vec_grid(n), TPB, 0, s>>>(
+                          n, P->d_npair_off.p, P->d_npair.p, P->ysub.p, P->d_diag_only.p, P->d_base.p, P->vals32.p,
+                          w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, init));
+    else
+      (note_launch(), k_cg_schwarz_gather<double><<<vec_grid(n), TPB, 0, s>>>(
+                          n, P->d_npair_off.p, P->d_npair.p, P->ysub.p, P->d_diag_only.p, P->d_base.p, P->vals.p,
+                          w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, init));
+    return;
+  }
   NodeRows PR = P->rows();
   PR.lanes = lanes_for(*P, p32);
   HOEFEM_LANES_DISPATCH(PR.lanes, {
@@ -330,7 +419,7 @@ void enqueue_iteration(CgWork& w, Operator A, const Precond* P, bool p32, cudaSt
 CgWork::Graph& graph_for(CgWork& w, Operator A, const Precond* P, bool p32) {
   // the key also holds the SpMV variants the graph was captured with
   const intptr_t variants = (intptr_t)lanes_for(*w.m, A.v32 != nullptr) * 1024 +
-                            (P && P->kind == PREC_SCHWARZ ? lanes_for(*P, p32) : 0);
+                            (P && P->kind == PREC_SCHWARZ ? (P->block_apply ? 1000 : lanes_for(*P, p32)) : 0);
   const void* key[4] = {A.v32 ? (const void*)A.v32 : (const void*)A.v64, (const void*)P, prec_key(P, p32),
                         (const void*)(intptr_t)(((P ? P->kind : 0) * 2 + (p32 ? 1 : 0)) + 8 * variants)};
   for (auto& g : w.graphs)
@@ -423,7 +512,8 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   }
   // online SpMV variant choice: candidate pairs (operator lanes, Schwarz lanes)
   const bool f32 = A.v32 != nullptr;
-  const bool schwarz = P && P->kind == PREC_SCHWARZ;
+  // (with the block apply the Schwarz SpMV variant plays no part)
+  const bool schwarz = P && P->kind == PREC_SCHWARZ && !P->block_apply;
   static const int cand_lanes[4] = {8, 16, 32, 132};
   const int ncand = schwarz ? 16 : 4;
   CgWork::Tuning& tu = w.tuning[f32 ? 1 : 0];

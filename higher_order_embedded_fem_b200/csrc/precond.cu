@@ -294,6 +294,22 @@ __global__ void __launch_bounds__(256) k_schwarz_scatter(const int* __restrict__
   }
 }
 
+// Symmetric part of every staged block (what the scatter adds), kept for the
+// block apply.
+__global__ void __launch_bounds__(256) k_schwarz_symmetrize(const int* __restrict__ sub_off,
+                                                            const long long* __restrict__ stage_off,
+                                                            const double* __restrict__ stage,
+                                                            double* __restrict__ sym) {
+  const int s = blockIdx.x;
+  const int dim = 3 * (sub_off[s + 1] - sub_off[s]);
+  const double* blk = stage + stage_off[s];
+  double* out = sym + stage_off[s];
+  for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) {
+    const int r = k / dim, c = k % dim;
+    out[k] = 0.5 * (blk[k] + blk[c * dim + r]);
+  }
+}
+
 __global__ void k_schwarz_untreated(int nun, const int* __restrict__ untreated, const long long* __restrict__ pbase,
                                     NodeRows A, const double* __restrict__ J, double* __restrict__ pv, int* err) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -453,6 +469,22 @@ void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes
   p.d_base.upload(p.base, st);
   p.d_diag_only.upload(p.diag_only, st);
   p.d_stage_off.upload(stage_off, st);
+  {
+    // node -> (subdomain, local node) incidences for the block apply
+    std::vector<int> poff(m.nv + 1, 0), pairs;
+    for (i64 s = 0; s < nsub; ++s)
+      for (i64 k = sub_off[s]; k < sub_off[s + 1]; ++k) poff[sub_nodes[k] + 1] += 1;
+    for (i64 a = 0; a < m.nv; ++a) poff[a + 1] += poff[a];
+    pairs.resize(poff[m.nv]);
+    std::vector<int> fill(poff.begin(), poff.end() - 1);
+    for (i64 s = 0; s < nsub; ++s)
+      for (i64 k = sub_off[s]; k < sub_off[s + 1]; ++k) pairs[fill[sub_nodes[k]]++] = (int)(3 * k);
+    p.d_npair_off.upload(poff, st);
+    p.d_npair.upload(pairs, st);
+    p.ysub.alloc(3 * sub_off[nsub]);
+    p.bsym.alloc(stage_off[nsub]);
+    p.block_apply = 3 * p.max_nodes <= 96;  // one thread per block row
+  }
   p.vals.alloc(p.nnz);
   p.vals.zero(st);
   p.staging.alloc(stage_off[nsub]);
@@ -511,6 +543,8 @@ void precond_update(Precond& p, const double* J, cudaStream_t s) {
                                                                            m.d_adj_off.p, m.d_base.p, J, p.d_stage_off.p,
                                                                            p.staging.p, p.d_err.p));
     HOEFEM_CUDA(cudaGetLastError());
+    (note_launch(), k_schwarz_symmetrize<<<(int)p.nsub, 256, 0, s>>>(p.d_sub_off.p, p.d_stage_off.p, p.staging.p,
+                                                                      p.bsym.p));
     const int nc = (int)p.color_off.size() - 1;
     for (int c = 0; c < nc; ++c) {
       int b = (int)p.color_off[c], cnt = (int)(p.color_off[c + 1] - b);
@@ -525,11 +559,19 @@ void precond_update(Precond& p, const double* J, cudaStream_t s) {
         (int)p.untreated.size(), p.d_untreated.p, p.d_base.p, A, J, p.vals.p, p.d_err.p));
   HOEFEM_CUDA(cudaGetLastError());
   check_err(p.d_err, s);
-  if (p.want_fp32) {
-    if (p.vals32.n < (size_t)p.nnz) p.vals32.alloc(p.nnz);
-    to_f32(p.vals.p, p.vals32.p, p.nnz, s);
-  }
+  if (p.want_fp32) precond_to_fp32(p, s);
   p.ready = true;
+}
+
+// FP32 copies of the Schwarz values: the assembled CSR and the symmetrized
+// blocks of the block apply (both, so that either apply can run in FP32).
+void precond_to_fp32(Precond& p, cudaStream_t s) {
+  if (p.vals32.n < (size_t)p.nnz) p.vals32.alloc(p.nnz);
+  to_f32(p.vals.p, p.vals32.p, p.nnz, s);
+  if (p.nsub > 0) {
+    if (p.bsym32.n < p.bsym.n) p.bsym32.alloc(p.bsym.n);
+    to_f32(p.bsym.p, p.bsym32.p, (long long)p.bsym.n, s);
+  }
 }
 
 void precond_apply(const Precond& p, const double* r, double* z, cudaStream_t s) {

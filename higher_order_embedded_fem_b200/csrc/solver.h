@@ -39,6 +39,15 @@ struct Precond {
   bool spmv_pinned = false;  // set explicitly by the caller: no autotuning
   DBuf<int> d_tnodes;      // nodes with subdomain rows (the rest are untreated, diagonal only)
   i64 tnodes_count = 0;
+  // Block apply (CG): the symmetrized inverted subdomain blocks (staging
+  // layout) applied as dense products into ysub (3 entries per subdomain
+  // node), then summed per node over its subdomains in subdomain order.
+  bool block_apply = true;
+  DBuf<double> bsym;
+  DBuf<float> bsym32;
+  DBuf<double> ysub;
+  DBuf<int> d_npair_off;  // nv + 1
+  DBuf<int> d_npair;      // ysub offset of every (subdomain, node) incidence, by node, subdomains ascending
   NodeRows rows() const;
 };
 
@@ -46,6 +55,7 @@ void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes
                             i64 nun);
 void precond_update(Precond& p, const double* system_vals, cudaStream_t s);
 void precond_apply(const Precond& p, const double* r, double* z, cudaStream_t s);
+void precond_to_fp32(Precond& p, cudaStream_t s);
 
 struct CgState {
   double bnorm, tol, zTr, pAp, rr, alpha, beta;

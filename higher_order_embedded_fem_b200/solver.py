@@ -75,6 +75,11 @@ class SchwarzPreconditioner(DiagonalPreconditioner):
         """8 / 16 / 32 lanes per node, +100 for the column-streaming traversal."""
         check(lib().hoefem_precond_set_spmv_variant(self._h, int(variant)))
 
+    def set_block_apply(self, on):
+        """CG applies the subdomain blocks as dense products (True, default) or
+        the assembled CSR matrix (False); both are P r up to rounding."""
+        check(lib().hoefem_precond_set_block_apply(self._h, 1 if on else 0))
+
     def spmv_variants(self):
         """(FP64-value variant, FP32-value variant) in use."""
         a, b = C.c_int32(), C.c_int32()

@@ -227,6 +227,12 @@ int hoefem_precond_update(hoefem_precond p, const double* system_values, int mem
 int hoefem_precond_apply(hoefem_precond p, const double* r, double* z, int mem);
 /* Schwarz pattern / values for inspection (nnz first, then the arrays). */
 int hoefem_precond_nnz(hoefem_precond p, int64_t* nnz);
+/* How the CG applies a Schwarz preconditioner (no reference counterpart; the
+   reference applies the assembled CSR matrix with MKL): on (default) = the
+   symmetrized inverted subdomain blocks as dense products, summed per node in
+   subdomain order; off = SpMV over the assembled values.  Both are P r; they
+   differ only in rounding.  hoefem_precond_apply always uses the CSR. */
+int hoefem_precond_set_block_apply(hoefem_precond p, int32_t on);
 /* SpMV variant of the Schwarz apply (as hoefem_model_set_spmv_variant);
    chosen by the autotuner at creation and by the CG's online choice
    otherwise. */

@@ -279,3 +279,27 @@ def test_schwarz_zero_diagonal_is_an_error():
     with pytest.raises(H.HoefemError) as ei:
         D.update(np.zeros(m.nnz))
     assert ei.value.status == "ZERO_DIAGONAL"
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_schwarz_block_apply_matches_assembled_apply(mixed):
+    # The CG's Schwarz apply as dense subdomain block products (default) and as
+    # the SpMV over the assembled values: the same P r up to rounding, so the
+    # Newton step agrees to the CG tolerance and the iteration counts match.
+    e, m, mat, ref = embedded_setup(6)
+    bc = e.nodes_below(2, 1e-9)
+    comp = H.SchwarzPreconditionerComponent.from_embedded_model(m, e.volume_fractions, 0.5)
+    P = comp.build(m)
+    integ = H.NewtonCgIntegrator3d(m, mat, 1000.0, bc, preconditioner=P)
+    integ.set_precision(mixed, 0.1)
+    u0 = H.scenes.random_normal(1, m.ndof(), 0.01 * e.cell_size)
+    out = []
+    for on in (True, False):
+        P.set_block_apply(on)
+        u, v = u0.copy(), np.zeros(m.ndof())
+        st = integ.step(u, v, 0.0, 1e-3)
+        out.append((u, v, st))
+    (ub, vb, sb), (uc, vc, sc) = out
+    assert sb["newton_iterations"] == sc["newton_iterations"]
+    assert abs(sb["total_cg_iterations"] - sc["total_cg_iterations"]) <= 2
+    assert rel(ub, uc) < 1e-8 and rel(vb, vc) < 1e-8
