@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(SCHWARZ_BLOCK_TPB) k_cg_schwarz_blocks(const i
                                                                          const int* __restrict__ sub_nodes,
                                                                          const long long* __restrict__ stage_off,
                                                                          const VB* __restrict__ B,
+                                                                         const int* __restrict__ slot,
                                                                          const double* __restrict__ r,
                                                                          double* __restrict__ y, const CgState* st,
                                                                          int init) {
@@ -141,15 +142,14 @@ __global__ void __launch_bounds__(SCHWARZ_BLOCK_TPB) k_cg_schwarz_blocks(const i
   double acc = 0.0;
 #pragma unroll 9
   for (int i = 0; i < dim; ++i) acc += (double)Bs[(size_t)i * dim + j] * rs[i];
-  y[3 * o + j] = acc;
+  y[3 * slot[o + j / 3] + j % 3] = acc;
 }
 
-// z = P r from the block products (each node: its subdomains' entries in
-// subdomain order; untreated nodes: their diagonal value times r) ; z.r ;
-// when `init` the last block stores zTr, otherwise it forms beta.
+// z = P r from the block products (each node: its consecutive slots, its
+// subdomains in ascending order; untreated nodes: their diagonal value times
+// r) ; z.r ; when `init` the last block stores zTr, otherwise it forms beta.
 template <class VP>
 __global__ void __launch_bounds__(TPB) k_cg_schwarz_gather(int n, const int* __restrict__ pair_off,
-                                                           const int* __restrict__ pair_y,
                                                            const double* __restrict__ y,
                                                            const unsigned char* __restrict__ diag_only,
                                                            const long long* __restrict__ pbase,
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(TPB) k_cg_schwarz_gather(int n, const int* __r
     if (diag_only[a]) {
       v = (double)pv[pbase[a] + i] * r[t];
     } else {
-      for (int q = pair_off[a]; q < pair_off[a + 1]; ++q) v += y[pair_y[q] + i];
+      for (int q = pair_off[a]; q < pair_off[a + 1]; ++q) v += y[3 * q + i];
     }
     z[t] = v;
     acc[0] += v * r[t];
@@ -369,20 +369,20 @@ void enqueue_prec_spmv(CgWork& w, const Precond* P, bool p32, int init, cudaStre
     if (P->nsub > 0) {
       if (p32)
         (note_launch(), k_cg_schwarz_blocks<float><<<(int)P->nsub, SCHWARZ_BLOCK_TPB, 0, s>>>(
-                            P->d_sub_off.p, P->d_sub_nodes.p, P->d_stage_off.p, P->bsym32.p, w.r.p, P->ysub.p, w.st.p,
+                            P->d_sub_off.p, P->d_sub_nodes.p, P->d_stage_off.p, P->bsym32.p, P->d_npair.p, w.r.p, P->ysub.p, w.st.p,
                             init));
       else
         (note_launch(), k_cg_schwarz_blocks<double><<<(int)P->nsub, SCHWARZ_BLOCK_TPB, 0, s>>>(
-                            P->d_sub_off.p, P->d_sub_nodes.p, P->d_stage_off.p, P->bsym.p, w.r.p, P->ysub.p, w.st.p,
+                            P->d_sub_off.p, P->d_sub_nodes.p, P->d_stage_off.p, P->bsym.p, P->d_npair.p, w.r.p, P->ysub.p, w.st.p,
                             init));
     }
     if (p32)
       (note_launch(), k_cg_schwarz_gather<float><<<vec_grid(n), TPB, 0, s>>>(
-                          n, P->d_npair_off.p, P->d_npair.p, P->ysub.p, P->d_diag_only.p, P->d_base.p, P->vals32.p,
+                          n, P->d_npair_off.p, P->ysub.p, P->d_diag_only.p, P->d_base.p, P->vals32.p,
                           w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, init));
     else
       (note_launch(), k_cg_schwarz_gather<double><<<vec_grid(n), TPB, 0, s>>>(
-                          n, P->d_npair_off.p, P->d_npair.p, P->ysub.p, P->d_diag_only.p, P->d_base.p, P->vals.p,
+                          n, P->d_npair_off.p, P->ysub.p, P->d_diag_only.p, P->d_base.p, P->vals.p,
                           w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, init));
     return;
   }

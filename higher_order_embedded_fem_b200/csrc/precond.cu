@@ -470,17 +470,17 @@ void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes
   p.d_diag_only.upload(p.diag_only, st);
   p.d_stage_off.upload(stage_off, st);
   {
-    // node -> (subdomain, local node) incidences for the block apply
-    std::vector<int> poff(m.nv + 1, 0), pairs;
+    // block apply: every (subdomain, node) incidence gets a slot; a node's
+    // slots are consecutive, its subdomains in ascending order
+    std::vector<int> poff(m.nv + 1, 0), slot(sub_off[nsub]);
     for (i64 s = 0; s < nsub; ++s)
       for (i64 k = sub_off[s]; k < sub_off[s + 1]; ++k) poff[sub_nodes[k] + 1] += 1;
     for (i64 a = 0; a < m.nv; ++a) poff[a + 1] += poff[a];
-    pairs.resize(poff[m.nv]);
     std::vector<int> fill(poff.begin(), poff.end() - 1);
     for (i64 s = 0; s < nsub; ++s)
-      for (i64 k = sub_off[s]; k < sub_off[s + 1]; ++k) pairs[fill[sub_nodes[k]]++] = (int)(3 * k);
+      for (i64 k = sub_off[s]; k < sub_off[s + 1]; ++k) slot[k] = fill[sub_nodes[k]]++;
     p.d_npair_off.upload(poff, st);
-    p.d_npair.upload(pairs, st);
+    p.d_npair.upload(slot, st);
     p.ysub.alloc(3 * sub_off[nsub]);
     p.bsym.alloc(stage_off[nsub]);
     p.block_apply = 3 * p.max_nodes <= 96;  // one thread per block row

@@ -46,8 +46,8 @@ struct Precond {
   DBuf<double> bsym;
   DBuf<float> bsym32;
   DBuf<double> ysub;
-  DBuf<int> d_npair_off;  // nv + 1
-  DBuf<int> d_npair;      // ysub offset of every (subdomain, node) incidence, by node, subdomains ascending
+  DBuf<int> d_npair_off;  // nv + 1: a node's slots in ysub (3 entries each)
+  DBuf<int> d_npair;      // slot of every (subdomain, node) incidence (sub_nodes order)
   NodeRows rows() const;
 };
 
