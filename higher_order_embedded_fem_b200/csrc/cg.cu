@@ -13,8 +13,11 @@
 // All reductions are deterministic: the node-row kernels fetch chunks of
 // nodes dynamically but sum each chunk in a fixed order and the chunks in
 // index order; the vector kernels use a fixed grid and sum block partials in
-// block order.  The SpMV variants of the operator and of the Schwarz apply
-// are chosen online per value precision by timing the first chunks.
+// block order.  A Schwarz preconditioner is applied either as dense products
+// with its symmetrized inverted subdomain blocks plus a per-node gather
+// (default) or as an SpMV over its assembled values.  The SpMV variants of
+// the operator (and of an assembled Schwarz apply) are chosen online per
+// value precision by timing the first chunks.
 #include <cuda_runtime.h>
 
 #include <algorithm>

@@ -6,9 +6,11 @@
 // force scatter); materials in fenris/src/solid/materials.rs.
 //
 // Layout: connectivity is SoA (conn[I * ne + e]) so that the lanes that own
-// the nodes of one element read it with one transaction per node.  One warp
-// owns a Tet10 element (4 elements per 128-thread CTA); one 128-thread CTA
-// owns a Hex27 element.  Per quadrature point the owning warp builds the
+// the nodes of one element read it with one transaction per node.  Forces:
+// one warp per Tet10 element with a lane per quadrature point (affine
+// geometry), eight warps per Hex27 element over its points.  Stiffness: 64
+// threads per Tet10 element (4 per CTA; the per-point phase one lane per
+// point), 384 per Hex27 element.  Per quadrature point the kernel builds the
 // per-node vectors a_I = sqrt(w |det J|) J^-T grad N_I, b_I = F a_I and
 // c_I = Cof(F) a_I (SNH) or S a_I (StVK); the stiffness block of a node pair
 // is then a closed-form rank-structured expression of those vectors (the
