@@ -130,15 +130,21 @@ __global__ void __launch_bounds__(SCHWARZ_BLOCK_TPB) k_cg_schwarz_blocks(const i
                                                                          const VB* __restrict__ B,
                                                                          const int* __restrict__ slot,
                                                                          const double* __restrict__ r,
+                                                                         const double* __restrict__ Ap,
                                                                          double* __restrict__ y, const CgState* st,
-                                                                         int init) {
+                                                                         int init, int update) {
   if (!init && st->done) return;
   __shared__ double rs[SCHWARZ_BLOCK_TPB];
   const int s = blockIdx.x;
   const int o = sub_off[s];
   const int dim = 3 * (sub_off[s + 1] - o);
   const int j = threadIdx.x;
-  if (j < dim) rs[j] = r[3 * sub_nodes[o + j / 3] + j % 3];
+  if (j < dim) {
+    // with `update`: the residual after this iteration's step, r - alpha Ap
+    // (the same expression the gather stores)
+    const int d = 3 * sub_nodes[o + j / 3] + j % 3;
+    rs[j] = update ? r[d] - st->alpha * Ap[d] : r[d];
+  }
   __syncthreads();
   if (j >= dim) return;
   const VB* Bs = B + stage_off[s];
@@ -151,33 +157,58 @@ __global__ void __launch_bounds__(SCHWARZ_BLOCK_TPB) k_cg_schwarz_blocks(const i
 // z = P r from the block products (each node: its consecutive slots, its
 // subdomains in ascending order; untreated nodes: their diagonal value times
 // r) ; z.r ; when `init` the last block stores zTr, otherwise it forms beta.
+// With `update` it also takes the CG step of this iteration first (x += alpha
+// p, r -= alpha Ap, r.r, iteration count and convergence, as k_cg_update):
+// the block products already used the updated residual.
 template <class VP>
 __global__ void __launch_bounds__(TPB) k_cg_schwarz_gather(int n, const int* __restrict__ pair_off,
                                                            const double* __restrict__ y,
                                                            const unsigned char* __restrict__ diag_only,
                                                            const long long* __restrict__ pbase,
-                                                           const VP* __restrict__ pv, const double* __restrict__ r,
-                                                           double* __restrict__ z, double* partials, unsigned* counter,
-                                                           CgState* st, int init) {
+                                                           const VP* __restrict__ pv, double* __restrict__ r,
+                                                           double* __restrict__ z, double* __restrict__ x,
+                                                           const double* __restrict__ p,
+                                                           const double* __restrict__ Ap, double* partials,
+                                                           unsigned* counter, CgState* st, int init, int update) {
   if (!init && st->done) return;
-  double acc[1] = {0.0};
+  const double alpha = update ? st->alpha : 0.0;
+  double acc[2] = {0.0, 0.0};  // r.r (update only), z.r
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    double ri = r[t];
+    if (update) {
+      x[t] = x[t] + alpha * p[t];
+      ri = r[t] - alpha * Ap[t];
+      r[t] = ri;
+      acc[0] += ri * ri;
+    }
     const int a = t / 3, i = t - 3 * a;
     double v = 0.0;
     if (diag_only[a]) {
-      v = (double)pv[pbase[a] + i] * r[t];
+      v = (double)pv[pbase[a] + i] * ri;
     } else {
       for (int q = pair_off[a]; q < pair_off[a + 1]; ++q) v += y[3 * q + i];
     }
     z[t] = v;
-    acc[0] += v * r[t];
+    acc[1] += v * ri;
   }
-  double tot[1];
-  if (grid_reduce_last_k<1>(acc, partials, counter, tot) && threadIdx.x == 0) {
-    if (init) st->zTr = tot[0];
-    else {
-      st->beta = tot[0] / st->zTr;
-      st->zTr = tot[0];
+  double tot[2];
+  if (grid_reduce_last_k<2>(acc, partials, counter, tot) && threadIdx.x == 0) {
+    if (init) {
+      st->zTr = tot[1];
+    } else if (update) {
+      st->rr = tot[0];
+      st->iters += 1;
+      if (sqrt(tot[0]) <= st->tol * st->bnorm) { st->done = 1; st->status = HOEFEM_OK; }
+      else if (st->max_iter >= 0 && st->iters >= st->max_iter) {
+        st->done = 1;
+        st->status = HOEFEM_CG_MAX_ITERATIONS;
+      } else {
+        st->beta = tot[1] / st->zTr;
+        st->zTr = tot[1];
+      }
+    } else {
+      st->beta = tot[1] / st->zTr;
+      st->zTr = tot[1];
     }
   }
 }
@@ -364,7 +395,8 @@ void enqueue_Ap(CgWork& w, Operator A, cudaStream_t s) {
   });
 }
 
-void enqueue_prec_spmv(CgWork& w, const Precond* P, bool p32, int init, cudaStream_t s) {
+// update (block apply only): fuse this iteration's x / r step into the apply
+void enqueue_prec_spmv(CgWork& w, const Precond* P, bool p32, int init, cudaStream_t s, int update = 0) {
   if (P->block_apply) {
     const int n = (int)w.n;
     HOEFEM_REQUIRE(!p32 || P->nsub == 0 || P->bsym32.p, HOEFEM_ERR_INVALID_ARGUMENT,
@@ -372,21 +404,21 @@ void enqueue_prec_spmv(CgWork& w, const Precond* P, bool p32, int init, cudaStre
     if (P->nsub > 0) {
       if (p32)
         (note_launch(), k_cg_schwarz_blocks<float><<<(int)P->nsub, SCHWARZ_BLOCK_TPB, 0, s>>>(
-                            P->d_sub_off.p, P->d_sub_nodes.p, P->d_stage_off.p, P->bsym32.p, P->d_npair.p, w.r.p, P->ysub.p, w.st.p,
-                            init));
+                            P->d_sub_off.p, P->d_sub_nodes.p, P->d_stage_off.p, P->bsym32.p, P->d_npair.p, w.r.p, w.Ap.p, P->ysub.p,
+                            w.st.p, init, update));
       else
         (note_launch(), k_cg_schwarz_blocks<double><<<(int)P->nsub, SCHWARZ_BLOCK_TPB, 0, s>>>(
-                            P->d_sub_off.p, P->d_sub_nodes.p, P->d_stage_off.p, P->bsym.p, P->d_npair.p, w.r.p, P->ysub.p, w.st.p,
-                            init));
+                            P->d_sub_off.p, P->d_sub_nodes.p, P->d_stage_off.p, P->bsym.p, P->d_npair.p, w.r.p, w.Ap.p, P->ysub.p,
+                            w.st.p, init, update));
     }
     if (p32)
       (note_launch(), k_cg_schwarz_gather<float><<<vec_grid(n), TPB, 0, s>>>(
                           n, P->d_npair_off.p, P->ysub.p, P->d_diag_only.p, P->d_base.p, P->vals32.p,
-                          w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, init));
+                          w.r.p, w.z.p, w.x.p, w.p.p, w.Ap.p, w.partials.p, w.counter.p, w.st.p, init, update));
     else
       (note_launch(), k_cg_schwarz_gather<double><<<vec_grid(n), TPB, 0, s>>>(
                           n, P->d_npair_off.p, P->ysub.p, P->d_diag_only.p, P->d_base.p, P->vals.p,
-                          w.r.p, w.z.p, w.partials.p, w.counter.p, w.st.p, init));
+                          w.r.p, w.z.p, w.x.p, w.p.p, w.Ap.p, w.partials.p, w.counter.p, w.st.p, init, update));
     return;
   }
   NodeRows PR = P->rows();
@@ -407,7 +439,9 @@ void enqueue_iteration(CgWork& w, Operator A, const Precond* P, bool p32, cudaSt
   const int vg = vec_grid(n);
   enqueue_Ap(w, A, s);
   const int kind = P ? P->kind : PREC_NONE;
-  if (kind == PREC_SCHWARZ) {
+  if (kind == PREC_SCHWARZ && P->block_apply) {
+    enqueue_prec_spmv(w, P, p32, 0, s, 1);  // the step fused into the apply
+  } else if (kind == PREC_SCHWARZ) {
     (note_launch(), k_cg_update<<<vg, TPB, 0, s>>>(n, 0, nullptr, w.x.p, w.r.p, w.p.p, w.Ap.p, w.z.p, w.partials.p,
                                                    w.counter.p, w.st.p));
     enqueue_prec_spmv(w, P, p32, 0, s);
