@@ -35,7 +35,13 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Newton-step ms & CG iters at 1e-6 rel res: learned/FP32 vs plain FP64 on 1 GPU"
 DT = 1e-3
-NEWTON_ITERS = 5  # Newton iterations of the benchmark step (GPU and oracle agree)
+# arithmetic of each variant (the line's `dtype` is the headline variant's)
+DTYPES = {
+    "plain": "f64",
+    "mixed": "mixed: f32 element stiffness arithmetic, f32 operator and Schwarz values in CG, f64 vectors, dot "
+             "products, residual replacement and CSR accumulation",
+    "learned": "mixed (as the mixed variant) + bf16 MLP inference with f32 accumulation",
+}
 
 
 def parse():
@@ -173,79 +179,64 @@ def max_over_ranks(x, world, device=None):
     return float(t.item())
 
 
-def cpu_reference_step(e, model, mat, bc, comp, u0, v0, cg_tol, threads):
-    """The oracle (FP64 CPU restatement of the reference path) on the same scene."""
+def workload_name(n, cg_tol):
+    """The workload string both arms report (identical by construction)."""
+    return ("embedded Hex27 hollow cylinder %d^3 (r 0.3-0.4), StVK E=5e5 nu=0.45, one backward-Euler Newton step "
+            "dt=1e-3, Schwarz-CG to %g" % (n, cg_tol))
+
+
+def oracle_step_sample(n, seed, cg_tol, threads):
+    """The reference path's CPU restatement (the oracle) on the benchmark scene,
+    built entirely on the oracle side (oracle/scenes.py, checked bit for bit
+    against the product's scene): returns (ref, u0, v0) ready for ref.step."""
     from oracle import oracle as O
+    from oracle import scenes as OS
 
     if threads:
         O.set_num_threads(threads)
-    b0, b1 = e.blocks
-    ref = O.Scene(e.vertices)
-    ref.add_block(O.ELEM_HEX27, b0.connectivity, b0.weights, b0.points)
-    ref.add_block(O.ELEM_HEX27, b1.connectivity, b1.weights, b1.points, qoff=b1.offsets)
-    ref.finalize_pattern()
-    ref.set_material(O.MAT_STVK, mat.lame.mu, mat.lame.lam, 1000.0)
-    ref.set_bc(bc)
-    ref.set_gravity(True)
-    ref.set_schwarz(comp.schwarz_connectivity, comp.untreated_nodes)
-    ref.set_solver(cg_tol, 500, 100)
-    ref.setup()
-    return ref
+    sc = OS.embedded_cylinder(n, 0.3, 0.4, 8, 27, seed)
+    u0, v0 = OS.sway_state(sc, 0.02, 0.01, 1000 + seed)
+    ref = OS.cylinder_reference_scene(sc, cg_tol=cg_tol)
+    return ref, u0, v0
 
 
-def newton_iteration_sample(ref, u0, v0, bc, cg_tol):
-    """A bounded sample of the reference path on the same scene: the first
-    Newton iteration of the step (eval_f, stiffness, Jacobian combination,
-    Schwarz update, Schwarz-CG to cg_tol, one line-search evaluation), all
-    in the oracle.  Returns (ms, cg iterations)."""
-    nd = u0.size
-    bmask = np.zeros(nd, dtype=bool)
-    for a in bc:
-        bmask[3 * a:3 * a + 3] = True
-    t0 = time.perf_counter()
-    up = u0 + DT * v0
-    up[bmask] = 0.0
-    F = -DT * ref.eval_f(up, v0)
-    F[bmask] = 0.0
-    J = ref.jacobian(ref.stiffness(up), DT)
-    ref.schwarz_update(J)
-    st, x, it = ref.cg(J, F, cg_tol, 500)
-    ref.eval_f(up - DT * x, v0 - x)
-    return (time.perf_counter() - t0) * 1e3, it
+def timed_oracle_steps(ref, u0, v0, warmup, steps):
+    """Whole backward-Euler steps of the oracle from the same initial state:
+    per-step wall ms, CG iterations and Newton iterations of the last step."""
+    for _ in range(warmup):
+        ref.step(u0, v0, 0.0, DT)
+    times, st = [], None
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        _, _, st = ref.step(u0, v0, 0.0, DT)
+        times.append((time.perf_counter() - t0) * 1e3)
+    return times, st
 
 
 def run_reference(args):
+    """`--impl reference`: the reference path's CPU restatement (the Rust
+    reference cannot be built here) on all host cores, whole Newton steps, no
+    product code on the path."""
     world, rank, local = dist_setup(args.gpus)
     if rank != 0:
         return
-    import higher_order_embedded_fem_b200 as H
     from oracle import oracle as O
 
-    e, model, mat, bc, comp, u0, v0 = workload(H, args.n, args.seed)
-    threads = os.cpu_count() or 1
-    ref = cpu_reference_step(e, model, mat, bc, comp, u0, v0, args.cg_tol, threads)
-    # each step: one Newton iteration of the step (a bounded sample), scaled by
-    # the step's Newton iteration count (the GPU path and the oracle both take
-    # NEWTON_ITERS iterations on this workload)
-    for _ in range(args.warmup):
-        newton_iteration_sample(ref, u0, v0, bc, args.cg_tol)
-    times, cgit = [], 0
-    for _ in range(args.steps):
-        t, cgit = newton_iteration_sample(ref, u0, v0, bc, args.cg_tol)
-        times.append(t * NEWTON_ITERS)
+    ref, u0, v0 = oracle_step_sample(args.n, args.seed, args.cg_tol, os.cpu_count() or 1)
+    times, st = timed_oracle_steps(ref, u0, v0, args.warmup, args.steps)
     ms = float(np.mean(times))
     line = {
         "metric": METRIC, "value": ms, "unit": "ms", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": "embedded Hex27 hollow cylinder %d^3, StVK, one BE Newton step, Schwarz-CG 1e-6"
-                   % args.n, "ndof": model.ndof(), "nnz": model.nnz},
-        "cg_iterations_first_newton_iteration": int(cgit), "newton_iterations": NEWTON_ITERS,
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene, built by the oracle)",
+        "config": {"workload": workload_name(args.n, args.cg_tol), "ndof": int(u0.size), "nnz": int(ref.nnz)},
+        "cg_iterations": int(sum(st["cg_iters"])), "newton_iterations": int(st["newton_iters"]),
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": O.num_threads(), "kind": "port",
-                         "sample": "first Newton iteration of the step (force, stiffness, Jacobian, Schwarz update, "
-                                   "Schwarz-CG to 1e-6, one line-search force evaluation) in the oracle with "
-                                   "OpenMP over the host cores, times the step's %d Newton iterations" % NEWTON_ITERS},
+                         "sample": "whole backward-Euler Newton steps of the oracle (C++ FP64 restatement of the "
+                                   "reference path, OpenMP over the host cores), %d timed after %d warm-up"
+                                   % (args.steps, args.warmup)},
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "step_ms": times,
     }
     print(json.dumps(line), flush=True)
 
@@ -311,12 +302,14 @@ def run_hoefem(args):
         ck = clocks.stop()
         ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world, dev)
         s_ = per[-1]
+        eng = integ.cg_engine_stats()
         variants[vname] = {
             "ms_per_step": ms, "cg_iterations": int(s_["total_cg_iterations"]),
             "newton_iterations": int(s_["newton_iterations"]), "residual_norm": s_["residual_norm"],
             "phase_ms": {"forces": s_["ms_assemble_forces"], "stiffness": s_["ms_assemble_stiffness"],
                          "precond_update": s_["ms_precond_update"], "cg": s_["ms_cg"], "total": s_["ms_total"]},
             "gpu_launches": int(launches), "clocks": ck, "u": ud.cpu().numpy(),
+            "cg_engine": eng,
         }
         if vname == "learned":
             variants[vname].update({"learned_accepted": int(s_["learned_accepted"]),
@@ -336,8 +329,9 @@ def run_hoefem(args):
         if vn in variants and "plain" in variants:
             up, um = variants["plain"]["u"], variants[vn]["u"]
             variants[vn]["rel_diff_u_vs_plain"] = float(np.abs(um - up).max() / np.abs(up).max())
-    for v in variants.values():
+    for vn_, v in variants.items():
         v.pop("u")
+        v["cg_roofline"] = cg_roofline(v, vn_)
 
     # end to end through the public API with pinned host buffers
     uh = torch.empty(model.ndof(), dtype=torch.float64, pin_memory=True).numpy()
@@ -355,19 +349,20 @@ def run_hoefem(args):
     e2e_ms = max_over_ranks(e2e_ms, world, dev)
     model.set_stream(stream.cuda_stream)
 
-    # roofline of the dominant kernel class: node-row SpMV of the CG operator
-    roof = spmv_roofline(H, model, integ, mat, ud, stream, args.roofline_reps)
+    # roofline of the dominant kernel: the persistent streamed CG of the headline
+    # variant (its CUDA-event device time over the step's iterations)
+    roof = cg_roofline(variants[head], head)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        ref = cpu_reference_step(e, model, mat, bc, comp, u0, v0, args.cg_tol, os.cpu_count())
         from oracle import oracle as O
 
-        t, cgit = newton_iteration_sample(ref, u0, v0, bc, args.cg_tol)
-        cpu = {"value": t * NEWTON_ITERS, "unit": "ms", "cores": O.num_threads(), "kind": "port",
-               "sample": "first Newton iteration of the step in the oracle (OpenMP over the host cores), %.0f ms, "
-                         "times the step's %d Newton iterations" % (t, NEWTON_ITERS),
-               "cg_iterations_first_newton_iteration": int(cgit)}
+        ref, ru0, rv0 = oracle_step_sample(args.n, args.seed, args.cg_tol, os.cpu_count())
+        times, rst = timed_oracle_steps(ref, ru0, rv0, 0, 1)
+        cpu = {"value": times[0], "unit": "ms", "cores": O.num_threads(), "kind": "port",
+               "sample": "one whole backward-Euler Newton step of the oracle on the same scene (OpenMP over the "
+                         "host cores)", "cg_iterations": int(sum(rst["cg_iters"])),
+               "newton_iterations": int(rst["newton_iters"])}
 
     if rank == 0:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
@@ -375,11 +370,10 @@ def run_hoefem(args):
         line = {
             "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene, replicas per rank)",
+            "vs_baseline": None, "dtype": DTYPES[head], "data": "synthetic (seeded scene, replicas per rank)",
             "variant": {"mixed": "mixed_fp32", "plain": "plain_fp64", "learned": "learned_mixed"}[head],
             "variants": variants,
-            "config": {"workload": "embedded Hex27 hollow cylinder %d^3 (r 0.3-0.4), StVK E=5e5 nu=0.45, one "
-                                   "backward-Euler Newton step dt=1e-3, Schwarz-CG to %g" % (args.n, args.cg_tol),
+            "config": {"workload": workload_name(args.n, args.cg_tol),
                        "ndof": model.ndof(), "nnz": model.nnz, "elements": model.num_elements,
                        "schwarz_subdomains": len(comp.schwarz_connectivity),
                        "l2": "inputs larger than L2 (CSR values %d MB)" % (model.nnz * 8 // 2 ** 20),
@@ -399,6 +393,28 @@ def run_hoefem(args):
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def cg_roofline(var, head):
+    """Streamed CG of one variant: algorithmic bytes per iteration = operator
+    tiles (values + neighbour lists + tile headers) + Schwarz block chunks, the
+    data an iteration must read from HBM (vectors, 1 MB each, stay in L2);
+    achieved = bytes x iterations / summed device time of the persistent
+    launches (CUDA events on the launch stream)."""
+    eng = var.get("cg_engine") or {}
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
+    if not eng.get("launches") or not eng.get("iterations") or not eng.get("device_ms"):
+        return None
+    per_it = eng["operator_bytes"] + eng["schwarz_bytes"]
+    ms_it = eng["device_ms"] / eng["iterations"]
+    gbs = per_it / (ms_it * 1e-3) / 1e9
+    kern = {"plain": "k_cg_stream<double,double,2>", "mixed": "k_cg_stream<float,float,2>",
+            "learned": "k_cg_stream<float,float,2>"}[head]
+    return {"kernel": kern + " (persistent streamed Schwarz-PCG)", "bound": "hbm", "achieved": gbs, "peak": peak,
+            "unit": "GB/s", "frac": gbs / peak, "traffic": None, "bytes_per_iteration": per_it,
+            "us_per_iteration": ms_it * 1e3, "iterations": eng["iterations"], "launches": eng["launches"],
+            "peak_source": "measured" if os.path.exists(peaks_path) else "fallback"}
 
 
 def spmv_roofline(H, model, integ, mat, ud, stream, reps):

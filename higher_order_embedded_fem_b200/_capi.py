@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(_HERE, "libhoefem.so")
 HOEFEM_OK = 0
 STATUS = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "CUDA", 3: "OUT_OF_MEMORY", 4: "SINGULAR", 5: "NONFINITE", 6: "PATTERN",
-    7: "ZERO_DIAGONAL", 8: "NOT_FINALIZED", 10: "CG_INDEFINITE_OPERATOR", 11: "CG_INDEFINITE_PRECONDITIONER",
+    7: "ZERO_DIAGONAL", 8: "NOT_FINALIZED", 9: "DEVICE_TIMEOUT", 10: "CG_INDEFINITE_OPERATOR", 11: "CG_INDEFINITE_PRECONDITIONER",
     12: "CG_MAX_ITERATIONS", 20: "NEWTON_MAX_ITERATIONS", 21: "LINE_SEARCH_FAILED", 22: "SUBSTEPPING_FAILED",
     31: "NO_DEVICE",
 }
@@ -53,6 +53,14 @@ class StepStats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class CgEngineStats(C.Structure):
+    _fields_ = [("launches", C.c_int64), ("iterations", C.c_int64), ("device_ms", C.c_double),
+                ("operator_bytes", C.c_int64), ("schwarz_bytes", C.c_int64)]
+
+
+CG_ENGINE = {"auto": 0, "chunked": 1, "streamed": 2}
 
 
 class SceneInfo(C.Structure):
@@ -105,6 +113,10 @@ SIGNATURES = {
     "hoefem_integrator_create": (C.c_int, [vp, C.POINTER(Material), dbl, vp, i64, C.c_int, dbl, vp, C.POINTER(vp)]),
     "hoefem_integrator_set_tolerances": (C.c_int, [vp, dbl, i64, i64]),
     "hoefem_integrator_set_precision": (C.c_int, [vp, C.c_int, dbl]),
+    "hoefem_integrator_set_cg_engine": (C.c_int, [vp, C.c_int, C.c_int]),
+    "hoefem_model_set_cg_engine": (C.c_int, [vp, C.c_int, C.c_int]),
+    "hoefem_integrator_cg_engine_stats": (C.c_int, [vp, vp]),
+    "hoefem_model_cg_engine_stats": (C.c_int, [vp, vp]),
     "hoefem_integrator_step": (C.c_int, [vp, vp, vp, dbl, dbl, C.c_int]),
     "hoefem_integrator_stats": (C.c_int, [vp, C.POINTER(StepStats)]),
     "hoefem_integrator_mass": (C.c_int, [vp, vp]),

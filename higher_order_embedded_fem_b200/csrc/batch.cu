@@ -626,7 +626,7 @@ struct Batch {
       K.zero(s);
       set_emask(active);
       launch_stiffness(m, MatDev{mat_kind, 0.0, 0.0}, us.p, K.p, s);
-      (note_launch(), k_combine2<<<148 * 8, TPB, 0, s>>>(m.nnz, -(-dt * dt), K.p, M.p, J.p));
+      (note_launch(), k_combine2<<<device_sms() * 8, TPB, 0, s>>>(m.nnz, -(-dt * dt), K.p, M.p, J.p));
       dirichlet(J.p);
       (note_launch(), k_diag_inv<<<(n + 255) / 256, 256, 0, s>>>(m.rows(), d_scene_of.p, J.p, diag.p, err.p));
       check_device_error(m);

@@ -23,6 +23,8 @@ void integrator_set_tolerances(Integrator* it, double tol, i64 cg_max, i64 newto
 void integrator_set_damping(Integrator* it, bool has_mass, double mass_coeff, bool has_stiffness,
                             double stiffness_coeff);
 void integrator_set_precision(Integrator* it, int precision, double delta);
+CgWork* integrator_cg(Integrator* it);
+const Precond* integrator_precond(Integrator* it);
 void integrator_set_learned(Integrator* it, Learned* l, int mode);
 int integrator_step(Integrator* it, double* ud, double* vd, double t, double dt);
 hoefem_step_stats integrator_stats(Integrator* it);
@@ -610,6 +612,9 @@ int hoefem_cg_solve(hoefem_model m, const double* system_values, hoefem_precond 
     m->cg->init(&mm);
   }
   CgWork& w = *m->cg;
+  w.stream_launches = 0;
+  w.stream_iterations = 0;
+  w.stream_ms_total = 0.0;
   View A(system_values, mm.nnz, mem, mm.stream, true);
   View B(b, mm.ndof, mem, mm.stream, true), X(x, mm.ndof, mem, mm.stream, true);
   HOEFEM_CUDA(cudaMemcpyAsync(w.b.p, B.d, mm.ndof * sizeof(double), cudaMemcpyDeviceToDevice, mm.stream));
@@ -635,6 +640,9 @@ int hoefem_cg_solve_mixed(hoefem_model m, const double* system_values, hoefem_pr
     m->cg->init(&mm);
   }
   CgWork& w = *m->cg;
+  w.stream_launches = 0;
+  w.stream_iterations = 0;
+  w.stream_ms_total = 0.0;
   View A(system_values, mm.nnz, mem, mm.stream, true);
   View B(b, mm.ndof, mem, mm.stream, true), X(x, mm.ndof, mem, mm.stream, true);
   DBuf<float> A32;
@@ -687,6 +695,54 @@ int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double 
                      delta > 0.0 && delta < 1.0,
                  HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
   integrator_set_precision(it->it, precision == HOEFEM_PRECISION_MIXED ? PRECISION_FP32 : PRECISION_FP64, delta);
+  API_END
+}
+
+static void set_engine(CgWork& w, int engine, int fp16) {
+  HOEFEM_REQUIRE(engine >= HOEFEM_CG_ENGINE_AUTO && engine <= HOEFEM_CG_ENGINE_STREAMED, HOEFEM_ERR_INVALID_ARGUMENT,
+                 "unknown CG engine");
+  w.stream_mode = engine;
+  w.schwarz_half = fp16 != 0;
+}
+
+static void engine_stats(const CgWork& w, const Precond* P, hoefem_cg_engine_stats* out) {
+  HOEFEM_REQUIRE(out, HOEFEM_ERR_INVALID_ARGUMENT, "null stats");
+  out->launches = w.stream_launches;
+  out->iterations = w.stream_iterations;
+  out->device_ms = w.stream_ms_total;
+  out->operator_bytes = w.sop32.vsize && w.last_f32 ? w.sop32.bytes : w.sop64.bytes;
+  out->schwarz_bytes = (P && P->kind == PREC_SCHWARZ) ? w.ssw.bytes : 0;
+}
+
+int hoefem_integrator_set_cg_engine(hoefem_integrator it, int engine, int schwarz_fp16) {
+  API_BEGIN
+  HOEFEM_REQUIRE(it, HOEFEM_ERR_INVALID_ARGUMENT, "null integrator");
+  set_engine(*integrator_cg(it->it), engine, schwarz_fp16);
+  API_END
+}
+
+int hoefem_model_set_cg_engine(hoefem_model m, int engine, int schwarz_fp16) {
+  API_BEGIN
+  Model& mm = device_model(m);
+  if (!m->cg) {
+    m->cg.reset(new CgWork());
+    m->cg->init(&mm);
+  }
+  set_engine(*m->cg, engine, schwarz_fp16);
+  API_END
+}
+
+int hoefem_integrator_cg_engine_stats(hoefem_integrator it, hoefem_cg_engine_stats* out) {
+  API_BEGIN
+  HOEFEM_REQUIRE(it, HOEFEM_ERR_INVALID_ARGUMENT, "null integrator");
+  engine_stats(*integrator_cg(it->it), integrator_precond(it->it), out);
+  API_END
+}
+
+int hoefem_model_cg_engine_stats(hoefem_model m, hoefem_cg_engine_stats* out) {
+  API_BEGIN
+  HOEFEM_REQUIRE(m && m->cg, HOEFEM_ERR_INVALID_ARGUMENT, "no CG has run on this model");
+  engine_stats(*m->cg, nullptr, out);
   API_END
 }
 

@@ -220,6 +220,7 @@ __global__ void k_cg_copy(int n, const double* __restrict__ a, double* __restric
 // Initial convergence test (loop head of cg.rs:419-441 before any update).
 __global__ void k_cg_init_check(CgState* st) {
   st->iters = 0;
+  st->beta = 0.0;  // first direction p = z (the streamed CG forms z + beta p)
   st->done = 0;
   st->status = HOEFEM_OK;
   if (st->bnorm == 0.0) {
@@ -343,7 +344,7 @@ void CgWork::init(Model* model) {
   n = model->ndof;
   x.alloc(n); b.alloc(n); r.alloc(n); z.alloc(n); p.alloc(n); Ap.alloc(n);
   // node-chunk partials (<= nv / 8 chunks) + block partials, K <= 2 values
-  partials.alloc(std::max<size_t>(4 * 148 * 16, 2 * ((size_t)model->nv / 8 + 2) + 2 * 4096));
+  partials.alloc(std::max<size_t>(reduce_partials_count(), 2 * ((size_t)model->nv / 8 + 2) + 2 * 4096));
   st.alloc(1);
   counter.alloc(1);
   HOEFEM_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), model->stream));
@@ -361,7 +362,7 @@ CgWork::~CgWork() {
 }
 
 void to_f32(const double* a, float* b, long long n, cudaStream_t s) {
-  (note_launch(), k_to_f32<<<148 * 8, 256, 0, s>>>(n, a, b));
+  (note_launch(), k_to_f32<<<device_sms() * 8, 256, 0, s>>>(n, a, b));
   HOEFEM_CUDA(cudaGetLastError());
 }
 
@@ -547,8 +548,53 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
     *iters = w.h_st->iters;
     return w.h_st->status;
   }
-  // online SpMV variant choice: candidate pairs (operator lanes, Schwarz lanes)
   const bool f32 = A.v32 != nullptr;
+  const bool streamed = cg_stream_usable(w, P);
+  HOEFEM_REQUIRE(streamed || w.stream_mode != 2, HOEFEM_ERR_INVALID_ARGUMENT,
+                 "the streamed CG cannot run this solve (preconditioner or device)");
+  if (streamed) {
+    // persistent streamed CG: the operator (FP64 values, FP32 in the mixed
+    // form) and the Schwarz blocks packed into their stream layouts, then one
+    // launch per residual replacement
+    const double* vals64 = A64 ? A64 : A.v64;
+    HOEFEM_REQUIRE(vals64, HOEFEM_ERR_INVALID_ARGUMENT, "streamed CG needs the FP64 operator values");
+    cg_stream_prepare(w, vals64, f32, P, p32, s);
+    cg_stream_arm(w, A64 ? delta : 0.0, s);
+    w.stream_ms = 0.f;
+    const i64 cap_s = max_iter >= 0 ? max_iter : 10 * (i64)n;
+    i64 nrep_s = 0;
+    for (;;) {
+      const i64 it0 = w.h_st->iters;
+      cg_stream_iterate(w, f32, P, p32, A64 != nullptr, s);
+      w.stream_iterations += w.h_st->iters - it0;
+      if (A64) {
+        const bool conv = w.h_st->done && w.h_st->status == HOEFEM_OK;
+        const bool trig = !w.h_st->done && w.h_st->replace;
+        if (conv || trig) {
+          (note_launch(), k_cg_save_ztr<<<1, 1, 0, s>>>(w.st.p));
+          true_residual(A64);
+          prec_init();
+          // resume after a converged recurrence: beta = z.r / z.r_old; the
+          // kernel forms the direction z + beta p itself
+          (note_launch(), k_cg_reliable<<<1, 1, 0, s>>>(w.st.p, conv ? 1 : 0));
+          cg_stream_arm(w, delta, s);
+          HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+          HOEFEM_CUDA(cudaStreamSynchronize(s));
+          ++nrep_s;
+        }
+      }
+      if (w.h_st->done) break;
+      if (w.h_st->iters >= cap_s) {
+        if (replacements) *replacements = nrep_s;
+        *iters = w.h_st->iters;
+        return HOEFEM_CG_MAX_ITERATIONS;
+      }
+    }
+    if (replacements) *replacements = nrep_s;
+    *iters = w.h_st->iters;
+    return w.h_st->status;
+  }
+  // online SpMV variant choice: candidate pairs (operator lanes, Schwarz lanes)
   // (with the block apply the Schwarz SpMV variant plays no part)
   const bool schwarz = P && P->kind == PREC_SCHWARZ && !P->block_apply;
   static const int cand_lanes[4] = {8, 16, 32, 132};

@@ -173,7 +173,7 @@ struct Integrator {
     HOEFEM_CUDA(cudaMemcpyAsync(bc.p, hb.data(), n, cudaMemcpyHostToDevice, s));
     for (auto* b : {&M, &K, &J}) b->alloc(m->nnz);
     for (auto* b : {&gforce, &up, &vn, &w, &F, &dx, &us, &vs, &f, &u, &v}) b->alloc(n);
-    partials.alloc(4 * 148 * 16);
+    partials.alloc(reduce_partials_count());
     scalars.alloc(8);
     counter.alloc(1);
     counter.zero(s);
@@ -423,6 +423,9 @@ struct Integrator {
     const int n = (int)m->ndof;
     stats = hoefem_step_stats{};
     ratio_sum = 0.0;
+    cg.stream_launches = 0;
+    cg.stream_iterations = 0;
+    cg.stream_ms_total = 0.0;
     stats.representative_force = rep_force;
     cudaEvent_t t0, t1;
     HOEFEM_CUDA(cudaEventCreate(&t0));
@@ -503,6 +506,8 @@ void integrator_set_tolerances(Integrator* it, double tol, i64 cg_max, i64 newto
 }
 int integrator_step(Integrator* it, double* ud, double* vd, double t, double dt) { return it->step(ud, vd, t, dt); }
 hoefem_step_stats integrator_stats(Integrator* it) { return it->stats; }
+CgWork* integrator_cg(Integrator* it) { return &it->cg; }
+const Precond* integrator_precond(Integrator* it) { return it->P; }
 const double* integrator_mass(Integrator* it) { return it->M.p; }
 void integrator_eval_f(Integrator* it, const double* ud, const double* vd, double* f) { it->eval_f(ud, vd, f); }
 

@@ -192,6 +192,10 @@ void jacobian_combination(const Model& m, double ck, const double* K, double cm,
 void dot_device(const double* a, const double* b, i64 n, double* out, double* partials, unsigned* counter,
                 cudaStream_t s);
 int reduce_blocks_for(i64 n);
+// Multiprocessor count of the current device, and the size of a partials
+// buffer that holds every deterministic grid reduction's block partials.
+int device_sms();
+size_t reduce_partials_count();
 
 void finalize_model(Model& m);
 void ensure_device(Model& m);

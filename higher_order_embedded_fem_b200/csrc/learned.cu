@@ -501,7 +501,7 @@ void Learned::setup(Model* model, const unsigned char* bc_mask, int num_sub, uin
   for (auto* b : {&Y3, &T, &dY3}) b->alloc((size_t)max_batch * NM);
   e.alloc(ndof);
   rtmp.alloc(ndof);
-  partials.alloc(4 * 148 * 16);
+  partials.alloc(reduce_partials_count());
   scal.alloc(8);
   counter.alloc(1);
   counter.zero(s);

@@ -115,16 +115,32 @@ __global__ void k_fill_u64(unsigned long long* p, unsigned long long v) { *p = v
 
 }  // namespace
 
-// Node-row kernels run 8 warps per block, 8 blocks per SM: a grid of at most
-// 148 * 8 blocks covers the GPU once and each warp strides over nodes.
+// Multiprocessor count of the current device (queried once per device).
+int device_sms() {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  HOEFEM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) dev = 0;
+  int v = cache[dev].load(std::memory_order_relaxed);
+  if (v <= 0) {
+    HOEFEM_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+    if (v <= 0) v = 1;
+    cache[dev].store(v, std::memory_order_relaxed);
+  }
+  return v;
+}
+
+size_t reduce_partials_count() { return (size_t)device_sms() * 64; }
+
 // Grid of the node-row kernels: with dynamic node scheduling, one CTA per
-// resident slot (8 CTAs of 256 threads per SM, 148 SMs) or fewer for small
-// matrices; the two-value deterministic reductions fit their partials buffer
-// (4 x 148 x 16 doubles).
+// resident slot (8 CTAs of 256 threads per SM) or fewer for small matrices;
+// the two-value deterministic reductions fit their partials buffer
+// (reduce_partials_count() doubles).
 int spmv_grid(int nv, int lanes) {
   int nodes_per_block = 8 * (32 / (lanes % 100));
   int g = (nv + nodes_per_block - 1) / nodes_per_block;
-  return g < 148 * 8 ? (g > 0 ? g : 1) : 148 * 8;
+  const int cap = device_sms() * 8;
+  return g < cap ? (g > 0 ? g : 1) : cap;
 }
 
 void spmv_node_rows(const NodeRows& A, const double* vals, const double* x, double* y, double alpha, double beta,
@@ -184,7 +200,7 @@ void jacobian_combination(const Model& m, double ck, const double* K, double cm,
                           const unsigned char* bc_dof, double* out, double* d_scratch, cudaStream_t s, double cd,
                           const double* D) {
   NodeRows A = m.rows();
-  (note_launch(), k_combine<<<148 * 8, 256, 0, s>>>(A, ck, K, cd, D, cm, M, out));
+  (note_launch(), k_combine<<<device_sms() * 8, 256, 0, s>>>(A, ck, K, cd, D, cm, M, out));
   if (bc_dof) {
     unsigned long long* first = reinterpret_cast<unsigned long long*>(d_scratch);
     (note_launch(), k_fill_u64<<<1, 1, 0, s>>>(first, ~0ull));
@@ -212,7 +228,8 @@ __global__ void __launch_bounds__(256) k_dot(const double* __restrict__ a, const
 int reduce_blocks_for(i64 n) {
   i64 g = (n + 1023) / 1024;
   if (g < 1) g = 1;
-  if (g > 148 * 4) g = 148 * 4;
+  const i64 cap = (i64)device_sms() * 4;
+  if (g > cap) g = cap;
   return (int)g;
 }
 

@@ -39,10 +39,9 @@ constexpr int MAX_DEVICES = 64;
 std::mutex g_noalloc_mutex;
 unsigned char* g_noalloc_ptr[MAX_DEVICES] = {};
 
-// Device address of this device's scratch, looked up once per device.
-unsigned char* noalloc_scratch() {
-  int dev = 0;
-  HOEFEM_CUDA(cudaGetDevice(&dev));
+// Device address of the scratch on device `dev`, looked up once per device
+// with that device current (the caller makes it current).
+unsigned char* noalloc_scratch(int dev) {
   HOEFEM_REQUIRE(dev >= 0 && dev < MAX_DEVICES, HOEFEM_ERR_INVALID_ARGUMENT, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   if (!g_noalloc_ptr[dev]) {
@@ -52,6 +51,20 @@ unsigned char* noalloc_scratch() {
   }
   return g_noalloc_ptr[dev];
 }
+
+// Makes `dev` current for the lifetime of the object and restores the
+// previous current device afterwards.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev) {
+    HOEFEM_CUDA(cudaGetDevice(&prev));
+    if (prev != dev) HOEFEM_CUDA(cudaSetDevice(dev));
+    else prev = -1;
+  }
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 }  // namespace
 
@@ -67,7 +80,9 @@ void jacobian_combination_noalloc(Model& m, double ck, const double* K, double c
   for (long long k = 0; k < num_bc; ++k)
     HOEFEM_REQUIRE(bc_nodes[k] >= 0 && bc_nodes[k] < m.nv, HOEFEM_ERR_INVALID_ARGUMENT,
                    "Dirichlet node out of range");
-  unsigned char* scratch = noalloc_scratch();
+  // the scratch, the stream and the model's buffers all belong to m.device
+  DeviceScope scope(m.device);
+  unsigned char* scratch = noalloc_scratch(m.device);
   cudaStream_t s = m.stream;
   unsigned char* mask = nullptr;
   if (num_bc > 0) {
@@ -75,7 +90,7 @@ void jacobian_combination_noalloc(Model& m, double ck, const double* K, double c
     mask = scratch + NOALLOC_MASK_OFF;
     HOEFEM_CUDA(cudaMemsetAsync(mask, 0, (size_t)m.ndof, s));
     HOEFEM_CUDA(cudaMemcpyAsync(nodes, bc_nodes, sizeof(long long) * num_bc, cudaMemcpyHostToDevice, s));
-    const int grid = (int)std::min<long long>((num_bc + 255) / 256, 148 * 8);
+    const int grid = (int)std::min<long long>((num_bc + 255) / 256, (long long)device_sms() * 8);
     (note_launch(), k_mark_bc_nodes<<<grid, 256, 0, s>>>(nodes, num_bc, mask));
     HOEFEM_CUDA(cudaGetLastError());
   }

@@ -61,6 +61,47 @@ struct CgState {
   double bnorm, tol, zTr, pAp, rr, alpha, beta;
   long long iters, max_iter;
   int done, status;
+  // streamed CG: residual-replacement trigger (rr <= delta2 * rr_ref), the
+  // flag it raises, and which direction buffer holds the current direction
+  double rr_ref, delta2;
+  int replace, pcur;
+};
+
+// One unit of a streamed kernel's work: `bytes` (multiple of 16, at most one
+// ring stage) at byte offset `off` of a stream buffer, plus kind-specific
+// fields (operator tile: a = first node; Schwarz chunk: a = subdomain,
+// b = first row, c = rows).
+struct CgsItem {
+  long long off;
+  int bytes, a, b, c;
+  int pad[2];
+};
+
+// Stream layouts of the persistent CG (cg_stream.cu): the operator as tiles
+// of whole node rows (header, neighbour lists, 9 value planes per node) and
+// the Schwarz blocks as row chunks, each split into contiguous per-CTA item
+// ranges balanced by bytes.
+struct CgStreamOp {
+  int vsize = 0;  // value bytes (8 FP64, 4 FP32); 0 = not built
+  int grid = 0;
+  DBuf<unsigned char> data;
+  DBuf<CgsItem> items;
+  DBuf<int> item_off;    // grid + 1
+  DBuf<int> node_range;  // grid + 1
+  DBuf<long long> val_off;  // per node: byte offset of its value planes
+  long long bytes = 0;      // streamed bytes per apply
+};
+struct CgStreamSchwarz {
+  int vsize = 0;  // 8, 4 or 2 (FP16 with a per-subdomain scale)
+  int grid = 0;
+  const void* built_for = nullptr;
+  DBuf<unsigned char> data;
+  DBuf<CgsItem> items;
+  DBuf<int> item_off;
+  DBuf<long long> chunk_base;  // per subdomain: byte offset of its first chunk
+  DBuf<int> rows_per_chunk;    // per subdomain
+  DBuf<double> scale;          // per subdomain (FP16 only)
+  long long bytes = 0;
 };
 
 struct CgWork {
@@ -89,6 +130,22 @@ struct CgWork {
   Tuning tuning[2];  // [0] FP64 values, [1] FP32 values
   bool online_tuning = true;
   int chunk = 8;
+  // Persistent streamed CG (cg_stream.cu): mode 0 automatic (used whenever
+  // the device, the preconditioner and the layouts allow), 1 off (graphs of
+  // kernel chunks), 2 required (error if it cannot run); schwarz_half stores
+  // the mixed-precision Schwarz blocks in FP16 with a per-subdomain scale.
+  int stream_mode = 0;
+  bool schwarz_half = false;
+  CgStreamOp sop64, sop32;
+  CgStreamSchwarz ssw;
+  DBuf<double> p2, spart;
+  DBuf<unsigned> sbar;
+  DBuf<int> serr;
+  long long stream_launches = 0, stream_iterations = 0;
+  float stream_ms = 0.f;         // device time of the persistent launches (last solve)
+  double stream_ms_total = 0.0;  // summed over solves until reset by the caller
+  bool last_f32 = false;         // precision of the last streamed solve
+  cudaEvent_t sev[2] = {nullptr, nullptr};
   // called on the host after every chunk of iterations (solver state synced)
   std::function<void(cudaStream_t)> on_chunk;
   void init(Model* model);
@@ -102,5 +159,19 @@ int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 ma
 int cg_solve_reliable(CgWork& w, const double* A64, const float* A32, const Precond* P, double tol, i64 max_iter,
                       double delta, i64* iters, i64* replacements, cudaStream_t s);
 void to_f32(const double* a, float* b, long long n, cudaStream_t s);
+
+// Streamed CG (cg_stream.cu).  cg_stream_usable: whether the persistent
+// kernel can run this solve; cg_stream_prepare packs the operator (FP64
+// values, converted to the stream precision) and the Schwarz blocks into
+// their stream layouts; cg_stream_iterate runs iterations from the current
+// state (x, r, z, zTr in w; direction = z + beta * w.p) until convergence,
+// an error outcome, the iteration limit or a residual-replacement trigger,
+// and leaves the current direction in w.p.
+bool cg_stream_usable(CgWork& w, const Precond* P);
+void cg_stream_prepare(CgWork& w, const double* A64, bool f32, const Precond* P, bool p32, cudaStream_t s);
+void cg_stream_iterate(CgWork& w, bool f32, const Precond* P, bool p32, bool reliable, cudaStream_t s);
+// Sets the residual-replacement reference rr_ref = rr (current state) and
+// delta^2, clears the replacement flag.
+void cg_stream_arm(CgWork& w, double delta, cudaStream_t s);
 
 }  // namespace hoefem

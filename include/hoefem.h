@@ -50,6 +50,9 @@ typedef enum {
      schwarz_precond.rs:203-210) */
   HOEFEM_ERR_ZERO_DIAGONAL = 7,
   HOEFEM_ERR_NOT_FINALIZED = 8,
+  /* a bounded device-side wait of a persistent kernel ran out (no
+     counterpart in the reference; the kernel wound down instead of spinning) */
+  HOEFEM_ERR_DEVICE_TIMEOUT = 9,
   /* CG outcomes, fenris/src/cg.rs:277-286 SolveErrorKind */
   HOEFEM_CG_INDEFINITE_OPERATOR = 10,
   HOEFEM_CG_INDEFINITE_PRECONDITIONER = 11,
@@ -182,7 +185,8 @@ int hoefem_jacobian_combination(hoefem_model m, double c_stiffness, const double
    they step (a host that reserves its device memory budget up front, or a
    real-time loop that must not wait on the allocator).  stiffness_values /
    mass_values (either may be NULL) and out are device pointers on the
-   current device (nnz each); bc_nodes is a host array.  Scratch (the
+   model's device (nnz each); bc_nodes is a host array.  The call runs on the
+   model's device and restores the caller's current device on return.  Scratch (the
    Dirichlet DOF mask, the node list and the diagonal-scale word) is a fixed
    array inside the library, one per device, sized for at most 4,194,304 DOFs
    and 262,144 Dirichlet nodes; larger inputs return
@@ -320,6 +324,34 @@ int hoefem_integrator_set_damping(hoefem_integrator it, int has_mass, double mas
    (an addition on top of its FP64 path). */
 typedef enum { HOEFEM_PRECISION_FP64 = 0, HOEFEM_PRECISION_MIXED = 1 } hoefem_precision;
 int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double delta);
+/* CG engine of the integrator's Jacobian solves and of hoefem_cg_solve /
+   hoefem_cg_solve_mixed on a model (no counterpart in the reference, whose CG
+   is one host loop).  HOEFEM_CG_ENGINE_AUTO (default): the persistent
+   streamed CG (one cooperative launch per solve, the operator and the Schwarz
+   blocks streamed through shared memory) whenever the device and the
+   preconditioner allow it (no preconditioner, diagonal, or Schwarz with
+   subdomains of at most 27 nodes), else CUDA graphs of kernel chunks;
+   HOEFEM_CG_ENGINE_CHUNKED: always the graphs; HOEFEM_CG_ENGINE_STREAMED:
+   the streamed CG or HOEFEM_ERR_INVALID_ARGUMENT.  schwarz_fp16 != 0: in the
+   mixed-precision form the streamed CG keeps the Schwarz blocks in FP16
+   scaled by each block's largest magnitude (products and sums stay FP64). */
+typedef enum {
+  HOEFEM_CG_ENGINE_AUTO = 0,
+  HOEFEM_CG_ENGINE_CHUNKED = 1,
+  HOEFEM_CG_ENGINE_STREAMED = 2
+} hoefem_cg_engine;
+int hoefem_integrator_set_cg_engine(hoefem_integrator it, int engine, int schwarz_fp16);
+int hoefem_model_set_cg_engine(hoefem_model m, int engine, int schwarz_fp16);
+/* Streamed-CG counters of the last step (integrator) or solve (model):
+   persistent launches, iterations they ran, their summed device time (ms) and
+   the bytes one iteration streams (operator tiles + Schwarz chunks). */
+typedef struct {
+  int64_t launches, iterations;
+  double device_ms;
+  int64_t operator_bytes, schwarz_bytes;
+} hoefem_cg_engine_stats;
+int hoefem_integrator_cg_engine_stats(hoefem_integrator it, hoefem_cg_engine_stats* out);
+int hoefem_model_cg_engine_stats(hoefem_model m, hoefem_cg_engine_stats* out);
 /* One time step: u, v (ndof) updated in place. */
 int hoefem_integrator_step(hoefem_integrator it, double* u, double* v, double t, double dt, int mem);
 int hoefem_integrator_stats(hoefem_integrator it, hoefem_step_stats* out);

@@ -206,7 +206,12 @@ def quadrature(ref):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) > 1:
+        ref = sys.argv[1]
+    elif os.environ.get("HOEFEM_REFERENCE_DIR"):
+        ref = os.environ["HOEFEM_REFERENCE_DIR"]
+    else:
+        sys.exit("usage: make_golden.py <reference checkout> (or set HOEFEM_REFERENCE_DIR)")
     data = dict(
         source="InteractiveComputerGraphics/higher_order_embedded_fem (test sources read as text)",
         mock_patterns=mock_patterns(ref),

@@ -30,6 +30,23 @@ def test_noalloc_jacobian_matches_allocating_entry_point():
         got = m.jacobian_combination_noalloc(torch.zeros_like(K), dt * dt, K, 1.0, M, bc)
         torch.cuda.synchronize()
         assert torch.equal(got, want)
+    # the point of the entry point: once its first call on the device has
+    # looked up the scratch address, further calls allocate no device memory
+    # (free device memory is unchanged; the check does see an allocation)
+    def free_bytes():
+        torch.cuda.synchronize()
+        return torch.cuda.mem_get_info()[0]
+
+    out = torch.zeros_like(K)
+    torch.cuda.empty_cache()
+    f0 = free_bytes()
+    for bc in bc_sets * 3:
+        m.jacobian_combination_noalloc(out, dt * dt, K, 1.0, M, bc)
+    assert free_bytes() == f0
+    probe = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    assert free_bytes() < f0
+    del probe
+    torch.cuda.empty_cache()
     # no Dirichlet nodes, mass only
     want = m.jacobian_combination(torch.zeros_like(K), 0.0, None, 1.0, M, ())
     got = m.jacobian_combination_noalloc(torch.zeros_like(K), 0.0, None, 1.0, M, ())
