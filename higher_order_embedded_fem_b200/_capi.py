@@ -48,7 +48,7 @@ class StepStats(C.Structure):
         ("residual_norm", C.c_double), ("representative_force", C.c_double), ("ms_assemble_forces", C.c_double),
         ("ms_assemble_stiffness", C.c_double), ("ms_precond_update", C.c_double), ("ms_cg", C.c_double),
         ("ms_total", C.c_double), ("learned_accepted", C.c_int64), ("learned_rejected", C.c_int64),
-        ("learned_residual_ratio", C.c_double), ("ms_learned", C.c_double),
+        ("learned_residual_ratio", C.c_double), ("ms_learned", C.c_double), ("line_search_backtracks", C.c_int64),
     ]
 
     def as_dict(self):
@@ -57,7 +57,7 @@ class StepStats(C.Structure):
 
 class CgEngineStats(C.Structure):
     _fields_ = [("launches", C.c_int64), ("iterations", C.c_int64), ("device_ms", C.c_double),
-                ("operator_bytes", C.c_int64), ("schwarz_bytes", C.c_int64)]
+                ("operator_bytes", C.c_int64), ("schwarz_bytes", C.c_int64), ("phase_us", C.c_double * 12)]
 
 
 CG_ENGINE = {"auto": 0, "chunked": 1, "streamed": 2}
@@ -117,6 +117,8 @@ SIGNATURES = {
     "hoefem_model_set_cg_engine": (C.c_int, [vp, C.c_int, C.c_int]),
     "hoefem_integrator_cg_engine_stats": (C.c_int, [vp, vp]),
     "hoefem_model_cg_engine_stats": (C.c_int, [vp, vp]),
+    "hoefem_integrator_set_cg_l2_keep": (C.c_int, [vp, i64]),
+    "hoefem_model_set_cg_l2_keep": (C.c_int, [vp, i64]),
     "hoefem_integrator_step": (C.c_int, [vp, vp, vp, dbl, dbl, C.c_int]),
     "hoefem_integrator_stats": (C.c_int, [vp, C.POINTER(StepStats)]),
     "hoefem_integrator_mass": (C.c_int, [vp, vp]),

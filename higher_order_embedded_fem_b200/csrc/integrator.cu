@@ -403,6 +403,7 @@ struct Integrator {
         if (g <= (1.0 - c * alpha) * g0) break;
         if (alpha < alpha_min) return HOEFEM_LINE_SEARCH_FAILED;
         alpha_prev = alpha;
+        stats.line_search_backtracks += 1;
         ++k;
         if (k < 4) alpha = initial[k];
         else { alpha = tail; tail *= 0.25; }

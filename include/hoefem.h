@@ -294,6 +294,9 @@ typedef struct {
   int64_t learned_rejected;
   double learned_residual_ratio;
   double ms_learned;
+  /* backtracking line search (newton.rs:171-248): reductions of alpha below 1
+     over all Newton iterations and substep attempts of the step */
+  int64_t line_search_backtracks;
 } hoefem_step_stats;
 
 /* precond: a preconditioner of this model (ownership stays with the caller),
@@ -332,26 +335,44 @@ int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double 
    preconditioner allow it (no preconditioner, diagonal, or Schwarz with
    subdomains of at most 27 nodes), else CUDA graphs of kernel chunks;
    HOEFEM_CG_ENGINE_CHUNKED: always the graphs; HOEFEM_CG_ENGINE_STREAMED:
-   the streamed CG or HOEFEM_ERR_INVALID_ARGUMENT.  schwarz_fp16 != 0: in the
-   mixed-precision form the streamed CG keeps the Schwarz blocks in FP16
-   scaled by each block's largest magnitude (products and sums stay FP64). */
+   the streamed CG or HOEFEM_ERR_INVALID_ARGUMENT.  options (bit mask):
+   HOEFEM_CG_SCHWARZ_FP16: in the mixed-precision form the streamed CG keeps
+   the Schwarz blocks in FP16 scaled by each block's largest magnitude
+   (products and sums stay FP64); HOEFEM_CG_PHASE_PROFILE: the streamed CG
+   records per-phase cycle counts (hoefem_cg_engine_stats.phase_us). */
 typedef enum {
   HOEFEM_CG_ENGINE_AUTO = 0,
   HOEFEM_CG_ENGINE_CHUNKED = 1,
   HOEFEM_CG_ENGINE_STREAMED = 2
 } hoefem_cg_engine;
-int hoefem_integrator_set_cg_engine(hoefem_integrator it, int engine, int schwarz_fp16);
-int hoefem_model_set_cg_engine(hoefem_model m, int engine, int schwarz_fp16);
+enum { HOEFEM_CG_SCHWARZ_FP16 = 1, HOEFEM_CG_PHASE_PROFILE = 2 };
+int hoefem_integrator_set_cg_engine(hoefem_integrator it, int engine, int options);
+int hoefem_model_set_cg_engine(hoefem_model m, int engine, int options);
 /* Streamed-CG counters of the last step (integrator) or solve (model):
    persistent launches, iterations they ran, their summed device time (ms) and
-   the bytes one iteration streams (operator tiles + Schwarz chunks). */
+   the bytes one iteration streams (operator tiles + Schwarz chunks); with
+   HOEFEM_CG_PHASE_PROFILE, microseconds per iteration (mean over CTAs) of:
+   [0] operator halo gather, [1] operator tiles, [2] of which waiting for
+   tile data, [3] CTA + grid barrier after the operator, [4] Schwarz residual
+   gather, [5] Schwarz chunks, [6] of which waiting for chunk data, [7] grid
+   barrier after the Schwarz products, [8] own-DOF update, [9] grid barrier
+   and reductions after it, [10] producer waiting for free stages, [11]
+   producer lifetime. */
 typedef struct {
   int64_t launches, iterations;
   double device_ms;
   int64_t operator_bytes, schwarz_bytes;
+  double phase_us[12];
 } hoefem_cg_engine_stats;
 int hoefem_integrator_cg_engine_stats(hoefem_integrator it, hoefem_cg_engine_stats* out);
 int hoefem_model_cg_engine_stats(hoefem_model m, hoefem_cg_engine_stats* out);
+/* L2 residency budget of the streamed CG (no counterpart in the reference):
+   bytes of each iteration's stream (over all CTAs; the Schwarz chunks first,
+   then operator tiles) copied with an evict-last L2 policy so that they are
+   still cached in the next iteration, the rest with evict-first.  bytes < 0:
+   the default, 60 % of the device's L2. */
+int hoefem_integrator_set_cg_l2_keep(hoefem_integrator it, int64_t bytes);
+int hoefem_model_set_cg_l2_keep(hoefem_model m, int64_t bytes);
 /* One time step: u, v (ndof) updated in place. */
 int hoefem_integrator_step(hoefem_integrator it, double* u, double* v, double t, double dt, int mem);
 int hoefem_integrator_stats(hoefem_integrator it, hoefem_step_stats* out);

@@ -1098,6 +1098,7 @@ struct Scene {
   std::vector<i64> cg_iters;
   std::vector<int> cg_status;
   i64 newton_iters = 0;
+  i64 ls_backtracks = 0;  // line-search reductions of alpha below 1 in the last step (all attempts)
   i64 num_substeps = 1;
   double last_residual = 0.0;
 };
@@ -1261,6 +1262,7 @@ static int backward_euler_step(Scene& s, double* u, double* v, double t0, double
       if (g <= (1.0 - c * alpha) * g0) break;
       if (alpha < alpha_min) return STEP_LINE_SEARCH_FAILED;
       alpha_prev = alpha;
+      ++s.ls_backtracks;
       ++k;
       if (k < 4) alpha = initial[k];
       else { alpha = tail; tail *= 0.25; }
@@ -1279,6 +1281,7 @@ static int integrate(Scene& s, double* u, double* v, double t, double dt) {
   const i64 n = s.model.pattern.nrows;
   s.cg_iters.clear();
   s.cg_status.clear();
+  s.ls_backtracks = 0;
   apply_bc_unknowns(s, u, v);
   const i64 max_substeps = 1000, factor = 5;
   std::vector<double> us(u, u + n), vs(v, v + n);
@@ -1943,6 +1946,7 @@ void oracle_scene_last_cg(void* sp, int64_t* iters, int32_t* status) {
   }
 }
 int64_t oracle_scene_last_substeps(void* sp) { return ((Scene*)sp)->num_substeps; }
+int64_t oracle_scene_last_ls_backtracks(void* sp) { return ((Scene*)sp)->ls_backtracks; }
 double oracle_scene_last_residual(void* sp) { return ((Scene*)sp)->last_residual; }
 void oracle_scene_destroy(void* sp) { delete (Scene*)sp; }
 

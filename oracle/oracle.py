@@ -98,6 +98,7 @@ def lib():
             "oracle_scene_last_num_cg": (C.c_int64, [vp]),
             "oracle_scene_last_cg": (None, [vp, i64p, i32p]),
             "oracle_scene_last_substeps": (C.c_int64, [vp]),
+            "oracle_scene_last_ls_backtracks": (C.c_int64, [vp]),
             "oracle_scene_last_residual": (C.c_double, [vp]),
             "oracle_scene_destroy": (None, [vp]),
             "oracle_embed_last_error": (C.c_char_p, []),
@@ -457,7 +458,8 @@ class Scene:
         L.oracle_scene_last_cg(self._h, its, sts)
         stats = dict(status=st, newton_iters=L.oracle_scene_last_newton_iters(self._h),
                      cg_iters=its[:ncg].tolist(), cg_status=sts[:ncg].tolist(),
-                     substeps=L.oracle_scene_last_substeps(self._h), residual=L.oracle_scene_last_residual(self._h))
+                     substeps=L.oracle_scene_last_substeps(self._h), residual=L.oracle_scene_last_residual(self._h),
+                     ls_backtracks=L.oracle_scene_last_ls_backtracks(self._h))
         return u, v, stats
 
 
