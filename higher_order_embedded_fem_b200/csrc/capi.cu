@@ -698,37 +698,59 @@ int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double 
   API_END
 }
 
-static void set_engine(CgWork& w, int engine, int fp16) {
+static void set_engine(CgWork& w, int engine, int options) {
   HOEFEM_REQUIRE(engine >= HOEFEM_CG_ENGINE_AUTO && engine <= HOEFEM_CG_ENGINE_STREAMED, HOEFEM_ERR_INVALID_ARGUMENT,
                  "unknown CG engine");
+  HOEFEM_REQUIRE((options & ~(HOEFEM_CG_SCHWARZ_FP16 | HOEFEM_CG_PHASE_PROFILE)) == 0, HOEFEM_ERR_INVALID_ARGUMENT,
+                 "unknown CG engine option");
   w.stream_mode = engine;
-  w.schwarz_half = fp16 != 0;
+  w.schwarz_half = (options & HOEFEM_CG_SCHWARZ_FP16) != 0;
+  w.phase_profile = (options & HOEFEM_CG_PHASE_PROFILE) != 0;
 }
 
-static void engine_stats(const CgWork& w, const Precond* P, hoefem_cg_engine_stats* out) {
+static void engine_stats(CgWork& w, const Precond* P, hoefem_cg_engine_stats* out) {
   HOEFEM_REQUIRE(out, HOEFEM_ERR_INVALID_ARGUMENT, "null stats");
   out->launches = w.stream_launches;
   out->iterations = w.stream_iterations;
   out->device_ms = w.stream_ms_total;
   out->operator_bytes = w.sop32.vsize && w.last_f32 ? w.sop32.bytes : w.sop64.bytes;
   out->schwarz_bytes = (P && P->kind == PREC_SCHWARZ) ? w.ssw.bytes : 0;
+  cg_stream_phase_us(w, out->phase_us);
 }
 
-int hoefem_integrator_set_cg_engine(hoefem_integrator it, int engine, int schwarz_fp16) {
+int hoefem_integrator_set_cg_engine(hoefem_integrator it, int engine, int options) {
   API_BEGIN
   HOEFEM_REQUIRE(it, HOEFEM_ERR_INVALID_ARGUMENT, "null integrator");
-  set_engine(*integrator_cg(it->it), engine, schwarz_fp16);
+  set_engine(*integrator_cg(it->it), engine, options);
   API_END
 }
 
-int hoefem_model_set_cg_engine(hoefem_model m, int engine, int schwarz_fp16) {
+int hoefem_model_set_cg_engine(hoefem_model m, int engine, int options) {
   API_BEGIN
   Model& mm = device_model(m);
   if (!m->cg) {
     m->cg.reset(new CgWork());
     m->cg->init(&mm);
   }
-  set_engine(*m->cg, engine, schwarz_fp16);
+  set_engine(*m->cg, engine, options);
+  API_END
+}
+
+int hoefem_integrator_set_cg_l2_keep(hoefem_integrator it, int64_t bytes) {
+  API_BEGIN
+  HOEFEM_REQUIRE(it, HOEFEM_ERR_INVALID_ARGUMENT, "null integrator");
+  integrator_cg(it->it)->l2_keep = bytes < 0 ? -1 : bytes;
+  API_END
+}
+
+int hoefem_model_set_cg_l2_keep(hoefem_model m, int64_t bytes) {
+  API_BEGIN
+  Model& mm = device_model(m);
+  if (!m->cg) {
+    m->cg.reset(new CgWork());
+    m->cg->init(&mm);
+  }
+  m->cg->l2_keep = bytes < 0 ? -1 : bytes;
   API_END
 }
 

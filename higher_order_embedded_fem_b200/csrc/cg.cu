@@ -549,16 +549,14 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
     return w.h_st->status;
   }
   const bool f32 = A.v32 != nullptr;
-  const bool streamed = cg_stream_usable(w, P);
+  const double* vals64 = A64 ? A64 : A.v64;
+  // persistent streamed CG: the operator (FP64 values, FP32 in the mixed
+  // form) and the Schwarz blocks packed into their stream layouts, then one
+  // launch per residual replacement
+  const bool streamed = vals64 && cg_stream_usable(w, P) && cg_stream_prepare(w, vals64, f32, P, p32, s);
   HOEFEM_REQUIRE(streamed || w.stream_mode != 2, HOEFEM_ERR_INVALID_ARGUMENT,
-                 "the streamed CG cannot run this solve (preconditioner or device)");
+                 "the streamed CG cannot run this solve (preconditioner, device or layout)");
   if (streamed) {
-    // persistent streamed CG: the operator (FP64 values, FP32 in the mixed
-    // form) and the Schwarz blocks packed into their stream layouts, then one
-    // launch per residual replacement
-    const double* vals64 = A64 ? A64 : A.v64;
-    HOEFEM_REQUIRE(vals64, HOEFEM_ERR_INVALID_ARGUMENT, "streamed CG needs the FP64 operator values");
-    cg_stream_prepare(w, vals64, f32, P, p32, s);
     cg_stream_arm(w, A64 ? delta : 0.0, s);
     w.stream_ms = 0.f;
     const i64 cap_s = max_iter >= 0 ? max_iter : 10 * (i64)n;

@@ -11,17 +11,33 @@
 // everything else (vectors, 1 MB each on the benchmark) stays in L2.  The
 // kernel keeps that stream flowing: one CTA per SM, a producer warp whose
 // lane 0 issues bulk asynchronous copies (cp.async.bulk, no multicast) of
-// 16 KB work items into a ring of shared-memory stages, cycling through the
-// CTA's fixed item list (its operator tiles, then its Schwarz chunks) across
-// iterations and gated only by free stages, and 12 consumer warps that
-// compute from the stages.  Stage k % NS belongs to consumer warp k % NW
-// (NS a multiple of NW), so each stage is used and released in order by one
-// warp.  Phases of an iteration, separated by grid barriers:
-//   P1  Ap = A p with the direction formed on the fly, p = z + beta p_old
-//       (double-buffered), stored for the CTA's own nodes; p.Ap partials
-//   P2  Schwarz block products y_s = B_s (r - alpha Ap)_s into node-major slots
-//   P3  own DOFs: x += alpha p, r -= alpha Ap, z = sum of the node's slots (or
-//       diag / identity), r.r and z.r partials
+// work items of up to 14 KB into a ring of shared-memory stages, cycling
+// through the CTA's fixed item list (its operator tiles, then its Schwarz
+// row records) across iterations and refilling each stage as soon as its
+// warp releases it (in any order across stages, so that one busy warp does
+// not hold up the others' copies), and 12 consumer warps that compute from
+// the stages.  Stage k % NS belongs to consumer warp k % NW (NS a multiple of
+// NW), so each stage is used and released in order by one warp.
+//
+// Work is partitioned by node: a CTA owns a contiguous node range, split into
+// segments whose halo (every neighbour node of the segment's nodes) fits in
+// shared memory.  The tiles' neighbour lists and the Schwarz records' column
+// lists are 16-bit indices into that halo, and the vectors an item needs are
+// gathered into it once per phase by all consumer threads, so the per-node
+// loops read shared memory only.  The Schwarz blocks are distributed by rows:
+// the 3 rows of a subdomain block that belong to a node are stored with the
+// node's owner, so z = P r of an own node is a sum of local row products and
+// an iteration needs two grid barriers:
+//   P1  per segment: direction p = z + beta p_old (double-buffered) on the
+//       halo, stored for the own nodes; Ap = A p for the own nodes; p.Ap
+//   --- grid barrier (alpha) ---
+//   P2  per segment: residual r' = r_old - alpha Ap on the halo (r is
+//       double-buffered: other CTAs still gather r_old while the owners
+//       write r_new); the own nodes' Schwarz rows y = B_s r'_s per
+//       incidence; then the own DOFs: x += alpha p, r_new = r', z = the sum
+//       of the node's rows in subdomain order (untreated nodes: 1 / a_ii;
+//       diagonal / identity preconditioners: z from r' directly); r.r, z.r
+//   --- grid barrier (beta, convergence) ---
 // Vectors this kernel writes are read through L2 only (ld.global.cg): another
 // SM's L1 may still hold lines from an earlier phase, and the grid barrier's
 // fences do not invalidate them.
@@ -47,14 +63,22 @@ namespace hoefem {
 
 namespace {
 
-constexpr int NW = 12;                 // consumer warps
-constexpr int NS = 12;                 // ring stages
-constexpr int STAGE = 16384;           // bytes per stage (and per work item)
+constexpr int NW = 12;                  // consumer warps
+constexpr int NS = 12;                  // ring stages
+constexpr int STAGE = 14336;            // bytes per stage (and per work item)
 constexpr int THREADS = 32 * (NW + 1);  // + the producer warp (the last one)
 constexpr int CONSUMERS = 32 * NW;
-constexpr int TILE_HDR = 16;  // int nodes, int first node, 2 x pad; then (record offset, degree) per node
-constexpr int MAX_DIM = 84;   // Schwarz block dimension bound (3 x 27 nodes, padded)
+// item headers: int records, int first node / slot, 2 x pad; then per record
+// an int4 (record offset, degree or block dimension, own halo index or slot, 0)
+constexpr int ITEM_HDR = 16;
+constexpr int MAX_DIM = 81;      // Schwarz block dimension bound (3 x 27 nodes)
+constexpr int HALO_MAX = 1280;   // halo nodes of one segment
+constexpr int ZMAX = 1536;       // Schwarz row results (3 per incidence) of one segment
+constexpr size_t SMEM_RING = (size_t)NS * STAGE;
+constexpr size_t SMEM_BYTES = SMEM_RING + (size_t)3 * HALO_MAX * 8 + (size_t)ZMAX * 8;
 static_assert(NS % NW == 0, "each ring stage must belong to one consumer warp");
+static_assert(STAGE % 16 == 0 && SMEM_RING % 16 == 0, "bulk copies need 16-byte sizes and offsets");
+static_assert(3 * HALO_MAX < 65536, "halo-local indices are 16-bit");
 
 __host__ __device__ constexpr long long align16(long long x) { return (x + 15) & ~15LL; }
 
@@ -63,21 +87,22 @@ struct Args {
   const CgsItem* op_items;
   const int* op_item_off;
   const int* node_range;
+  const CgsSeg* segs;
+  const int* seg_off;
+  const int* halo;
   const unsigned char* sw;
   const CgsItem* sw_items;
   const int* sw_item_off;
-  const int* sub_off;
-  const int* sub_nodes;
-  const int* slot;      // slot of every (subdomain, node) incidence
-  const int* pair_off;  // nv + 1: a node's slots
+  const double* sw_scale;  // FP16 blocks: per-subdomain scale
+  const int* slot_sub;     // per slot: subdomain (FP16 scale lookup)
+  const int* pair_off;     // nv + 1: a node's slots (Schwarz incidences, subdomains ascending)
   const unsigned char* diag_only;
   const long long* pbase;
-  const double* pvals;     // assembled Schwarz values (untreated nodes' 1 / a_ii)
-  const double* sw_scale;  // FP16 blocks: per-subdomain scale
-  const double* dinv;      // diagonal preconditioner
-  double* ysub;
+  const double* pvals;  // assembled Schwarz values (untreated nodes' 1 / a_ii)
+  const double* dinv;   // diagonal preconditioner
   double* x;
-  double* r;
+  double* r0;
+  double* r1;
   double* z;
   double* Ap;
   double* pb0;
@@ -87,11 +112,11 @@ struct Args {
   unsigned* bar;
   int* err;  // [0] abort flag, [1] error code
   int reliable;
+  unsigned long long* prof;  // optional: 16 cycle counters per CTA (phase profile)
 };
 
 // The direction and the residual step, written once so that every use of a
-// value (neighbour gathers, own-node stores, block products, the update)
-// rounds identically.
+// value (halo gathers, own-node stores, the update) rounds identically.
 __device__ __forceinline__ double cg_dir(double z, double beta, double pold) { return __fma_rn(beta, pold, z); }
 __device__ __forceinline__ double cg_res(double r, double alpha, double ap) { return __fma_rn(-alpha, ap, r); }
 
@@ -134,16 +159,60 @@ __device__ __forceinline__ double sum_partials(const double* part, int G, int la
   return warp_sum(v);
 }
 
+// Gather batches: each thread first issues the loads of GB entries, then
+// computes and stores, so that GB L2 round trips overlap instead of chaining.
+constexpr int GB = 8;
+
+// For t < n3 (halo entry t / 3, component t % 3, DOF g = 3 halo[t / 3] + t % 3):
+// mode 0: s[t] = va + c vb at g (the direction z + beta p_old), also stored to
+// pnew for g in [d0, d1); mode 1: s[t] = va - c vb at g (r_old - alpha Ap).
+template <int MODE>
+__device__ __forceinline__ void gather_halo(const int* __restrict__ halo, int n3, int d0, int d1,
+                                            const double* __restrict__ va, const double* __restrict__ vb, double c,
+                                            double* __restrict__ s, double* __restrict__ pnew) {
+  for (int t0 = (int)threadIdx.x; t0 < n3; t0 += GB * CONSUMERS) {
+    int g[GB];
+#pragma unroll
+    for (int u = 0; u < GB; ++u) {
+      const int t = t0 + u * CONSUMERS;
+      g[u] = -1;
+      if (t < n3) {
+        const int hl = t / 3;
+        g[u] = 3 * __ldg(halo + hl) + (t - 3 * hl);
+      }
+    }
+    double a[GB], b[GB];
+#pragma unroll
+    for (int u = 0; u < GB; ++u) {
+      a[u] = g[u] >= 0 ? __ldcg(va + g[u]) : 0.0;
+      b[u] = g[u] >= 0 ? __ldcg(vb + g[u]) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < GB; ++u) {
+      if (g[u] < 0) continue;
+      if (MODE == 0) {
+        const double dv = cg_dir(a[u], c, b[u]);
+        s[t0 + u * CONSUMERS] = dv;
+        if (g[u] >= d0 && g[u] < d1) pnew[g[u]] = dv;
+      } else {
+        s[t0 + u * CONSUMERS] = cg_res(a[u], c, b[u]);
+      }
+    }
+  }
+}
+
 template <class VA, class VB, int PK>
 __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
   extern __shared__ __align__(128) unsigned char ring[];
+  double* s_halo = reinterpret_cast<double*>(ring + SMEM_RING);  // 3 x HALO_MAX
+  double* s_zp = s_halo + 3 * HALO_MAX;                           // ZMAX
   __shared__ __align__(8) uint64_t full[NS];
   __shared__ __align__(8) uint64_t empty[NS];
   __shared__ volatile int s_stop;
   __shared__ int s_fail, s_gok;
   __shared__ double s_red[NW][2];
-  __shared__ double s_rs[NW][MAX_DIM];
   __shared__ double s_bc[3];
+  __shared__ unsigned long long s_prof[16];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = blockIdx.x, G = gridDim.x;
   if (threadIdx.x == 0) {
@@ -153,52 +222,105 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
     }
     s_stop = 0;
     s_fail = 0;
+    for (int i = 0; i < 16; ++i) s_prof[i] = 0ull;
     pipe::mbar_fence_init();
   }
   __syncthreads();
+  // phase profile: thread 0 times its own path through the phases, the
+  // producer its idle polling
+  const bool prof = A.prof != nullptr;
+  const bool timer = prof && threadIdx.x == 0;
+  auto tick = [&]() -> unsigned long long { return timer ? (unsigned long long)clock64() : 0ull; };
+  auto tock = [&](int slot, unsigned long long t0) {
+    if (timer) s_prof[slot] += (unsigned long long)clock64() - t0;
+  };
   const int op0 = A.op_item_off[c], nop = A.op_item_off[c + 1] - op0;
   const int sw0 = PK == 2 ? A.sw_item_off[c] : 0;
   const int nsw = PK == 2 ? A.sw_item_off[c + 1] - sw0 : 0;
   const int per = nop + nsw;
 
   if (warp == NW) {
-    // ---- producer: cycle through the CTA's items, gated by free stages ----
+    // ---- producer: each stage s carries items s, s + NS, s + 2 NS, ... (the
+    // CTA's items cycled over the iterations); a stage is refilled as soon as
+    // its warp has released it, whatever the other stages are doing ----
     if (lane != 0) return;
-    long long k = 0;
+    const unsigned long long tp0 = prof ? (unsigned long long)clock64() : 0ull;
+    unsigned long long twait = 0ull, tw = tp0;
+    const uint64_t pol_keep = pipe::policy_evict_last(), pol_stream = pipe::policy_evict_first();
+    long long next[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) next[i] = i;
     bool late = false;
+    uint64_t t_idle = 0;
     while (per > 0 && !s_stop) {
-      const int j = (int)(k % per);
-      const CgsItem it = j < nop ? A.op_items[op0 + j] : A.sw_items[sw0 + (j - nop)];
-      const unsigned char* src = (j < nop ? A.op : A.sw) + it.off;
-      const int s = (int)(k % NS);
-      const long long use = k / NS;
-      if (use > 0 && !pipe::mbar_wait(&empty[s], (unsigned)((use - 1) & 1), &s_stop)) {
-        late = !s_stop;
-        break;
+      bool progress = false;
+#pragma unroll
+      for (int st = 0; st < NS; ++st) {
+        const long long k = next[st];
+        const long long use = k / NS;
+        if (use > 0 && !pipe::mbar_test(&empty[st], (unsigned)((use - 1) & 1))) continue;
+        const int j = (int)(k % per);
+        const CgsItem it = j < nop ? A.op_items[op0 + j] : A.sw_items[sw0 + (j - nop)];
+        const unsigned char* src = (j < nop ? A.op : A.sw) + it.off;
+        pipe::mbar_arrive_expect_tx(&full[st], (unsigned)it.bytes);
+        pipe::bulk_g2s_hint(ring + (size_t)st * STAGE, src, (unsigned)it.bytes, &full[st],
+                            it.keep ? pol_keep : pol_stream);
+        next[st] = k + NS;
+        progress = true;
       }
-      pipe::mbar_arrive_expect_tx(&full[s], (unsigned)it.bytes);
-      pipe::bulk_g2s(ring + (size_t)s * STAGE, src, (unsigned)it.bytes, &full[s]);
-      ++k;
+      if (progress) {
+        t_idle = 0;
+        if (prof) tw = (unsigned long long)clock64();
+      } else {
+        const uint64_t now = pipe::clock_ns();
+        if (t_idle == 0) {
+          t_idle = now;
+        } else if (now - t_idle > pipe::HOEFEM_WAIT_NS) {
+          late = true;
+          break;
+        }
+        if (prof) {
+          const unsigned long long c1 = (unsigned long long)clock64();
+          twait += c1 - tw;
+          tw = c1;
+        }
+      }
     }
-    if (late) {
+    if (late && !s_stop) {
       atomicExch(&A.err[0], 1);
       atomicCAS(&A.err[1], 0, (int)HOEFEM_ERR_DEVICE_TIMEOUT);
     }
-    // the copies still in flight (the last NS issued) land before the CTA exits
-    for (long long q = k > NS ? k - NS : 0; q < k; ++q) pipe::mbar_wait(&full[q % NS], (unsigned)((q / NS) & 1));
+    // the copies still in flight (each stage's last issued item) land before
+    // the CTA exits
+#pragma unroll
+    for (int st = 0; st < NS; ++st) {
+      const long long k = next[st] - NS;
+      if (k >= 0) pipe::mbar_wait(&full[st], (unsigned)((k / NS) & 1));
+    }
+    if (prof) {
+      atomicAdd(A.prof + 16 * c + 10, twait);
+      atomicAdd(A.prof + 16 * c + 11, (unsigned long long)clock64() - tp0);
+    }
     return;
   }
 
   // ---- consumers ----
   const int w = warp;
-  const int n0 = A.node_range[c], n1 = A.node_range[c + 1];
+  const int sg0 = A.seg_off[c], sg1 = A.seg_off[c + 1];
   CgState* st = A.st;
   double zTr = st->zTr, beta = st->beta, alpha = st->alpha, pAp = st->pAp, rr = st->rr;
   const double bnorm = st->bnorm, tol = st->tol, rr_ref = st->rr_ref, delta2 = st->delta2;
   long long iters = st->iters;
   const long long max_iter = st->max_iter;
-  int status = HOEFEM_OK, done = 0, replace = 0, pcur = 0;
+  int status = HOEFEM_OK, done = 0, replace = 0, pcur = 0, rcur = 0;
   long long it = 0;
+  // a lane's Schwarz columns j = lane + 32 p: record node j / 3, component j % 3
+  int jn[3], jc[3];
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    jn[p] = (lane + 32 * p) / 3;
+    jc[p] = (lane + 32 * p) % 3;
+  }
   auto fail = [&]() {
     s_fail = 1;
     atomicExch(&A.err[0], 1);
@@ -216,52 +338,93 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
     const long long kb = it * per;
     const double* pold = (it & 1) ? A.pb1 : A.pb0;
     double* pnew = (it & 1) ? A.pb0 : A.pb1;
-    // ---- P1: Ap = A p, p = z + beta p_old, p.Ap ----
+    const double* rold = (it & 1) ? A.r1 : A.r0;
+    double* rnew = (it & 1) ? A.r0 : A.r1;
+    // ---- P1: p = z + beta p_old on each segment's halo, Ap = A p, p.Ap ----
     double acc = 0.0;
-    for (int j = first_item(kb, 0, w); j < nop; j += NW) {
-      const long long k = kb + j;
-      const int s = (int)(k % NS);
-      if (!warp_wait(&full[s], (unsigned)((k / NS) & 1))) {
-        if (lane == 0) fail();
-        break;
-      }
-      const unsigned char* t = ring + (size_t)s * STAGE;
-      const int nn = *(const int*)t;
-      const int a0 = *(const int*)(t + 4);
-      for (int q = 0; q < nn; ++q) {
-        const int2 h = *(const int2*)(t + TILE_HDR + 8 * q);
-        const int d = h.y;
-        const int* adj = (const int*)(t + h.x);
-        const VA* v = (const VA*)(t + h.x + align16(4LL * d));
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-#pragma unroll 2
-        for (int e = lane; e < d; e += 32) {
-          const int b3 = 3 * adj[e];
-          const double q0 = cg_dir(__ldcg(A.z + b3), beta, __ldcg(pold + b3));
-          const double q1 = cg_dir(__ldcg(A.z + b3 + 1), beta, __ldcg(pold + b3 + 1));
-          const double q2 = cg_dir(__ldcg(A.z + b3 + 2), beta, __ldcg(pold + b3 + 2));
-          s0 += ldv(v + e) * q0 + ldv(v + d + e) * q1 + ldv(v + 2 * d + e) * q2;
-          s1 += ldv(v + 3 * d + e) * q0 + ldv(v + 4 * d + e) * q1 + ldv(v + 5 * d + e) * q2;
-          s2 += ldv(v + 6 * d + e) * q0 + ldv(v + 7 * d + e) * q1 + ldv(v + 8 * d + e) * q2;
+    for (int sg = sg0; sg < sg1; ++sg) {
+      const CgsSeg S = A.segs[sg];
+      unsigned long long t0 = tick();
+      pipe::named_sync(1, CONSUMERS);  // the previous segment is done with the halo
+      gather_halo<0>(A.halo + S.halo_off, 3 * S.halo_n, 3 * S.n0, 3 * S.n1, A.z, pold, beta, s_halo, pnew);
+      pipe::named_sync(1, CONSUMERS);
+      tock(0, t0);
+      t0 = tick();
+      for (int j = first_item(kb, S.j0, w); j < S.j1; j += NW) {
+        const long long k = kb + j;
+        const int s = (int)(k % NS);
+        const unsigned long long tw = tick();
+        if (!warp_wait(&full[s], (unsigned)((k / NS) & 1))) {
+          if (lane == 0) fail();
+          break;
         }
-        s0 = warp_sum(s0);
-        s1 = warp_sum(s1);
-        s2 = warp_sum(s2);
-        if (lane == 0) {
-          const int a3 = 3 * (a0 + q);
-          const double sv[3] = {s0, s1, s2};
+        tock(2, tw);
+        const unsigned char* t = ring + (size_t)s * STAGE;
+        const int nn = *(const int*)t;
+        const int a0 = *(const int*)(t + 4);
+        // two node rows at a time: their loads and reductions interleave
+        for (int q = 0; q < nn; q += 2) {
+          const bool two = q + 1 < nn;
+          const int4 h0 = *(const int4*)(t + ITEM_HDR + 16 * q);
+          const int4 h1 = two ? *(const int4*)(t + ITEM_HDR + 16 * (q + 1)) : make_int4(0, 0, 0, 0);
+          const unsigned short* loc0 = (const unsigned short*)(t + h0.x);
+          const unsigned short* loc1 = (const unsigned short*)(t + h1.x);
+          const VA* v0 = (const VA*)(t + h0.x + align16(2LL * h0.y));
+          const VA* v1 = (const VA*)(t + h1.x + align16(2LL * h1.y));
+          const int d0 = h0.y, d1 = h1.y;
+          double a00 = 0.0, a01 = 0.0, a02 = 0.0, a10 = 0.0, a11 = 0.0, a12 = 0.0;
+          const int dm = max(d0, d1);
+          for (int e = lane; e < dm; e += 32) {
+            if (e < d0) {
+              const double* pd = s_halo + loc0[e];
+              const double q0 = pd[0], q1 = pd[1], q2 = pd[2];
+              a00 += ldv(v0 + e) * q0 + ldv(v0 + d0 + e) * q1 + ldv(v0 + 2 * d0 + e) * q2;
+              a01 += ldv(v0 + 3 * d0 + e) * q0 + ldv(v0 + 4 * d0 + e) * q1 + ldv(v0 + 5 * d0 + e) * q2;
+              a02 += ldv(v0 + 6 * d0 + e) * q0 + ldv(v0 + 7 * d0 + e) * q1 + ldv(v0 + 8 * d0 + e) * q2;
+            }
+            if (e < d1) {
+              const double* pd = s_halo + loc1[e];
+              const double q0 = pd[0], q1 = pd[1], q2 = pd[2];
+              a10 += ldv(v1 + e) * q0 + ldv(v1 + d1 + e) * q1 + ldv(v1 + 2 * d1 + e) * q2;
+              a11 += ldv(v1 + 3 * d1 + e) * q0 + ldv(v1 + 4 * d1 + e) * q1 + ldv(v1 + 5 * d1 + e) * q2;
+              a12 += ldv(v1 + 6 * d1 + e) * q0 + ldv(v1 + 7 * d1 + e) * q1 + ldv(v1 + 8 * d1 + e) * q2;
+            }
+          }
 #pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            const double pa = cg_dir(__ldcg(A.z + a3 + i), beta, __ldcg(pold + a3 + i));
-            pnew[a3 + i] = pa;
-            A.Ap[a3 + i] = sv[i];
-            acc += pa * sv[i];
+          for (int o = 16; o > 0; o >>= 1) {
+            a00 += __shfl_xor_sync(0xffffffffu, a00, o);
+            a01 += __shfl_xor_sync(0xffffffffu, a01, o);
+            a02 += __shfl_xor_sync(0xffffffffu, a02, o);
+            a10 += __shfl_xor_sync(0xffffffffu, a10, o);
+            a11 += __shfl_xor_sync(0xffffffffu, a11, o);
+            a12 += __shfl_xor_sync(0xffffffffu, a12, o);
+          }
+          if (lane == 0) {
+            const int a3 = 3 * (a0 + q);
+            const double* pa = s_halo + h0.z;
+            A.Ap[a3] = a00;
+            A.Ap[a3 + 1] = a01;
+            A.Ap[a3 + 2] = a02;
+            acc += pa[0] * a00;
+            acc += pa[1] * a01;
+            acc += pa[2] * a02;
+            if (two) {
+              const double* pb = s_halo + h1.z;
+              A.Ap[a3 + 3] = a10;
+              A.Ap[a3 + 4] = a11;
+              A.Ap[a3 + 5] = a12;
+              acc += pb[0] * a10;
+              acc += pb[1] * a11;
+              acc += pb[2] * a12;
+            }
           }
         }
+        __syncwarp();
+        if (lane == 0) pipe::mbar_arrive(&empty[s]);
       }
-      __syncwarp();
-      if (lane == 0) pipe::mbar_arrive(&empty[s]);
+      tock(1, t0);
     }
+    unsigned long long tb = tick();
     if (lane == 0) s_red[w][0] = acc;
     pipe::named_sync(1, CONSUMERS);
     if (threadIdx.x == 0) {
@@ -278,85 +441,104 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
       if (lane == 0) s_bc[0] = t;
     }
     pipe::named_sync(1, CONSUMERS);
+    tock(3, tb);
     pAp = s_bc[0];
-    if (pAp <= 0.0) {
+    if (pAp <= 0.0 || zTr <= 0.0) {
       done = 1;
-      status = HOEFEM_CG_INDEFINITE_OPERATOR;
+      status = pAp <= 0.0 ? HOEFEM_CG_INDEFINITE_OPERATOR : HOEFEM_CG_INDEFINITE_PRECONDITIONER;
       pcur = (int)((it + 1) & 1);
-      break;
-    }
-    if (zTr <= 0.0) {
-      done = 1;
-      status = HOEFEM_CG_INDEFINITE_PRECONDITIONER;
-      pcur = (int)((it + 1) & 1);
+      rcur = (int)(it & 1);
       break;
     }
     alpha = zTr / pAp;
-    // ---- P2: Schwarz block products on the updated residual ----
-    if (PK == 2) {
-      for (int j = first_item(kb, nop, w); j < per; j += NW) {
-        const long long k = kb + j;
-        const int s = (int)(k % NS);
-        if (!warp_wait(&full[s], (unsigned)((k / NS) & 1))) {
-          if (lane == 0) fail();
-          break;
-        }
-        const CgsItem itm = A.sw_items[sw0 + (j - nop)];
-        const int sd = itm.a, row0 = itm.b, nrows = itm.c;
-        const int o = A.sub_off[sd];
-        const int dim = 3 * (A.sub_off[sd + 1] - o);
-        double* rs = s_rs[w];
-        for (int jj = lane; jj < dim; jj += 32) {
-          const int dd = 3 * A.sub_nodes[o + jj / 3] + jj % 3;
-          rs[jj] = cg_res(__ldcg(A.r + dd), alpha, __ldcg(A.Ap + dd));
-        }
-        __syncwarp();
-        const VB* blk = (const VB*)(ring + (size_t)s * STAGE);
-        const double sc = sizeof(VB) == 2 ? A.sw_scale[sd] : 1.0;
-        for (int i = lane; i < nrows; i += 32) {
-          const VB* row = blk + (size_t)i * dim;
-          double b0 = 0.0, b1 = 0.0, b2 = 0.0;
-          for (int jj = 0; jj < dim; jj += 3) {
-            b0 += ldv(row + jj) * rs[jj];
-            b1 += ldv(row + jj + 1) * rs[jj + 1];
-            b2 += ldv(row + jj + 2) * rs[jj + 2];
-          }
-          const int gi = row0 + i;
-          A.ysub[3 * A.slot[o + gi / 3] + gi % 3] = ((b0 + b1) + b2) * sc;
-        }
-        __syncwarp();
-        if (lane == 0) pipe::mbar_arrive(&empty[s]);
-      }
-      if (!grid_sync()) {
-        ok = false;
-        break;
-      }
-    }
-    // ---- P3: own DOFs: x, r, z, r.r, z.r ----
+    // ---- P2: r' on the halo, Schwarz rows, own DOFs ----
     double racc = 0.0, zacc = 0.0;
-    for (int t = 3 * n0 + (int)threadIdx.x; t < 3 * n1; t += CONSUMERS) {
-      const double pc = __ldcg(pnew + t);
-      A.x[t] = __fma_rn(alpha, pc, __ldcg(A.x + t));
-      const double rn = cg_res(__ldcg(A.r + t), alpha, __ldcg(A.Ap + t));
-      A.r[t] = rn;
-      double zv;
+    for (int sg = sg0; sg < sg1; ++sg) {
+      const CgsSeg S = A.segs[sg];
+      unsigned long long t0 = tick();
       if (PK == 2) {
-        const int a = t / 3, i = t - 3 * a;
-        if (A.diag_only[a]) {
-          zv = A.pvals[A.pbase[a] + i] * rn;
-        } else {
-          zv = 0.0;
-          for (int q = A.pair_off[a]; q < A.pair_off[a + 1]; ++q) zv += __ldcg(A.ysub + 3 * q + i);
+        pipe::named_sync(1, CONSUMERS);  // the previous segment is done with the halo and s_zp
+        gather_halo<1>(A.halo + S.halo_off, 3 * S.halo_n, 0, 0, rold, A.Ap, alpha, s_halo, nullptr);
+        pipe::named_sync(1, CONSUMERS);
+        tock(4, t0);
+        t0 = tick();
+        for (int j = first_item(kb, nop + S.sj0, w); j < nop + S.sj1; j += NW) {
+          const long long k = kb + j;
+          const int s = (int)(k % NS);
+          const unsigned long long tw = tick();
+          if (!warp_wait(&full[s], (unsigned)((k / NS) & 1))) {
+            if (lane == 0) fail();
+            break;
+          }
+          tock(6, tw);
+          const unsigned char* t = ring + (size_t)s * STAGE;
+          const int nr = *(const int*)t;
+          for (int q = 0; q < nr; ++q) {
+            const int4 h = *(const int4*)(t + ITEM_HDR + 16 * q);
+            const int dim = h.y;
+            const unsigned short* cols = (const unsigned short*)(t + h.x);
+            const VB* v = (const VB*)(t + h.x + align16(2LL * (dim / 3)));
+            double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+#pragma unroll
+            for (int p = 0; p < 3; ++p) {
+              const int j2 = lane + 32 * p;
+              if (j2 < dim) {
+                const double rv = s_halo[cols[jn[p]] + jc[p]];
+                y0 += ldv(v + j2) * rv;
+                y1 += ldv(v + dim + j2) * rv;
+                y2 += ldv(v + 2 * dim + j2) * rv;
+              }
+            }
+            y0 = warp_sum(y0);
+            y1 = warp_sum(y1);
+            y2 = warp_sum(y2);
+            if (lane == 0) {
+              const double sc = sizeof(VB) == 2 ? A.sw_scale[__ldg(A.slot_sub + h.z)] : 1.0;
+              double* zp = s_zp + 3 * (h.z - S.q0);
+              zp[0] = y0 * sc;
+              zp[1] = y1 * sc;
+              zp[2] = y2 * sc;
+            }
+          }
+          __syncwarp();
+          if (lane == 0) pipe::mbar_arrive(&empty[s]);
         }
-      } else if (PK == 1) {
-        zv = A.dinv[t] * rn;
-      } else {
-        zv = rn;
+        pipe::named_sync(1, CONSUMERS);  // every row result of the segment is in s_zp
+        tock(5, t0);
       }
-      A.z[t] = zv;
-      racc += rn * rn;
-      zacc += zv * rn;
+      // own DOFs of the segment
+      t0 = tick();
+      for (int t = 3 * S.n0 + (int)threadIdx.x; t < 3 * S.n1; t += CONSUMERS) {
+        const int a = t / 3, i = t - 3 * a;
+        const double pc = __ldcg(pnew + t);
+        const double xv = __ldcg(A.x + t);
+        double rn;
+        if (PK == 2) rn = s_halo[3 * (S.own_lo + a - S.n0) + i];
+        else rn = cg_res(__ldcg(rold + t), alpha, __ldcg(A.Ap + t));
+        double zv;
+        if (PK == 2) {
+          if (__ldg(A.diag_only + a)) {
+            zv = __ldg(A.pvals + __ldg(A.pbase + a) + i) * rn;
+          } else {
+            // the node's subdomains in ascending order (zero if it has none)
+            zv = 0.0;
+            const int q1 = __ldg(A.pair_off + a + 1);
+            for (int q = __ldg(A.pair_off + a); q < q1; ++q) zv += s_zp[3 * (q - S.q0) + i];
+          }
+        } else if (PK == 1) {
+          zv = __ldg(A.dinv + t) * rn;
+        } else {
+          zv = rn;
+        }
+        A.x[t] = __fma_rn(alpha, pc, xv);
+        rnew[t] = rn;
+        A.z[t] = zv;
+        racc += rn * rn;
+        zacc += zv * rn;
+      }
+      tock(8, t0);
     }
+    unsigned long long tu = tick();
     racc = warp_sum(racc);
     zacc = warp_sum(zacc);
     if (lane == 0) {
@@ -386,11 +568,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
       }
     }
     pipe::named_sync(1, CONSUMERS);
+    tock(9, tu);
     rr = s_bc[1];
     const double zr = s_bc[2];
     iters += 1;
     ++it;
     pcur = (int)(it & 1);
+    rcur = (int)(it & 1);
     if (sqrt(rr) <= tol * bnorm) {
       done = 1;
       status = HOEFEM_OK;
@@ -420,46 +604,53 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
       st->status = status;
       st->replace = replace;
       st->pcur = pcur;
+      st->rcur = rcur;
     } else {
       st->done = 1;
       st->status = HOEFEM_ERR_DEVICE_TIMEOUT;
       st->replace = 0;
       st->pcur = 0;
+      st->rcur = 0;
     }
   }
   pipe::named_sync(1, CONSUMERS);
-  if (threadIdx.x == 0) s_stop = 1;
+  if (threadIdx.x == 0) {
+    s_stop = 1;
+    if (prof) {
+      for (int i = 0; i < 10; ++i) atomicAdd(A.prof + 16 * c + i, s_prof[i]);
+      atomicAdd(A.prof + 16 * c + 12, (unsigned long long)it);
+    }
+  }
 }
 
 // ---- stream layouts -----------------------------------------------------------
 
-// Tile headers and neighbour lists (once per layout).
-__global__ void k_op_layout(int ntiles, const CgsItem* __restrict__ items, const int* __restrict__ adj_off,
-                            const int* __restrict__ adj, const long long* __restrict__ val_off,
-                            unsigned char* __restrict__ data) {
-  const int tile = blockIdx.x;
-  if (tile >= ntiles) return;
-  const CgsItem it = items[tile];
+// Item headers and 16-bit halo-local index lists (once per layout): for an
+// operator tile the neighbour lists, for a Schwarz row item the subdomain node
+// lists.  Record r of an item (global record first + r) starts at
+// idx_off[first + r]; its header holds (offset in the item, field_y, field_z).
+__global__ void k_item_layout(int nitems, const CgsItem* __restrict__ items, const long long* __restrict__ idx_off,
+                              const int* __restrict__ nidx_off, const unsigned short* __restrict__ idx,
+                              const int* __restrict__ field_y, const int* __restrict__ field_z,
+                              unsigned char* __restrict__ data) {
+  const int item = blockIdx.x;
+  if (item >= nitems) return;
+  const CgsItem it = items[item];
   unsigned char* t = data + it.off;
-  const int nn = it.b;
+  const int nr = it.b, first = it.a;
   if (threadIdx.x == 0) {
-    ((int*)t)[0] = nn;
-    ((int*)t)[1] = it.a;
+    ((int*)t)[0] = nr;
+    ((int*)t)[1] = first;
     ((int*)t)[2] = 0;
     ((int*)t)[3] = 0;
   }
-  for (int q = threadIdx.x; q < nn; q += blockDim.x) {
-    const int a = it.a + q;
-    const int d = adj_off[a + 1] - adj_off[a];
-    const long long rec = val_off[a] - align16(4LL * d) - it.off;
-    ((int2*)(t + TILE_HDR))[q] = make_int2((int)rec, d);
-  }
+  for (int q = threadIdx.x; q < nr; q += blockDim.x)
+    ((int4*)(t + ITEM_HDR))[q] = make_int4((int)(idx_off[first + q] - it.off), field_y[first + q], field_z[first + q], 0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
-  for (int q = warp; q < nn; q += nwarp) {
-    const int a = it.a + q;
-    const int o = adj_off[a], d = adj_off[a + 1] - o;
-    int* dst = (int*)(data + val_off[a] - align16(4LL * d));
-    for (int e = lane; e < d; e += 32) dst[e] = adj[o + e];
+  for (int q = warp; q < nr; q += nwarp) {
+    const int o = nidx_off[first + q], n = nidx_off[first + q + 1] - o;
+    unsigned short* dst = (unsigned short*)(data + idx_off[first + q]);
+    for (int e = lane; e < n; e += 32) dst[e] = idx[o + e];
   }
 }
 
@@ -484,38 +675,48 @@ __global__ void __launch_bounds__(256) k_op_pack(int nv, const long long* __rest
   }
 }
 
-// Schwarz blocks (symmetrized inverses, row-major dim x dim at stage_off[s])
-// into row chunks; FP16 blocks are divided by their largest magnitude first.
-template <class V>
-__global__ void __launch_bounds__(256) k_sw_pack(const int* __restrict__ sub_off, const long long* __restrict__ stage_off,
-                                                 const double* __restrict__ B, const long long* __restrict__ chunk_base,
-                                                 const int* __restrict__ rpc, double* __restrict__ scale,
-                                                 unsigned char* __restrict__ data) {
+// Largest magnitude of each subdomain block (FP16 scale).
+__global__ void __launch_bounds__(256) k_sw_scale(const int* __restrict__ sub_off,
+                                                  const long long* __restrict__ stage_off,
+                                                  const double* __restrict__ B, double* __restrict__ scale) {
   const int s = blockIdx.x;
   const int dim = 3 * (sub_off[s + 1] - sub_off[s]);
   const double* src = B + stage_off[s];
-  const int rows = rpc[s];
-  const long long cbytes = align16((long long)rows * dim * (long long)sizeof(V));
-  double inv = 1.0;
-  if (sizeof(V) == 2) {
-    __shared__ double s_max[8];
-    double m = 0.0;
-    for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) m = fmax(m, fabs(src[k]));
+  __shared__ double s_max[8];
+  double m = 0.0;
+  for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) m = fmax(m, fabs(src[k]));
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
-    __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
     double mx = 0.0;
     for (int i = 0; i < (int)(blockDim.x >> 5); ++i) mx = fmax(mx, s_max[i]);
-    if (mx > 0.0) inv = 1.0 / mx;
-    if (threadIdx.x == 0) scale[s] = mx > 0.0 ? mx : 1.0;
+    scale[s] = mx > 0.0 ? mx : 1.0;
   }
-  for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) {
-    const int row = k / dim, col = k - row * dim;
-    const int ch = row / rows, rin = row - ch * rows;
-    V* dst = (V*)(data + chunk_base[s] + ch * cbytes);
-    if constexpr (sizeof(V) == 2) dst[rin * dim + col] = __float2half_rn((float)(src[k] * inv));
-    else dst[rin * dim + col] = (V)src[k];
+}
+
+// Schwarz rows into the slot records: slot q (subdomain s, local node I) gets
+// rows 3I .. 3I + 2 of the symmetrized inverted block (row-major dim x dim at
+// stage_off[s]), FP16 divided by the block's scale.  One warp per slot.
+template <class V>
+__global__ void __launch_bounds__(256) k_sw_pack(int nslot, const int* __restrict__ slot_sub,
+                                                 const int* __restrict__ slot_local, const int* __restrict__ sub_off,
+                                                 const long long* __restrict__ stage_off, const double* __restrict__ B,
+                                                 const double* __restrict__ scale,
+                                                 const long long* __restrict__ rec_val_off,
+                                                 unsigned char* __restrict__ data) {
+  const int lane = threadIdx.x & 31;
+  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nslot; q += (gridDim.x * blockDim.x) >> 5) {
+    const int s = slot_sub[q], I = slot_local[q];
+    const int dim = 3 * (sub_off[s + 1] - sub_off[s]);
+    const double* src = B + stage_off[s] + (long long)3 * I * dim;
+    V* dst = (V*)(data + rec_val_off[q]);
+    const double inv = sizeof(V) == 2 ? 1.0 / scale[s] : 1.0;
+    for (int k = lane; k < 3 * dim; k += 32) {
+      if constexpr (sizeof(V) == 2) dst[k] = __float2half_rn((float)(src[k] * inv));
+      else dst[k] = (V)src[k];
+    }
   }
 }
 
@@ -524,10 +725,10 @@ __global__ void k_cg_stream_arm(CgState* st, double delta2) {
   st->delta2 = delta2;
   st->replace = 0;
   st->pcur = 0;
+  st->rcur = 0;
 }
 
-// Splits `n` items with byte sizes `bytes` into G contiguous groups of about
-// equal bytes: off[0..G].
+// Splits items into G contiguous groups of about equal bytes: off[0..G].
 void split_items(const std::vector<CgsItem>& items, int G, std::vector<int>& off) {
   long long total = 0;
   for (auto& it : items) total += it.bytes;
@@ -541,33 +742,112 @@ void split_items(const std::vector<CgsItem>& items, int G, std::vector<int>& off
   while (g <= G) off[g++] = (int)items.size();
 }
 
-// Operator layout for value size vsize; false if a node row does not fit a
-// stage (the streamed CG is then not used).
-bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, cudaStream_t s) {
+// Packs consecutive records (byte sizes rec[r], each 16-aligned) into items of
+// at most STAGE bytes with a header; item.a = first record, item.b = records;
+// the records' absolute offsets go to rec_off.  False if one record alone
+// does not fit.
+bool pack_items(const std::vector<long long>& rec, long long& pos, std::vector<CgsItem>& items,
+                std::vector<long long>& rec_off) {
+  const size_t n = rec.size();
+  size_t a = 0;
+  while (a < n) {
+    size_t b = a;
+    long long recs = 0;
+    while (b < n) {
+      const long long hdr = align16(ITEM_HDR + 16 * (long long)(b - a + 1));
+      if (hdr + recs + rec[b] > STAGE) break;
+      recs += rec[b];
+      ++b;
+    }
+    if (b == a) return false;
+    const long long hdr = align16(ITEM_HDR + 16 * (long long)(b - a));
+    long long o = pos + hdr;
+    for (size_t q = a; q < b; ++q) {
+      rec_off[q] = o;
+      o += rec[q];
+    }
+    CgsItem it{};
+    it.off = pos;
+    it.bytes = (int)(hdr + recs);
+    it.a = (int)a;
+    it.b = (int)(b - a);
+    items.push_back(it);
+    pos = o;
+    a = b;
+  }
+  return true;
+}
+
+// Incidence (slot) structure of a Schwarz preconditioner in node-major slot
+// order: the slots of node a are [pair_off[a], pair_off[a+1]), its subdomains
+// ascending; slot_sub / slot_local give (subdomain, local node index).
+void schwarz_slots(const Precond& P, i64 nv, std::vector<int>& pair_off, std::vector<int>& slot_sub,
+                   std::vector<int>& slot_local) {
+  pair_off.assign(nv + 1, 0);
+  for (i64 k = 0; k < P.sub_off[P.nsub]; ++k) pair_off[P.sub_nodes[k] + 1] += 1;
+  for (i64 a = 0; a < nv; ++a) pair_off[a + 1] += pair_off[a];
+  std::vector<int> fill(pair_off.begin(), pair_off.end() - 1);
+  slot_sub.assign(P.sub_off[P.nsub], 0);
+  slot_local.assign(P.sub_off[P.nsub], 0);
+  for (i64 s = 0; s < P.nsub; ++s)
+    for (i64 k = P.sub_off[s]; k < P.sub_off[s + 1]; ++k) {
+      const int q = fill[P.sub_nodes[k]]++;
+      slot_sub[q] = (int)s;
+      slot_local[q] = (int)(k - P.sub_off[s]);
+    }
+}
+
+// Operator layout for value size vsize (and, with a Schwarz preconditioner,
+// segments that also bound its incidences); false if a node row does not fit
+// a stage or a halo.  Tiles are runs of consecutive nodes; the CTAs get
+// contiguous tile ranges of about equal bytes; a CTA's tiles are cut into
+// segments whose halo fits HALO_MAX nodes and whose Schwarz incidences fit
+// ZMAX / 3.
+bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P, cudaStream_t s) {
   const i64 nv = m.nv;
+  for (i64 q = 0; q < nv; ++q)
+    HOEFEM_REQUIRE(m.diag_slot[q] >= 0, HOEFEM_ERR_PATTERN, "streamed CG: a node row without its diagonal block");
+  std::vector<int> pair_off, slot_sub, slot_local;
+  const bool sw = P && P->kind == PREC_SCHWARZ && P->nsub > 0;
+  if (sw) schwarz_slots(*P, nv, pair_off, slot_sub, slot_local);
+  auto incid = [&](i64 a) { return sw ? pair_off[a + 1] - pair_off[a] : 0; };
+  auto rec_bytes = [&](i64 a) {
+    const long long d = m.adj_off[a + 1] - m.adj_off[a];
+    return align16(2 * d) + align16(9 * d * vsize);
+  };
+  // tiles: runs of nodes within a stage and a halo
   std::vector<CgsItem> items;
-  std::vector<long long> val_off(nv);
+  std::vector<long long> val_off(nv), idx_off(nv);
+  std::vector<int> stamp(nv, -1);
   long long pos = 0;
   i64 a = 0;
+  int tile_id = 0;
   while (a < nv) {
     const long long start = pos;
     long long recs = 0;
+    int uniq = 0, inc = 0;
     i64 b = a;
     std::vector<long long> rec_rel;
     while (b < nv) {
-      const long long d = m.adj_off[b + 1] - m.adj_off[b];
-      const long long rec = align16(4 * d) + align16(9 * d * vsize);
-      const long long hdr = align16(TILE_HDR + 8 * (b - a + 1));
+      const long long rec = rec_bytes(b);
+      const long long hdr = align16(ITEM_HDR + 16 * (b - a + 1));
       if (hdr + recs + rec > STAGE) break;
+      int add = 0;
+      for (int e = m.adj_off[b]; e < m.adj_off[b + 1]; ++e) add += stamp[m.adj[e]] != tile_id;
+      if (uniq + add > HALO_MAX || 3 * (inc + incid(b)) > ZMAX) break;
+      for (int e = m.adj_off[b]; e < m.adj_off[b + 1]; ++e) stamp[m.adj[e]] = tile_id;
+      uniq += add;
+      inc += incid(b);
       rec_rel.push_back(recs);
       recs += rec;
       ++b;
     }
-    if (b == a) return false;  // one node row exceeds a stage
-    const long long hdr = align16(TILE_HDR + 8 * (b - a));
+    if (b == a) return false;  // one node row exceeds a stage or a halo
+    const long long hdr = align16(ITEM_HDR + 16 * (b - a));
     for (i64 q = a; q < b; ++q) {
       const long long d = m.adj_off[q + 1] - m.adj_off[q];
-      val_off[q] = start + hdr + rec_rel[q - a] + align16(4 * d);
+      idx_off[q] = start + hdr + rec_rel[q - a];
+      val_off[q] = idx_off[q] + align16(2 * d);
     }
     CgsItem it{};
     it.off = start;
@@ -577,63 +857,229 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, cudaStream_t s) 
     items.push_back(it);
     pos = start + hdr + recs;
     a = b;
+    ++tile_id;
   }
   std::vector<int> off, nrange(G + 1);
   split_items(items, G, off);
   for (int g = 0; g <= G; ++g) nrange[g] = off[g] < (int)items.size() ? items[off[g]].a : (int)nv;
+  // segments: halo-local neighbour indices (sorted halo, times 3), own halo index
+  std::vector<CgsSeg> segs;
+  std::vector<int> seg_off(G + 1, 0), halo;
+  std::vector<unsigned short> loc_adj(m.adj.size());
+  std::vector<int> self_loc(nv, 0), deg(nv);
+  std::vector<int> local(nv, -1);
+  std::fill(stamp.begin(), stamp.end(), -1);
+  int seg_id = 0;
+  for (int g = 0; g < G; ++g) {
+    seg_off[g] = (int)segs.size();
+    int j = off[g];
+    while (j < off[g + 1]) {
+      std::vector<int> hs;
+      int j1 = j, inc = 0;
+      while (j1 < off[g + 1]) {
+        const CgsItem& it = items[j1];
+        int add = 0, tinc = 0;
+        for (i64 q = it.a; q < it.a + it.b; ++q) {
+          tinc += incid(q);
+          for (int e = m.adj_off[q]; e < m.adj_off[q + 1]; ++e)
+            if (stamp[m.adj[e]] != seg_id) {
+              stamp[m.adj[e]] = seg_id;
+              ++add;
+              hs.push_back(m.adj[e]);
+            }
+        }
+        if ((int)hs.size() > HALO_MAX || 3 * (inc + tinc) > ZMAX) {
+          if (j1 == j) return false;
+          for (int r = 0; r < add; ++r) {
+            stamp[hs.back()] = -1;
+            hs.pop_back();
+          }
+          break;
+        }
+        inc += tinc;
+        ++j1;
+      }
+      std::sort(hs.begin(), hs.end());
+      for (size_t h = 0; h < hs.size(); ++h) local[hs[h]] = (int)h;
+      CgsSeg S{};
+      S.j0 = j - off[g];
+      S.j1 = j1 - off[g];
+      S.halo_off = (int)halo.size();
+      S.halo_n = (int)hs.size();
+      S.n0 = items[j].a;
+      S.n1 = items[j1 - 1].a + items[j1 - 1].b;
+      S.own_lo = local[S.n0];
+      S.q0 = sw ? pair_off[S.n0] : 0;
+      S.q1 = sw ? pair_off[S.n1] : 0;
+      halo.insert(halo.end(), hs.begin(), hs.end());
+      for (int t = j; t < j1; ++t)
+        for (i64 q = items[t].a; q < items[t].a + items[t].b; ++q) {
+          for (int e = m.adj_off[q]; e < m.adj_off[q + 1]; ++e)
+            loc_adj[e] = (unsigned short)(3 * local[m.adj[e]]);
+          self_loc[q] = 3 * local[q];  // every node is its own neighbour (diagonal block)
+          deg[q] = m.adj_off[q + 1] - m.adj_off[q];
+        }
+      segs.push_back(S);
+      ++seg_id;
+      j = j1;
+    }
+  }
+  seg_off[G] = (int)segs.size();
   L.data.alloc(pos);
   L.items.upload(items, s);
   L.item_off.upload(off, s);
+  L.h_items = items;
+  L.h_item_off = off;
+  L.h_segs = segs;
+  L.h_seg_off = seg_off;
+  L.h_halo = halo;
+  L.keep_applied = -1;
   L.node_range.upload(nrange, s);
   L.val_off.upload(val_off, s);
+  L.segs.upload(segs, s);
+  L.seg_off.upload(seg_off, s);
+  L.halo.upload(halo, s);
+  DBuf<unsigned short> d_loc;
+  DBuf<int> d_self, d_deg;
+  DBuf<long long> d_idx_off;
+  d_loc.upload(loc_adj, s);
+  d_self.upload(self_loc, s);
+  d_deg.upload(deg, s);
+  d_idx_off.upload(idx_off, s);
   L.bytes = pos;
   L.grid = G;
-  (note_launch(), k_op_layout<<<(int)items.size(), 256, 0, s>>>((int)items.size(), L.items.p, m.d_adj_off.p,
-                                                                  m.d_adj.p, L.val_off.p, L.data.p));
+  (note_launch(), k_item_layout<<<(int)items.size(), 256, 0, s>>>((int)items.size(), L.items.p, d_idx_off.p,
+                                                                    m.d_adj_off.p, d_loc.p, d_deg.p, d_self.p,
+                                                                    L.data.p));
   HOEFEM_CUDA(cudaGetLastError());
   HOEFEM_CUDA(cudaStreamSynchronize(s));
   L.vsize = vsize;
+  L.seg_for = sw ? (const void*)P : nullptr;
   return true;
 }
 
-void build_sw_layout(CgStreamSchwarz& L, const Precond& P, int vsize, int G, cudaStream_t s) {
-  std::vector<CgsItem> items;
-  std::vector<long long> base(P.nsub);
-  std::vector<int> rpc(P.nsub);
-  long long pos = 0;
-  for (i64 sd = 0; sd < P.nsub; ++sd) {
-    const int dim = (int)(3 * (P.sub_off[sd + 1] - P.sub_off[sd]));
-    const int maxrows = std::max(1, STAGE / (dim * vsize));
-    const int nch = (dim + maxrows - 1) / maxrows;
-    const int rows = (dim + nch - 1) / nch;
-    const long long cbytes = align16((long long)rows * dim * vsize);
-    base[sd] = pos;
-    rpc[sd] = rows;
-    for (int ch = 0; ch < nch; ++ch) {
-      const int r0 = ch * rows, r1 = std::min(dim, r0 + rows);
-      CgsItem it{};
-      it.off = pos + ch * cbytes;
-      it.bytes = (int)align16((long long)(r1 - r0) * dim * vsize);
-      it.a = (int)sd;
-      it.b = r0;
-      it.c = r1 - r0;
-      items.push_back(it);
-    }
-    pos += nch * cbytes;
+// Schwarz row records in the segments of the operator layout L: for each
+// segment the slots of its nodes (node-major), each record the 16-bit
+// halo-local indices (times 3) of the subdomain's nodes and its 3 block rows.
+bool build_sw_layout(CgStreamSchwarz& S, const Precond& P, CgStreamOp& L, int vsize, i64 nv, cudaStream_t s) {
+  std::vector<int> pair_off, slot_sub, slot_local;
+  schwarz_slots(P, nv, pair_off, slot_sub, slot_local);
+  const i64 nslot = (i64)slot_sub.size();
+  std::vector<long long> rec(nslot), rec_off(nslot), val_off(nslot);
+  std::vector<int> cols_off(nslot + 1, 0), dims(nslot), slot_id(nslot);
+  for (i64 q = 0; q < nslot; ++q) {
+    const int ns = (int)(P.sub_off[slot_sub[q] + 1] - P.sub_off[slot_sub[q]]);
+    dims[q] = 3 * ns;
+    slot_id[q] = (int)q;
+    rec[q] = align16(2LL * ns) + align16(3LL * (3 * ns) * vsize);
+    cols_off[q + 1] = cols_off[q] + ns;
   }
-  std::vector<int> off;
-  split_items(items, G, off);
-  L.data.alloc(pos);
-  L.items.upload(items, s);
-  L.item_off.upload(off, s);
-  L.chunk_base.upload(base, s);
-  L.rows_per_chunk.upload(rpc, s);
-  L.scale.alloc(std::max<i64>(P.nsub, 1));
-  L.bytes = pos;
-  L.grid = G;
-  L.vsize = vsize;
-  L.built_for = &P;
+  std::vector<unsigned short> cols(cols_off[nslot]);
+  std::vector<int> local(nv, -1);
+  const int G = L.grid;
+  std::vector<CgsItem> items;
+  std::vector<int> item_off(G + 1, 0);
+  std::vector<CgsSeg> segs = L.h_segs;
+  long long pos = 0;
+  for (int g = 0; g < G; ++g) {
+    item_off[g] = (int)items.size();
+    for (int sg = L.h_seg_off[g]; sg < L.h_seg_off[g + 1]; ++sg) {
+      CgsSeg& Sg = segs[sg];
+      for (int h = 0; h < Sg.halo_n; ++h) local[L.h_halo[Sg.halo_off + h]] = h;
+      const int q0 = pair_off[Sg.n0], q1 = pair_off[Sg.n1];
+      bool inside = true;
+      for (int q = q0; q < q1 && inside; ++q) {
+        const i64 sd = slot_sub[q];
+        for (i64 k = P.sub_off[sd]; k < P.sub_off[sd + 1]; ++k) {
+          const int l = local[P.sub_nodes[k]];
+          if (l < 0) {
+            inside = false;  // a subdomain node outside the segment's halo
+            break;
+          }
+          cols[cols_off[q] + (k - P.sub_off[sd])] = (unsigned short)(3 * l);
+        }
+      }
+      for (int h = 0; h < Sg.halo_n; ++h) local[L.h_halo[Sg.halo_off + h]] = -1;
+      if (!inside) return false;
+      Sg.sj0 = (int)items.size() - item_off[g];
+      if (q1 > q0) {
+        std::vector<long long> r(rec.begin() + q0, rec.begin() + q1), ro(q1 - q0);
+        const size_t first = items.size();
+        if (!pack_items(r, pos, items, ro)) return false;
+        for (size_t i = first; i < items.size(); ++i) items[i].a += q0;  // first slot of the item
+        for (int q = q0; q < q1; ++q) {
+          rec_off[q] = ro[q - q0];
+          val_off[q] = rec_off[q] + align16(2LL * (dims[q] / 3));
+        }
+      }
+      Sg.sj1 = (int)items.size() - item_off[g];
+    }
+  }
+  item_off[G] = (int)items.size();
+  S.data.alloc(pos);
+  S.items.upload(items, s);
+  S.item_off.upload(item_off, s);
+  S.h_items = items;
+  S.h_item_off = item_off;
+  S.keep_applied = -1;
+  S.rec_val_off.upload(val_off, s);
+  S.slot_sub.upload(slot_sub, s);
+  S.slot_local.upload(slot_local, s);
+  S.scale.alloc(std::max<i64>(P.nsub, 1));
+  // the segments now carry their Schwarz item ranges
+  L.h_segs = segs;
+  L.segs.upload(segs, s);
+  DBuf<unsigned short> d_cols;
+  DBuf<int> d_cols_off, d_dims, d_slot;
+  DBuf<long long> d_rec_off;
+  d_cols.upload(cols, s);
+  d_cols_off.upload(cols_off, s);
+  d_dims.upload(dims, s);
+  d_slot.upload(slot_id, s);
+  d_rec_off.upload(rec_off, s);
+  if (!items.empty())
+    (note_launch(), k_item_layout<<<(int)items.size(), 256, 0, s>>>((int)items.size(), S.items.p, d_rec_off.p,
+                                                                      d_cols_off.p, d_cols.p, d_dims.p, d_slot.p,
+                                                                      S.data.p));
+  HOEFEM_CUDA(cudaGetLastError());
   HOEFEM_CUDA(cudaStreamSynchronize(s));
+  S.bytes = pos;
+  S.grid = G;
+  S.vsize = vsize;
+  S.built_for = &P;
+  S.op_for = &L;
+  return true;
+}
+
+// L2 keep flags for a budget of `budget` bytes over all CTAs: each CTA keeps
+// up to budget / G bytes, its Schwarz records first, then its operator tiles
+// from the start of its list.
+void apply_keep(CgStreamOp& L, CgStreamSchwarz* S, long long budget, cudaStream_t s) {
+  const int G = L.grid;
+  const long long per = budget / G;
+  for (auto& it : L.h_items) it.keep = 0;
+  if (S)
+    for (auto& it : S->h_items) it.keep = 0;
+  for (int c = 0; c < G; ++c) {
+    long long rem = per;
+    if (S)
+      for (int j = S->h_item_off[c]; j < S->h_item_off[c + 1]; ++j)
+        if (S->h_items[j].bytes <= rem) {
+          S->h_items[j].keep = 1;
+          rem -= S->h_items[j].bytes;
+        }
+    for (int j = L.h_item_off[c]; j < L.h_item_off[c + 1]; ++j)
+      if (L.h_items[j].bytes <= rem) {
+        L.h_items[j].keep = 1;
+        rem -= L.h_items[j].bytes;
+      }
+  }
+  L.items.upload(L.h_items, s);
+  L.keep_applied = budget;
+  if (S) {
+    S->items.upload(S->h_items, s);
+    S->keep_applied = budget;
+  }
 }
 
 template <class VA, class VB, int PK>
@@ -642,7 +1088,7 @@ void launch_engine(const Args& args, int G, cudaStream_t s) {
   static bool configured[64] = {};
   int dev = 0;
   HOEFEM_CUDA(cudaGetDevice(&dev));
-  const size_t smem = (size_t)NS * STAGE;
+  const size_t smem = SMEM_BYTES;
   if (dev >= 0 && dev < 64 && !configured[dev]) {
     HOEFEM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
@@ -664,18 +1110,53 @@ bool cg_stream_usable(CgWork& w, const Precond* P) {
   HOEFEM_CUDA(cudaGetDevice(&dev));
   HOEFEM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
   if (!coop || w.m->nv == 0) return false;
-  if (P && P->kind == PREC_SCHWARZ && (!P->block_apply || P->nsub == 0 || 3 * P->max_nodes > MAX_DIM)) return false;
+  if (P && P->kind == PREC_SCHWARZ && (P->nsub == 0 || 3 * P->max_nodes > MAX_DIM)) return false;
   return true;
 }
 
-void cg_stream_prepare(CgWork& w, const double* A64, bool f32, const Precond* P, bool p32, cudaStream_t s) {
+bool cg_stream_prepare(CgWork& w, const double* A64, bool f32, const Precond* P, bool p32, cudaStream_t s) {
   Model& m = *w.m;
   const int G = device_sms();
   CgStreamOp& L = f32 ? w.sop32 : w.sop64;
   const int vsize = f32 ? 4 : 8;
-  if (L.vsize != vsize || L.grid != G) {
-    if (!build_op_layout(L, m, vsize, G, s))
-      throw Error(HOEFEM_ERR_INVALID_ARGUMENT, "a node row exceeds the streamed CG's stage size");
+  const bool sw = P && P->kind == PREC_SCHWARZ && P->nsub > 0;
+  const void* seg_for = sw ? (const void*)P : nullptr;
+  if (L.vsize != vsize || L.grid != G || L.seg_for != seg_for) {
+    if (L.vsize == -vsize && L.seg_for == seg_for) return false;  // layout known not to fit
+    if (!build_op_layout(L, m, vsize, G, P, s)) {
+      L.vsize = -vsize;
+      L.seg_for = seg_for;
+      return false;
+    }
+    w.ssw.vsize = 0;  // the Schwarz records follow the operator segments
+  }
+  if (sw) {
+    const int sv = p32 ? (w.schwarz_half ? 2 : 4) : 8;
+    CgStreamSchwarz& S = w.ssw;
+    if (S.vsize != sv || S.grid != G || S.built_for != (const void*)P || S.op_for != (const void*)&L) {
+      if (!build_sw_layout(S, *P, L, sv, m.nv, s)) {
+        S.vsize = 0;
+        return false;
+      }
+    }
+    const int nslot = (int)P->sub_off[P->nsub];
+    const int ng = std::min(std::max(1, (nslot + 7) / 8), device_sms() * 8);
+    if (sv == 2)
+      (note_launch(), k_sw_scale<<<(int)P->nsub, 256, 0, s>>>(P->d_sub_off.p, P->d_stage_off.p, P->bsym.p,
+                                                               S.scale.p));
+    if (sv == 8)
+      (note_launch(), k_sw_pack<double><<<ng, 256, 0, s>>>(nslot, S.slot_sub.p, S.slot_local.p, P->d_sub_off.p,
+                                                            P->d_stage_off.p, P->bsym.p, S.scale.p,
+                                                            S.rec_val_off.p, S.data.p));
+    else if (sv == 4)
+      (note_launch(), k_sw_pack<float><<<ng, 256, 0, s>>>(nslot, S.slot_sub.p, S.slot_local.p, P->d_sub_off.p,
+                                                           P->d_stage_off.p, P->bsym.p, S.scale.p,
+                                                           S.rec_val_off.p, S.data.p));
+    else
+      (note_launch(), k_sw_pack<__half><<<ng, 256, 0, s>>>(nslot, S.slot_sub.p, S.slot_local.p, P->d_sub_off.p,
+                                                            P->d_stage_off.p, P->bsym.p, S.scale.p,
+                                                            S.rec_val_off.p, S.data.p));
+    HOEFEM_CUDA(cudaGetLastError());
   }
   const int ng = std::max(1, (int)((m.nv + 7) / 8));
   if (f32)
@@ -685,23 +1166,13 @@ void cg_stream_prepare(CgWork& w, const double* A64, bool f32, const Precond* P,
     (note_launch(), k_op_pack<double><<<std::min(ng, device_sms() * 8), 256, 0, s>>>(
                         (int)m.nv, m.d_base.p, m.d_adj_off.p, L.val_off.p, A64, L.data.p));
   HOEFEM_CUDA(cudaGetLastError());
-  if (P && P->kind == PREC_SCHWARZ && P->nsub > 0) {
-    const int sv = p32 ? (w.schwarz_half ? 2 : 4) : 8;
-    CgStreamSchwarz& S = w.ssw;
-    if (S.vsize != sv || S.grid != G || S.built_for != (const void*)P) build_sw_layout(S, *P, sv, G, s);
-    const int ns = (int)P->nsub;
-    if (sv == 8)
-      (note_launch(), k_sw_pack<double><<<ns, 256, 0, s>>>(P->d_sub_off.p, P->d_stage_off.p, P->bsym.p,
-                                                            S.chunk_base.p, S.rows_per_chunk.p, S.scale.p, S.data.p));
-    else if (sv == 4)
-      (note_launch(), k_sw_pack<float><<<ns, 256, 0, s>>>(P->d_sub_off.p, P->d_stage_off.p, P->bsym.p,
-                                                           S.chunk_base.p, S.rows_per_chunk.p, S.scale.p, S.data.p));
-    else
-      (note_launch(), k_sw_pack<__half><<<ns, 256, 0, s>>>(P->d_sub_off.p, P->d_stage_off.p, P->bsym.p,
-                                                            S.chunk_base.p, S.rows_per_chunk.p, S.scale.p, S.data.p));
-    HOEFEM_CUDA(cudaGetLastError());
+  {
+    const long long budget = w.l2_keep < 0 ? 0 : w.l2_keep;
+    CgStreamSchwarz* S = sw ? &w.ssw : nullptr;
+    if (L.keep_applied != budget || (S && S->keep_applied != budget)) apply_keep(L, S, budget, s);
   }
   if (w.p2.n < (size_t)w.n) w.p2.alloc(w.n);
+  if (w.r2.n < (size_t)w.n) w.r2.alloc(w.n);
   if (w.spart.n < (size_t)(3 * G)) w.spart.alloc(3 * G);
   if (!w.sbar.p) w.sbar.alloc(1);
   if (!w.serr.p) w.serr.alloc(2);
@@ -709,6 +1180,31 @@ void cg_stream_prepare(CgWork& w, const double* A64, bool f32, const Precond* P,
     HOEFEM_CUDA(cudaEventCreate(&w.sev[0]));
     HOEFEM_CUDA(cudaEventCreate(&w.sev[1]));
   }
+  return true;
+}
+
+void cg_stream_phase_us(CgWork& w, double* out) {
+  for (int i = 0; i < 12; ++i) out[i] = 0.0;
+  if (!w.phase_profile || !w.sprof.p) return;
+  std::vector<unsigned long long> h(w.sprof.n);
+  HOEFEM_CUDA(cudaMemcpy(h.data(), w.sprof.p, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  const int G = (int)(w.sprof.n / 16);
+  unsigned long long its = 0;
+  for (int c = 0; c < G; ++c) its = std::max(its, h[16 * c + 12]);
+  if (w.sclock_khz <= 0.0) {
+    int dev = 0, khz = 0;
+    HOEFEM_CUDA(cudaGetDevice(&dev));
+    HOEFEM_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev));
+    w.sclock_khz = khz > 0 ? khz : 1.0;
+  }
+  if (its > 0) {
+    for (int i = 0; i < 12; ++i) {
+      double sum = 0.0;
+      for (int c = 0; c < G; ++c) sum += (double)h[16 * c + i];
+      out[i] = sum / G / (double)its / (w.sclock_khz * 1e-3);
+    }
+  }
+  HOEFEM_CUDA(cudaMemset(w.sprof.p, 0, w.sprof.n * sizeof(unsigned long long)));
 }
 
 void cg_stream_arm(CgWork& w, double delta, cudaStream_t s) {
@@ -717,6 +1213,7 @@ void cg_stream_arm(CgWork& w, double delta, cudaStream_t s) {
 }
 
 void cg_stream_iterate(CgWork& w, bool f32, const Precond* P, bool p32, bool reliable, cudaStream_t s) {
+  (void)p32;
   Model& m = *w.m;
   CgStreamOp& L = f32 ? w.sop32 : w.sop64;
   const int G = L.grid;
@@ -726,25 +1223,24 @@ void cg_stream_iterate(CgWork& w, bool f32, const Precond* P, bool p32, bool rel
   a.op_items = L.items.p;
   a.op_item_off = L.item_off.p;
   a.node_range = L.node_range.p;
-  if (P && P->kind == PREC_SCHWARZ) {
-    a.sub_off = P->d_sub_off.p;
-    a.sub_nodes = P->d_sub_nodes.p;
-    a.slot = P->d_npair.p;
+  a.segs = L.segs.p;
+  a.seg_off = L.seg_off.p;
+  a.halo = L.halo.p;
+  if (pk == 2) {
+    a.sw = w.ssw.data.p;
+    a.sw_items = w.ssw.items.p;
+    a.sw_item_off = w.ssw.item_off.p;
+    a.sw_scale = w.ssw.scale.p;
+    a.slot_sub = w.ssw.slot_sub.p;
     a.pair_off = P->d_npair_off.p;
     a.diag_only = P->d_diag_only.p;
     a.pbase = P->d_base.p;
     a.pvals = P->vals.p;
-    a.ysub = P->ysub.p;
-    if (P->nsub > 0) {
-      a.sw = w.ssw.data.p;
-      a.sw_items = w.ssw.items.p;
-      a.sw_item_off = w.ssw.item_off.p;
-      a.sw_scale = w.ssw.scale.p;
-    }
   }
-  if (P && P->kind == PREC_DIAGONAL) a.dinv = P->diag.p;
+  if (pk == 1) a.dinv = P->diag.p;
   a.x = w.x.p;
-  a.r = w.r.p;
+  a.r0 = w.r.p;
+  a.r1 = w.r2.p;
   a.z = w.z.p;
   a.Ap = w.Ap.p;
   a.pb0 = w.p.p;
@@ -754,6 +1250,13 @@ void cg_stream_iterate(CgWork& w, bool f32, const Precond* P, bool p32, bool rel
   a.bar = w.sbar.p;
   a.err = w.serr.p;
   a.reliable = reliable ? 1 : 0;
+  if (w.phase_profile) {
+    if (w.sprof.n < (size_t)(16 * G)) {
+      w.sprof.alloc(16 * G);
+      w.sprof.zero(s);
+    }
+    a.prof = w.sprof.p;
+  }
   HOEFEM_CUDA(cudaMemsetAsync(w.sbar.p, 0, sizeof(unsigned), s));
   HOEFEM_CUDA(cudaMemsetAsync(w.serr.p, 0, 2 * sizeof(int), s));
   HOEFEM_CUDA(cudaEventRecord(w.sev[0], s));
@@ -783,8 +1286,11 @@ void cg_stream_iterate(CgWork& w, bool f32, const Precond* P, bool p32, bool rel
   w.stream_launches += 1;
   w.last_f32 = f32;
   if (herr[0] || herr[1]) throw Error(herr[1] ? herr[1] : HOEFEM_ERR_DEVICE_TIMEOUT, "streamed CG: device wait ran out");
+  // the current direction and residual back into w.p / w.r
   if (w.h_st->pcur == 1)
     HOEFEM_CUDA(cudaMemcpyAsync(w.p.p, w.p2.p, sizeof(double) * m.ndof, cudaMemcpyDeviceToDevice, s));
+  if (w.h_st->rcur == 1)
+    HOEFEM_CUDA(cudaMemcpyAsync(w.r.p, w.r2.p, sizeof(double) * m.ndof, cudaMemcpyDeviceToDevice, s));
 }
 
 }  // namespace hoefem

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <functional>
+#include <vector>
 
 #include "internal.h"
 
@@ -64,23 +65,38 @@ struct CgState {
   // streamed CG: residual-replacement trigger (rr <= delta2 * rr_ref), the
   // flag it raises, and which direction buffer holds the current direction
   double rr_ref, delta2;
-  int replace, pcur;
+  int replace, pcur, rcur, pad;
 };
 
 // One unit of a streamed kernel's work: `bytes` (multiple of 16, at most one
 // ring stage) at byte offset `off` of a stream buffer, plus kind-specific
-// fields (operator tile: a = first node; Schwarz chunk: a = subdomain,
-// b = first row, c = rows).
+// fields (operator tile: a = first node, b = nodes; Schwarz chunk:
+// a = subdomain, b = first row, c = rows) and keep = 1 for items whose copy
+// asks L2 to keep the lines (evict last) rather than stream them.
 struct CgsItem {
   long long off;
   int bytes, a, b, c;
-  int pad[2];
+  int keep, pad;
+};
+
+// A run of a CTA's own nodes [n0, n1) that share one staged halo (`halo_n`
+// nodes listed from `halo_off` of the halo array, sorted; the own nodes are
+// halo entries own_lo ..): its operator tiles are the CTA's items [j0, j1),
+// its Schwarz row items the CTA's Schwarz items [sj0, sj1), covering the
+// subdomain incidences (node-major slots) [q0, q1) of its nodes.
+struct CgsSeg {
+  int j0, j1;
+  int halo_off, halo_n;
+  int n0, n1;
+  int sj0, sj1;
+  int q0, q1;
+  int own_lo, pad;
 };
 
 // Stream layouts of the persistent CG (cg_stream.cu): the operator as tiles
-// of whole node rows (header, neighbour lists, 9 value planes per node) and
-// the Schwarz blocks as row chunks, each split into contiguous per-CTA item
-// ranges balanced by bytes.
+// of whole node rows (header, 16-bit halo-local neighbour indices, 9 value
+// planes per node) and the Schwarz blocks as row chunks, each split into
+// contiguous per-CTA item ranges balanced by bytes and into halo segments.
 struct CgStreamOp {
   int vsize = 0;  // value bytes (8 FP64, 4 FP32); 0 = not built
   int grid = 0;
@@ -89,19 +105,37 @@ struct CgStreamOp {
   DBuf<int> item_off;    // grid + 1
   DBuf<int> node_range;  // grid + 1
   DBuf<long long> val_off;  // per node: byte offset of its value planes
+  DBuf<CgsSeg> segs;
+  DBuf<int> seg_off;  // grid + 1
+  DBuf<int> halo;     // halo node lists of the segments
   long long bytes = 0;      // streamed bytes per apply
+  std::vector<CgsItem> h_items;  // host copies (L2 keep flags)
+  std::vector<int> h_item_off;
+  std::vector<CgsSeg> h_segs;  // host copies (the Schwarz layout follows the segments)
+  std::vector<int> h_seg_off, h_halo;
+  long long keep_applied = -1;
+  const void* seg_for = nullptr;  // the preconditioner whose incidences bound the segments
 };
+// Schwarz blocks distributed by rows: every subdomain incidence (subdomain
+// s, its local node I; node-major slot order) is a record of the block's rows
+// 3I .. 3I + 2 plus the halo-local indices of the subdomain's nodes, stored
+// with the operator segment that owns the node.
 struct CgStreamSchwarz {
   int vsize = 0;  // 8, 4 or 2 (FP16 with a per-subdomain scale)
   int grid = 0;
   const void* built_for = nullptr;
+  const void* op_for = nullptr;  // the operator layout whose segments it follows
   DBuf<unsigned char> data;
   DBuf<CgsItem> items;
   DBuf<int> item_off;
-  DBuf<long long> chunk_base;  // per subdomain: byte offset of its first chunk
-  DBuf<int> rows_per_chunk;    // per subdomain
-  DBuf<double> scale;          // per subdomain (FP16 only)
+  DBuf<long long> rec_val_off;  // per slot: byte offset of its 3 rows
+  DBuf<int> slot_sub;           // per slot: subdomain
+  DBuf<int> slot_local;         // per slot: local node index in the subdomain
+  DBuf<double> scale;           // per subdomain (FP16 only)
   long long bytes = 0;
+  std::vector<CgsItem> h_items;
+  std::vector<int> h_item_off;
+  long long keep_applied = -1;
 };
 
 struct CgWork {
@@ -138,13 +172,22 @@ struct CgWork {
   bool schwarz_half = false;
   CgStreamOp sop64, sop32;
   CgStreamSchwarz ssw;
-  DBuf<double> p2, spart;
+  DBuf<double> p2, r2, spart;
   DBuf<unsigned> sbar;
   DBuf<int> serr;
   long long stream_launches = 0, stream_iterations = 0;
   float stream_ms = 0.f;         // device time of the persistent launches (last solve)
   double stream_ms_total = 0.0;  // summed over solves until reset by the caller
   bool last_f32 = false;         // precision of the last streamed solve
+  bool phase_profile = false;    // per-phase cycle counters in the streamed CG
+  // L2 residency budget of the streamed CG (bytes over all CTAs; -1: default,
+  // a share of the device's L2): that many bytes of each iteration's stream,
+  // the Schwarz chunks first, are copied with an evict-last policy so that
+  // they are still in L2 in the next iteration, the rest evict-first
+  long long l2_keep = -1;
+  long long l2_keep_applied = -2;
+  DBuf<unsigned long long> sprof;  // grid x 16 counters (cycles), summed over launches
+  double sclock_khz = 0.0;
   cudaEvent_t sev[2] = {nullptr, nullptr};
   // called on the host after every chunk of iterations (solver state synced)
   std::function<void(cudaStream_t)> on_chunk;
@@ -168,8 +211,12 @@ void to_f32(const double* a, float* b, long long n, cudaStream_t s);
 // an error outcome, the iteration limit or a residual-replacement trigger,
 // and leaves the current direction in w.p.
 bool cg_stream_usable(CgWork& w, const Precond* P);
-void cg_stream_prepare(CgWork& w, const double* A64, bool f32, const Precond* P, bool p32, cudaStream_t s);
+// (false: the layouts do not fit the kernel's stages or halos)
+bool cg_stream_prepare(CgWork& w, const double* A64, bool f32, const Precond* P, bool p32, cudaStream_t s);
 void cg_stream_iterate(CgWork& w, bool f32, const Precond* P, bool p32, bool reliable, cudaStream_t s);
+// Per-phase microseconds per iteration of the streamed CG since the last
+// reset (zeros without HOEFEM_CG_PHASE_PROFILE); resets the counters.
+void cg_stream_phase_us(CgWork& w, double* out12);
 // Sets the residual-replacement reference rr_ref = rr (current state) and
 // delta^2, clears the replacement flag.
 void cg_stream_arm(CgWork& w, double delta, cudaStream_t s);

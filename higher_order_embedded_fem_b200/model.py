@@ -79,16 +79,23 @@ class _Model:
         """8 / 16 / 32 lanes per node, +100 for the column-streaming traversal."""
         check(lib().hoefem_model_set_spmv_variant(self._h, int(variant)))
 
-    def set_cg_engine(self, engine="auto", schwarz_fp16=False):
+    def set_cg_engine(self, engine="auto", schwarz_fp16=False, phase_profile=False):
         """CG engine of ConjugateGradient solves on this model ("auto",
         "chunked", "streamed"; see hoefem_model_set_cg_engine)."""
-        check(lib().hoefem_model_set_cg_engine(self._h, _capi.CG_ENGINE[engine], 1 if schwarz_fp16 else 0))
+        check(lib().hoefem_model_set_cg_engine(self._h, _capi.CG_ENGINE[engine],
+                                                         (1 if schwarz_fp16 else 0) | (2 if phase_profile else 0)))
+
+    def set_cg_l2_keep(self, nbytes=-1):
+        """L2 residency budget (bytes) of the streamed CG; -1: 60 percent of L2."""
+        check(lib().hoefem_model_set_cg_l2_keep(self._h, int(nbytes)))
 
     def cg_engine_stats(self):
         """Streamed-CG counters of the last ConjugateGradient solve."""
         s = _capi.CgEngineStats()
         check(lib().hoefem_model_cg_engine_stats(self._h, C.byref(s)))
-        return {f: getattr(s, f) for f, _ in s._fields_}
+        out = {f: getattr(s, f) for f, _ in s._fields_}
+        out["phase_us"] = list(out["phase_us"])
+        return out
 
     def set_stream(self, stream):
         """Run this model's work on a CUDA stream handle (int), None: own stream."""

@@ -251,19 +251,26 @@ class NewtonCgIntegrator3d:
         hoefem_integrator_set_precision)."""
         check(lib().hoefem_integrator_set_precision(self._h, 1 if mixed else 0, float(delta)))
 
-    def set_cg_engine(self, engine="auto", schwarz_fp16=False):
+    def set_cg_engine(self, engine="auto", schwarz_fp16=False, phase_profile=False):
         """CG engine of the Jacobian solves: "auto" (persistent streamed CG
         where possible), "chunked" (CUDA graphs of kernel chunks) or
         "streamed" (error if it cannot run); schwarz_fp16 keeps the Schwarz
         blocks of the mixed form in scaled FP16 (hoefem_integrator_set_cg_engine)."""
-        check(lib().hoefem_integrator_set_cg_engine(self._h, _capi.CG_ENGINE[engine], 1 if schwarz_fp16 else 0))
+        check(lib().hoefem_integrator_set_cg_engine(self._h, _capi.CG_ENGINE[engine],
+                                                         (1 if schwarz_fp16 else 0) | (2 if phase_profile else 0)))
+
+    def set_cg_l2_keep(self, nbytes=-1):
+        """L2 residency budget (bytes) of the streamed CG; -1: 60 percent of L2."""
+        check(lib().hoefem_integrator_set_cg_l2_keep(self._h, int(nbytes)))
 
     def cg_engine_stats(self):
         """Streamed-CG counters of the last step: launches, iterations, device
         ms and the bytes one iteration streams."""
         s = _capi.CgEngineStats()
         check(lib().hoefem_integrator_cg_engine_stats(self._h, C.byref(s)))
-        return {f: getattr(s, f) for f, _ in s._fields_}
+        out = {f: getattr(s, f) for f, _ in s._fields_}
+        out["phase_us"] = list(out["phase_us"])
+        return out
 
     def step(self, u, v, t, dt):
         """Advances (u, v) in place by dt; returns the step statistics."""
