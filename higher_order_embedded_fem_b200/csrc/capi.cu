@@ -716,6 +716,10 @@ static void engine_stats(CgWork& w, const Precond* P, hoefem_cg_engine_stats* ou
   out->operator_bytes = w.sop32.vsize && w.last_f32 ? w.sop32.bytes : w.sop64.bytes;
   out->schwarz_bytes = (P && P->kind == PREC_SCHWARZ) ? w.ssw.bytes : 0;
   cg_stream_phase_us(w, out->phase_us);
+  const CgWork::EngineTune& et = w.etune[w.last_tune];
+  out->auto_us_per_iteration[0] = et.us_per_it[0];
+  out->auto_us_per_iteration[1] = et.us_per_it[1];
+  out->auto_choice = et.choice;
 }
 
 int hoefem_integrator_set_cg_engine(hoefem_integrator it, int engine, int options) {

@@ -355,6 +355,8 @@ CgWork::~CgWork() {
   for (auto& g : graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   if (h_st) cudaFreeHost(h_st);
+  for (auto* e : {&tev[0], &tev[1], &sev[0], &sev[1]})
+    if (*e) cudaEventDestroy(*e);
   for (auto& t : tuning) {
     if (t.e0) cudaEventDestroy(t.e0);
     if (t.e1) cudaEventDestroy(t.e1);
@@ -553,10 +555,35 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   // persistent streamed CG: the operator (FP64 values, FP32 in the mixed
   // form) and the Schwarz blocks packed into their stream layouts, then one
   // launch per residual replacement
-  const bool streamed = vals64 && cg_stream_usable(w, P) && cg_stream_prepare(w, vals64, f32, P, p32, s);
+  const int pk = !P ? 0 : (P->kind == PREC_DIAGONAL ? 1 : 2);
+  CgWork::EngineTune& et = w.etune[(f32 ? 3 : 0) + pk];
+  w.last_tune = (f32 ? 3 : 0) + pk;
+  bool want_stream = w.stream_mode == 2;
+  if (w.stream_mode == 0) want_stream = et.choice >= 0 ? et.choice == 1 : et.phase == 1;
+  const bool streamed =
+      want_stream && vals64 && cg_stream_usable(w, P) && cg_stream_prepare(w, vals64, f32, P, p32, s);
   HOEFEM_REQUIRE(streamed || w.stream_mode != 2, HOEFEM_ERR_INVALID_ARGUMENT,
                  "the streamed CG cannot run this solve (preconditioner, device or layout)");
+  if (w.stream_mode == 0 && want_stream && !streamed) et.choice = 0;  // cannot stream: chunked from now on
+  if (!w.tev[0]) {
+    HOEFEM_CUDA(cudaEventCreate(&w.tev[0]));
+    HOEFEM_CUDA(cudaEventCreate(&w.tev[1]));
+  }
+  // automatic engine choice: one timed sample per engine (iteration loop only)
+  const i64 it_start = w.h_st->iters;
+  auto sample = [&](int engine) {
+    if (w.stream_mode != 0 || et.choice >= 0 || et.phase != engine) return;
+    HOEFEM_CUDA(cudaEventRecord(w.tev[1], s));
+    HOEFEM_CUDA(cudaEventSynchronize(w.tev[1]));
+    const i64 n_it = w.h_st->iters - it_start;
+    if (n_it < 20) return;
+    float ms = 0.f;
+    HOEFEM_CUDA(cudaEventElapsedTime(&ms, w.tev[0], w.tev[1]));
+    et.us_per_it[engine] = 1e3 * ms / (double)n_it;
+    if (++et.phase == 2) et.choice = et.us_per_it[1] < et.us_per_it[0] ? 1 : 0;
+  };
   if (streamed) {
+    HOEFEM_CUDA(cudaEventRecord(w.tev[0], s));
     cg_stream_arm(w, A64 ? delta : 0.0, s);
     w.stream_ms = 0.f;
     const i64 cap_s = max_iter >= 0 ? max_iter : 10 * (i64)n;
@@ -588,6 +615,7 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
         return HOEFEM_CG_MAX_ITERATIONS;
       }
     }
+    sample(1);
     if (replacements) *replacements = nrep_s;
     *iters = w.h_st->iters;
     return w.h_st->status;
@@ -617,6 +645,9 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   const i64 cap = max_iter >= 0 ? max_iter : 10 * (i64)n;
   const i64 max_chunks = (cap + w.chunk - 1) / w.chunk + 2;
   double rr_ref = w.h_st->rr;
+  // the engine sample of this solve counts only if the SpMV variants were already tuned
+  const bool sample_chunked = tu.done;
+  HOEFEM_CUDA(cudaEventRecord(w.tev[0], s));
   i64 nrep = 0;
   for (i64 c = 0; c < max_chunks; ++c) {
     const i64 it0 = w.h_st->iters;
@@ -661,6 +692,7 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
     if (w.on_chunk && !w.h_st->done) w.on_chunk(s);
     if (w.h_st->done) break;
   }
+  if (sample_chunked) sample(0);
   if (replacements) *replacements = nrep;
   *iters = w.h_st->iters;
   if (!w.h_st->done) return HOEFEM_CG_MAX_ITERATIONS;

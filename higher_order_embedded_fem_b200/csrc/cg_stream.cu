@@ -68,8 +68,9 @@ constexpr int NS = 12;                  // ring stages
 constexpr int STAGE = 14336;            // bytes per stage (and per work item)
 constexpr int THREADS = 32 * (NW + 1);  // + the producer warp (the last one)
 constexpr int CONSUMERS = 32 * NW;
-// item headers: int records, int first node / slot, 2 x pad; then per record
-// an int4 (record offset, degree or block dimension, own halo index or slot, 0)
+// item headers: int records, int first record, 2 x pad; then per record an
+// int4: operator tiles (record offset, degree, 3 x own halo index, node),
+// Schwarz items (record offset, block dimension, slot, 0)
 constexpr int ITEM_HDR = 16;
 constexpr int MAX_DIM = 81;      // Schwarz block dimension bound (3 x 27 nodes)
 constexpr int HALO_MAX = 1280;   // halo nodes of one segment
@@ -314,13 +315,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
   const long long max_iter = st->max_iter;
   int status = HOEFEM_OK, done = 0, replace = 0, pcur = 0, rcur = 0;
   long long it = 0;
-  // a lane's Schwarz columns j = lane + 32 p: record node j / 3, component j % 3
-  int jn[3], jc[3];
-#pragma unroll
-  for (int p = 0; p < 3; ++p) {
-    jn[p] = (lane + 32 * p) / 3;
-    jc[p] = (lane + 32 * p) % 3;
-  }
+  const int grp = lane >> 3, gl = lane & 7;  // operator tiles: node group and its lane
   auto fail = [&]() {
     s_fail = 1;
     atomicExch(&A.err[0], 1);
@@ -361,62 +356,38 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
         tock(2, tw);
         const unsigned char* t = ring + (size_t)s * STAGE;
         const int nn = *(const int*)t;
-        const int a0 = *(const int*)(t + 4);
-        // two node rows at a time: their loads and reductions interleave
-        for (int q = 0; q < nn; q += 2) {
-          const bool two = q + 1 < nn;
-          const int4 h0 = *(const int4*)(t + ITEM_HDR + 16 * q);
-          const int4 h1 = two ? *(const int4*)(t + ITEM_HDR + 16 * (q + 1)) : make_int4(0, 0, 0, 0);
-          const unsigned short* loc0 = (const unsigned short*)(t + h0.x);
-          const unsigned short* loc1 = (const unsigned short*)(t + h1.x);
-          const VA* v0 = (const VA*)(t + h0.x + align16(2LL * h0.y));
-          const VA* v1 = (const VA*)(t + h1.x + align16(2LL * h1.y));
-          const int d0 = h0.y, d1 = h1.y;
-          double a00 = 0.0, a01 = 0.0, a02 = 0.0, a10 = 0.0, a11 = 0.0, a12 = 0.0;
-          const int dm = max(d0, d1);
-          for (int e = lane; e < dm; e += 32) {
-            if (e < d0) {
-              const double* pd = s_halo + loc0[e];
-              const double q0 = pd[0], q1 = pd[1], q2 = pd[2];
-              a00 += ldv(v0 + e) * q0 + ldv(v0 + d0 + e) * q1 + ldv(v0 + 2 * d0 + e) * q2;
-              a01 += ldv(v0 + 3 * d0 + e) * q0 + ldv(v0 + 4 * d0 + e) * q1 + ldv(v0 + 5 * d0 + e) * q2;
-              a02 += ldv(v0 + 6 * d0 + e) * q0 + ldv(v0 + 7 * d0 + e) * q1 + ldv(v0 + 8 * d0 + e) * q2;
-            }
-            if (e < d1) {
-              const double* pd = s_halo + loc1[e];
-              const double q0 = pd[0], q1 = pd[1], q2 = pd[2];
-              a10 += ldv(v1 + e) * q0 + ldv(v1 + d1 + e) * q1 + ldv(v1 + 2 * d1 + e) * q2;
-              a11 += ldv(v1 + 3 * d1 + e) * q0 + ldv(v1 + 4 * d1 + e) * q1 + ldv(v1 + 5 * d1 + e) * q2;
-              a12 += ldv(v1 + 6 * d1 + e) * q0 + ldv(v1 + 7 * d1 + e) * q1 + ldv(v1 + 8 * d1 + e) * q2;
-            }
+        // four node rows per pass, 8 lanes each (records sorted by degree, so
+        // the four have similar lengths); 3-level reductions per group
+        for (int q0 = 0; q0 < nn; q0 += 4) {
+          const int q = q0 + grp;
+          const bool has = q < nn;
+          const int4 h = has ? *(const int4*)(t + ITEM_HDR + 16 * q) : make_int4(0, 0, 0, 0);
+          const int d = h.y;
+          const unsigned short* loc = (const unsigned short*)(t + h.x);
+          const VA* v = (const VA*)(t + h.x + align16(2LL * d));
+          double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+          for (int e = gl; e < d; e += 8) {
+            const double* pd = s_halo + loc[e];
+            const double q0v = pd[0], q1v = pd[1], q2v = pd[2];
+            s0 += ldv(v + e) * q0v + ldv(v + d + e) * q1v + ldv(v + 2 * d + e) * q2v;
+            s1 += ldv(v + 3 * d + e) * q0v + ldv(v + 4 * d + e) * q1v + ldv(v + 5 * d + e) * q2v;
+            s2 += ldv(v + 6 * d + e) * q0v + ldv(v + 7 * d + e) * q1v + ldv(v + 8 * d + e) * q2v;
           }
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            a00 += __shfl_xor_sync(0xffffffffu, a00, o);
-            a01 += __shfl_xor_sync(0xffffffffu, a01, o);
-            a02 += __shfl_xor_sync(0xffffffffu, a02, o);
-            a10 += __shfl_xor_sync(0xffffffffu, a10, o);
-            a11 += __shfl_xor_sync(0xffffffffu, a11, o);
-            a12 += __shfl_xor_sync(0xffffffffu, a12, o);
+          for (int o = 4; o > 0; o >>= 1) {
+            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
           }
-          if (lane == 0) {
-            const int a3 = 3 * (a0 + q);
-            const double* pa = s_halo + h0.z;
-            A.Ap[a3] = a00;
-            A.Ap[a3 + 1] = a01;
-            A.Ap[a3 + 2] = a02;
-            acc += pa[0] * a00;
-            acc += pa[1] * a01;
-            acc += pa[2] * a02;
-            if (two) {
-              const double* pb = s_halo + h1.z;
-              A.Ap[a3 + 3] = a10;
-              A.Ap[a3 + 4] = a11;
-              A.Ap[a3 + 5] = a12;
-              acc += pb[0] * a10;
-              acc += pb[1] * a11;
-              acc += pb[2] * a12;
-            }
+          if (has && gl == 0) {
+            const int a3 = 3 * h.w;
+            const double* pa = s_halo + h.z;
+            A.Ap[a3] = s0;
+            A.Ap[a3 + 1] = s1;
+            A.Ap[a3 + 2] = s2;
+            acc += pa[0] * s0;
+            acc += pa[1] * s1;
+            acc += pa[2] * s2;
           }
         }
         __syncwarp();
@@ -425,6 +396,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
       tock(1, t0);
     }
     unsigned long long tb = tick();
+    acc = warp_sum(acc);
     if (lane == 0) s_red[w][0] = acc;
     pipe::named_sync(1, CONSUMERS);
     if (threadIdx.x == 0) {
@@ -473,32 +445,22 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
           tock(6, tw);
           const unsigned char* t = ring + (size_t)s * STAGE;
           const int nr = *(const int*)t;
-          for (int q = 0; q < nr; ++q) {
+          // one block row per lane: row i of record q is sum_m B[i][3m + c] r'(node m, c)
+          for (int rho = lane; rho < 3 * nr; rho += 32) {
+            const int q = rho / 3, i = rho - 3 * q;
             const int4 h = *(const int4*)(t + ITEM_HDR + 16 * q);
-            const int dim = h.y;
+            const int dim = h.y, ns = dim / 3;
             const unsigned short* cols = (const unsigned short*)(t + h.x);
-            const VB* v = (const VB*)(t + h.x + align16(2LL * (dim / 3)));
-            double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-#pragma unroll
-            for (int p = 0; p < 3; ++p) {
-              const int j2 = lane + 32 * p;
-              if (j2 < dim) {
-                const double rv = s_halo[cols[jn[p]] + jc[p]];
-                y0 += ldv(v + j2) * rv;
-                y1 += ldv(v + dim + j2) * rv;
-                y2 += ldv(v + 2 * dim + j2) * rv;
-              }
+            const VB* v = (const VB*)(t + h.x + align16(2LL * ns)) + (size_t)i * dim;
+            double b0 = 0.0, b1 = 0.0, b2 = 0.0;
+            for (int m = 0; m < ns; ++m) {
+              const double* hr = s_halo + cols[m];
+              b0 += ldv(v + 3 * m) * hr[0];
+              b1 += ldv(v + 3 * m + 1) * hr[1];
+              b2 += ldv(v + 3 * m + 2) * hr[2];
             }
-            y0 = warp_sum(y0);
-            y1 = warp_sum(y1);
-            y2 = warp_sum(y2);
-            if (lane == 0) {
-              const double sc = sizeof(VB) == 2 ? A.sw_scale[__ldg(A.slot_sub + h.z)] : 1.0;
-              double* zp = s_zp + 3 * (h.z - S.q0);
-              zp[0] = y0 * sc;
-              zp[1] = y1 * sc;
-              zp[2] = y2 * sc;
-            }
+            const double sc = sizeof(VB) == 2 ? A.sw_scale[__ldg(A.slot_sub + h.z)] : 1.0;
+            s_zp[3 * (h.z - S.q0) + i] = ((b0 + b1) + b2) * sc;
           }
           __syncwarp();
           if (lane == 0) pipe::mbar_arrive(&empty[s]);
@@ -625,14 +587,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
 
 // ---- stream layouts -----------------------------------------------------------
 
-// Item headers and 16-bit halo-local index lists (once per layout): for an
-// operator tile the neighbour lists, for a Schwarz row item the subdomain node
-// lists.  Record r of an item (global record first + r) starts at
-// idx_off[first + r]; its header holds (offset in the item, field_y, field_z).
-__global__ void k_item_layout(int nitems, const CgsItem* __restrict__ items, const long long* __restrict__ idx_off,
-                              const int* __restrict__ nidx_off, const unsigned short* __restrict__ idx,
-                              const int* __restrict__ field_y, const int* __restrict__ field_z,
-                              unsigned char* __restrict__ data) {
+// Item headers and 16-bit halo-local index lists (once per layout).  The
+// records are numbered in stream order; record r of item (first = item.a)
+// is first + r: its index list (rec_count[.] entries from idx[rec_src[.]])
+// goes to rec_idx_off[.] and its header is (offset in the item, fy, fz, fw).
+__global__ void k_item_layout(int nitems, const CgsItem* __restrict__ items, const long long* __restrict__ rec_idx_off,
+                              const int* __restrict__ rec_src, const int* __restrict__ rec_count,
+                              const unsigned short* __restrict__ idx, const int* __restrict__ fy,
+                              const int* __restrict__ fz, const int* __restrict__ fw, unsigned char* __restrict__ data) {
   const int item = blockIdx.x;
   if (item >= nitems) return;
   const CgsItem it = items[item];
@@ -645,11 +607,12 @@ __global__ void k_item_layout(int nitems, const CgsItem* __restrict__ items, con
     ((int*)t)[3] = 0;
   }
   for (int q = threadIdx.x; q < nr; q += blockDim.x)
-    ((int4*)(t + ITEM_HDR))[q] = make_int4((int)(idx_off[first + q] - it.off), field_y[first + q], field_z[first + q], 0);
+    ((int4*)(t + ITEM_HDR))[q] =
+        make_int4((int)(rec_idx_off[first + q] - it.off), fy[first + q], fz[first + q], fw[first + q]);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
   for (int q = warp; q < nr; q += nwarp) {
-    const int o = nidx_off[first + q], n = nidx_off[first + q + 1] - o;
-    unsigned short* dst = (unsigned short*)(data + idx_off[first + q]);
+    const int o = rec_src[first + q], n = rec_count[first + q];
+    unsigned short* dst = (unsigned short*)(data + rec_idx_off[first + q]);
     for (int e = lane; e < n; e += 32) dst[e] = idx[o + e];
   }
 }
@@ -818,7 +781,7 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
   // tiles: runs of nodes within a stage and a halo
   std::vector<CgsItem> items;
   std::vector<long long> val_off(nv), idx_off(nv);
-  std::vector<int> stamp(nv, -1);
+  std::vector<int> stamp(nv, -1), rec_node;
   long long pos = 0;
   i64 a = 0;
   int tile_id = 0;
@@ -844,16 +807,26 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
     }
     if (b == a) return false;  // one node row exceeds a stage or a halo
     const long long hdr = align16(ITEM_HDR + 16 * (b - a));
-    for (i64 q = a; q < b; ++q) {
+    // records in order of decreasing degree (groups of four similar rows)
+    std::vector<i64> order;
+    for (i64 q = a; q < b; ++q) order.push_back(q);
+    std::stable_sort(order.begin(), order.end(), [&](i64 x, i64 y) {
+      return m.adj_off[x + 1] - m.adj_off[x] > m.adj_off[y + 1] - m.adj_off[y];
+    });
+    long long o = start + hdr;
+    for (i64 q : order) {
       const long long d = m.adj_off[q + 1] - m.adj_off[q];
-      idx_off[q] = start + hdr + rec_rel[q - a];
+      idx_off[q] = o;
       val_off[q] = idx_off[q] + align16(2 * d);
+      o += rec_bytes(q);
+      rec_node.push_back((int)q);
     }
     CgsItem it{};
     it.off = start;
     it.bytes = (int)(hdr + recs);
-    it.a = (int)a;
+    it.a = (int)(rec_node.size() - order.size());  // first record (stream order)
     it.b = (int)(b - a);
+    it.c = (int)a;  // first node
     items.push_back(it);
     pos = start + hdr + recs;
     a = b;
@@ -861,7 +834,7 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
   }
   std::vector<int> off, nrange(G + 1);
   split_items(items, G, off);
-  for (int g = 0; g <= G; ++g) nrange[g] = off[g] < (int)items.size() ? items[off[g]].a : (int)nv;
+  for (int g = 0; g <= G; ++g) nrange[g] = off[g] < (int)items.size() ? items[off[g]].c : (int)nv;
   // segments: halo-local neighbour indices (sorted halo, times 3), own halo index
   std::vector<CgsSeg> segs;
   std::vector<int> seg_off(G + 1, 0), halo;
@@ -879,7 +852,7 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
       while (j1 < off[g + 1]) {
         const CgsItem& it = items[j1];
         int add = 0, tinc = 0;
-        for (i64 q = it.a; q < it.a + it.b; ++q) {
+        for (i64 q = it.c; q < it.c + it.b; ++q) {
           tinc += incid(q);
           for (int e = m.adj_off[q]; e < m.adj_off[q + 1]; ++e)
             if (stamp[m.adj[e]] != seg_id) {
@@ -906,14 +879,14 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
       S.j1 = j1 - off[g];
       S.halo_off = (int)halo.size();
       S.halo_n = (int)hs.size();
-      S.n0 = items[j].a;
-      S.n1 = items[j1 - 1].a + items[j1 - 1].b;
+      S.n0 = items[j].c;
+      S.n1 = items[j1 - 1].c + items[j1 - 1].b;
       S.own_lo = local[S.n0];
       S.q0 = sw ? pair_off[S.n0] : 0;
       S.q1 = sw ? pair_off[S.n1] : 0;
       halo.insert(halo.end(), hs.begin(), hs.end());
       for (int t = j; t < j1; ++t)
-        for (i64 q = items[t].a; q < items[t].a + items[t].b; ++q) {
+        for (i64 q = items[t].c; q < items[t].c + items[t].b; ++q) {
           for (int e = m.adj_off[q]; e < m.adj_off[q + 1]; ++e)
             loc_adj[e] = (unsigned short)(3 * local[m.adj[e]]);
           self_loc[q] = 3 * local[q];  // every node is its own neighbour (diagonal block)
@@ -939,18 +912,31 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
   L.segs.upload(segs, s);
   L.seg_off.upload(seg_off, s);
   L.halo.upload(halo, s);
+  // per record (stream order): its node's list and header fields
+  std::vector<long long> r_idx_off(nv);
+  std::vector<int> r_src(nv), r_cnt(nv), r_y(nv), r_z(nv);
+  for (i64 r = 0; r < nv; ++r) {
+    const int q = rec_node[r];
+    r_idx_off[r] = idx_off[q];
+    r_src[r] = m.adj_off[q];
+    r_cnt[r] = deg[q];
+    r_y[r] = deg[q];
+    r_z[r] = self_loc[q];
+  }
   DBuf<unsigned short> d_loc;
-  DBuf<int> d_self, d_deg;
+  DBuf<int> d_src, d_cnt, d_y, d_z, d_w;
   DBuf<long long> d_idx_off;
   d_loc.upload(loc_adj, s);
-  d_self.upload(self_loc, s);
-  d_deg.upload(deg, s);
-  d_idx_off.upload(idx_off, s);
+  d_src.upload(r_src, s);
+  d_cnt.upload(r_cnt, s);
+  d_y.upload(r_y, s);
+  d_z.upload(r_z, s);
+  d_w.upload(rec_node, s);
+  d_idx_off.upload(r_idx_off, s);
   L.bytes = pos;
   L.grid = G;
-  (note_launch(), k_item_layout<<<(int)items.size(), 256, 0, s>>>((int)items.size(), L.items.p, d_idx_off.p,
-                                                                    m.d_adj_off.p, d_loc.p, d_deg.p, d_self.p,
-                                                                    L.data.p));
+  (note_launch(), k_item_layout<<<(int)items.size(), 256, 0, s>>>((int)items.size(), L.items.p, d_idx_off.p, d_src.p,
+                                                                    d_cnt.p, d_loc.p, d_y.p, d_z.p, d_w.p, L.data.p));
   HOEFEM_CUDA(cudaGetLastError());
   HOEFEM_CUDA(cudaStreamSynchronize(s));
   L.vsize = vsize;
@@ -1029,18 +1015,22 @@ bool build_sw_layout(CgStreamSchwarz& S, const Precond& P, CgStreamOp& L, int vs
   // the segments now carry their Schwarz item ranges
   L.h_segs = segs;
   L.segs.upload(segs, s);
+  std::vector<int> ncols(nslot), zeros(nslot, 0);
+  for (i64 q = 0; q < nslot; ++q) ncols[q] = cols_off[q + 1] - cols_off[q];
   DBuf<unsigned short> d_cols;
-  DBuf<int> d_cols_off, d_dims, d_slot;
+  DBuf<int> d_cols_off, d_ncols, d_dims, d_slot, d_zero;
   DBuf<long long> d_rec_off;
   d_cols.upload(cols, s);
   d_cols_off.upload(cols_off, s);
+  d_ncols.upload(ncols, s);
   d_dims.upload(dims, s);
   d_slot.upload(slot_id, s);
+  d_zero.upload(zeros, s);
   d_rec_off.upload(rec_off, s);
   if (!items.empty())
     (note_launch(), k_item_layout<<<(int)items.size(), 256, 0, s>>>((int)items.size(), S.items.p, d_rec_off.p,
-                                                                      d_cols_off.p, d_cols.p, d_dims.p, d_slot.p,
-                                                                      S.data.p));
+                                                                      d_cols_off.p, d_ncols.p, d_cols.p, d_dims.p,
+                                                                      d_slot.p, d_zero.p, S.data.p));
   HOEFEM_CUDA(cudaGetLastError());
   HOEFEM_CUDA(cudaStreamSynchronize(s));
   S.bytes = pos;
@@ -1105,7 +1095,7 @@ void launch_engine(const Args& args, int G, cudaStream_t s) {
 }  // namespace
 
 bool cg_stream_usable(CgWork& w, const Precond* P) {
-  if (w.stream_mode != 2 || w.on_chunk) return false;
+  if (w.stream_mode == 1 || w.on_chunk) return false;
   int dev = 0, coop = 0;
   HOEFEM_CUDA(cudaGetDevice(&dev));
   HOEFEM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));

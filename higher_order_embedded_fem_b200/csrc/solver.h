@@ -170,6 +170,18 @@ struct CgWork {
   // the mixed-precision Schwarz blocks in FP16 with a per-subdomain scale.
   int stream_mode = 0;
   bool schwarz_half = false;
+  // automatic engine choice per (operator precision, preconditioner kind):
+  // the first solves with at least 20 iterations are timed on the chunked
+  // engine (once its SpMV variants are tuned), then on the streamed one; the
+  // faster per-iteration time decides for the later solves
+  struct EngineTune {
+    int phase = 0;  // 0: sample chunked, 1: sample streamed, 2: decided
+    double us_per_it[2] = {0.0, 0.0};
+    int choice = -1;  // 0 chunked, 1 streamed
+  };
+  EngineTune etune[6];
+  int last_tune = 0;  // entry of the last solve
+  cudaEvent_t tev[2] = {nullptr, nullptr};
   CgStreamOp sop64, sop32;
   CgStreamSchwarz ssw;
   DBuf<double> p2, r2, spart;

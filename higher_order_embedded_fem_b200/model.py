@@ -86,7 +86,7 @@ class _Model:
                                                          (1 if schwarz_fp16 else 0) | (2 if phase_profile else 0)))
 
     def set_cg_l2_keep(self, nbytes=-1):
-        """L2 residency budget (bytes) of the streamed CG; -1: 60 percent of L2."""
+        """L2 residency budget (bytes) of the streamed CG; -1: the default (0)."""
         check(lib().hoefem_model_set_cg_l2_keep(self._h, int(nbytes)))
 
     def cg_engine_stats(self):
@@ -95,6 +95,7 @@ class _Model:
         check(lib().hoefem_model_cg_engine_stats(self._h, C.byref(s)))
         out = {f: getattr(s, f) for f, _ in s._fields_}
         out["phase_us"] = list(out["phase_us"])
+        out["auto_us_per_iteration"] = list(out["auto_us_per_iteration"])
         return out
 
     def set_stream(self, stream):

@@ -252,15 +252,16 @@ class NewtonCgIntegrator3d:
         check(lib().hoefem_integrator_set_precision(self._h, 1 if mixed else 0, float(delta)))
 
     def set_cg_engine(self, engine="auto", schwarz_fp16=False, phase_profile=False):
-        """CG engine of the Jacobian solves: "auto" (persistent streamed CG
-        where possible), "chunked" (CUDA graphs of kernel chunks) or
-        "streamed" (error if it cannot run); schwarz_fp16 keeps the Schwarz
-        blocks of the mixed form in scaled FP16 (hoefem_integrator_set_cg_engine)."""
+        """CG engine of the Jacobian solves: "auto" (the faster engine, timed
+        on the first solves), "chunked" (CUDA graphs of kernel chunks) or
+        "streamed" (persistent streamed CG; error if it cannot run);
+        schwarz_fp16 keeps the Schwarz blocks of the mixed form in scaled FP16;
+        phase_profile records per-phase times (hoefem_integrator_set_cg_engine)."""
         check(lib().hoefem_integrator_set_cg_engine(self._h, _capi.CG_ENGINE[engine],
                                                          (1 if schwarz_fp16 else 0) | (2 if phase_profile else 0)))
 
     def set_cg_l2_keep(self, nbytes=-1):
-        """L2 residency budget (bytes) of the streamed CG; -1: 60 percent of L2."""
+        """L2 residency budget (bytes) of the streamed CG; -1: the default (0)."""
         check(lib().hoefem_integrator_set_cg_l2_keep(self._h, int(nbytes)))
 
     def cg_engine_stats(self):
@@ -270,6 +271,7 @@ class NewtonCgIntegrator3d:
         check(lib().hoefem_integrator_cg_engine_stats(self._h, C.byref(s)))
         out = {f: getattr(s, f) for f, _ in s._fields_}
         out["phase_us"] = list(out["phase_us"])
+        out["auto_us_per_iteration"] = list(out["auto_us_per_iteration"])
         return out
 
     def step(self, u, v, t, dt):

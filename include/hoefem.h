@@ -329,13 +329,15 @@ typedef enum { HOEFEM_PRECISION_FP64 = 0, HOEFEM_PRECISION_MIXED = 1 } hoefem_pr
 int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double delta);
 /* CG engine of the integrator's Jacobian solves and of hoefem_cg_solve /
    hoefem_cg_solve_mixed on a model (no counterpart in the reference, whose CG
-   is one host loop).  HOEFEM_CG_ENGINE_AUTO (default): the persistent
-   streamed CG (one cooperative launch per solve, the operator and the Schwarz
-   blocks streamed through shared memory) whenever the device and the
-   preconditioner allow it (no preconditioner, diagonal, or Schwarz with
-   subdomains of at most 27 nodes), else CUDA graphs of kernel chunks;
-   HOEFEM_CG_ENGINE_CHUNKED: always the graphs; HOEFEM_CG_ENGINE_STREAMED:
-   the streamed CG or HOEFEM_ERR_INVALID_ARGUMENT.  options (bit mask):
+   is one host loop).  Two engines run the same recurrence: CUDA graphs of
+   kernel chunks, and the persistent streamed CG (one cooperative launch per
+   solve, the operator and the Schwarz blocks streamed through shared memory;
+   for no preconditioner, diagonal, or Schwarz with subdomains of at most 27
+   nodes).  HOEFEM_CG_ENGINE_AUTO (default): the first solves with at least
+   20 iterations are timed on each engine, per operator precision and
+   preconditioner kind, and the faster one is kept; HOEFEM_CG_ENGINE_CHUNKED:
+   always the graphs; HOEFEM_CG_ENGINE_STREAMED: the streamed CG or
+   HOEFEM_ERR_INVALID_ARGUMENT.  options (bit mask):
    HOEFEM_CG_SCHWARZ_FP16: in the mixed-precision form the streamed CG keeps
    the Schwarz blocks in FP16 scaled by each block's largest magnitude
    (products and sums stay FP64); HOEFEM_CG_PHASE_PROFILE: the streamed CG
@@ -357,12 +359,17 @@ int hoefem_model_set_cg_engine(hoefem_model m, int engine, int options);
    gather, [5] Schwarz chunks, [6] of which waiting for chunk data, [7] grid
    barrier after the Schwarz products, [8] own-DOF update, [9] grid barrier
    and reductions after it, [10] producer waiting for free stages, [11]
-   producer lifetime. */
+   producer lifetime.  Automatic engine choice for the last solve's operator
+   precision and preconditioner kind: the sampled microseconds per iteration
+   of the chunked and the streamed engine (0 until sampled) and the choice
+   (-1 undecided, 0 chunked, 1 streamed). */
 typedef struct {
   int64_t launches, iterations;
   double device_ms;
   int64_t operator_bytes, schwarz_bytes;
   double phase_us[12];
+  double auto_us_per_iteration[2];
+  int32_t auto_choice;
 } hoefem_cg_engine_stats;
 int hoefem_integrator_cg_engine_stats(hoefem_integrator it, hoefem_cg_engine_stats* out);
 int hoefem_model_cg_engine_stats(hoefem_model m, hoefem_cg_engine_stats* out);
@@ -370,7 +377,8 @@ int hoefem_model_cg_engine_stats(hoefem_model m, hoefem_cg_engine_stats* out);
    bytes of each iteration's stream (over all CTAs; the Schwarz chunks first,
    then operator tiles) copied with an evict-last L2 policy so that they are
    still cached in the next iteration, the rest with evict-first.  bytes < 0:
-   the default, 60 % of the device's L2. */
+   the default, 0 (on the benchmark cylinder every kept budget measured
+   slower than streaming everything). */
 int hoefem_integrator_set_cg_l2_keep(hoefem_integrator it, int64_t bytes);
 int hoefem_model_set_cg_l2_keep(hoefem_model m, int64_t bytes);
 /* One time step: u, v (ndof) updated in place. */

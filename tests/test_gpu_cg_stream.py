@@ -193,3 +193,21 @@ def test_cg_first_iterates_match_numpy_recurrence(engine, prec):
             cg.solve_with_guess(b, x)
         assert ei.value.kind == H.SolveErrorKind.MaxIterationsReached and ei.value.output.num_iterations == k
         assert rel(x, numpy_pcg_iterates(A, apply_p, b, k)) < 1e-10, (k, rel(x, numpy_pcg_iterates(A, apply_p, b, k)))
+
+
+def test_auto_engine_times_both_engines_and_keeps_the_faster():
+    m, ref, P, J, b = schwarz_system(8)
+    m.set_cg_engine("auto")
+    xs = []
+    for _ in range(5):
+        x = np.zeros(m.ndof())
+        (H.ConjugateGradient(m).with_operator(J).with_preconditioner(P)
+         .with_stopping_criterion(H.RelativeResidualCriterion(1e-8)).with_max_iter(5000).solve_with_guess(b, x))
+        xs.append(x)
+    st = m.cg_engine_stats()
+    us = st["auto_us_per_iteration"]
+    assert st["auto_choice"] in (0, 1) and us[0] > 0 and us[1] > 0
+    assert st["auto_choice"] == (1 if us[1] < us[0] else 0)
+    # whichever engine runs, the solutions agree to the solve's tolerance
+    for x in xs[1:]:
+        assert rel(x, xs[0]) < 1e-6
