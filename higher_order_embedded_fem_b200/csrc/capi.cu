@@ -947,7 +947,7 @@ int hoefem_learned_predict(hoefem_learned l, const double* r, double* x0, int me
 
 int hoefem_integrator_set_learned(hoefem_integrator it, hoefem_learned l, int mode) {
   API_BEGIN
-  HOEFEM_REQUIRE(it && mode >= 0 && mode <= 3, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  HOEFEM_REQUIRE(it && mode >= 0 && mode <= 4, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
   HOEFEM_REQUIRE(!l || l->model == it->model, HOEFEM_ERR_INVALID_ARGUMENT, "learned correction of another model");
   integrator_set_learned(it->it, l ? &l->l : nullptr, mode);
   API_END

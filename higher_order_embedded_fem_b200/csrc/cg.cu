@@ -26,6 +26,7 @@
 
 #include "internal.h"
 #include "kernels_common.cuh"
+#include "learned.h"
 #include "solver.h"
 
 namespace hoefem {
@@ -326,6 +327,64 @@ __global__ void k_cg_reliable(CgState* st, int resume) {
   st->beta = st->zTr / st->pAp;
 }
 
+// ---- flexible CG with the learned coarse correction ------------------------
+
+// r_old = r; zr_old = z.r of this iteration (before the update).
+__global__ void k_fcg_save(int n, const double* __restrict__ r, double* __restrict__ r_old, CgState* st) {
+  if (st->done) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->zr_old = st->zTr;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) r_old[i] = r[i];
+}
+
+// z.r, z.r_old, c.r, c.r_old; the last block keeps the correction c if
+// c.r > 0, scaled by w = min(1, z.r / c.r) so that the coarse term never
+// outweighs the Schwarz term along r (the network predicts the coarse part
+// of the error, which the Schwarz term partly contains already); then
+// z' = z + w c, z'.r is the new zTr and (init = 0)
+// beta = (z'.r - z'.r_old) / zr_old.
+__global__ void __launch_bounds__(256) k_fcg_dots(int n, const double* __restrict__ z, const double* __restrict__ c,
+                                                  const double* __restrict__ r, const double* __restrict__ r_old,
+                                                  double* partials, unsigned* counter, CgState* st, int init) {
+  if (!init && st->done) return;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double ri = r[i], zi = z[i], ci = c[i];
+    acc[0] += zi * ri;
+    acc[2] += ci * ri;
+    if (!init) {
+      const double ro = r_old[i];
+      acc[1] += zi * ro;
+      acc[3] += ci * ro;
+    }
+  }
+  double tot[4];
+  if (grid_reduce_last_k<4>(acc, partials, counter, tot) && threadIdx.x == 0) {
+    const bool keep = tot[2] > 0.0;
+    const double wgt = keep ? fmin(1.0, fmax(tot[0], 0.0) / tot[2]) : 0.0;
+    st->learned_flag = keep ? 1 : 0;
+    st->learned_weight = wgt;
+    if (keep) st->learned_kept += 1;
+    else st->learned_dropped += 1;
+    const double zr = tot[0] + wgt * tot[2];
+    if (!init) {
+      const double zro = tot[1] + wgt * tot[3];
+      st->beta = (zr - zro) / st->zr_old;
+    }
+    st->zTr = zr;
+  }
+}
+
+// p = z + w c + beta p (init: p = z + w c).
+__global__ void __launch_bounds__(256) k_fcg_p(int n, const double* __restrict__ z, const double* __restrict__ c,
+                                               double* __restrict__ p, const CgState* st, int init) {
+  if (!init && st->done) return;
+  const double f = st->learned_flag ? st->learned_weight : 0.0, beta = st->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double zi = z[i] + f * c[i];
+    p[i] = init ? zi : zi + beta * p[i];
+  }
+}
+
 int vec_grid(i64 n) { return reduce_blocks_for(n); }
 
 __global__ void k_axpy(int n, double a, const double* __restrict__ x, double* __restrict__ y) {
@@ -357,6 +416,7 @@ CgWork::~CgWork() {
   if (h_st) cudaFreeHost(h_st);
   for (auto* e : {&tev[0], &tev[1], &sev[0], &sev[1]})
     if (*e) cudaEventDestroy(*e);
+  if (fcg_exec) cudaGraphExecDestroy(fcg_exec);
   for (auto& t : tuning) {
     if (t.e0) cudaEventDestroy(t.e0);
     if (t.e1) cudaEventDestroy(t.e1);
@@ -715,6 +775,103 @@ int cg_solve_reliable(CgWork& w, const double* A64, const float* A32, const Prec
                       double delta, i64* iters, i64* replacements, cudaStream_t s) {
   const bool p32 = P && P->kind == PREC_SCHWARZ && P->vals32.p;
   return run_pcg(w, Operator{nullptr, A32}, P, p32, tol, max_iter, iters, s, A64, delta, replacements);
+}
+
+// Flexible PCG with the learned two-level preconditioner (Notay's flexible CG
+// recurrence, since the network makes the preconditioner depend on r): per
+// iteration Ap and alpha as PCG, x / r updated, z = P r (the Schwarz or
+// diagonal apply of the plain solver), c = the network's coarse correction of
+// r, kept only if c.r > 0 (otherwise the iteration is the plain PCG step with
+// the flexible beta), p = z + c + beta p.  No host round trip inside an
+// iteration: the chunks of iterations are replayed as CUDA graphs, as in the
+// plain solver.
+int cg_solve_learned(CgWork& w, const double* vals, const Precond* P, Learned* L, double tol, i64 max_iter,
+                     i64* iters, i64* kept, i64* dropped, cudaStream_t s) {
+  HOEFEM_REQUIRE(L && L->trained, HOEFEM_ERR_INVALID_ARGUMENT, "learned correction not trained");
+  HOEFEM_REQUIRE(!P || P->ready, HOEFEM_ERR_INVALID_ARGUMENT, "preconditioner has not been updated");
+  NodeRows R = w.m->rows();
+  const int n = (int)w.n;
+  const int vg = vec_grid(n);
+  const int kind = P ? P->kind : PREC_NONE;
+  if (w.r_old.n < (size_t)n) w.r_old.alloc(n);
+  double* c = L->e.p;
+  CgState init{};
+  init.tol = tol;
+  init.max_iter = max_iter;
+  HOEFEM_CUDA(cudaMemcpyAsync(w.st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
+  R.lanes = lanes_for(*w.m, false);
+  HOEFEM_LANES_DISPATCH(R.lanes, {
+    const int sg = spmv_grid(R.nv, LN);
+    (note_launch(), k_cg_init<LN, double><<<sg, TPB, 0, s>>>(R, vals, w.x.p, w.b.p, w.r.p, w.partials.p, w.st.p));
+  });
+  auto plain_prec = [&](cudaStream_t cs) {
+    if (kind == PREC_SCHWARZ) enqueue_prec_spmv(w, P, false, 1, cs);
+    else
+      (note_launch(), k_cg_prec_vec<<<vg, TPB, 0, cs>>>(n, kind == PREC_DIAGONAL ? 1 : 0,
+                                                        kind == PREC_DIAGONAL ? P->diag.p : nullptr, w.r.p, w.z.p,
+                                                        w.partials.p, w.counter.p, w.st.p, 1));
+  };
+  plain_prec(s);
+  L->predict_device(w.r.p, &w.st.p->rr, c, s);
+  (note_launch(), k_fcg_dots<<<vg, TPB, 0, s>>>(n, w.z.p, c, w.r.p, nullptr, w.partials.p, w.counter.p, w.st.p, 1));
+  (note_launch(), k_fcg_p<<<vg, TPB, 0, s>>>(n, w.z.p, c, w.p.p, w.st.p, 1));
+  (note_launch(), k_cg_init_check<<<1, 1, 0, s>>>(w.st.p));
+  HOEFEM_CUDA(cudaGetLastError());
+  HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+  HOEFEM_CUDA(cudaStreamSynchronize(s));
+  auto finish = [&](int status) {
+    *iters = w.h_st->iters;
+    *kept = w.h_st->learned_kept;
+    *dropped = w.h_st->learned_dropped;
+    return status;
+  };
+  if (w.h_st->done == 2) {
+    HOEFEM_CUDA(cudaMemsetAsync(w.x.p, 0, sizeof(double) * n, s));
+    return finish(HOEFEM_OK);
+  }
+  if (w.h_st->done) return finish(w.h_st->status);
+  // one graph of w.chunk iterations
+  if (!w.fcg_exec || w.fcg_key[0] != (const void*)vals || w.fcg_key[1] != (const void*)P ||
+      w.fcg_key[2] != (const void*)L) {
+    if (w.fcg_exec) cudaGraphExecDestroy(w.fcg_exec);
+    w.fcg_exec = nullptr;
+    cudaStream_t cs;
+    HOEFEM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    HOEFEM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    g_capture_count = 0;
+    for (int k = 0; k < w.chunk; ++k) {
+      enqueue_Ap(w, Operator{vals, nullptr}, cs);
+      (note_launch(), k_fcg_save<<<vg, TPB, 0, cs>>>(n, w.r.p, w.r_old.p, w.st.p));
+      (note_launch(), k_cg_update<<<vg, TPB, 0, cs>>>(n, 0, nullptr, w.x.p, w.r.p, w.p.p, w.Ap.p, w.z.p,
+                                                      w.partials.p, w.counter.p, w.st.p));
+      plain_prec(cs);
+      L->predict_device(w.r.p, &w.st.p->rr, c, cs);
+      (note_launch(), k_fcg_dots<<<vg, TPB, 0, cs>>>(n, w.z.p, c, w.r.p, w.r_old.p, w.partials.p, w.counter.p,
+                                                     w.st.p, 0));
+      (note_launch(), k_fcg_p<<<vg, TPB, 0, cs>>>(n, w.z.p, c, w.p.p, w.st.p, 0));
+    }
+    w.fcg_kernels = g_capture_count;
+    g_capture_count = -1;
+    HOEFEM_CUDA(cudaStreamEndCapture(cs, &g));
+    HOEFEM_CUDA(cudaGraphInstantiate(&w.fcg_exec, g, 0));
+    cudaGraphDestroy(g);
+    cudaStreamDestroy(cs);
+    w.fcg_key[0] = vals;
+    w.fcg_key[1] = P;
+    w.fcg_key[2] = L;
+  }
+  const i64 cap = max_iter >= 0 ? max_iter : 10 * (i64)n;
+  const i64 max_chunks = (cap + w.chunk - 1) / w.chunk + 2;
+  for (i64 ch = 0; ch < max_chunks; ++ch) {
+    HOEFEM_CUDA(cudaGraphLaunch(w.fcg_exec, s));
+    g_launch_count.fetch_add(w.fcg_kernels, std::memory_order_relaxed);
+    HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+    HOEFEM_CUDA(cudaStreamSynchronize(s));
+    if (w.h_st->done) break;
+  }
+  if (!w.h_st->done) return finish(HOEFEM_CG_MAX_ITERATIONS);
+  return finish(w.h_st->status);
 }
 
 }  // namespace hoefem

@@ -125,7 +125,8 @@ struct Integrator {
   double delta = 0.1;  // reliable-update threshold of the mixed CG
   DBuf<float> J32;
   Learned* learned = nullptr;
-  int learned_mode = 0;  // 0 off, 1 warm start, 2 collect (b, x*), 3 collect (b, x*) and CG iterates
+  int learned_mode = 0;  // 0 off, 1 warm start, 2 collect (b, x*), 3 collect (b, x*) and CG iterates,
+                         // 4 two-level preconditioner (flexible CG, FP64)
   DBuf<double> x0, r0;
   std::vector<DBuf<double>*> snaps;  // collected (x_k, r_k) pairs of the current solve
   double ratio_sum = 0.0;
@@ -270,7 +271,12 @@ struct Integrator {
     i64 it = 0;
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
     int st;
-    if (precision == PRECISION_FP32) {
+    if (learned && learned_mode == 4 && learned->trained && precision == PRECISION_FP64) {
+      i64 kept = 0, dropped = 0;
+      st = cg_solve_learned(cg, J.p, P, learned, cg_tol, cg_max, &it, &kept, &dropped, s);
+      stats.learned_accepted += kept;
+      stats.learned_rejected += dropped;
+    } else if (precision == PRECISION_FP32) {
       if (J32.n < (size_t)m->nnz) J32.alloc(m->nnz);
       to_f32(J.p, J32.p, m->nnz, s);
       i64 reps = 0;

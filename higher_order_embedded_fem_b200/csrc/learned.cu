@@ -177,6 +177,8 @@ __global__ void k_apply(int S, const int* __restrict__ sub_off, const int* __res
   }
 }
 
+__global__ void k_sqrt_to(const double* __restrict__ rr, double* __restrict__ out) { *out = sqrt(fmax(*rr, 0.0)); }
+
 __global__ void k_sub(int n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ c) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) c[i] = a[i] - b[i];
 }
@@ -707,6 +709,20 @@ void Learned::predict(const double* r, double* x0, cudaStream_t s) {
   (note_launch(), k_unstandardise<<<(S * NM + 255) / 256, 256, 0, s>>>(S, NM, t_mean.p, t_std.p, Y3.p));
   HOEFEM_CUDA(cudaMemsetAsync(x0, 0, sizeof(double) * m->ndof, s));
   apply(Y3.p, rn, x0, s);
+}
+
+void Learned::predict_device(const double* r, const double* rr, double* x0, cudaStream_t s) {
+  const int ndof = (int)m->ndof;
+  (note_launch(), k_sqrt_to<<<1, 1, 0, s>>>(rr, scal.p));
+  (note_launch(), k_global_proj<<<NG, 256, 0, s>>>(ndof, d_psi.p, r, d_gproj.p));
+  (note_launch(), k_features<<<S, 256, 0, s>>>(S, d_sub_off.p, d_sub_dofs.p, d_phi.p, r, d_gproj.p, d_centroid.p,
+                                               scal.p, X.p));
+  (note_launch(), k_standardise<<<(S * F + 255) / 256, 256, 0, s>>>(S, F, x_mean.p, x_std.p, X.p));
+  forward(X.p, S, use_bf16 != 0, s);
+  (note_launch(), k_unstandardise<<<(S * NM + 255) / 256, 256, 0, s>>>(S, NM, t_mean.p, t_std.p, Y3.p));
+  HOEFEM_CUDA(cudaMemsetAsync(x0, 0, sizeof(double) * ndof, s));
+  (note_launch(), k_apply<<<S, 256, 0, s>>>(S, d_sub_off.p, d_sub_dofs.p, d_phi.p, Y3.p, scal.p, x0));
+  HOEFEM_CUDA(cudaGetLastError());
 }
 
 }  // namespace hoefem

@@ -61,6 +61,9 @@ struct Learned {
   void train(long long steps, int batch, float lr, uint64_t seed, float* loss_hist, cudaStream_t s);
   // prediction for residual r: writes x0 (device FP64)
   void predict(const double* r, double* x0, cudaStream_t s);
+  // the same without a host round trip (graph-capturable): ||r|| = sqrt(*rr)
+  // read on the device
+  void predict_device(const double* r, const double* rr, double* x0, cudaStream_t s);
 };
 
 }  // namespace hoefem

@@ -66,6 +66,11 @@ struct CgState {
   // flag it raises, and which direction buffer holds the current direction
   double rr_ref, delta2;
   int replace, pcur, rcur, pad;
+  // flexible CG with the learned coarse correction: z_k.r_k of the previous
+  // iteration, whether this iteration's correction was kept, and the counts
+  double zr_old, learned_weight;
+  long long learned_kept, learned_dropped;
+  int learned_flag, pad2;
 };
 
 // One unit of a streamed kernel's work: `bytes` (multiple of 16, at most one
@@ -182,6 +187,11 @@ struct CgWork {
   EngineTune etune[6];
   int last_tune = 0;  // entry of the last solve
   cudaEvent_t tev[2] = {nullptr, nullptr};
+  // flexible CG with the learned correction: r_k, its graph and what it was captured for
+  DBuf<double> r_old;
+  cudaGraphExec_t fcg_exec = nullptr;
+  const void* fcg_key[3] = {nullptr, nullptr, nullptr};
+  long long fcg_kernels = 0;
   CgStreamOp sop64, sop32;
   CgStreamSchwarz ssw;
   DBuf<double> p2, r2, spart;
@@ -214,6 +224,14 @@ int cg_solve(CgWork& w, const double* vals, const Precond* P, double tol, i64 ma
 int cg_solve_reliable(CgWork& w, const double* A64, const float* A32, const Precond* P, double tol, i64 max_iter,
                       double delta, i64* iters, i64* replacements, cudaStream_t s);
 void to_f32(const double* a, float* b, long long n, cudaStream_t s);
+
+struct Learned;
+// Flexible PCG (FP64) with the two-level preconditioner z = P r + c(r), c the
+// learned coarse correction of the current residual, kept in an iteration
+// only if c.r > 0; beta = z_{k+1}.(r_{k+1} - r_k) / z_k.r_k.  kept / dropped
+// count the iterations with and without the correction.
+int cg_solve_learned(CgWork& w, const double* vals, const Precond* P, Learned* L, double tol, i64 max_iter,
+                     i64* iters, i64* kept, i64* dropped, cudaStream_t s);
 
 // Streamed CG (cg_stream.cu).  cg_stream_usable: whether the persistent
 // kernel can run this solve; cg_stream_prepare packs the operator (FP64

@@ -240,7 +240,9 @@ class NewtonCgIntegrator3d:
     def set_learned(self, learned, mode=1):
         """mode 1: guarded learned warm start; 2: collect (b, x*) training pairs
         from this integrator's plain FP64 CG solves; 3: as 2 plus the CG
-        iterates (r_k, x* - x_k); 0 / learned=None: off."""
+        iterates (r_k, x* - x_k); 4: two-level preconditioner (the network's
+        coarse correction beside Schwarz in every CG iteration, flexible CG);
+        0 / learned=None: off."""
         self._learned = learned
         check(lib().hoefem_integrator_set_learned(self._h, learned._h if learned is not None else None,
                                                   int(mode) if learned is not None else 0))

@@ -428,7 +428,12 @@ int hoefem_learned_set_weights(hoefem_learned l, const float* w);
 int hoefem_learned_predict(hoefem_learned l, const double* r, double* x0, int mem);
 /* mode 0: off, 1: warm start with the guard, 2: collect training pairs from
    the integrator's plain FP64 CG solves (right-hand side b with the converged
-   solution), 3: as 2 plus every CG chunk's iterate (r_k, x* - x_k). */
+   solution), 3: as 2 plus every CG chunk's iterate (r_k, x* - x_k), 4:
+   two-level preconditioner beside the Schwarz (or diagonal) one in the FP64
+   Jacobian solves: flexible PCG with z = P r + c(r), the network's coarse
+   correction c(r) of every iteration's residual kept only when c.r > 0
+   (hoefem_step_stats.learned_accepted / learned_rejected count the
+   iterations with and without it). */
 int hoefem_integrator_set_learned(hoefem_integrator it, hoefem_learned l, int mode);
 
 /* ------------------------------------------------------------------------ */

@@ -88,3 +88,42 @@ def test_training_on_cg_pairs_and_heldout_gain():
     print("plain CG iterations %d, learned %d (accepted %d, residual ratio %.3f)" % (
         plain["total_cg_iterations"], learned["total_cg_iterations"], learned["learned_accepted"],
         learned["learned_residual_ratio"]))
+
+
+def test_two_level_learned_preconditioner_solves_the_step_at_dt_1e2():
+    # dt = 1e-2: a stiffer Jacobian, where a coarse correction on this coarse
+    # space could pay (the exact Galerkin one saves about a third of the
+    # Schwarz-CG iterations, test_coarse_space_ceiling.py).  The network,
+    # trained on (r_k, x* - x_k) pairs of plain Schwarz-CG solves of other
+    # seeds, is applied beside Schwarz in every iteration (flexible CG).  The
+    # step must reach the same solution; the iteration counts are reported:
+    # the correction varies nonlinearly with r from one iteration to the next,
+    # which costs the flexible recurrence its conjugacy, and it takes far more
+    # iterations than plain Schwarz-CG.
+    dt = 1e-2
+    e, m, mat = _model(10)
+    comp = H.SchwarzPreconditionerComponent.from_embedded_model(m, e.volume_fractions, 0.5)
+    L = H.LearnedCoarseCorrection(m, e.nodes_below(2, 1e-9), num_subdomains=32, seed=5)
+    it = _integrator(e, m, mat, comp)
+    it.set_tolerances(1e-6, 5000, 100)
+    it.set_learned(L, 3)
+    for seed in range(6):
+        u, v = _state(e, m, 200 + seed, amp=0.01 + 0.004 * seed)
+        it.step(u, v, 0.0, dt)
+    assert L.num_pairs() > 0
+    hist = L.train(1500, batch=256, lr=1e-3, seed=0)
+    assert np.mean(hist[-50:]) < 0.5 * np.mean(hist[:10])
+    u0, v0 = _state(e, m, 4242, amp=0.017)
+    it.set_learned(None)
+    u, v = u0.copy(), v0.copy()
+    plain = it.step(u, v, 0.0, dt)
+    it.set_learned(L, 4)
+    ul, vl = u0.copy(), v0.copy()
+    two = it.step(ul, vl, 0.0, dt)
+    print("dt 1e-2: Schwarz-CG %d iterations (%d Newton), learned two-level %d (%d Newton; correction kept in %d "
+          "of %d iterations)" % (plain["total_cg_iterations"], plain["newton_iterations"], two["total_cg_iterations"],
+                                 two["newton_iterations"], two["learned_accepted"],
+                                 two["learned_accepted"] + two["learned_rejected"]))
+    assert two["learned_accepted"] > 0
+    assert two["residual_norm"] <= dt * 1e-5 * two["representative_force"]
+    assert np.abs(ul - u).max() <= 1e-5 * np.abs(u).max()
