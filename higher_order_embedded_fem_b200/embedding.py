@@ -54,6 +54,7 @@ class Embedding:
 
     def __init__(self, handle, num_cells):
         self._h = handle
+        self._lib = lib()  # kept for __del__ at interpreter exit
         cls = np.zeros(num_cells, dtype=np.int32)
         cut = np.zeros(num_cells)
         ne, ni, nf = C.c_int64(), C.c_int64(), C.c_int64()
@@ -66,8 +67,8 @@ class Embedding:
         self.interface_cells = np.nonzero(cls == 2)[0]
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            lib().hoefem_embedding_destroy(self._h)
+        if getattr(self, "_h", None) and getattr(self, "_lib", None) is not None:
+            self._lib.hoefem_embedding_destroy(self._h)
             self._h = None
 
 

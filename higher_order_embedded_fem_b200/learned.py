@@ -22,6 +22,7 @@ class LearnedCoarseCorrection:
         check(lib().hoefem_learned_create(model._h, bc.ctypes.data if bc.size else None, bc.size, num_subdomains,
                                           seed, C.byref(h)))
         self._h = h
+        self._lib = lib()  # kept for __del__ at interpreter exit
         self.num_subdomains = num_subdomains
         n = C.c_int64()
         check(lib().hoefem_learned_num_params(h, C.byref(n)))
@@ -29,8 +30,8 @@ class LearnedCoarseCorrection:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            lib().hoefem_learned_destroy(h)
+        if h and getattr(self, "_lib", None) is not None:
+            self._lib.hoefem_learned_destroy(h)
             self._h = None
 
     def num_pairs(self):

@@ -33,14 +33,15 @@ class _Model:
         h = C.c_void_p()
         check(lib().hoefem_model_create(X.ctypes.data, X.shape[0], C.byref(h)))
         self._h = h
+        self._lib = lib()  # kept for __del__ at interpreter exit
         self.num_vertices = X.shape[0]
         self.vertices = X
         self._blocks = []
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            lib().hoefem_model_destroy(h)
+        if h and getattr(self, "_lib", None) is not None:
+            self._lib.hoefem_model_destroy(h)
             self._h = None
 
     def _add_block(self, kind, connectivity, weights, points, offsets=None):

@@ -28,11 +28,12 @@ class DiagonalPreconditioner:
         h = C.c_void_p()
         check(lib().hoefem_precond_create_diagonal(model._h, C.byref(h)))
         self._h = h
+        self._lib = lib()  # kept for __del__ at interpreter exit
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            lib().hoefem_precond_destroy(h)
+        if h and getattr(self, "_lib", None) is not None:
+            self._lib.hoefem_precond_destroy(h)
             self._h = None
 
     def update(self, system_values):
@@ -69,6 +70,7 @@ class SchwarzPreconditioner(DiagonalPreconditioner):
                                                   len(subs), un.ctypes.data if un.size else None, un.size,
                                                   C.byref(h)))
         self._h = h
+        self._lib = lib()  # kept for __del__ at interpreter exit
         self.num_subdomains = len(subs)
 
     def set_spmv_variant(self, variant):
@@ -220,11 +222,12 @@ class NewtonCgIntegrator3d:
                                              1 if gravity_enabled else 0, float(gravity),
                                              preconditioner._h if preconditioner is not None else None, C.byref(h)))
         self._h = h
+        self._lib = lib()  # kept for __del__ at interpreter exit
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            lib().hoefem_integrator_destroy(h)
+        if h and getattr(self, "_lib", None) is not None:
+            self._lib.hoefem_integrator_destroy(h)
             self._h = None
 
     def set_tolerances(self, cg_tol=1e-5, cg_max_iter=500, newton_max_iter=100):
@@ -330,6 +333,7 @@ class BatchedNewtonCgIntegrator3d:
         check(lib().hoefem_batch_create(handles, ns, descs, float(density), off.ctypes.data, flat.ctypes.data,
                                         1 if gravity_enabled else 0, float(gravity), C.byref(h)))
         self._h = h
+        self._lib = lib()  # kept for __del__ at interpreter exit
         self.num_scenes = ns
         ndof = C.c_int64()
         nnz = C.c_int64()
@@ -340,8 +344,8 @@ class BatchedNewtonCgIntegrator3d:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            lib().hoefem_batch_destroy(h)
+        if h and getattr(self, "_lib", None) is not None:
+            self._lib.hoefem_batch_destroy(h)
             self._h = None
 
     def set_stream(self, stream):
