@@ -335,7 +335,7 @@ def run_hoefem(args):
             variants[vn]["rel_diff_u_vs_plain"] = float(np.abs(um - up).max() / np.abs(up).max())
     for vn_, v in variants.items():
         v.pop("u")
-        v["cg_roofline"] = cg_roofline(v, vn_)
+        v["cg_roofline"] = cg_roofline(v, vn_, args.schwarz_fp16)
 
     # end to end through the public API with pinned host buffers
     uh = torch.empty(model.ndof(), dtype=torch.float64, pin_memory=True).numpy()
@@ -355,7 +355,7 @@ def run_hoefem(args):
 
     # roofline of the dominant kernel: the persistent streamed CG of the headline
     # variant (its CUDA-event device time over the step's iterations)
-    roof = cg_roofline(variants[head], head)
+    roof = cg_roofline(variants[head], head, args.schwarz_fp16)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -399,7 +399,7 @@ def run_hoefem(args):
         torch.distributed.destroy_process_group()
 
 
-def cg_roofline(var, head):
+def cg_roofline(var, head, fp16=False):
     """Streamed CG of one variant: algorithmic bytes per iteration = operator
     tiles (values + neighbour lists + tile headers) + Schwarz block chunks, the
     data an iteration must read from HBM (vectors, 1 MB each, stay in L2);
@@ -415,8 +415,20 @@ def cg_roofline(var, head):
     gbs = per_it / (ms_it * 1e-3) / 1e9
     kern = {"plain": "k_cg_stream<double,double,2>", "mixed": "k_cg_stream<float,float,2>",
             "learned": "k_cg_stream<float,float,2>"}[head]
+    if fp16 and head != "plain":
+        kern = kern.replace("float,float", "float,__half")
+    # DRAM bytes per iteration of the same kernel on this workload, from an ncu
+    # capture of all its launches in a bench run (dram__bytes_read.sum +
+    # dram__bytes_write.sum summed over the launches / the iterations they ran)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "k_cg_stream_traffic_embedded_cylinder_n24.json")
+    if os.path.exists(tpath):
+        t = json.load(open(tpath)).get("kernels", {}).get(kern)
+        if t and t.get("bytes_per_iteration_algorithmic") == per_it:
+            traffic = t["dram_bytes_per_iteration"]
     return {"kernel": kern + " (persistent streamed Schwarz-PCG)", "bound": "hbm", "achieved": gbs, "peak": peak,
-            "unit": "GB/s", "frac": gbs / peak, "traffic": None, "bytes_per_iteration": per_it,
+            "unit": "GB/s", "frac": gbs / peak, "traffic": traffic, "traffic_unit": "DRAM bytes per CG iteration",
+            "bytes_per_iteration": per_it,
             "us_per_iteration": ms_it * 1e3, "iterations": eng["iterations"], "launches": eng["launches"],
             "peak_source": "measured" if os.path.exists(peaks_path) else "fallback"}
 
@@ -656,6 +668,39 @@ def run_tet10(args):
                       "u": ud.cpu().numpy()}
     up, um = out["plain"].pop("u"), out["mixed"].pop("u")
     out["mixed"]["rel_diff_u_vs_plain"] = float(np.abs(um - up).max() / np.abs(up).max())
+    # the FP32 element stiffness alone (device arrays; adds into K), tensor
+    # cores (element blocks + gather) vs the CUDA-core colored kernels, and
+    # the FP64 kernels; CUDA events on the model's stream
+    stiff = {}
+    Kd = torch.zeros(model.nnz, dtype=torch.float64, device=dev)
+    reps = max(3, args.steps)
+    for name, path, f32 in (("fp32_tensor_cores", "auto", True), ("fp32_cuda_cores", "cuda_cores", True),
+                            ("fp64_cuda_cores", "auto", False)):
+        model.set_stiffness_path(path)
+        for _ in range(3):
+            model.assemble_stiffness_into_precision(Kd, u0d, mat, f32)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(reps):
+            model.assemble_stiffness_into_precision(Kd, u0d, mat, f32)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        stiff[name] = ev0.elapsed_time(ev1) / reps
+    model.set_stiffness_path("auto")
+    del Kd
+    ntiles = -(-model.num_elements // 14)
+    # tensor work the kernel issues: per 14-element tile 2 K chunks x 8 K steps
+    # x 3 products of M 128, N 64, K 8 (TF32)
+    tflop = 3 * 2 * 128 * 64 * 128 * ntiles / 1e12
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    bf16 = json.load(open(peaks_path))["bf16_tflops"] if os.path.exists(peaks_path) else 1590.0
+    stiff["tensor_roofline"] = {
+        "kernel": "k_stiffness_tc + k_stiffness_gather", "bound": "tensor", "unit": "TFLOP/s",
+        "achieved": tflop / (stiff["fp32_tensor_cores"] * 1e-3), "peak": bf16 / 2,
+        "frac": tflop / (stiff["fp32_tensor_cores"] * 1e-3) / (bf16 / 2),
+        "peak_source": "measured bf16 dense / 2 (TF32 rate)" if os.path.exists(peaks_path) else "fallback / 2",
+        "tflop_per_launch": tflop, "traffic": None}
     # element arithmetic errors at u0 against the FP64 oracle (host arrays)
     K64 = model.assemble_stiffness_into_par(np.zeros(model.nnz), u0, mat)
     K32 = model.assemble_stiffness_into_precision(np.zeros(model.nnz), u0, mat, True)
@@ -680,7 +725,7 @@ def run_tet10(args):
                                    "one BE Newton step dt=1e-3, diagonal PCG to %g" % args.cg_tol,
                        "elements": int(model.num_elements), "ndof": int(model.ndof()), "nnz": int(model.nnz)},
             "variants": out, "speedup_mixed_vs_plain": out["plain"]["ms_per_step"] / out["mixed"]["ms_per_step"],
-            "errors": errs}
+            "stiffness_ms": stiff, "errors": errs}
     print(json.dumps(line), flush=True)
 
 

@@ -62,6 +62,7 @@ class CgEngineStats(C.Structure):
 
 
 CG_ENGINE = {"auto": 0, "chunked": 1, "streamed": 2}
+STIFFNESS_PATH = {"auto": 0, "cuda_cores": 1}
 
 
 class SceneInfo(C.Structure):
@@ -83,6 +84,7 @@ SIGNATURES = {
     "hoefem_model_set_stream": (C.c_int, [vp, vp]),
     "hoefem_model_autotune": (C.c_int, [vp, C.POINTER(C.c_int32)]),
     "hoefem_model_set_spmv_variant": (C.c_int, [vp, C.c_int32]),
+    "hoefem_model_set_stiffness_path": (C.c_int, [vp, C.c_int]),
     "hoefem_model_sizes": (C.c_int, [vp, pi64, pi64, pi64, pi64]),
     "hoefem_model_pattern": (C.c_int, [vp, vp, vp]),
     "hoefem_model_num_colors": (C.c_int, [vp, C.c_int, pi64]),

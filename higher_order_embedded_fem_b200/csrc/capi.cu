@@ -282,6 +282,15 @@ int hoefem_model_set_spmv_variant(hoefem_model m, int32_t variant) {
   API_END
 }
 
+int hoefem_model_set_stiffness_path(hoefem_model m, int path) {
+  API_BEGIN
+  Model& mm = device_model(m);
+  HOEFEM_REQUIRE(path == HOEFEM_STIFFNESS_AUTO || path == HOEFEM_STIFFNESS_CUDA_CORES, HOEFEM_ERR_INVALID_ARGUMENT,
+                 "unknown stiffness path");
+  mm.stiffness_path = path == HOEFEM_STIFFNESS_AUTO ? STIFFNESS_AUTO : STIFFNESS_CUDA_CORES;
+  API_END
+}
+
 int hoefem_model_get_spmv_variants(hoefem_model m, int32_t* fp64_values, int32_t* fp32_values) {
   API_BEGIN
   Model& mm = model_of(m);

@@ -73,10 +73,12 @@ constexpr int CONSUMERS = 32 * NW;
 // Schwarz items (record offset, block dimension, slot, 0)
 constexpr int ITEM_HDR = 16;
 constexpr int MAX_DIM = 81;      // Schwarz block dimension bound (3 x 27 nodes)
-constexpr int HALO_MAX = 1280;   // halo nodes of one segment
+constexpr int HALO_MAX = 1152;   // halo nodes of one segment
 constexpr int ZMAX = 1536;       // Schwarz row results (3 per incidence) of one segment
 constexpr size_t SMEM_RING = (size_t)NS * STAGE;
-constexpr size_t SMEM_BYTES = SMEM_RING + (size_t)3 * HALO_MAX * 8 + (size_t)ZMAX * 8;
+// ring, FP64 halo (3 per node), Schwarz row results, FP32 halo (4 per node)
+constexpr size_t SMEM_BYTES = SMEM_RING + (size_t)3 * HALO_MAX * 8 + (size_t)ZMAX * 8 + (size_t)HALO_MAX * 16;
+static_assert(SMEM_BYTES + 2048 <= 227 * 1024, "shared memory (dynamic + static)");
 static_assert(NS % NW == 0, "each ring stage must belong to one consumer warp");
 static_assert(STAGE % 16 == 0 && SMEM_RING % 16 == 0, "bulk copies need 16-byte sizes and offsets");
 static_assert(3 * HALO_MAX < 65536, "halo-local indices are 16-bit");
@@ -160,6 +162,11 @@ __device__ __forceinline__ double sum_partials(const double* part, int G, int la
   return warp_sum(v);
 }
 
+// Halo node of a halo-local DOF index 3 hl (hl < HALO_MAX): hl = x / 3 by a
+// multiply and shift, exact for x < 98,304.
+__device__ __forceinline__ int halo_node(int x) { return (x * 43691) >> 17; }
+static_assert(3 * HALO_MAX < 98304, "halo_node range");
+
 // Gather batches: each thread first issues the loads of GB entries, then
 // computes and stores, so that GB L2 round trips overlap instead of chaining.
 constexpr int GB = 8;
@@ -167,10 +174,13 @@ constexpr int GB = 8;
 // For t < n3 (halo entry t / 3, component t % 3, DOF g = 3 halo[t / 3] + t % 3):
 // mode 0: s[t] = va + c vb at g (the direction z + beta p_old), also stored to
 // pnew for g in [d0, d1); mode 1: s[t] = va - c vb at g (r_old - alpha Ap).
+// With s32 non-null the value is also stored rounded to FP32 at s32[4 (t / 3) + t % 3]
+// (the FP32 halo of the FP32-value products).
 template <int MODE>
 __device__ __forceinline__ void gather_halo(const int* __restrict__ halo, int n3, int d0, int d1,
                                             const double* __restrict__ va, const double* __restrict__ vb, double c,
-                                            double* __restrict__ s, double* __restrict__ pnew) {
+                                            double* __restrict__ s, double* __restrict__ pnew,
+                                            float* __restrict__ s32 = nullptr) {
   for (int t0 = (int)threadIdx.x; t0 < n3; t0 += GB * CONSUMERS) {
     int g[GB];
 #pragma unroll
@@ -191,12 +201,18 @@ __device__ __forceinline__ void gather_halo(const int* __restrict__ halo, int n3
 #pragma unroll
     for (int u = 0; u < GB; ++u) {
       if (g[u] < 0) continue;
+      const int t = t0 + u * CONSUMERS;
+      double dv;
       if (MODE == 0) {
-        const double dv = cg_dir(a[u], c, b[u]);
-        s[t0 + u * CONSUMERS] = dv;
+        dv = cg_dir(a[u], c, b[u]);
         if (g[u] >= d0 && g[u] < d1) pnew[g[u]] = dv;
       } else {
-        s[t0 + u * CONSUMERS] = cg_res(a[u], c, b[u]);
+        dv = cg_res(a[u], c, b[u]);
+      }
+      s[t] = dv;
+      if (s32) {
+        const int hl = t / 3;
+        s32[4 * hl + (t - 3 * hl)] = (float)dv;
       }
     }
   }
@@ -207,6 +223,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
   extern __shared__ __align__(128) unsigned char ring[];
   double* s_halo = reinterpret_cast<double*>(ring + SMEM_RING);  // 3 x HALO_MAX
   double* s_zp = s_halo + 3 * HALO_MAX;                           // ZMAX
+  float4* s_h32 = reinterpret_cast<float4*>(s_zp + ZMAX);          // HALO_MAX
+  constexpr bool OP32 = sizeof(VA) == 4, SW32 = sizeof(VB) < 8;
   __shared__ __align__(8) uint64_t full[NS];
   __shared__ __align__(8) uint64_t empty[NS];
   __shared__ volatile int s_stop;
@@ -341,7 +359,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
       const CgsSeg S = A.segs[sg];
       unsigned long long t0 = tick();
       pipe::named_sync(1, CONSUMERS);  // the previous segment is done with the halo
-      gather_halo<0>(A.halo + S.halo_off, 3 * S.halo_n, 3 * S.n0, 3 * S.n1, A.z, pold, beta, s_halo, pnew);
+      gather_halo<0>(A.halo + S.halo_off, 3 * S.halo_n, 3 * S.n0, 3 * S.n1, A.z, pold, beta, s_halo, pnew,
+                     OP32 ? reinterpret_cast<float*>(s_h32) : nullptr);
       pipe::named_sync(1, CONSUMERS);
       tock(0, t0);
       t0 = tick();
@@ -366,18 +385,40 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
           const unsigned short* loc = (const unsigned short*)(t + h.x);
           const VA* v = (const VA*)(t + h.x + align16(2LL * d));
           double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-          for (int e = gl; e < d; e += 8) {
-            const double* pd = s_halo + loc[e];
-            const double q0v = pd[0], q1v = pd[1], q2v = pd[2];
-            s0 += ldv(v + e) * q0v + ldv(v + d + e) * q1v + ldv(v + 2 * d + e) * q2v;
-            s1 += ldv(v + 3 * d + e) * q0v + ldv(v + 4 * d + e) * q1v + ldv(v + 5 * d + e) * q2v;
-            s2 += ldv(v + 6 * d + e) * q0v + ldv(v + 7 * d + e) * q1v + ldv(v + 8 * d + e) * q2v;
-          }
+          if constexpr (OP32) {
+            // FP32 values times the FP32 halo (one 16-byte load per block),
+            // FP32 sums: the products carry the values' own rounding
+            float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+            const float* vf = reinterpret_cast<const float*>(v);
+            for (int e = gl; e < d; e += 8) {
+              const float4 pv = s_h32[halo_node(loc[e])];
+              f0 += vf[e] * pv.x + vf[d + e] * pv.y + vf[2 * d + e] * pv.z;
+              f1 += vf[3 * d + e] * pv.x + vf[4 * d + e] * pv.y + vf[5 * d + e] * pv.z;
+              f2 += vf[6 * d + e] * pv.x + vf[7 * d + e] * pv.y + vf[8 * d + e] * pv.z;
+            }
 #pragma unroll
-          for (int o = 4; o > 0; o >>= 1) {
-            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+            for (int o = 4; o > 0; o >>= 1) {
+              f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+              f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+              f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+            }
+            s0 = f0;
+            s1 = f1;
+            s2 = f2;
+          } else {
+            for (int e = gl; e < d; e += 8) {
+              const double* pd = s_halo + loc[e];
+              const double q0v = pd[0], q1v = pd[1], q2v = pd[2];
+              s0 += ldv(v + e) * q0v + ldv(v + d + e) * q1v + ldv(v + 2 * d + e) * q2v;
+              s1 += ldv(v + 3 * d + e) * q0v + ldv(v + 4 * d + e) * q1v + ldv(v + 5 * d + e) * q2v;
+              s2 += ldv(v + 6 * d + e) * q0v + ldv(v + 7 * d + e) * q1v + ldv(v + 8 * d + e) * q2v;
+            }
+#pragma unroll
+            for (int o = 4; o > 0; o >>= 1) {
+              s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+              s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+              s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+            }
           }
           if (has && gl == 0) {
             const int a3 = 3 * h.w;
@@ -430,7 +471,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
       unsigned long long t0 = tick();
       if (PK == 2) {
         pipe::named_sync(1, CONSUMERS);  // the previous segment is done with the halo and s_zp
-        gather_halo<1>(A.halo + S.halo_off, 3 * S.halo_n, 0, 0, rold, A.Ap, alpha, s_halo, nullptr);
+        gather_halo<1>(A.halo + S.halo_off, 3 * S.halo_n, 0, 0, rold, A.Ap, alpha, s_halo, nullptr,
+                       SW32 ? reinterpret_cast<float*>(s_h32) : nullptr);
         pipe::named_sync(1, CONSUMERS);
         tock(4, t0);
         t0 = tick();
@@ -453,11 +495,24 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
             const unsigned short* cols = (const unsigned short*)(t + h.x);
             const VB* v = (const VB*)(t + h.x + align16(2LL * ns)) + (size_t)i * dim;
             double b0 = 0.0, b1 = 0.0, b2 = 0.0;
-            for (int m = 0; m < ns; ++m) {
-              const double* hr = s_halo + cols[m];
-              b0 += ldv(v + 3 * m) * hr[0];
-              b1 += ldv(v + 3 * m + 1) * hr[1];
-              b2 += ldv(v + 3 * m + 2) * hr[2];
+            if constexpr (SW32) {
+              float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+              for (int m = 0; m < ns; ++m) {
+                const float4 hr = s_h32[halo_node(cols[m])];
+                c0 += (float)v[3 * m] * hr.x;
+                c1 += (float)v[3 * m + 1] * hr.y;
+                c2 += (float)v[3 * m + 2] * hr.z;
+              }
+              b0 = c0;
+              b1 = c1;
+              b2 = c2;
+            } else {
+              for (int m = 0; m < ns; ++m) {
+                const double* hr = s_halo + cols[m];
+                b0 += ldv(v + 3 * m) * hr[0];
+                b1 += ldv(v + 3 * m + 1) * hr[1];
+                b2 += ldv(v + 3 * m + 2) * hr[2];
+              }
             }
             const double sc = sizeof(VB) == 2 ? A.sw_scale[__ldg(A.slot_sub + h.z)] : 1.0;
             s_zp[3 * (h.z - S.q0) + i] = ((b0 + b1) + b2) * sc;

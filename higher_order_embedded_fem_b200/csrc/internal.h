@@ -130,8 +130,20 @@ struct Block {
   std::vector<int> escene;   // optional element -> scene (batched scenes)
   DBuf<int> d_escene;
   const unsigned char* scene_active = nullptr;  // non-owning device mask, per scene
+  // tensor-core stiffness (stiffness_tc.cu), built on first use: the reference
+  // gradient operator (TF32 hi / lo image), the per-slot gather map and the
+  // element blocks
+  mutable DBuf<float> d_tc_psi, d_tc_ke;
+  mutable DBuf<int> d_tc_off, d_tc_ent;
+  mutable int tc_nch = 0;
+  mutable bool tc_ready = false;
   BlockDev dev() const;
 };
+
+// Element stiffness implementation: automatic (tensor cores for the blocks
+// they cover: Tet10 with one quadrature rule of at most 14 points, FP32
+// element arithmetic), or the CUDA-core kernels only.
+enum StiffnessPath { STIFFNESS_AUTO = 0, STIFFNESS_CUDA_CORES = 1 };
 
 struct Model {
   int device = 0;
@@ -154,6 +166,7 @@ struct Model {
   int spmv_lanes = 32;    // SpMV variant for FP64 values (autotuned)
   int spmv_lanes32 = 0;   // SpMV variant for FP32 values (0: as spmv_lanes)
   bool spmv_pinned = false;  // set explicitly by the caller: no autotuning
+  int stiffness_path = STIFFNESS_AUTO;
   NodeRows rows() const;
   ~Model();
 };
@@ -171,6 +184,12 @@ enum Precision { PRECISION_FP64 = 0, PRECISION_FP32 = 1 };
 void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s,
                       int precision = PRECISION_FP64);
 void launch_mass(const Model& m, double density, double* vals, cudaStream_t s);
+// Tensor-core Tet10 stiffness (stiffness_tc.cu): eligibility of a block for
+// FP32 element arithmetic, and the launch (element blocks on the tensor
+// cores, then the gather into vals, adding).
+bool stiffness_tc_eligible(const Model& m, const Block& blk);
+void launch_stiffness_tc(const Model& m, const Block& blk, const MatDev& mat, const double* u, double* vals,
+                         cudaStream_t s);
 // Stiffness with every element matrix projected onto PSD (negative eigenvalues
 // set to zero) before the colored scatter; adds into vals.
 void launch_stiffness_projected(Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s);

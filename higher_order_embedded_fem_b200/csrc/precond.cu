@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(256, 2) k_schwarz_gj(
     const double* __restrict__ J, const long long* __restrict__ stage_off, double* __restrict__ stage,
     int* __restrict__ fallback) {
   constexpr int M = 16 * T;
-  __shared__ double s_row[2][M], s_col[2][M];
+  __shared__ double s_row[2][M], s_col[2][M], s_piv[2];
   __shared__ int s_g[27], s_rl[27];
   __shared__ long long s_jb[27];
   __shared__ double s_red;
@@ -116,6 +116,11 @@ __global__ void __launch_bounds__(256, 2) k_schwarz_gj(
   block_sum<1>(v1);
   if (threadIdx.x == 0) s_red = sqrt(v1[0]);
   bool ok = true;
+  // Step k: the owners of pivot row and column publish them (the pivot
+  // itself separately; in its place 1 in the row and -1 in the column) and
+  // zero their copies, so that one FMA a_ij - c_i r_j / piv per entry gives the
+  // Gauss-Jordan step everywhere: row k -> r_j / piv, column k -> -c_i / piv,
+  // pivot -> 1 / piv, the rest the rank-1 update.
   for (int k = 0; k < dim; ++k) {
     const int buf = k & 1;
     const int kq = k >> 4, kr = k & 15;
@@ -124,7 +129,12 @@ __global__ void __launch_bounds__(256, 2) k_schwarz_gj(
       for (int ii = 0; ii < T; ++ii)
         if (ii == kq) {
 #pragma unroll
-          for (int jj = 0; jj < T; ++jj) s_row[buf][tx + 16 * jj] = a[ii][jj];
+          for (int jj = 0; jj < T; ++jj) {
+            const bool pk = (tx == kr) && (jj == kq);
+            s_row[buf][tx + 16 * jj] = pk ? 1.0 : a[ii][jj];
+            if (pk) s_piv[buf] = a[ii][jj];
+            a[ii][jj] = 0.0;
+          }
         }
     }
     if (tx == kr) {
@@ -132,11 +142,14 @@ __global__ void __launch_bounds__(256, 2) k_schwarz_gj(
       for (int jj = 0; jj < T; ++jj)
         if (jj == kq) {
 #pragma unroll
-          for (int ii = 0; ii < T; ++ii) s_col[buf][ty + 16 * ii] = a[ii][jj];
+          for (int ii = 0; ii < T; ++ii) {
+            s_col[buf][ty + 16 * ii] = ((ty == kr) && (ii == kq)) ? -1.0 : a[ii][jj];
+            a[ii][jj] = 0.0;
+          }
         }
     }
     __syncthreads();
-    const double piv = s_row[buf][k];
+    const double piv = s_piv[buf];
     if (!(piv > 0.0) || !isfinite(piv)) {
       ok = false;
       break;
@@ -148,17 +161,9 @@ __global__ void __launch_bounds__(256, 2) k_schwarz_gj(
 #pragma unroll
     for (int ii = 0; ii < T; ++ii) ci[ii] = s_col[buf][ty + 16 * ii];
 #pragma unroll
-    for (int ii = 0; ii < T; ++ii) {
-      const bool rowk = (ii == kq) && (ty == kr);
+    for (int ii = 0; ii < T; ++ii)
 #pragma unroll
-      for (int jj = 0; jj < T; ++jj) {
-        const bool colk = (jj == kq) && (tx == kr);
-        double v = a[ii][jj] - ci[ii] * rj[jj];
-        if (rowk) v = colk ? inv : rj[jj];
-        else if (colk) v = -ci[ii] * inv;
-        a[ii][jj] = v;
-      }
-    }
+      for (int jj = 0; jj < T; ++jj) a[ii][jj] = __fma_rn(-ci[ii], rj[jj], a[ii][jj]);
   }
   double fi = 0.0;
   if (ok) {

@@ -80,6 +80,12 @@ class _Model:
         """8 / 16 / 32 lanes per node, +100 for the column-streaming traversal."""
         check(lib().hoefem_model_set_spmv_variant(self._h, int(variant)))
 
+    def set_stiffness_path(self, path="auto"):
+        """FP32 element stiffness implementation: "auto" (Tet10 blocks on the
+        tensor cores where they qualify) or "cuda_cores"
+        (hoefem_model_set_stiffness_path)."""
+        check(lib().hoefem_model_set_stiffness_path(self._h, _capi.STIFFNESS_PATH[path]))
+
     def set_cg_engine(self, engine="auto", schwarz_fp16=False, phase_profile=False):
         """CG engine of ConjugateGradient solves on this model ("auto",
         "chunked", "streamed"; see hoefem_model_set_cg_engine)."""
