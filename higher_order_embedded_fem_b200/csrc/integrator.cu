@@ -79,6 +79,34 @@ __global__ void k_scale(int n, double a, double* __restrict__ x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] *= a;
 }
 
+// Learned warm start on the device (w: [0] F.F, [1] d.J d, [2] d.F, [3] r0.r0,
+// [4] accepted, [5] rejected, [6] sum of sqrt(r0.r0 / F.F), [7] alpha).
+__global__ void k_warm_alpha(double* w) {
+  const double dJd = w[1], db = w[2];
+  w[7] = (dJd > 0.0 && db > 0.0) ? db / dJd : 0.0;
+}
+// r0 = F - alpha J d (r0 holds J d on entry)
+__global__ void k_warm_residual(int n, const double* __restrict__ w, double* __restrict__ r0,
+                                const double* __restrict__ F) {
+  const double a = w[7];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) r0[i] = -a * r0[i] + F[i];
+}
+// x = alpha d if alpha > 0 and ||r0|| < ||F|| (x is zero on entry); counters
+__global__ void k_warm_accept(int n, double* __restrict__ w, const double* __restrict__ d, double* __restrict__ x) {
+  const double a = w[7], rr = w[3], bb = w[0];
+  const bool keep = a > 0.0 && rr < bb;
+  if (keep)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = a * d[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (keep) {
+      w[4] += 1.0;
+      w[6] += sqrt(rr / bb);
+    } else {
+      w[5] += 1.0;
+    }
+  }
+}
+
 __global__ void k_neg(int n, double* __restrict__ x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] *= -1.0;
 }
@@ -127,9 +155,10 @@ struct Integrator {
   Learned* learned = nullptr;
   int learned_mode = 0;  // 0 off, 1 warm start, 2 collect (b, x*), 3 collect (b, x*) and CG iterates,
                          // 4 two-level preconditioner (flexible CG, FP64)
-  DBuf<double> x0, r0;
+  DBuf<double> x0, r0, lw;
+  cudaEvent_t lev[2] = {nullptr, nullptr};
+  bool lev_pending = false;
   std::vector<DBuf<double>*> snaps;  // collected (x_k, r_k) pairs of the current solve
-  double ratio_sum = 0.0;
   double rep_force = 0.0;
   // damping D = gamma M + alpha K_proj(u) from the (sub)step's initial state
   // (compute_damping_matrix_into, system_assembly.rs:145-193)
@@ -148,6 +177,8 @@ struct Integrator {
   ~Integrator() {
     if (h_scalar) cudaFreeHost(h_scalar);
     for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : lev)
       if (e) cudaEventDestroy(e);
   }
 
@@ -288,6 +319,7 @@ struct Integrator {
     HOEFEM_CUDA(cudaEventRecord(ev[1], s));
     HOEFEM_CUDA(cudaEventSynchronize(ev[1]));
     stats.ms_cg += elapsed();
+    account_warm_start();
     stats.num_cg_solves += 1;
     stats.total_cg_iterations += it;
     if (it > stats.max_cg_iterations) stats.max_cg_iterations = it;
@@ -303,31 +335,37 @@ struct Integrator {
   // scaled by the energy-optimal alpha = d.F / d.J d (the minimiser of the
   // J-norm error along d), kept only if ||F - alpha J d|| < ||F||.
   void warm_start(cudaStream_t s) {
+    // all on the device, no host synchronisation: the prediction from the
+    // residual and its norm, the energy-optimal scale, the guard, and x set
+    // only when the guard passes; the counters are read after the step
     const int n = (int)m->ndof;
-    HOEFEM_CUDA(cudaEventRecord(ev[0], s));
     if (x0.n < (size_t)n) { x0.alloc(n); r0.alloc(n); }
-    learned->predict(F.p, x0.p, s);
+    if (!lw.p) {
+      lw.alloc(8);
+      for (auto& e : lev) HOEFEM_CUDA(cudaEventCreate(&e));
+    }
+    HOEFEM_CUDA(cudaEventRecord(lev[0], s));
+    dot_device(F.p, F.p, n, lw.p + 0, partials.p, counter.p, s);
+    learned->predict_device(F.p, lw.p + 0, x0.p, s);
     spmv_node_rows(m->rows(), J.p, x0.p, r0.p, 1.0, 0.0, s);
-    const double dJd = dot(x0.p, r0.p), db = dot(x0.p, F.p), bb = norm_sq(F.p);
-    double rr = bb;
-    const double alpha = (dJd > 0.0 && db > 0.0) ? db / dJd : 0.0;
-    if (alpha > 0.0) {
-      // r0 = F - alpha J d, x0 = alpha d
-      (note_launch(), k_axpby<<<grid(), TPB, 0, s>>>(n, -alpha, r0.p, F.p));
-      (note_launch(), k_scale<<<grid(), TPB, 0, s>>>(n, alpha, x0.p));
-      rr = norm_sq(r0.p);
-    }
-    HOEFEM_CUDA(cudaEventRecord(ev[1], s));
-    HOEFEM_CUDA(cudaEventSynchronize(ev[1]));
-    stats.ms_learned += elapsed();
-    if (alpha > 0.0 && rr < bb) {
-      (note_launch(), k_copy<<<grid(), TPB, 0, s>>>(n, x0.p, cg.x.p));
-      stats.learned_accepted += 1;
-      ratio_sum += std::sqrt(rr / bb);
-      stats.learned_residual_ratio = ratio_sum / stats.learned_accepted;
-    } else {
-      stats.learned_rejected += 1;
-    }
+    dot_device(x0.p, r0.p, n, lw.p + 1, partials.p, counter.p, s);
+    dot_device(x0.p, F.p, n, lw.p + 2, partials.p, counter.p, s);
+    (note_launch(), k_warm_alpha<<<1, 1, 0, s>>>(lw.p));
+    (note_launch(), k_warm_residual<<<grid(), TPB, 0, s>>>(n, lw.p, r0.p, F.p));
+    dot_device(r0.p, r0.p, n, lw.p + 3, partials.p, counter.p, s);
+    (note_launch(), k_warm_accept<<<grid(), TPB, 0, s>>>(n, lw.p, x0.p, cg.x.p));
+    HOEFEM_CUDA(cudaEventRecord(lev[1], s));
+    lev_pending = true;
+  }
+
+  // Time of the last warm start (its events have completed once the solve has
+  // been waited for).
+  void account_warm_start() {
+    if (!lev_pending) return;
+    float ms = 0.f;
+    HOEFEM_CUDA(cudaEventElapsedTime(&ms, lev[0], lev[1]));
+    stats.ms_learned += ms;
+    lev_pending = false;
   }
 
   // Training-pair collection: snapshot (x_k, r_k) after every CG chunk.
@@ -429,7 +467,7 @@ struct Integrator {
     cudaStream_t s = m->stream;
     const int n = (int)m->ndof;
     stats = hoefem_step_stats{};
-    ratio_sum = 0.0;
+    if (lw.p) lw.zero(s);
     cg.stream_launches = 0;
     cg.stream_iterations = 0;
     cg.stream_ms_total = 0.0;
@@ -470,6 +508,13 @@ struct Integrator {
     float ms = 0.f;
     HOEFEM_CUDA(cudaEventElapsedTime(&ms, t0, t1));
     stats.ms_total = ms;
+    if (lw.p && learned_mode == 1) {
+      double h[8];
+      HOEFEM_CUDA(cudaMemcpy(h, lw.p, sizeof(h), cudaMemcpyDeviceToHost));
+      stats.learned_accepted += (i64)h[4];
+      stats.learned_rejected += (i64)h[5];
+      if (h[4] > 0.0) stats.learned_residual_ratio = h[6] / h[4];
+    }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     return result;

@@ -350,9 +350,12 @@ int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double 
    always the graphs; HOEFEM_CG_ENGINE_STREAMED: the streamed CG or
    HOEFEM_ERR_INVALID_ARGUMENT.  options (bit mask):
    HOEFEM_CG_SCHWARZ_FP16: in the mixed-precision form the streamed CG keeps
-   the Schwarz blocks in FP16 scaled by each block's largest magnitude
-   (products and sums stay FP64); HOEFEM_CG_PHASE_PROFILE: the streamed CG
-   records per-phase cycle counts (hoefem_cg_engine_stats.phase_us). */
+   the Schwarz blocks in FP16 scaled by each block's largest magnitude;
+   HOEFEM_CG_PHASE_PROFILE: the streamed CG records per-phase cycle counts
+   (hoefem_cg_engine_stats.phase_us).  In the mixed-precision form the
+   streamed CG multiplies the FP32 (or FP16) operator and Schwarz values with
+   an FP32 copy of the direction / residual and sums a row's products in FP32;
+   the vectors, the dot products and the CG recurrence stay FP64. */
 typedef enum {
   HOEFEM_CG_ENGINE_AUTO = 0,
   HOEFEM_CG_ENGINE_CHUNKED = 1,
