@@ -679,10 +679,18 @@ void launch_stiffness_staged(const Model& m, const Block& blk, const MatDev& mat
 }
 
 void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s,
-                      int precision) {
+                      int precision, bool assign) {
   init_pairs();
+  const bool f32 = precision == PRECISION_FP32;
+  if (assign) {
+    if (f32 && m.blocks.size() == 1 && stiffness_tc_eligible(m, *m.blocks[0])) {
+      launch_stiffness_tc(m, *m.blocks[0], mat, u, vals, s, true);
+      HOEFEM_CUDA(cudaGetLastError());
+      return;
+    }
+    HOEFEM_CUDA(cudaMemsetAsync(vals, 0, sizeof(double) * (size_t)m.nnz, s));
+  }
   for (const Block* bp : m.blocks) {
-    const bool f32 = precision == PRECISION_FP32;
     if (f32 && stiffness_tc_eligible(m, *bp)) {
       launch_stiffness_tc(m, *bp, mat, u, vals, s);
       continue;

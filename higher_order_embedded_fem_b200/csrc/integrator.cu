@@ -280,8 +280,7 @@ struct Integrator {
     const unsigned char* bcp = bc_nodes.empty() ? nullptr : bc.p;
     HOEFEM_CUDA(cudaEventRecord(ev[0], s));
     (note_launch(), k_be_state<<<grid(), TPB, 0, s>>>(n, up.p, vn.p, w.p, dt, bcp, us.p, vs.p));
-    K.zero(s);
-    launch_stiffness(*m, mat, us.p, K.p, s, precision);
+    launch_stiffness(*m, mat, us.p, K.p, s, precision, /*assign=*/true);
     // J = gamma M - beta D - alpha K with alpha = -dt^2, beta = -dt, gamma = 1
     jacobian_combination(*m, -(-dt * dt), K.p, 1.0, M.p, bcp, J.p, scalars.p + 4, s, -(-dt),
                          has_damping ? D.p : nullptr);

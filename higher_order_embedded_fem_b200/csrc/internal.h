@@ -133,7 +133,7 @@ struct Block {
   // tensor-core stiffness (stiffness_tc.cu), built on first use: the reference
   // gradient operator (TF32 hi / lo image), the per-slot gather map and the
   // element blocks
-  mutable DBuf<float> d_tc_psi, d_tc_ke;
+  mutable DBuf<float> d_tc_psi, d_tc_grad, d_tc_ke;
   mutable DBuf<int> d_tc_off, d_tc_ent;
   mutable int tc_nch = 0;
   mutable bool tc_ready = false;
@@ -180,16 +180,18 @@ struct MatDev {
 void launch_forces(const Model& m, const MatDev& mat, const double* u, double* f, cudaStream_t s);
 enum Precision { PRECISION_FP64 = 0, PRECISION_FP32 = 1 };
 // Element stiffness with the element arithmetic in FP64 or FP32; the CSR
-// values are accumulated in FP64 either way.
+// values are accumulated in FP64 either way.  Adds into vals, or with assign
+// stores K(u) (a single tensor-core block writes every entry; otherwise vals
+// is cleared first).
 void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s,
-                      int precision = PRECISION_FP64);
+                      int precision = PRECISION_FP64, bool assign = false);
 void launch_mass(const Model& m, double density, double* vals, cudaStream_t s);
 // Tensor-core Tet10 stiffness (stiffness_tc.cu): eligibility of a block for
 // FP32 element arithmetic, and the launch (element blocks on the tensor
 // cores, then the gather into vals, adding).
 bool stiffness_tc_eligible(const Model& m, const Block& blk);
 void launch_stiffness_tc(const Model& m, const Block& blk, const MatDev& mat, const double* u, double* vals,
-                         cudaStream_t s);
+                         cudaStream_t s, bool assign = false);
 // Stiffness with every element matrix projected onto PSD (negative eigenvalues
 // set to zero) before the colored scatter; adds into vals.
 void launch_stiffness_projected(Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s);

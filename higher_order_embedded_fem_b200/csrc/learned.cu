@@ -108,14 +108,30 @@ double mode_value(int k, double x, double y, double z, int& comp) {
 // ---- device kernels --------------------------------------------------------------
 constexpr int TPB = 256;
 
-// G[g] = psi_g . r   (one block per global mode)
-__global__ void k_global_proj(int n, const float* __restrict__ psi, const double* __restrict__ r, float* G) {
-  const float* p = psi + (size_t)blockIdx.x * n;
+// G[g] = psi_g . r in two deterministic passes: block (c, g) sums DOF chunk c
+// of mode g into part[g * C + c], then one thread per mode adds its C chunk
+// sums in chunk order (one block per mode alone was latency-bound: 29 blocks
+// for 29 x ndof products).
+constexpr int GP_CHUNKS = 32;
+static_assert(Learned::NG <= 32, "one warp sums the global modes");
+__global__ void k_global_proj(int n, const float* __restrict__ psi, const double* __restrict__ r,
+                              double* __restrict__ part) {
+  const int c = blockIdx.x, g = blockIdx.y;
+  const int chunk = (n + GP_CHUNKS - 1) / GP_CHUNKS;
+  const int i0 = c * chunk, i1 = min(n, i0 + chunk);
+  const float* p = psi + (size_t)g * n;
   double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += (double)p[i] * r[i];
+  for (int i = i0 + (int)threadIdx.x; i < i1; i += blockDim.x) acc += (double)p[i] * r[i];
   double v[1] = {acc};
   block_sum<1>(v);
-  if (threadIdx.x == 0) G[blockIdx.x] = (float)v[0];
+  if (threadIdx.x == 0) part[g * GP_CHUNKS + c] = v[0];
+}
+__global__ void k_global_proj_sum(int ng, const double* __restrict__ part, float* __restrict__ G) {
+  const int g = threadIdx.x;
+  if (g >= ng) return;
+  double s = 0.0;
+  for (int c = 0; c < GP_CHUNKS; ++c) s += part[g * GP_CHUNKS + c];
+  G[g] = (float)s;
 }
 
 // X[s] = [Phi_s^T r_s / rn, G / rn, centroid_s]
@@ -471,6 +487,7 @@ void Learned::setup(Model* model, const unsigned char* bc_mask, int num_sub, uin
   d_psi.upload(Gf, s);
   d_centroid.upload(centroid, s);
   d_gproj.alloc(NG);
+  d_gpart.alloc((size_t)NG * GP_CHUNKS);
   // MLP parameters (He initialisation, seeded)
   n_params = (size_t)F * H + H + (size_t)H * H + H + (size_t)H * NM + NM;
   std::vector<float> p0(n_params, 0.f);
@@ -514,7 +531,8 @@ void Learned::setup(Model* model, const unsigned char* bc_mask, int num_sub, uin
 double Learned::features(const double* r, float* Xout, cudaStream_t s) {
   const int ndof = (int)m->ndof;
   (note_launch(), k_norm<<<1, 1024, 0, s>>>(ndof, r, scal.p));
-  (note_launch(), k_global_proj<<<NG, 256, 0, s>>>(ndof, d_psi.p, r, d_gproj.p));
+  (note_launch(), k_global_proj<<<dim3(GP_CHUNKS, NG), 256, 0, s>>>(ndof, d_psi.p, r, d_gpart.p));
+  (note_launch(), k_global_proj_sum<<<1, 32, 0, s>>>(NG, d_gpart.p, d_gproj.p));
   (note_launch(), k_features<<<S, 256, 0, s>>>(S, d_sub_off.p, d_sub_dofs.p, d_phi.p, r, d_gproj.p, d_centroid.p,
                                                scal.p, Xout));
   HOEFEM_CUDA(cudaGetLastError());
@@ -714,7 +732,8 @@ void Learned::predict(const double* r, double* x0, cudaStream_t s) {
 void Learned::predict_device(const double* r, const double* rr, double* x0, cudaStream_t s) {
   const int ndof = (int)m->ndof;
   (note_launch(), k_sqrt_to<<<1, 1, 0, s>>>(rr, scal.p));
-  (note_launch(), k_global_proj<<<NG, 256, 0, s>>>(ndof, d_psi.p, r, d_gproj.p));
+  (note_launch(), k_global_proj<<<dim3(GP_CHUNKS, NG), 256, 0, s>>>(ndof, d_psi.p, r, d_gpart.p));
+  (note_launch(), k_global_proj_sum<<<1, 32, 0, s>>>(NG, d_gpart.p, d_gproj.p));
   (note_launch(), k_features<<<S, 256, 0, s>>>(S, d_sub_off.p, d_sub_dofs.p, d_phi.p, r, d_gproj.p, d_centroid.p,
                                                scal.p, X.p));
   (note_launch(), k_standardise<<<(S * F + 255) / 256, 256, 0, s>>>(S, F, x_mean.p, x_std.p, X.p));

@@ -24,6 +24,7 @@ struct Learned {
   DBuf<float> d_psi;        // global modes: NG x ndof
   DBuf<float> d_centroid;
   DBuf<float> d_gproj;      // NG global projections of the current residual
+  DBuf<double> d_gpart;     // their per-chunk partial sums
   // MLP (FP32 master weights, Adam moments); layout: W1 F x H, b1 H, W2 H x H, b2 H, W3 H x NM, b3 NM
   size_t n_params = 0;
   DBuf<float> params, grads, adam_m, adam_v;

@@ -67,8 +67,10 @@ constexpr int TC_MAXCH = 2;         // chunks (quadrature points <= 14)
 constexpr int TC_NP = 55;           // Tet10 node pairs I >= J
 constexpr int TC_M = 128, TC_N = 64, TC_KC = 64;
 constexpr int TC_ITEMS = TC_EPT * TC_PPC;  // (element, point) items per chunk
-constexpr int TC_ITEM_F = 40;       // floats per item: v[3][9], T[9], s1..s4
-constexpr int TC_EL_F = 48;         // floats per element: u[30], Ji[9], detJ, mu, lam, X[4x3] staged first
+constexpr int TC_QMAX = TC_PPC * TC_MAXCH;  // quadrature points per element
+constexpr int TC_TITEMS = TC_EPT * TC_QMAX; // (element, point) items per tile
+constexpr int TC_ITEM_F = 41;       // floats per item: v[3][9], T[9], s1..s4 (odd stride: no bank conflicts)
+constexpr int TC_EL_F = 44;         // floats per element: u[30], Ji[9], detJ, mu, lam (corners staged at 30..41 first)
 constexpr int EPI_WARPS = 4, MMA_WARP = 4, PROD_WARPS = 8;
 constexpr int PROD0 = 32 * (EPI_WARPS + 1);
 constexpr int PRODUCERS = 32 * PROD_WARPS;
@@ -78,12 +80,11 @@ constexpr int B_SPLIT = TC_N * TC_KC * 4;      // 16 KB: one split of one chunk 
 constexpr int OFF_B = 0;                                   // B: [hi, lo][chunk] 64 KB
 constexpr int OFF_A = OFF_B + 2 * TC_MAXCH * B_SPLIT;      // A: [buffer][hi, lo] 128 KB
 constexpr int OFF_ITEM = OFF_A + 2 * 2 * A_SPLIT;
-constexpr int OFF_EL = OFF_ITEM + TC_ITEMS * TC_ITEM_F * 4;
-constexpr int OFF_X = OFF_EL + TC_EPT * TC_EL_F * 4;       // corners, 14 x 12 floats
-constexpr size_t TC_SMEM = (size_t)OFF_X + TC_EPT * 12 * 4;
+constexpr int OFF_EL = OFF_ITEM + TC_TITEMS * TC_ITEM_F * 4;
+constexpr size_t TC_SMEM = (size_t)OFF_EL + TC_EPT * TC_EL_F * 4;
 constexpr int TMEM_COLS = 2 * TC_N;
-static_assert(TC_SMEM <= 227 * 1024, "shared memory");
-static_assert(TC_ITEMS <= PRODUCERS, "one producer thread per item");
+static_assert(TC_SMEM + 256 <= 227 * 1024, "shared memory (dynamic + static)");
+static_assert(TC_TITEMS <= PRODUCERS, "one producer thread per item of a tile");
 
 // Byte offset of (row, k) in a K-major no-swizzle UMMA operand tile with 64
 // K columns: 8 x 16-byte core matrices, K-adjacent core matrices 128 B apart
@@ -148,6 +149,7 @@ struct TcArgs {
   const double* X;
   const double* u;
   const float* psi;  // [hi, lo][chunk][B_SPLIT / 4]
+  const float* grad; // reference gradients [point][node][3]
   float* ke;         // [ne][55][9]
   MatDev mat;
   int* err;
@@ -156,7 +158,7 @@ struct TcArgs {
 };
 
 __global__ void __launch_bounds__(TC_THREADS, 1) k_stiffness_tc(TcArgs A) {
-  extern __shared__ __align__(1024) unsigned char sm[];
+  extern __shared__ __align__(128) unsigned char sm[];
   __shared__ __align__(8) uint64_t afull[2], afree[2], accfull[2], accfree[2];
   __shared__ uint32_t s_tmem;
   __shared__ volatile int s_abort;
@@ -211,14 +213,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_stiffness_tc(TcArgs A) {
     const int pt = threadIdx.x - PROD0;
     float* s_item = reinterpret_cast<float*>(sm + OFF_ITEM);
     float* s_el = reinterpret_cast<float*>(sm + OFF_EL);
-    float* s_X = reinterpret_cast<float*>(sm + OFF_X);
     for (int g = 0; g < nchunks && !s_abort; ++g) {
       const int tl = g / nch, c = g % nch;
       const int tile = (int)blockIdx.x + tl * (int)gridDim.x;
       const int e0 = tile * TC_EPT;
       const int nel = min(TC_EPT, b.ne - e0);
       if (c == 0) {
-        // element data of the tile: node displacements, corners, J^-1, det J
+        // element data of the tile: node displacements and corners, then
+        // J^-1, det J and the Lame parameters (over the corners)
         for (int x = pt; x < nel * 10; x += PRODUCERS) {
           const int el = x / 10, I = x % 10;
           const int gn = b.conn[I * b.ne + e0 + el];
@@ -226,15 +228,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_stiffness_tc(TcArgs A) {
           for (int k = 0; k < 3; ++k) s_el[el * TC_EL_F + 3 * I + k] = (float)A.u[3 * gn + k];
           if (I < 4) {
 #pragma unroll
-            for (int k = 0; k < 3; ++k) s_X[el * 12 + 3 * I + k] = (float)A.X[3 * gn + k];
+            for (int k = 0; k < 3; ++k) s_el[el * TC_EL_F + 30 + 3 * I + k] = (float)A.X[3 * gn + k];
           }
         }
         pipe::named_sync(1, PRODUCERS);
         if (pt < nel) {
-          float J[9], Ji[9];
-          tet4_jacobian(s_X + pt * 12, J);
-          const float dJ = inv3(J, Ji);
           float* E = s_el + pt * TC_EL_F;
+          float X[12], J[9], Ji[9];
+#pragma unroll
+          for (int k = 0; k < 12; ++k) X[k] = E[30 + k];
+          tet4_jacobian(X, J);
+          const float dJ = inv3(J, Ji);
 #pragma unroll
           for (int k = 0; k < 9; ++k) E[30 + k] = Ji[k];
           E[39] = dJ;
@@ -243,31 +247,35 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_stiffness_tc(TcArgs A) {
           E[41] = (float)(b.emat ? b.emat[2 * e + 1] : A.mat.lambda);
         }
         pipe::named_sync(1, PRODUCERS);
-      }
-      // stage 1: per (element, point) state of this chunk
-      {
-        const int el = pt / TC_PPC, ql = pt % TC_PPC, q = c * TC_PPC + ql;
-        if (pt < TC_ITEMS && el < nel && q < b.nq) {
+        // stage 1: the state of every (element, point) item of the tile, item
+        // el * 14 + q: F = I + H J^-1 with H = sum_I u_I (dN_I/dxi)^T, the
+        // material, the vectors a^(m), F a^(m), M1 a^(m) and the pair scalars
+        const int el = pt / TC_QMAX, q = pt % TC_QMAX;
+        if (pt < TC_TITEMS && el < nel && q < b.nq) {
           const float* E = s_el + el * TC_EL_F;
-          const float xi[3] = {(float)b.qp[3 * q], (float)b.qp[3 * q + 1], (float)b.qp[3 * q + 2]};
           const float w = (float)b.qw[q];
           const float* Ji = E + 30;
           const float dJ = E[39];
-          float F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+          const float* gq = A.grad + q * 30;
+          float H[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
           for (int I = 0; I < 10; ++I) {
-            float gr[3], G[3];
-            tet10_grad(I, xi, gr);
+            const float g0 = __ldg(gq + 3 * I), g1 = __ldg(gq + 3 * I + 1), g2 = __ldg(gq + 3 * I + 2);
 #pragma unroll
-            for (int k = 0; k < 3; ++k) G[k] = Ji[k] * gr[0] + Ji[3 + k] * gr[1] + Ji[6 + k] * gr[2];
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc)
-#pragma unroll
-              for (int k = 0; k < 3; ++k) F[3 * cc + k] += E[3 * I + cc] * G[k];
+            for (int cc = 0; cc < 3; ++cc) {
+              const float uc = E[3 * I + cc];
+              H[3 * cc] += uc * g0;
+              H[3 * cc + 1] += uc * g1;
+              H[3 * cc + 2] += uc * g2;
+            }
           }
-          F[0] += 1.f;
-          F[4] += 1.f;
-          F[8] += 1.f;
+          float F[9];
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+              F[3 * cc + k] = H[3 * cc] * Ji[k] + H[3 * cc + 1] * Ji[3 + k] + H[3 * cc + 2] * Ji[6 + k] +
+                              (cc == k ? 1.f : 0.f);
           QpState<float> st;
           float* it = s_item + pt * TC_ITEM_F;
           if (dJ == 0.f || !material_state(A.mat.kind, F, E[40], E[41], st, false)) {
@@ -305,9 +313,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_stiffness_tc(TcArgs A) {
       // stage 2: the 9 pair blocks (m, n) of every item, split into hi / lo
       float* a_hi = reinterpret_cast<float*>(sm + OFF_A + bi * 2 * A_SPLIT);
       float* a_lo = reinterpret_cast<float*>(sm + OFF_A + bi * 2 * A_SPLIT + A_SPLIT);
+      // task = (ql * 9 + mn) * 14 + el: the lanes of a warp take different
+      // elements of one (point, m, n), so their stores land in different banks
       for (int task = pt; task < TC_ITEMS * 9; task += PRODUCERS) {
-        const int item = task / 9, mn = task % 9;
-        const int el = item / TC_PPC, ql = item % TC_PPC, q = c * TC_PPC + ql;
+        const int el = task % TC_EPT, r2 = task / TC_EPT;
+        const int mn = r2 % 9, ql = r2 / 9, q = c * TC_PPC + ql;
+        const int item = el * TC_QMAX + q;
         if (el >= nel || q >= b.nq) continue;
         const float* it = s_item + item * TC_ITEM_F;
         QpPair<float> qp;
@@ -409,12 +420,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_stiffness_tc(TcArgs A) {
   }
 }
 
+constexpr int GU = 2;  // contributions loaded together in the gather
+
 // Warp per node row: every 3 x 3 block of the row summed over its element
-// contributions (element order), added into the CSR values.
+// contributions (element order), added into the CSR values (assign: stored).
 __global__ void __launch_bounds__(256) k_stiffness_gather(int nv, const int* __restrict__ adj_off,
                                                           const long long* __restrict__ base,
                                                           const int* __restrict__ off, const int* __restrict__ ent,
-                                                          const float* __restrict__ ke, double* __restrict__ vals) {
+                                                          const float* __restrict__ ke, double* __restrict__ vals,
+                                                          int assign) {
   const int a = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (a >= nv) return;
   const int s0 = adj_off[a], deg = adj_off[a + 1] - s0;
@@ -422,29 +436,43 @@ __global__ void __launch_bounds__(256) k_stiffness_gather(int nv, const int* __r
   double* row = vals + base[a];
   for (int s = lane; s < deg; s += 32) {
     const int k0 = off[s0 + s], k1 = off[s0 + s + 1];
-    if (k0 == k1) continue;
+    if (k0 == k1 && !assign) continue;
     double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int k = k0; k < k1; ++k) {
-      const int code = ent[k];
-      const float* kb = ke + (size_t)(code >> 1) * 9;
-      float v[9];
+    // two contributions at a time: their codes, then all their loads, then
+    // the sums in contribution order
+    for (int k = k0; k < k1; k += GU) {
+      int code[GU];
 #pragma unroll
-      for (int i = 0; i < 9; ++i) v[i] = __ldg(kb + i);
-      if (code & 1) {
+      for (int u = 0; u < GU; ++u) code[u] = k + u < k1 ? __ldg(ent + k + u) : -1;
+      float v[GU][9];
 #pragma unroll
-        for (int i = 0; i < 3; ++i)
+      for (int u = 0; u < GU; ++u) {
+        const float* kb = ke + (size_t)(code[u] >> 1) * 9;
 #pragma unroll
-          for (int j = 0; j < 3; ++j) acc[3 * i + j] += (double)v[3 * j + i];
-      } else {
+        for (int i = 0; i < 9; ++i) v[u][i] = code[u] >= 0 ? __ldg(kb + i) : 0.f;
+      }
 #pragma unroll
-        for (int i = 0; i < 9; ++i) acc[i] += (double)v[i];
+      for (int u = 0; u < GU; ++u) {
+        if (code[u] < 0) break;
+        if (code[u] & 1) {
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) acc[3 * i + j] += (double)v[u][3 * j + i];
+        } else {
+#pragma unroll
+          for (int i = 0; i < 9; ++i) acc[i] += (double)v[u][i];
+        }
       }
     }
     double* o = row + 3 * s;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) o[i * rl + j] += acc[3 * i + j];
+      for (int j = 0; j < 3; ++j) {
+        if (assign) o[i * rl + j] = acc[3 * i + j];
+        else o[i * rl + j] += acc[3 * i + j];
+      }
   }
 }
 
@@ -513,6 +541,15 @@ void prepare_tc(const Model& m, const Block& blk, cudaStream_t s) {
         }
     }
   blk.d_tc_psi.upload(img, s);
+  // reference gradients per point and node (FP32), read by the point states
+  std::vector<float> grad((size_t)nq * 30);
+  for (int q = 0; q < nq; ++q)
+    for (int I = 0; I < 10; ++I) {
+      double g[3];
+      tet10_grad_host(I, &blk.qp[3 * q], g);
+      for (int k = 0; k < 3; ++k) grad[(size_t)q * 30 + 3 * I + k] = (float)g[k];
+    }
+  blk.d_tc_grad.upload(grad, s);
   // gather map: per pattern slot, (element, pair, transposed) in element order
   const size_t nslot = m.adj.size();
   HOEFEM_REQUIRE(blk.ne * (i64)TC_NP * 2 < (i64)2147483647, HOEFEM_ERR_INVALID_ARGUMENT,
@@ -560,7 +597,7 @@ bool stiffness_tc_eligible(const Model& m, const Block& blk) {
 }
 
 void launch_stiffness_tc(const Model& m, const Block& blk, const MatDev& mat, const double* u, double* vals,
-                         cudaStream_t s) {
+                         cudaStream_t s, bool assign) {
   if (!blk.tc_ready) prepare_tc(m, blk, s);
   static bool attr[64] = {};
   int dev = 0;
@@ -574,6 +611,7 @@ void launch_stiffness_tc(const Model& m, const Block& blk, const MatDev& mat, co
   a.X = m.d_X.p;
   a.u = u;
   a.psi = blk.d_tc_psi.p;
+  a.grad = blk.d_tc_grad.p;
   a.ke = blk.d_tc_ke.p;
   a.mat = mat;
   a.err = m.d_err.p;
@@ -584,7 +622,8 @@ void launch_stiffness_tc(const Model& m, const Block& blk, const MatDev& mat, co
   HOEFEM_CUDA(cudaGetLastError());
   const int nv = (int)m.nv;
   (note_launch(), k_stiffness_gather<<<(nv + 7) / 8, 256, 0, s>>>(nv, m.d_adj_off.p, m.d_base.p, blk.d_tc_off.p,
-                                                                     blk.d_tc_ent.p, blk.d_tc_ke.p, vals));
+                                                                     blk.d_tc_ent.p, blk.d_tc_ke.p, vals,
+                                                                     assign ? 1 : 0));
   HOEFEM_CUDA(cudaGetLastError());
 }
 
