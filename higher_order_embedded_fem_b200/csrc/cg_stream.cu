@@ -888,38 +888,7 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
     ++tile_id;
   }
   std::vector<int> off, nrange(G + 1);
-  if (sw && G > 1) {
-    // 2G contiguous chunks of about equal operator bytes; CTA g takes the
-    // chunk with the g-th most Schwarz row entries and the one with the g-th
-    // fewest, so that both phases of an iteration are balanced (contiguous
-    // ranges alone leave the Schwarz work of the busiest CTA ~1.5x the mean
-    // on the benchmark cylinder)
-    std::vector<int> coff;
-    split_items(items, 2 * G, coff);
-    std::vector<long long> csw(2 * G, 0);
-    for (int c = 0; c < 2 * G; ++c)
-      for (int j = coff[c]; j < coff[c + 1]; ++j)
-        for (i64 q = items[j].c; q < items[j].c + items[j].b; ++q)
-          for (int k = pair_off[q]; k < pair_off[q + 1]; ++k)
-            csw[c] += 9LL * (P->sub_off[slot_sub[k] + 1] - P->sub_off[slot_sub[k]]);
-    std::vector<int> order(2 * G);
-    for (int c = 0; c < 2 * G; ++c) order[c] = c;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return csw[x] > csw[y]; });
-    std::vector<CgsItem> paired;
-    paired.reserve(items.size());
-    off.assign(G + 1, 0);
-    for (int g = 0; g < G; ++g) {
-      off[g] = (int)paired.size();
-      int c0 = order[g], c1 = order[2 * G - 1 - g];
-      if (c1 < c0) std::swap(c0, c1);
-      for (int c : {c0, c1})
-        for (int j = coff[c]; j < coff[c + 1]; ++j) paired.push_back(items[j]);
-    }
-    off[G] = (int)paired.size();
-    items.swap(paired);
-  } else {
-    split_items(items, G, off);
-  }
+  split_items(items, G, off);
   for (int g = 0; g <= G; ++g) nrange[g] = off[g] < (int)items.size() ? items[off[g]].c : (int)nv;
   // segments: halo-local neighbour indices (sorted halo, times 3), own halo index
   std::vector<CgsSeg> segs;
@@ -937,8 +906,6 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
       int j1 = j, inc = 0;
       while (j1 < off[g + 1]) {
         const CgsItem& it = items[j1];
-        // a segment covers consecutive nodes (a CTA may hold two node ranges)
-        if (j1 > j && it.c != items[j1 - 1].c + items[j1 - 1].b) break;
         int add = 0, tinc = 0;
         for (i64 q = it.c; q < it.c + it.b; ++q) {
           tinc += incid(q);

@@ -26,7 +26,7 @@
 // FP32 in tensor memory (the dropped lo.lo term is below FP32 rounding).
 //
 // The kernel (one CTA per SM, persistent over the element tiles):
-//   8 producer warps: per K chunk, the per-point state (F, material, the
+//   16 producer warps: per K chunk, the per-point state (F, material, the
 //     vectors a, F a, M1 a of m = 0..2) of the chunk's 98 (element, point)
 //     items, then the 9 pair blocks of each item, split, into the chunk's A
 //     operand (hi, lo) in the UMMA K-major no-swizzle layout; two chunk
@@ -71,10 +71,10 @@ constexpr int TC_QMAX = TC_PPC * TC_MAXCH;  // quadrature points per element
 constexpr int TC_TITEMS = TC_EPT * TC_QMAX; // (element, point) items per tile
 constexpr int TC_ITEM_F = 41;       // floats per item: v[3][9], T[9], s1..s4 (odd stride: no bank conflicts)
 constexpr int TC_EL_F = 44;         // floats per element: u[30], Ji[9], detJ, mu, lam (corners staged at 30..41 first)
-constexpr int EPI_WARPS = 4, MMA_WARP = 4, PROD_WARPS = 8;
+constexpr int EPI_WARPS = 4, MMA_WARP = 4, PROD_WARPS = 16;
 constexpr int PROD0 = 32 * (EPI_WARPS + 1);
 constexpr int PRODUCERS = 32 * PROD_WARPS;
-constexpr int TC_THREADS = PROD0 + PRODUCERS;  // 416
+constexpr int TC_THREADS = PROD0 + PRODUCERS;  // 672
 constexpr int A_SPLIT = TC_M * TC_KC * 4;      // 32 KB: one split of one chunk buffer
 constexpr int B_SPLIT = TC_N * TC_KC * 4;      // 16 KB: one split of one chunk of Psi
 constexpr int OFF_B = 0;                                   // B: [hi, lo][chunk] 64 KB
