@@ -213,6 +213,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_stiffness_tc(TcArgs A) {
     const int pt = threadIdx.x - PROD0;
     float* s_item = reinterpret_cast<float*>(sm + OFF_ITEM);
     float* s_el = reinterpret_cast<float*>(sm + OFF_EL);
+    // the next tile's node displacements and corners are loaded into
+    // registers one tile ahead (producer thread pt < 140 holds node pt % 10 of
+    // element pt / 10), so their global latency overlaps the current tile
+    static_assert(TC_EPT * 10 <= PRODUCERS, "one producer thread per element node");
+    double pu[3] = {0, 0, 0}, px[3] = {0, 0, 0};
+    auto prefetch = [&](int tile) {
+      const int e0 = tile * TC_EPT;
+      if (tile < A.ntiles && pt < min(TC_EPT, b.ne - e0) * 10) {
+        const int el = pt / 10, I = pt % 10;
+        const int gn = b.conn[I * b.ne + e0 + el];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) pu[k] = A.u[3 * gn + k];
+        if (I < 4) {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) px[k] = A.X[3 * gn + k];
+        }
+      }
+    };
+    prefetch((int)blockIdx.x);
     for (int g = 0; g < nchunks && !s_abort; ++g) {
       const int tl = g / nch, c = g % nch;
       const int tile = (int)blockIdx.x + tl * (int)gridDim.x;
@@ -221,16 +240,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_stiffness_tc(TcArgs A) {
       if (c == 0) {
         // element data of the tile: node displacements and corners, then
         // J^-1, det J and the Lame parameters (over the corners)
-        for (int x = pt; x < nel * 10; x += PRODUCERS) {
-          const int el = x / 10, I = x % 10;
-          const int gn = b.conn[I * b.ne + e0 + el];
+        if (pt < nel * 10) {
+          const int el = pt / 10, I = pt % 10;
 #pragma unroll
-          for (int k = 0; k < 3; ++k) s_el[el * TC_EL_F + 3 * I + k] = (float)A.u[3 * gn + k];
+          for (int k = 0; k < 3; ++k) s_el[el * TC_EL_F + 3 * I + k] = (float)pu[k];
           if (I < 4) {
 #pragma unroll
-            for (int k = 0; k < 3; ++k) s_el[el * TC_EL_F + 30 + 3 * I + k] = (float)A.X[3 * gn + k];
+            for (int k = 0; k < 3; ++k) s_el[el * TC_EL_F + 30 + 3 * I + k] = (float)px[k];
           }
         }
+        prefetch(tile + (int)gridDim.x);
         pipe::named_sync(1, PRODUCERS);
         if (pt < nel) {
           float* E = s_el + pt * TC_EL_F;
