@@ -652,7 +652,10 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
       const i64 it0 = w.h_st->iters;
       cg_stream_iterate(w, f32, P, p32, A64 != nullptr, s);
       w.stream_iterations += w.h_st->iters - it0;
-      if (A64) {
+      // a launch that ran no iteration found the solve finished by the
+      // replacement before it
+      const bool ran = w.h_st->iters > it0;
+      if (A64 && ran) {
         const bool conv = w.h_st->done && w.h_st->status == HOEFEM_OK;
         const bool trig = !w.h_st->done && w.h_st->replace;
         if (conv || trig) {
@@ -660,12 +663,13 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
           true_residual(A64);
           prec_init();
           // resume after a converged recurrence: beta = z.r / z.r_old; the
-          // kernel forms the direction z + beta p itself
+          // kernel forms the direction z + beta p itself.  No host round trip
+          // here: if the true residual meets the tolerance, the next launch
+          // returns at once and the loop ends on its state.
           (note_launch(), k_cg_reliable<<<1, 1, 0, s>>>(w.st.p, conv ? 1 : 0));
           cg_stream_arm(w, delta, s);
-          HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
-          HOEFEM_CUDA(cudaStreamSynchronize(s));
           ++nrep_s;
+          continue;
         }
       }
       if (w.h_st->done) break;

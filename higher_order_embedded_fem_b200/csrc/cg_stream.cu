@@ -232,6 +232,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_cg_stream(Args A) {
   __shared__ double s_red[NW][2];
   __shared__ double s_bc[3];
   __shared__ unsigned long long s_prof[16];
+  // a solve that an earlier kernel finished (the true residual after a
+  // replacement met the tolerance) runs no iteration: uniform over the grid
+  if (*(const volatile int*)&A.st->done) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = blockIdx.x, G = gridDim.x;
   if (threadIdx.x == 0) {
