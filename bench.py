@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--roofline-reps", type=int, default=20)
-    ap.add_argument("--delta", type=float, default=0.1, help="mixed variant: reliable-update threshold")
+    ap.add_argument("--delta", type=float, default=1e-3,
+                    help="mixed variant: reliable-update threshold (residual drop between FP64 replacements)")
     ap.add_argument("--cg-engine", default="auto", choices=["auto", "chunked", "streamed"],
                     help="CG engine of the Jacobian solves (hoefem_integrator_set_cg_engine)")
     ap.add_argument("--schwarz-fp16", action="store_true", help="mixed variants: FP16 Schwarz blocks in the streamed CG")

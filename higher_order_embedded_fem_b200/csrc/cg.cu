@@ -558,6 +558,17 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   const int n = (int)w.n;
   const int kind = P ? P->kind : PREC_NONE;
   HOEFEM_REQUIRE(!P || P->ready, HOEFEM_ERR_INVALID_ARGUMENT, "preconditioner has not been updated");
+  // automatic engine choice: each engine's first solve builds its one-time
+  // structures (graphs, stream layouts) and is not timed; its second solve of
+  // at least 20 iterations is timed whole (set-up, packing, replacements and
+  // launches included), per iteration
+  const int pk = !P ? 0 : (P->kind == PREC_DIAGONAL ? 1 : 2);
+  CgWork::EngineTune& et = w.etune[(A.v32 != nullptr ? 3 : 0) + pk];
+  if (!w.tev[0]) {
+    HOEFEM_CUDA(cudaEventCreate(&w.tev[0]));
+    HOEFEM_CUDA(cudaEventCreate(&w.tev[1]));
+  }
+  if (w.stream_mode == 0 && et.choice < 0) HOEFEM_CUDA(cudaEventRecord(w.tev[0], s));
   CgState init{};
   init.tol = tol;
   init.max_iter = max_iter;
@@ -615,35 +626,31 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   // persistent streamed CG: the operator (FP64 values, FP32 in the mixed
   // form) and the Schwarz blocks packed into their stream layouts, then one
   // launch per residual replacement
-  const int pk = !P ? 0 : (P->kind == PREC_DIAGONAL ? 1 : 2);
-  CgWork::EngineTune& et = w.etune[(f32 ? 3 : 0) + pk];
   w.last_tune = (f32 ? 3 : 0) + pk;
   bool want_stream = w.stream_mode == 2;
-  if (w.stream_mode == 0) want_stream = et.choice >= 0 ? et.choice == 1 : et.phase == 1;
+  if (w.stream_mode == 0) want_stream = et.choice >= 0 ? et.choice == 1 : et.phase >= 2;
   const bool streamed =
       want_stream && vals64 && cg_stream_usable(w, P) && cg_stream_prepare(w, vals64, f32, P, p32, s);
   HOEFEM_REQUIRE(streamed || w.stream_mode != 2, HOEFEM_ERR_INVALID_ARGUMENT,
                  "the streamed CG cannot run this solve (preconditioner, device or layout)");
   if (w.stream_mode == 0 && want_stream && !streamed) et.choice = 0;  // cannot stream: chunked from now on
-  if (!w.tev[0]) {
-    HOEFEM_CUDA(cudaEventCreate(&w.tev[0]));
-    HOEFEM_CUDA(cudaEventCreate(&w.tev[1]));
-  }
-  // automatic engine choice: one timed sample per engine (iteration loop only)
-  const i64 it_start = w.h_st->iters;
+  // phases: 0 chunked set-up solve, 1 chunked timed, 2 streamed set-up, 3 streamed timed
   auto sample = [&](int engine) {
-    if (w.stream_mode != 0 || et.choice >= 0 || et.phase != engine) return;
+    if (w.stream_mode != 0 || et.choice >= 0 || (et.phase >= 2) != (engine == 1)) return;
+    if ((et.phase & 1) == 0) {
+      ++et.phase;
+      return;
+    }
     HOEFEM_CUDA(cudaEventRecord(w.tev[1], s));
     HOEFEM_CUDA(cudaEventSynchronize(w.tev[1]));
-    const i64 n_it = w.h_st->iters - it_start;
+    const i64 n_it = w.h_st->iters;
     if (n_it < 20) return;
     float ms = 0.f;
     HOEFEM_CUDA(cudaEventElapsedTime(&ms, w.tev[0], w.tev[1]));
     et.us_per_it[engine] = 1e3 * ms / (double)n_it;
-    if (++et.phase == 2) et.choice = et.us_per_it[1] < et.us_per_it[0] ? 1 : 0;
+    if (++et.phase == 4) et.choice = et.us_per_it[1] < et.us_per_it[0] ? 1 : 0;
   };
   if (streamed) {
-    HOEFEM_CUDA(cudaEventRecord(w.tev[0], s));
     cg_stream_arm(w, A64 ? delta : 0.0, s);
     w.stream_ms = 0.f;
     const i64 cap_s = max_iter >= 0 ? max_iter : 10 * (i64)n;
@@ -711,7 +718,6 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   double rr_ref = w.h_st->rr;
   // the engine sample of this solve counts only if the SpMV variants were already tuned
   const bool sample_chunked = tu.done;
-  HOEFEM_CUDA(cudaEventRecord(w.tev[0], s));
   i64 nrep = 0;
   for (i64 c = 0; c < max_chunks; ++c) {
     const i64 it0 = w.h_st->iters;

@@ -180,7 +180,7 @@ struct CgWork {
   // engine (once its SpMV variants are tuned), then on the streamed one; the
   // faster per-iteration time decides for the later solves
   struct EngineTune {
-    int phase = 0;  // 0: sample chunked, 1: sample streamed, 2: decided
+    int phase = 0;  // 0 / 1: chunked set-up / timed solve, 2 / 3: streamed set-up / timed, 4: decided
     double us_per_it[2] = {0.0, 0.0};
     int choice = -1;  // 0 chunked, 1 streamed
   };

@@ -250,9 +250,10 @@ class NewtonCgIntegrator3d:
         check(lib().hoefem_integrator_set_learned(self._h, learned._h if learned is not None else None,
                                                   int(mode) if learned is not None else 0))
 
-    def set_precision(self, mixed, delta=0.1):
+    def set_precision(self, mixed, delta=1e-3):
         """mixed=True: FP32 element stiffness, FP32 operator / Schwarz apply in
-        a reliable-update PCG with FP64 vectors (see
+        a reliable-update PCG with FP64 vectors, the recurrence residual
+        replaced by the FP64 one after every drop by `delta` (see
         hoefem_integrator_set_precision)."""
         check(lib().hoefem_integrator_set_precision(self._h, 1 if mixed else 0, float(delta)))
 

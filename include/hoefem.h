@@ -271,8 +271,12 @@ int hoefem_cg_solve(hoefem_model m, const double* system_values, hoefem_precond 
    preconditioner values; vectors, dot products and residual updates FP64.
    The recurrence residual is replaced by the true FP64 residual b - A x
    (reliable update) whenever it has dropped by the factor `delta` (0 < delta
-   < 1, e.g. 0.1) since the last replacement, and before the solve stops, so
-   ||b - A x|| <= tol ||b|| holds in FP64.  No counterpart in the reference. */
+   < 1) since the last replacement, and before the solve stops, so
+   ||b - A x|| <= tol ||b|| holds in FP64.  Each replacement costs an FP64
+   operator product and a preconditioner apply (and, on the streamed engine, a
+   new launch): on the benchmark cylinder delta = 1e-3 needs 3 launches per
+   solve instead of 7 at 0.1, with the same iteration count.  No counterpart
+   in the reference. */
 int hoefem_cg_solve_mixed(hoefem_model m, const double* system_values, hoefem_precond p, const double* b, double* x,
                           double tol, int64_t max_iter, double delta, int64_t* iterations, int mem);
 
@@ -344,9 +348,11 @@ int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double 
    kernel chunks, and the persistent streamed CG (one cooperative launch per
    solve, the operator and the Schwarz blocks streamed through shared memory;
    for no preconditioner, diagonal, or Schwarz with subdomains of at most 27
-   nodes).  HOEFEM_CG_ENGINE_AUTO (default): the first solves with at least
-   20 iterations are timed on each engine, per operator precision and
-   preconditioner kind, and the faster one is kept; HOEFEM_CG_ENGINE_CHUNKED:
+   nodes).  HOEFEM_CG_ENGINE_AUTO (default): per operator precision and
+   preconditioner kind, each engine's first solve sets it up (graphs, stream
+   layouts) and its next solve of at least 20 iterations is timed whole
+   (the solve's set-up, value packing, residual replacements and launches
+   included); the engine with the lower time per iteration is kept; HOEFEM_CG_ENGINE_CHUNKED:
    always the graphs; HOEFEM_CG_ENGINE_STREAMED: the streamed CG or
    HOEFEM_ERR_INVALID_ARGUMENT.  options (bit mask):
    HOEFEM_CG_SCHWARZ_FP16: in the mixed-precision form the streamed CG keeps
@@ -374,8 +380,8 @@ int hoefem_model_set_cg_engine(hoefem_model m, int engine, int options);
    barrier after the Schwarz products, [8] own-DOF update, [9] grid barrier
    and reductions after it, [10] producer waiting for free stages, [11]
    producer lifetime.  Automatic engine choice for the last solve's operator
-   precision and preconditioner kind: the sampled microseconds per iteration
-   of the chunked and the streamed engine (0 until sampled) and the choice
+   precision and preconditioner kind: the sampled whole-solve microseconds per
+   iteration of the chunked and the streamed engine (0 until sampled) and the choice
    (-1 undecided, 0 chunked, 1 streamed). */
 typedef struct {
   int64_t launches, iterations;

@@ -199,7 +199,9 @@ def test_auto_engine_times_both_engines_and_keeps_the_faster():
     m, ref, P, J, b = schwarz_system(8)
     m.set_cg_engine("auto")
     xs = []
-    for _ in range(5):
+    # per engine one set-up solve and one timed solve (after the chunked
+    # engine's online SpMV-variant tuning)
+    for _ in range(8):
         x = np.zeros(m.ndof())
         (H.ConjugateGradient(m).with_operator(J).with_preconditioner(P)
          .with_stopping_criterion(H.RelativeResidualCriterion(1e-8)).with_max_iter(5000).solve_with_guess(b, x))
