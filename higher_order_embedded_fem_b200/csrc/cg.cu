@@ -564,6 +564,11 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   // launches included), per iteration
   const int pk = !P ? 0 : (P->kind == PREC_DIAGONAL ? 1 : 2);
   CgWork::EngineTune& et = w.etune[(A.v32 != nullptr ? 3 : 0) + pk];
+  // below ~220 nodes per SM the streamed kernel's two grid barriers per
+  // iteration cost more than the graphs' launches, and sampling it (a stream
+  // layout built on the host) costs more than a short-lived solver can win:
+  // the chunked engine without sampling
+  if (w.stream_mode == 0 && et.choice < 0 && w.m->nv < (i64)CgWork::STREAM_MIN_NODES) et.choice = 0;
   if (!w.tev[0]) {
     HOEFEM_CUDA(cudaEventCreate(&w.tev[0]));
     HOEFEM_CUDA(cudaEventCreate(&w.tev[1]));

@@ -179,6 +179,8 @@ struct CgWork {
   // the first solves with at least 20 iterations are timed on the chunked
   // engine (once its SpMV variants are tuned), then on the streamed one; the
   // faster per-iteration time decides for the later solves
+  // automatic engine choice: models with fewer nodes use the chunked engine
+  static constexpr int STREAM_MIN_NODES = 32768;
   struct EngineTune {
     int phase = 0;  // 0 / 1: chunked set-up / timed solve, 2 / 3: streamed set-up / timed, 4: decided
     double us_per_it[2] = {0.0, 0.0};

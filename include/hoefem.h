@@ -348,7 +348,8 @@ int hoefem_integrator_set_precision(hoefem_integrator it, int precision, double 
    kernel chunks, and the persistent streamed CG (one cooperative launch per
    solve, the operator and the Schwarz blocks streamed through shared memory;
    for no preconditioner, diagonal, or Schwarz with subdomains of at most 27
-   nodes).  HOEFEM_CG_ENGINE_AUTO (default): per operator precision and
+   nodes).  HOEFEM_CG_ENGINE_AUTO (default): models with fewer than 32,768
+   nodes use the graphs; for larger ones, per operator precision and
    preconditioner kind, each engine's first solve sets it up (graphs, stream
    layouts) and its next solve of at least 20 iterations is timed whole
    (the solve's set-up, value packing, residual replacements and launches

@@ -195,21 +195,47 @@ def test_cg_first_iterates_match_numpy_recurrence(engine, prec):
         assert rel(x, numpy_pcg_iterates(A, apply_p, b, k)) < 1e-10, (k, rel(x, numpy_pcg_iterates(A, apply_p, b, k)))
 
 
-def test_auto_engine_times_both_engines_and_keeps_the_faster():
+def test_auto_engine_small_model_keeps_the_graphs():
+    # below 32,768 nodes the automatic choice is the chunked engine, unsampled
     m, ref, P, J, b = schwarz_system(8)
     m.set_cg_engine("auto")
     xs = []
-    # per engine one set-up solve and one timed solve (after the chunked
-    # engine's online SpMV-variant tuning)
-    for _ in range(8):
+    for _ in range(3):
         x = np.zeros(m.ndof())
         (H.ConjugateGradient(m).with_operator(J).with_preconditioner(P)
          .with_stopping_criterion(H.RelativeResidualCriterion(1e-8)).with_max_iter(5000).solve_with_guess(b, x))
         xs.append(x)
     st = m.cg_engine_stats()
+    assert st["auto_choice"] == 0 and st["launches"] == 0
+    assert st["auto_us_per_iteration"] == [0.0, 0.0]
+    for x in xs[1:]:
+        assert np.array_equal(x, xs[0])
+
+
+def test_auto_engine_times_both_engines_and_keeps_the_faster():
+    # the benchmark cylinder (44,296 nodes): per engine a set-up solve and a
+    # timed whole solve, then the faster engine for the rest
+    e = H.scenes.embedded_cylinder(24, 0.3, 0.4, 8, 27, 2)
+    b0, b1 = e.blocks
+    m = H.EmbeddedModel3d(e.vertices, b0.connectivity, b1.connectivity, (b0.weights, b0.points),
+                          (b1.offsets, b1.weights, b1.points))
+    mat = H.StVKMaterial(H.YoungPoisson(5e5, 0.45))
+    comp = H.SchwarzPreconditionerComponent.from_embedded_model(m, e.volume_fractions, 0.5)
+    integ = H.NewtonCgIntegrator3d(m, mat, 1000.0, e.nodes_below(2, 1e-9), preconditioner=comp.build(m))
+    integ.set_tolerances(1e-6, 500, 100)
+    integ.set_precision(True)
+    integ.set_cg_engine("auto")
+    X = e.vertices
+    u0 = np.zeros_like(X)
+    u0[:, 0] = 0.02 * X[:, 2] ** 2
+    u0 = u0.reshape(-1)
+    us_ = []
+    for _ in range(2):
+        u, v = u0.copy(), np.zeros_like(u0)
+        integ.step(u, v, 0.0, 1e-3)
+        us_.append(u)
+    st = integ.cg_engine_stats()
     us = st["auto_us_per_iteration"]
     assert st["auto_choice"] in (0, 1) and us[0] > 0 and us[1] > 0
     assert st["auto_choice"] == (1 if us[1] < us[0] else 0)
-    # whichever engine runs, the solutions agree to the solve's tolerance
-    for x in xs[1:]:
-        assert rel(x, xs[0]) < 1e-6
+    assert rel(us_[1], us_[0]) < 1e-6
