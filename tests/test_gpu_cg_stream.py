@@ -208,8 +208,9 @@ def test_auto_engine_small_model_keeps_the_graphs():
     st = m.cg_engine_stats()
     assert st["auto_choice"] == 0 and st["launches"] == 0
     assert st["auto_us_per_iteration"] == [0.0, 0.0]
+    # (the first solves also tune the SpMV variant, so they differ in rounding)
     for x in xs[1:]:
-        assert np.array_equal(x, xs[0])
+        assert rel(x, xs[0]) < 1e-6
 
 
 def test_auto_engine_times_both_engines_and_keeps_the_faster():
