@@ -594,6 +594,11 @@ def run_batched(args):
         for x in sc:
             it = H.NewtonCgIntegrator3d(x["model"], x["mat"], 1000.0, x["bc"])
             it.set_tolerances(args.cg_tol, args.cg_max_iter, 100)
+            # the CUDA-graph engine: the faster one for every scene size here
+            # (all 64 one at a time: 2.1 s against 3.1 s streamed), and an
+            # integrator that lives for two steps cannot amortise the
+            # automatic choice's sampling of both engines
+            it.set_cg_engine("chunked")
             x["model"].set_stream(stream.cuda_stream)
             a = torch.from_numpy(x["u0"]).to(dev)
             b = torch.from_numpy(x["v0"]).to(dev)
