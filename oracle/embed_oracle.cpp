@@ -5,8 +5,9 @@
 // classification of background cells against an embedded volumetric mesh,
 // cut-cell quadrature in the background element's reference coordinates, and
 // moment-fitting quadrature simplification.  Used only by tests/ and by
-// bench.py's CPU leg as the checker of the CUDA path in
-// higher_order_embedded_fem_b200/csrc/embed.cu; the product never links it.
+// bench.py's CPU leg, as the reference the CUDA path in
+// higher_order_embedded_fem_b200/csrc/embed.cu is compared with; the product
+// never links it.
 //
 // Reference (fenris):
 //   embed_mesh_3d_with_opts / embed_in_cell      src/embedding/embedding3d.rs:57-196

@@ -2,8 +2,8 @@
 // hoefem_oracle.cpp — TEST INFRASTRUCTURE ONLY.
 //
 // FP64 CPU restatement of the reference's per-step hot path
-// (InteractiveComputerGraphics/higher_order_embedded_fem), used as the parity
-// checker for the CUDA library and as the timed CPU baseline.  Nothing in the
+// (InteractiveComputerGraphics/higher_order_embedded_fem): the CUDA library's
+// results are compared with it, and it is the timed CPU baseline.  Nothing in the
 // product (higher_order_embedded_fem_b200/) links or calls this file; only
 // tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg do.
 //

@@ -1,8 +1,8 @@
 """ctypes wrapper of liboracle.so — TEST INFRASTRUCTURE ONLY.
 
-The FP64 CPU restatement of the reference path (hoefem_oracle.cpp).  It is the
-parity checker for the CUDA library and the timed CPU baseline; the product
-package never imports it.
+The FP64 CPU restatement of the reference path (hoefem_oracle.cpp).  The
+CUDA library's results are compared with it, and it is the timed CPU
+baseline; the product package never imports it.
 """
 import ctypes as C
 import os
