@@ -681,6 +681,14 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
           (note_launch(), k_cg_reliable<<<1, 1, 0, s>>>(w.st.p, conv ? 1 : 0));
           cg_stream_arm(w, delta, s);
           ++nrep_s;
+          if (conv) {
+            // the recurrence claimed convergence: the true residual usually
+            // confirms it, so wait for the verdict instead of launching a
+            // kernel that would return at once
+            HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+            HOEFEM_CUDA(cudaStreamSynchronize(s));
+            if (w.h_st->done) break;
+          }
           continue;
         }
       }

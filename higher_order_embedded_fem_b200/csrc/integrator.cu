@@ -158,6 +158,10 @@ struct Integrator {
   DBuf<double> x0, r0, lw;
   cudaEvent_t lev[2] = {nullptr, nullptr};
   bool lev_pending = false;
+  // the warm start's kernels as one CUDA graph (captured per learned model)
+  cudaGraphExec_t ws_exec = nullptr;
+  const void* ws_key = nullptr;
+  long long ws_kernels = 0;
   std::vector<DBuf<double>*> snaps;  // collected (x_k, r_k) pairs of the current solve
   double rep_force = 0.0;
   // damping D = gamma M + alpha K_proj(u) from the (sub)step's initial state
@@ -180,6 +184,7 @@ struct Integrator {
       if (e) cudaEventDestroy(e);
     for (auto& e : lev)
       if (e) cudaEventDestroy(e);
+    if (ws_exec) cudaGraphExecDestroy(ws_exec);
   }
 
   int grid() const { return reduce_blocks_for(m->ndof); }
@@ -336,14 +341,40 @@ struct Integrator {
   void warm_start(cudaStream_t s) {
     // all on the device, no host synchronisation: the prediction from the
     // residual and its norm, the energy-optimal scale, the guard, and x set
-    // only when the guard passes; the counters are read after the step
+    // only when the guard passes; the counters are read after the step.  The
+    // ~20 small kernels run as one CUDA graph (fixed buffers per integrator).
     const int n = (int)m->ndof;
     if (x0.n < (size_t)n) { x0.alloc(n); r0.alloc(n); }
     if (!lw.p) {
       lw.alloc(8);
       for (auto& e : lev) HOEFEM_CUDA(cudaEventCreate(&e));
     }
+    if (!ws_exec || ws_key != (const void*)learned) {
+      if (ws_exec) cudaGraphExecDestroy(ws_exec);
+      ws_exec = nullptr;
+      cudaStream_t cs;
+      HOEFEM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      cudaGraph_t g;
+      HOEFEM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      g_capture_count = 0;
+      enqueue_warm_start(cs);
+      ws_kernels = g_capture_count;
+      g_capture_count = -1;
+      HOEFEM_CUDA(cudaStreamEndCapture(cs, &g));
+      HOEFEM_CUDA(cudaGraphInstantiate(&ws_exec, g, 0));
+      HOEFEM_CUDA(cudaGraphDestroy(g));
+      HOEFEM_CUDA(cudaStreamDestroy(cs));
+      ws_key = (const void*)learned;
+    }
     HOEFEM_CUDA(cudaEventRecord(lev[0], s));
+    HOEFEM_CUDA(cudaGraphLaunch(ws_exec, s));
+    g_launch_count.fetch_add(ws_kernels, std::memory_order_relaxed);
+    HOEFEM_CUDA(cudaEventRecord(lev[1], s));
+    lev_pending = true;
+  }
+
+  void enqueue_warm_start(cudaStream_t s) {
+    const int n = (int)m->ndof;
     dot_device(F.p, F.p, n, lw.p + 0, partials.p, counter.p, s);
     learned->predict_device(F.p, lw.p + 0, x0.p, s);
     spmv_node_rows(m->rows(), J.p, x0.p, r0.p, 1.0, 0.0, s);
@@ -353,8 +384,6 @@ struct Integrator {
     (note_launch(), k_warm_residual<<<grid(), TPB, 0, s>>>(n, lw.p, r0.p, F.p));
     dot_device(r0.p, r0.p, n, lw.p + 3, partials.p, counter.p, s);
     (note_launch(), k_warm_accept<<<grid(), TPB, 0, s>>>(n, lw.p, x0.p, cg.x.p));
-    HOEFEM_CUDA(cudaEventRecord(lev[1], s));
-    lev_pending = true;
   }
 
   // Time of the last warm start (its events have completed once the solve has
