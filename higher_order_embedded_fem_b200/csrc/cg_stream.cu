@@ -749,15 +749,18 @@ __global__ void k_cg_stream_arm(CgState* st, double delta2) {
   st->rcur = 0;
 }
 
-// Splits items into G contiguous groups of about equal bytes: off[0..G].
-void split_items(const std::vector<CgsItem>& items, int G, std::vector<int>& off) {
+// Splits items into G contiguous groups of about equal weight (the item's
+// bytes, plus extra[i] when given): off[0..G].
+void split_items(const std::vector<CgsItem>& items, int G, std::vector<int>& off,
+                 const std::vector<long long>* extra = nullptr) {
+  auto weight = [&](size_t i) { return (long long)items[i].bytes + (extra ? (*extra)[i] : 0LL); };
   long long total = 0;
-  for (auto& it : items) total += it.bytes;
+  for (size_t i = 0; i < items.size(); ++i) total += weight(i);
   off.assign(G + 1, 0);
   long long cum = 0;
   int g = 1;
   for (size_t i = 0; i < items.size(); ++i) {
-    cum += items[i].bytes;
+    cum += weight(i);
     while (g < G && cum * (long long)G >= total * (long long)g) off[g++] = (int)(i + 1);
   }
   while (g <= G) off[g++] = (int)items.size();
@@ -891,7 +894,18 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
     ++tile_id;
   }
   std::vector<int> off, nrange(G + 1);
-  split_items(items, G, off);
+  // CTA ranges of about equal operator + Schwarz bytes (the Schwarz rows at
+  // the operator's value size): the producer streams both through one ring,
+  // so a CTA's iteration costs about their sum
+  std::vector<long long> swb;
+  if (sw) {
+    swb.assign(items.size(), 0);
+    for (size_t j = 0; j < items.size(); ++j)
+      for (i64 q = items[j].c; q < items[j].c + items[j].b; ++q)
+        for (int k = pair_off[q]; k < pair_off[q + 1]; ++k)
+          swb[j] += 9LL * (P->sub_off[slot_sub[k] + 1] - P->sub_off[slot_sub[k]]) * vsize;
+  }
+  split_items(items, G, off, sw ? &swb : nullptr);
   for (int g = 0; g <= G; ++g) nrange[g] = off[g] < (int)items.size() ? items[off[g]].c : (int)nv;
   // segments: halo-local neighbour indices (sorted halo, times 3), own halo index
   std::vector<CgsSeg> segs;
