@@ -678,14 +678,15 @@ def run_tet10(args):
                       "u": ud.cpu().numpy()}
     up, um = out["plain"].pop("u"), out["mixed"].pop("u")
     out["mixed"]["rel_diff_u_vs_plain"] = float(np.abs(um - up).max() / np.abs(up).max())
-    # the FP32 element stiffness alone (device arrays; adds into K), tensor
-    # cores (element blocks + gather) vs the CUDA-core colored kernels, and
-    # the FP64 kernels; CUDA events on the model's stream
+    # the element stiffness alone (device arrays; adds into K); CUDA events on
+    # the model's stream
     stiff = {}
     Kd = torch.zeros(model.nnz, dtype=torch.float64, device=dev)
     reps = max(3, args.steps)
-    for name, path, f32 in (("fp32_tensor_cores", "auto", True), ("fp32_cuda_cores", "cuda_cores", True),
-                            ("fp64_cuda_cores", "auto", False)):
+    # auto: FP32 on the tensor cores, FP64 on the CUDA cores with staged
+    # node-pair blocks and the gather; cuda_cores: the colored scatter kernels
+    for name, path, f32 in (("fp32_tensor_cores", "auto", True), ("fp32_colored", "cuda_cores", True),
+                            ("fp64_staged_pairs", "auto", False), ("fp64_colored", "cuda_cores", False)):
         model.set_stiffness_path(path)
         for _ in range(3):
             model.assemble_stiffness_into_precision(Kd, u0d, mat, f32)

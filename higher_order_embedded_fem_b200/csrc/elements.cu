@@ -324,7 +324,8 @@ __global__ void __launch_bounds__(StiffCfg<NN>::TPB, 2) k_stiffness(const BlockD
                                                                     const int* __restrict__ adj_off,
                                                                     const long long* __restrict__ base,
                                                                     double* __restrict__ vals, MatDev mat, int* err,
-                                                                    double* __restrict__ stage) {
+                                                                    double* __restrict__ stage,
+                                                                    R* __restrict__ pblk = nullptr) {
   using C = StiffCfg<NN>;
   constexpr int TPE = C::TPE, EPC = C::EPC, QT = C::QT, WPE = TPE / 32;
   constexpr int NP = PairTable<NN>::NP;
@@ -486,6 +487,20 @@ __global__ void __launch_bounds__(StiffCfg<NN>::TPB, 2) k_stiffness(const BlockD
     if (t == 0) set_error(err, HOEFEM_ERR_SINGULAR);
     return;
   }
+  if (pblk) {
+    // the element's node-pair blocks, pblk[(e NP + p) 9 + 3 i + j], for the
+    // gather into the CSR values
+    R* o = pblk + (size_t)e * NP * 9;
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      const int p = t + k * TPE;
+      if (p < NP) {
+#pragma unroll
+        for (int ab = 0; ab < 9; ++ab) o[(size_t)p * 9 + ab] = acc[k][ab];
+      }
+    }
+    return;
+  }
   if (stage) {
     // dense element matrix (row-major 3NN x 3NN) instead of the scatter
     constexpr int D = 3 * NN;
@@ -641,7 +656,7 @@ void launch_forces(const Model& m, const MatDev& mat, const double* u, double* f
 
 template <int NN, class R>
 void launch_stiffness_kind(const Model& m, const Block& blk, const MatDev& mat, const double* u, double* vals,
-                           cudaStream_t s, double* stage = nullptr) {
+                           cudaStream_t s, double* stage = nullptr, R* pblk = nullptr) {
   using C = StiffCfg<NN>;
   constexpr size_t smem = stiffness_smem<NN, R>();
   static bool attr_set[64] = {};
@@ -652,13 +667,13 @@ void launch_stiffness_kind(const Model& m, const Block& blk, const MatDev& mat, 
     attr_set[dev] = true;
   }
   BlockDev bd = blk.dev();
-  if (stage) {
+  if (stage || pblk) {
     // all elements at once (no scatter, no coloring needed)
     const int cnt = (int)blk.ne;
     if (cnt > 0)
       (note_launch(), k_stiffness<NN, R><<<(cnt + C::EPC - 1) / C::EPC, C::TPB, smem, s>>>(
                           bd, blk.d_color_elems.p, cnt, m.d_X.p, u, m.d_adj_off.p, m.d_base.p, vals, mat, m.d_err.p,
-                          stage));
+                          stage, pblk));
     return;
   }
   for_each_color(blk, [&](const int* elems, int cnt) {
@@ -682,17 +697,29 @@ void launch_stiffness(const Model& m, const MatDev& mat, const double* u, double
                       int precision, bool assign) {
   init_pairs();
   const bool f32 = precision == PRECISION_FP32;
-  if (assign) {
-    if (f32 && m.blocks.size() == 1 && stiffness_tc_eligible(m, *m.blocks[0])) {
-      launch_stiffness_tc(m, *m.blocks[0], mat, u, vals, s, true);
-      HOEFEM_CUDA(cudaGetLastError());
-      return;
-    }
-    HOEFEM_CUDA(cudaMemsetAsync(vals, 0, sizeof(double) * (size_t)m.nnz, s));
-  }
+  // a single block whose gather writes every entry stores instead of adding
+  const bool one = m.blocks.size() == 1;
+  const bool gathered = one && ((f32 && stiffness_tc_eligible(m, *m.blocks[0])) || stiffness_pairs_eligible(m, *m.blocks[0]));
+  if (assign && !gathered) HOEFEM_CUDA(cudaMemsetAsync(vals, 0, sizeof(double) * (size_t)m.nnz, s));
+  const bool store = assign && gathered;
   for (const Block* bp : m.blocks) {
     if (f32 && stiffness_tc_eligible(m, *bp)) {
-      launch_stiffness_tc(m, *bp, mat, u, vals, s);
+      launch_stiffness_tc(m, *bp, mat, u, vals, s, store);
+      continue;
+    }
+    if (stiffness_pairs_eligible(m, *bp)) {
+      // every element of the block in one launch, node-pair blocks staged,
+      // then the gather into the CSR values
+      void* pb = stiffness_pair_buffer(m, *bp, f32, s);
+      if (bp->kind == HOEFEM_ELEM_TET10) {
+        if (f32) launch_stiffness_kind<10, float>(m, *bp, mat, u, nullptr, s, nullptr, (float*)pb);
+        else launch_stiffness_kind<10, double>(m, *bp, mat, u, nullptr, s, nullptr, (double*)pb);
+      } else {
+        if (f32) launch_stiffness_kind<27, float>(m, *bp, mat, u, nullptr, s, nullptr, (float*)pb);
+        else launch_stiffness_kind<27, double>(m, *bp, mat, u, nullptr, s, nullptr, (double*)pb);
+      }
+      HOEFEM_CUDA(cudaGetLastError());
+      stiffness_gather_pairs(m, *bp, f32, vals, store, s);
       continue;
     }
     if (bp->kind == HOEFEM_ELEM_TET10) {

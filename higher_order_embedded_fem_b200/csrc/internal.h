@@ -135,8 +135,9 @@ struct Block {
   // element blocks
   mutable DBuf<float> d_tc_psi, d_tc_grad, d_tc_ke;
   mutable DBuf<int> d_tc_off, d_tc_ent;
+  mutable DBuf<double> d_pb64;  // FP64 node-pair blocks of the staged CUDA-core path
   mutable int tc_nch = 0;
-  mutable bool tc_ready = false;
+  mutable bool tc_ready = false, gmap_ready = false;
   BlockDev dev() const;
 };
 
@@ -192,6 +193,12 @@ void launch_mass(const Model& m, double density, double* vals, cudaStream_t s);
 bool stiffness_tc_eligible(const Model& m, const Block& blk);
 void launch_stiffness_tc(const Model& m, const Block& blk, const MatDev& mat, const double* u, double* vals,
                          cudaStream_t s, bool assign = false);
+// CUDA-core element stiffness of a whole block in one launch into staged
+// node-pair blocks, then the same gather (not for batched scenes): the
+// block's pair buffer (FP32 or FP64 blocks), and the gather into vals.
+bool stiffness_pairs_eligible(const Model& m, const Block& blk);
+void* stiffness_pair_buffer(const Model& m, const Block& blk, bool f32, cudaStream_t s);
+void stiffness_gather_pairs(const Model& m, const Block& blk, bool f32, double* vals, bool assign, cudaStream_t s);
 // Stiffness with every element matrix projected onto PSD (negative eigenvalues
 // set to zero) before the colored scatter; adds into vals.
 void launch_stiffness_projected(Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s);

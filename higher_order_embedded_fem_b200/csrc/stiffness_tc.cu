@@ -443,10 +443,11 @@ constexpr int GU = 2;  // contributions loaded together in the gather
 
 // Warp per node row: every 3 x 3 block of the row summed over its element
 // contributions (element order), added into the CSR values (assign: stored).
+template <class KT>
 __global__ void __launch_bounds__(256) k_stiffness_gather(int nv, const int* __restrict__ adj_off,
                                                           const long long* __restrict__ base,
                                                           const int* __restrict__ off, const int* __restrict__ ent,
-                                                          const float* __restrict__ ke, double* __restrict__ vals,
+                                                          const KT* __restrict__ ke, double* __restrict__ vals,
                                                           int assign) {
   const int a = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (a >= nv) return;
@@ -463,12 +464,12 @@ __global__ void __launch_bounds__(256) k_stiffness_gather(int nv, const int* __r
       int code[GU];
 #pragma unroll
       for (int u = 0; u < GU; ++u) code[u] = k + u < k1 ? __ldg(ent + k + u) : -1;
-      float v[GU][9];
+      KT v[GU][9];
 #pragma unroll
       for (int u = 0; u < GU; ++u) {
-        const float* kb = ke + (size_t)(code[u] >> 1) * 9;
+        const KT* kb = ke + (size_t)(code[u] >> 1) * 9;
 #pragma unroll
-        for (int i = 0; i < 9; ++i) v[u][i] = code[u] >= 0 ? __ldg(kb + i) : 0.f;
+        for (int i = 0; i < 9; ++i) v[u][i] = code[u] >= 0 ? __ldg(kb + i) : KT(0);
       }
 #pragma unroll
       for (int u = 0; u < GU; ++u) {
@@ -529,10 +530,56 @@ float tf32_host(float x) {
   return r;
 }
 
-int pair_index10(int I, int J) {  // I >= J, pairs ordered J-major (J = 0: I = 0..9, J = 1: I = 1..9, ...)
-  int p = 0;
-  for (int j = 0; j < J; ++j) p += 10 - j;
-  return p + (I - J);
+// Node pair (I >= J) of an element with nn nodes, ordered J-major (J = 0:
+// I = 0..nn-1, J = 1: I = 1..nn-1, ...), as the element kernels number them.
+int pair_index(int nn, int I, int J) { return J * nn - J * (J - 1) / 2 + (I - J); }
+
+// Gather map of a block: per pattern slot, the (element, pair, transposed)
+// contributions in element order, as ((e NP + p) << 1) | transposed.
+void prepare_gather_map(const Model& m, const Block& blk, cudaStream_t s) {
+  if (blk.gmap_ready) return;
+  const int nn = blk.nn, np = nn * (nn + 1) / 2;
+  const size_t nslot = m.adj.size();
+  HOEFEM_REQUIRE(blk.ne * (i64)np * 2 < (i64)2147483647, HOEFEM_ERR_INVALID_ARGUMENT,
+                 "too many elements for the stiffness gather map");
+  std::vector<int> off(nslot + 1, 0);
+  std::vector<int> slot((size_t)blk.ne * nn * nn);
+  for (i64 e = 0; e < blk.ne; ++e) {
+    const i64* c = blk.conn.data() + e * nn;
+    for (int I = 0; I < nn; ++I) {
+      const int* b0 = m.adj.data() + m.adj_off[c[I]];
+      const int* b1 = m.adj.data() + m.adj_off[c[I] + 1];
+      for (int J = 0; J < nn; ++J) {
+        const int* it = std::lower_bound(b0, b1, (int)c[J]);
+        HOEFEM_REQUIRE(it != b1 && *it == (int)c[J], HOEFEM_ERR_PATTERN, "element node missing from pattern");
+        const int sl = (int)(it - m.adj.data());
+        slot[((size_t)e * nn + I) * nn + J] = sl;
+        off[sl + 1]++;
+      }
+    }
+  }
+  for (size_t i = 0; i < nslot; ++i) off[i + 1] += off[i];
+  std::vector<int> ent(off[nslot]);
+  std::vector<int> fill(off.begin(), off.end() - 1);
+  for (i64 e = 0; e < blk.ne; ++e)
+    for (int I = 0; I < nn; ++I)
+      for (int J = 0; J < nn; ++J) {
+        const int sl = slot[((size_t)e * nn + I) * nn + J];
+        const int t = I < J ? 1 : 0;
+        const int p = t ? pair_index(nn, J, I) : pair_index(nn, I, J);
+        ent[fill[sl]++] = (int)(((e * np + p) << 1) | t);
+      }
+  blk.d_tc_off.upload(off, s);
+  blk.d_tc_ent.upload(ent, s);
+  blk.gmap_ready = true;
+}
+
+template <class KT>
+void launch_gather(const Model& m, const Block& blk, const KT* ke, double* vals, bool assign, cudaStream_t s) {
+  const int nv = (int)m.nv;
+  (note_launch(), k_stiffness_gather<KT><<<(nv + 7) / 8, 256, 0, s>>>(nv, m.d_adj_off.p, m.d_base.p, blk.d_tc_off.p,
+                                                                         blk.d_tc_ent.p, ke, vals, assign ? 1 : 0));
+  HOEFEM_CUDA(cudaGetLastError());
 }
 
 void prepare_tc(const Model& m, const Block& blk, cudaStream_t s) {
@@ -548,7 +595,7 @@ void prepare_tc(const Model& m, const Block& blk, cudaStream_t s) {
       for (int I = 0; I < 10; ++I) tet10_grad_host(I, &blk.qp[3 * q], gr[I]);
       for (int J = 0; J < 10; ++J)
         for (int I = J; I < 10; ++I) {
-          const int p = pair_index10(I, J);
+          const int p = pair_index(10, I, J);
           for (int mm = 0; mm < 3; ++mm)
             for (int nn = 0; nn < 3; ++nn) {
               const float x = (float)(gr[I][mm] * gr[J][nn]);
@@ -569,39 +616,7 @@ void prepare_tc(const Model& m, const Block& blk, cudaStream_t s) {
       for (int k = 0; k < 3; ++k) grad[(size_t)q * 30 + 3 * I + k] = (float)g[k];
     }
   blk.d_tc_grad.upload(grad, s);
-  // gather map: per pattern slot, (element, pair, transposed) in element order
-  const size_t nslot = m.adj.size();
-  HOEFEM_REQUIRE(blk.ne * (i64)TC_NP * 2 < (i64)2147483647, HOEFEM_ERR_INVALID_ARGUMENT,
-                 "too many elements for the tensor-core stiffness map");
-  std::vector<int> off(nslot + 1, 0);
-  std::vector<int> slot((size_t)blk.ne * 100);
-  for (i64 e = 0; e < blk.ne; ++e) {
-    const i64* c = blk.conn.data() + e * 10;
-    for (int I = 0; I < 10; ++I) {
-      const int* b0 = m.adj.data() + m.adj_off[c[I]];
-      const int* b1 = m.adj.data() + m.adj_off[c[I] + 1];
-      for (int J = 0; J < 10; ++J) {
-        const int* it = std::lower_bound(b0, b1, (int)c[J]);
-        HOEFEM_REQUIRE(it != b1 && *it == (int)c[J], HOEFEM_ERR_PATTERN, "element node missing from pattern");
-        const int sl = (int)(it - m.adj.data());
-        slot[(size_t)e * 100 + I * 10 + J] = sl;
-        off[sl + 1]++;
-      }
-    }
-  }
-  for (size_t i = 0; i < nslot; ++i) off[i + 1] += off[i];
-  std::vector<int> ent(off[nslot]);
-  std::vector<int> fill(off.begin(), off.end() - 1);
-  for (i64 e = 0; e < blk.ne; ++e)
-    for (int I = 0; I < 10; ++I)
-      for (int J = 0; J < 10; ++J) {
-        const int sl = slot[(size_t)e * 100 + I * 10 + J];
-        const int t = I < J ? 1 : 0;
-        const int p = t ? pair_index10(J, I) : pair_index10(I, J);
-        ent[fill[sl]++] = (int)(((e * TC_NP + p) << 1) | t);
-      }
-  blk.d_tc_off.upload(off, s);
-  blk.d_tc_ent.upload(ent, s);
+  prepare_gather_map(m, blk, s);
   blk.d_tc_ke.alloc((size_t)blk.ne * TC_NP * 9);
   blk.tc_nch = nch;
   blk.tc_ready = true;
@@ -639,11 +654,28 @@ void launch_stiffness_tc(const Model& m, const Block& blk, const MatDev& mat, co
   const int grid = std::min(device_sms(), a.ntiles);
   (note_launch(), k_stiffness_tc<<<grid, TC_THREADS, TC_SMEM, s>>>(a));
   HOEFEM_CUDA(cudaGetLastError());
-  const int nv = (int)m.nv;
-  (note_launch(), k_stiffness_gather<<<(nv + 7) / 8, 256, 0, s>>>(nv, m.d_adj_off.p, m.d_base.p, blk.d_tc_off.p,
-                                                                     blk.d_tc_ent.p, blk.d_tc_ke.p, vals,
-                                                                     assign ? 1 : 0));
-  HOEFEM_CUDA(cudaGetLastError());
+  launch_gather<float>(m, blk, blk.d_tc_ke.p, vals, assign, s);
+}
+
+bool stiffness_pairs_eligible(const Model& m, const Block& blk) {
+  if (m.stiffness_path == STIFFNESS_CUDA_CORES) return false;
+  return blk.escene.empty() && blk.scene_active == nullptr && blk.ne > 0;
+}
+
+void* stiffness_pair_buffer(const Model& m, const Block& blk, bool f32, cudaStream_t s) {
+  prepare_gather_map(m, blk, s);
+  const size_t n = (size_t)blk.ne * (blk.nn * (blk.nn + 1) / 2) * 9;
+  if (f32) {
+    if (blk.d_tc_ke.n < n) blk.d_tc_ke.alloc(n);
+    return blk.d_tc_ke.p;
+  }
+  if (blk.d_pb64.n < n) blk.d_pb64.alloc(n);
+  return blk.d_pb64.p;
+}
+
+void stiffness_gather_pairs(const Model& m, const Block& blk, bool f32, double* vals, bool assign, cudaStream_t s) {
+  if (f32) launch_gather<float>(m, blk, blk.d_tc_ke.p, vals, assign, s);
+  else launch_gather<double>(m, blk, blk.d_pb64.p, vals, assign, s);
 }
 
 }  // namespace hoefem

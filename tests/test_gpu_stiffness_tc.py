@@ -6,7 +6,9 @@ Box sizes: 6 elements (one partial tile), 162 (a partial last tile, fewer
 tiles than SMs), 3,072 (one or two tiles per CTA) and 6,000 (up to three
 tiles per CTA, so both accumulators and both chunk buffers are reused).
 Tolerance: 1e-5 relative to the largest entry, the FP32 element arithmetic
-bound the CUDA-core kernel meets as well."""
+bound the CUDA-core kernel meets as well.  Also the staged node-pair path of
+the CUDA-core kernels (one launch per block, then the same gather) in FP64
+(1e-10 against the oracle) and FP32, Tet10 and embedded Hex27."""
 import numpy as np
 import pytest
 
@@ -79,3 +81,34 @@ def test_tc_mixed_newton_step_matches_cuda_core_step():
     (ua, sa), (uc, sc) = out["auto"], out["cuda_cores"]
     assert sa["newton_iterations"] == sc["newton_iterations"]
     assert rel(ua, uc) < 1e-6
+
+
+@pytest.mark.parametrize("scene", ["tet10", "embedded"])
+@pytest.mark.parametrize("mat_kind", [O.MAT_SNH, O.MAT_STVK])
+def test_staged_pair_stiffness_matches_oracle_and_colored(scene, mat_kind):
+    # whole-block launches into node-pair blocks, then the gather (automatic
+    # path for FP64 and for FP32 blocks the tensor cores do not take), against
+    # the colored scatter and the oracle
+    from test_gpu_parity import embedded_setup
+
+    if scene == "tet10":
+        s, m, mat, ref = tet10_setup(5, mat_kind)
+        h = s.cell_size
+    else:
+        s, m, mat, ref = embedded_setup(8, mat_kind)
+        h = s.cell_size
+    u = H.scenes.random_normal(11, m.ndof(), 0.01 * h)
+    Kr = ref.stiffness(u)
+    out = {}
+    for path in ("auto", "cuda_cores"):
+        m.set_stiffness_path(path)
+        out[path] = (m.assemble_stiffness_into_par(np.zeros(m.nnz), u, mat),
+                     m.assemble_stiffness_into_precision(np.zeros(m.nnz), u, mat, True))
+    m.set_stiffness_path("auto")
+    (a64, a32), (c64, c32) = out["auto"], out["cuda_cores"]
+    assert rel(a64, Kr) < 1e-10 and rel(a64, c64) < 1e-12
+    assert rel(a32, Kr) < 1e-5 and rel(c32, Kr) < 1e-5
+    # adds into the values
+    init = H.scenes.random_normal(12, m.nnz, 1.0)
+    K = m.assemble_stiffness_into_par(init.copy(), u, mat)
+    assert np.abs(K - (init + a64)).max() <= 1e-12 * np.abs(a64).max()
