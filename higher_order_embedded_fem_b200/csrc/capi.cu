@@ -560,6 +560,7 @@ int hoefem_precond_set_block_apply(hoefem_precond p, int32_t on) {
   HOEFEM_REQUIRE(!on || 3 * p->p.max_nodes <= 96, HOEFEM_ERR_INVALID_ARGUMENT,
                  "block apply supports subdomains of at most 32 nodes");
   p->p.block_apply = on != 0;
+  if (!on) precond_assemble(p->p, p->p.m->stream);  // the SpMV apply reads every entry
   API_END
 }
 
@@ -596,6 +597,7 @@ int hoefem_precond_values(hoefem_precond p, double* values) {
   HOEFEM_REQUIRE(p && values, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
   const Precond& pp = p->p;
   HOEFEM_REQUIRE(pp.ready, HOEFEM_ERR_INVALID_ARGUMENT, "preconditioner has not been updated");
+  precond_assemble(pp, pp.m->stream);
   const double* src = pp.kind == PREC_SCHWARZ ? pp.vals.p : pp.diag.p;
   size_t n = pp.kind == PREC_SCHWARZ ? (size_t)pp.nnz : (size_t)pp.m->ndof;
   HOEFEM_CUDA(cudaMemcpyAsync(values, src, n * sizeof(double), cudaMemcpyDeviceToHost, pp.m->stream));

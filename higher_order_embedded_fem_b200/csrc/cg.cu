@@ -558,6 +558,7 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
   const int n = (int)w.n;
   const int kind = P ? P->kind : PREC_NONE;
   HOEFEM_REQUIRE(!P || P->ready, HOEFEM_ERR_INVALID_ARGUMENT, "preconditioner has not been updated");
+  if (P && !P->block_apply) precond_assemble(*P, s);  // the SpMV apply reads every entry
   // automatic engine choice: each engine's first solve builds its one-time
   // structures (graphs, stream layouts) and is not timed; its second solve of
   // at least 20 iterations is timed whole (set-up, packing, replacements and
@@ -812,6 +813,7 @@ int cg_solve_learned(CgWork& w, const double* vals, const Precond* P, Learned* L
                      i64* iters, i64* kept, i64* dropped, cudaStream_t s) {
   HOEFEM_REQUIRE(L && L->trained, HOEFEM_ERR_INVALID_ARGUMENT, "learned correction not trained");
   HOEFEM_REQUIRE(!P || P->ready, HOEFEM_ERR_INVALID_ARGUMENT, "preconditioner has not been updated");
+  if (P && !P->block_apply) precond_assemble(*P, s);  // the SpMV apply reads every entry
   NodeRows R = w.m->rows();
   const int n = (int)w.n;
   const int vg = vec_grid(n);

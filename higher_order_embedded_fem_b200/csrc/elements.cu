@@ -39,7 +39,8 @@ constexpr int TPB = 128;
 template <int NN>
 __global__ void __launch_bounds__(TPB) k_forces(const BlockDev b, const int* __restrict__ elems, int count,
                                                 const double* __restrict__ X, const double* __restrict__ u,
-                                                double* __restrict__ f, MatDev mat, int* err) {
+                                                double* __restrict__ f, MatDev mat, int* err,
+                                                double* __restrict__ fst = nullptr) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int idx = blockIdx.x * (TPB / 32) + warp;
   __shared__ double s_corner[TPB / 32][24];
@@ -105,7 +106,10 @@ __global__ void __launch_bounds__(TPB) k_forces(const BlockDev b, const int* __r
   }
   if (own) {
 #pragma unroll
-    for (int i = 0; i < 3; ++i) f[3 * g + i] += fl[i];
+    for (int i = 0; i < 3; ++i) {
+      if (fst) fst[((size_t)e * NN + lane) * 3 + i] = fl[i];
+      else f[3 * g + i] += fl[i];
+    }
   }
 }
 
@@ -120,7 +124,8 @@ constexpr int T10_FSTRIDE = 31;  // doubles per point row (30 used; odd stride)
 
 __global__ void __launch_bounds__(TPB) k_forces_tet10(const BlockDev b, const int* __restrict__ elems, int count,
                                                       const double* __restrict__ X, const double* __restrict__ u,
-                                                      double* __restrict__ f, MatDev mat, int* err) {
+                                                      double* __restrict__ f, MatDev mat, int* err,
+                                                      double* __restrict__ fst = nullptr) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int idx = blockIdx.x * (TPB / 32) + warp;
   __shared__ double s_corner[TPB / 32][12];
@@ -191,7 +196,8 @@ __global__ void __launch_bounds__(TPB) k_forces_tet10(const BlockDev b, const in
     for (int i = 0; i < 3; ++i) {
       double acc = 0.0;
       for (int q = 0; q < nq; ++q) acc += s_f[warp][q * T10_FSTRIDE + 3 * lane + i];
-      f[3 * g + i] += acc;
+      if (fst) fst[((size_t)e * 10 + lane) * 3 + i] = acc;
+      else f[3 * g + i] += acc;
     }
   }
 }
@@ -206,7 +212,8 @@ constexpr int FW = 8;
 
 __global__ void __launch_bounds__(32 * FW, 2) k_forces_hex27(const BlockDev b, const int* __restrict__ elems, int count,
                                                          const double* __restrict__ X, const double* __restrict__ u,
-                                                         double* __restrict__ f, MatDev mat, int* err) {
+                                                         double* __restrict__ f, MatDev mat, int* err,
+                                                         double* __restrict__ fst = nullptr) {
   constexpr int NN = 27;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __shared__ double s_corner[24];
@@ -274,8 +281,12 @@ __global__ void __launch_bounds__(32 * FW, 2) k_forces_hex27(const BlockDev b, c
     double acc = 0.0;
 #pragma unroll
     for (int w = 0; w < FW; ++w) acc += s_f[w][I][i];
-    const int gI = b.conn[I * b.ne + e];
-    f[3 * gI + i] += acc;
+    if (fst) {
+      fst[((size_t)e * NN + I) * 3 + i] = acc;
+    } else {
+      const int gI = b.conn[I * b.ne + e];
+      f[3 * gI + i] += acc;
+    }
   }
 }
 
@@ -641,15 +652,25 @@ void for_each_color(const Block& blk, F&& fn) {
 void launch_forces(const Model& m, const MatDev& mat, const double* u, double* f, cudaStream_t s) {
   for (const Block* bp : m.blocks) {
     BlockDev bd = bp->dev();
-    for_each_color(*bp, [&](const int* elems, int cnt) {
+    auto launch = [&](const int* elems, int cnt, double* fst) {
       int grid = (cnt + TPB / 32 - 1) / (TPB / 32);
       if (bp->kind == HOEFEM_ELEM_TET10 && bd.uniform && bd.nq <= 32)
-        (note_launch(), k_forces_tet10<<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p));
+        (note_launch(), k_forces_tet10<<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p, fst));
       else if (bp->kind == HOEFEM_ELEM_TET10)
-        (note_launch(), k_forces<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p));
+        (note_launch(), k_forces<10><<<grid, TPB, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p, fst));
       else
-        (note_launch(), k_forces_hex27<<<cnt, 32 * FW, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p));
-    });
+        (note_launch(), k_forces_hex27<<<cnt, 32 * FW, 0, s>>>(bd, elems, cnt, m.d_X.p, u, f, mat, m.d_err.p, fst));
+    };
+    if (stiffness_pairs_eligible(m, *bp)) {
+      // every element in one launch into per-element node forces, then the
+      // per-node gather (element order)
+      double* fst = forces_stage_buffer(m, *bp, s);
+      if (bp->ne > 0) launch(bp->d_color_elems.p, (int)bp->ne, fst);
+      HOEFEM_CUDA(cudaGetLastError());
+      forces_gather(m, *bp, f, s);
+    } else {
+      for_each_color(*bp, [&](const int* elems, int cnt) { launch(elems, cnt, nullptr); });
+    }
   }
   HOEFEM_CUDA(cudaGetLastError());
 }

@@ -136,8 +136,10 @@ struct Block {
   mutable DBuf<float> d_tc_psi, d_tc_grad, d_tc_ke;
   mutable DBuf<int> d_tc_off, d_tc_ent;
   mutable DBuf<double> d_pb64;  // FP64 node-pair blocks of the staged CUDA-core path
+  mutable DBuf<double> d_fst;   // staged element node forces
+  mutable DBuf<int> d_noff, d_nent;  // per node: its (element, local node) incidences
   mutable int tc_nch = 0;
-  mutable bool tc_ready = false, gmap_ready = false;
+  mutable bool tc_ready = false, gmap_ready = false, nmap_ready = false;
   BlockDev dev() const;
 };
 
@@ -199,6 +201,10 @@ void launch_stiffness_tc(const Model& m, const Block& blk, const MatDev& mat, co
 bool stiffness_pairs_eligible(const Model& m, const Block& blk);
 void* stiffness_pair_buffer(const Model& m, const Block& blk, bool f32, cudaStream_t s);
 void stiffness_gather_pairs(const Model& m, const Block& blk, bool f32, double* vals, bool assign, cudaStream_t s);
+// Staged element forces of a whole block (same eligibility): the buffer
+// (element-major node forces) and the per-node gather adding into f.
+double* forces_stage_buffer(const Model& m, const Block& blk, cudaStream_t s);
+void forces_gather(const Model& m, const Block& blk, double* f, cudaStream_t s);
 // Stiffness with every element matrix projected onto PSD (negative eigenvalues
 // set to zero) before the colored scatter; adds into vals.
 void launch_stiffness_projected(Model& m, const MatDev& mat, const double* u, double* vals, cudaStream_t s);

@@ -330,6 +330,17 @@ __global__ void k_schwarz_untreated(int nun, const int* __restrict__ untreated, 
   else atomicCAS(err, 0, HOEFEM_ERR_ZERO_DIAGONAL);
 }
 
+// Zero the entries of every node row that is not diagonal-only (the
+// subdomain entries, before the scatter adds the blocks into them).
+__global__ void k_zero_block_rows(int nv, const long long* __restrict__ pbase,
+                                  const unsigned char* __restrict__ diag_only, double* __restrict__ pv) {
+  for (int a = blockIdx.x; a < nv; a += gridDim.x) {
+    if (diag_only[a]) continue;
+    const long long b0 = pbase[a], b1 = pbase[a + 1];
+    for (long long k = b0 + threadIdx.x; k < b1; k += blockDim.x) pv[k] = 0.0;
+  }
+}
+
 __global__ void k_diag_inverse(NodeRows A, const double* __restrict__ J, double* __restrict__ d, int* err) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 3 * A.nv) return;
@@ -516,6 +527,19 @@ static void check_err(DBuf<int>& e, cudaStream_t s) {
   }
 }
 
+// Adds the symmetric part of every staged block into the assembled values
+// (one launch per Schwarz color: no two blocks of a color share a node).
+static void scatter_blocks(Precond& p, cudaStream_t s) {
+  const int nc = (int)p.color_off.size() - 1;
+  for (int c = 0; c < nc; ++c) {
+    int b = (int)p.color_off[c], cnt = (int)(p.color_off[c + 1] - b);
+    if (cnt)
+      (note_launch(), k_schwarz_scatter<<<cnt, 256, 0, s>>>(p.d_color_subs.p + b, cnt, p.d_sub_off.p, p.d_sub_nodes.p,
+                                                             p.d_gmap_off.p, p.d_smap.p, p.d_adj_off.p, p.d_stage_off.p,
+                                                             p.staging.p, p.vals.p));
+  }
+}
+
 void precond_update(Precond& p, const double* J, cudaStream_t s) {
   Model& m = *p.m;
   NodeRows A = m.rows();
@@ -528,7 +552,9 @@ void precond_update(Precond& p, const double* J, cudaStream_t s) {
     p.ready = true;
     return;
   }
-  p.vals.zero(s);
+  // with the block apply the subdomain entries are scattered on demand
+  const bool lazy = p.block_apply && p.nsub > 0;
+  if (!lazy) p.vals.zero(s);
   if (p.nsub > 0) {
     HOEFEM_CUDA(cudaMemsetAsync(p.d_fallback.p, 0, sizeof(int), s));
     const int dmax = 3 * p.max_nodes;
@@ -550,14 +576,7 @@ void precond_update(Precond& p, const double* J, cudaStream_t s) {
     HOEFEM_CUDA(cudaGetLastError());
     (note_launch(), k_schwarz_symmetrize<<<(int)p.nsub, 256, 0, s>>>(p.d_sub_off.p, p.d_stage_off.p, p.staging.p,
                                                                       p.bsym.p));
-    const int nc = (int)p.color_off.size() - 1;
-    for (int c = 0; c < nc; ++c) {
-      int b = (int)p.color_off[c], cnt = (int)(p.color_off[c + 1] - b);
-      if (cnt)
-        (note_launch(), k_schwarz_scatter<<<cnt, 256, 0, s>>>(p.d_color_subs.p + b, cnt, p.d_sub_off.p, p.d_sub_nodes.p,
-                                              p.d_gmap_off.p, p.d_smap.p, p.d_adj_off.p, p.d_stage_off.p,
-                                              p.staging.p, p.vals.p));
-    }
+    if (!lazy) scatter_blocks(p, s);
   }
   if (!p.untreated.empty())
     (note_launch(), k_schwarz_untreated<<<(int)((3 * p.untreated.size() + 255) / 256), 256, 0, s>>>(
@@ -565,7 +584,20 @@ void precond_update(Precond& p, const double* J, cudaStream_t s) {
   HOEFEM_CUDA(cudaGetLastError());
   check_err(p.d_err, s);
   if (p.want_fp32) precond_to_fp32(p, s);
+  p.vals_complete = !lazy;
   p.ready = true;
+}
+
+void precond_assemble(const Precond& p, cudaStream_t s) {
+  if (p.kind != PREC_SCHWARZ || !p.ready || p.vals_complete) return;
+  Precond& q = const_cast<Precond&>(p);
+  const int nv = (int)q.m->nv;
+  (note_launch(), k_zero_block_rows<<<std::min(nv, device_sms() * 16), 128, 0, s>>>(nv, q.d_base.p, q.d_diag_only.p,
+                                                                                  q.vals.p));
+  scatter_blocks(q, s);
+  if (q.vals32.p) to_f32(q.vals.p, q.vals32.p, q.nnz, s);
+  HOEFEM_CUDA(cudaGetLastError());
+  q.vals_complete = true;
 }
 
 // FP32 copies of the Schwarz values: the assembled CSR and the symmetrized
@@ -585,6 +617,7 @@ void precond_apply(const Precond& p, const double* r, double* z, cudaStream_t s)
     int n = (int)p.m->ndof;
     (note_launch(), k_mul<<<reduce_blocks_for(n), 256, 0, s>>>(n, p.diag.p, r, z));
   } else {
+    precond_assemble(p, s);
     NodeRows PR = p.rows();
     HOEFEM_LANES_DISPATCH(PR.lanes,
                           (note_launch(), k_spmv_plain<LN><<<spmv_grid(PR.nv, LN), 256, 0, s>>>(PR, p.vals.p, r, z)));

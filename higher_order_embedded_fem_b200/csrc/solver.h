@@ -44,6 +44,11 @@ struct Precond {
   // layout) applied as dense products into ysub (3 entries per subdomain
   // node), then summed per node over its subdomains in subdomain order.
   bool block_apply = true;
+  // With the block apply the CG reads the symmetrized blocks and, from the
+  // assembled values, only the untreated (diagonal-only) entries, which every
+  // update writes; the subdomain entries are scattered into the values when
+  // something reads them (precond_assemble).
+  mutable bool vals_complete = false;
   DBuf<double> bsym;
   DBuf<float> bsym32;
   DBuf<double> ysub;
@@ -55,6 +60,9 @@ struct Precond {
 void precond_create_schwarz(Precond& p, const i64* sub_off, const i64* sub_nodes, i64 nsub, const i64* untreated,
                             i64 nun);
 void precond_update(Precond& p, const double* system_vals, cudaStream_t s);
+// Completes the assembled values (subdomain entries) if an update left them
+// out; before any read of P's CSR values.
+void precond_assemble(const Precond& p, cudaStream_t s);
 void precond_apply(const Precond& p, const double* r, double* z, cudaStream_t s);
 void precond_to_fp32(Precond& p, cudaStream_t s);
 

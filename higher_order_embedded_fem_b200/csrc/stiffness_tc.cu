@@ -574,6 +574,35 @@ void prepare_gather_map(const Model& m, const Block& blk, cudaStream_t s) {
   blk.gmap_ready = true;
 }
 
+// Per node, its (element, local node) incidences in element order, as
+// e nn + I: the gather of staged element forces.
+void prepare_node_map(const Model& m, const Block& blk, cudaStream_t s) {
+  if (blk.nmap_ready) return;
+  const int nn = blk.nn;
+  HOEFEM_REQUIRE(blk.ne * (i64)nn < (i64)2147483647, HOEFEM_ERR_INVALID_ARGUMENT, "too many elements for the force map");
+  std::vector<int> off(m.nv + 1, 0);
+  for (i64 k = 0; k < blk.ne * nn; ++k) off[blk.conn[k] + 1]++;
+  for (i64 a = 0; a < m.nv; ++a) off[a + 1] += off[a];
+  std::vector<int> ent(off[m.nv]);
+  std::vector<int> fill(off.begin(), off.end() - 1);
+  for (i64 k = 0; k < blk.ne * nn; ++k) ent[fill[blk.conn[k]]++] = (int)k;  // k = e nn + I
+  blk.d_noff.upload(off, s);
+  blk.d_nent.upload(ent, s);
+  blk.nmap_ready = true;
+}
+
+__global__ void __launch_bounds__(256) k_forces_gather(int n3, const int* __restrict__ off, const int* __restrict__ ent,
+                                                       const double* __restrict__ fst, double* __restrict__ f) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n3) return;
+  const int a = t / 3, i = t - 3 * a;
+  const int k0 = off[a], k1 = off[a + 1];
+  if (k0 == k1) return;
+  double acc = 0.0;
+  for (int k = k0; k < k1; ++k) acc += fst[(size_t)__ldg(ent + k) * 3 + i];
+  f[t] += acc;
+}
+
 template <class KT>
 void launch_gather(const Model& m, const Block& blk, const KT* ke, double* vals, bool assign, cudaStream_t s) {
   const int nv = (int)m.nv;
@@ -671,6 +700,19 @@ void* stiffness_pair_buffer(const Model& m, const Block& blk, bool f32, cudaStre
   }
   if (blk.d_pb64.n < n) blk.d_pb64.alloc(n);
   return blk.d_pb64.p;
+}
+
+double* forces_stage_buffer(const Model& m, const Block& blk, cudaStream_t s) {
+  prepare_node_map(m, blk, s);
+  const size_t n = (size_t)blk.ne * blk.nn * 3;
+  if (blk.d_fst.n < n) blk.d_fst.alloc(n);
+  return blk.d_fst.p;
+}
+
+void forces_gather(const Model& m, const Block& blk, double* f, cudaStream_t s) {
+  const int n3 = (int)(3 * m.nv);
+  (note_launch(), k_forces_gather<<<(n3 + 255) / 256, 256, 0, s>>>(n3, blk.d_noff.p, blk.d_nent.p, blk.d_fst.p, f));
+  HOEFEM_CUDA(cudaGetLastError());
 }
 
 void stiffness_gather_pairs(const Model& m, const Block& blk, bool f32, double* vals, bool assign, cudaStream_t s) {
