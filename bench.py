@@ -685,8 +685,9 @@ def run_tet10(args):
     reps = max(3, args.steps)
     # auto: FP32 on the tensor cores, FP64 on the CUDA cores with staged
     # node-pair blocks and the gather; cuda_cores: the colored scatter kernels
-    for name, path, f32 in (("fp32_tensor_cores", "auto", True), ("fp32_colored", "cuda_cores", True),
-                            ("fp64_staged_pairs", "auto", False), ("fp64_colored", "cuda_cores", False)):
+    for name, path, f32 in (("fp32_tensor_cores", "auto", True), ("fp32_staged_pairs", "staged", True),
+                            ("fp32_colored", "cuda_cores", True), ("fp64_staged_pairs", "auto", False),
+                            ("fp64_colored", "cuda_cores", False)):
         model.set_stiffness_path(path)
         for _ in range(3):
             model.assemble_stiffness_into_precision(Kd, u0d, mat, f32)

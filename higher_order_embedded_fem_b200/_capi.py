@@ -62,7 +62,7 @@ class CgEngineStats(C.Structure):
 
 
 CG_ENGINE = {"auto": 0, "chunked": 1, "streamed": 2}
-STIFFNESS_PATH = {"auto": 0, "cuda_cores": 1}
+STIFFNESS_PATH = {"auto": 0, "cuda_cores": 1, "staged": 2}
 
 
 class SceneInfo(C.Structure):

@@ -285,9 +285,10 @@ int hoefem_model_set_spmv_variant(hoefem_model m, int32_t variant) {
 int hoefem_model_set_stiffness_path(hoefem_model m, int path) {
   API_BEGIN
   Model& mm = device_model(m);
-  HOEFEM_REQUIRE(path == HOEFEM_STIFFNESS_AUTO || path == HOEFEM_STIFFNESS_CUDA_CORES, HOEFEM_ERR_INVALID_ARGUMENT,
-                 "unknown stiffness path");
-  mm.stiffness_path = path == HOEFEM_STIFFNESS_AUTO ? STIFFNESS_AUTO : STIFFNESS_CUDA_CORES;
+  HOEFEM_REQUIRE(path == HOEFEM_STIFFNESS_AUTO || path == HOEFEM_STIFFNESS_CUDA_CORES || path == HOEFEM_STIFFNESS_STAGED,
+                 HOEFEM_ERR_INVALID_ARGUMENT, "unknown stiffness path");
+  mm.stiffness_path = path == HOEFEM_STIFFNESS_AUTO ? STIFFNESS_AUTO
+                      : path == HOEFEM_STIFFNESS_STAGED ? STIFFNESS_STAGED : STIFFNESS_CUDA_CORES;
   API_END
 }
 

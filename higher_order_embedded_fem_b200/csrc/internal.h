@@ -143,10 +143,11 @@ struct Block {
   BlockDev dev() const;
 };
 
-// Element stiffness implementation: automatic (tensor cores for the blocks
-// they cover: Tet10 with one quadrature rule of at most 14 points, FP32
-// element arithmetic), or the CUDA-core kernels only.
-enum StiffnessPath { STIFFNESS_AUTO = 0, STIFFNESS_CUDA_CORES = 1 };
+// Element stiffness / force implementation: automatic (tensor cores for the
+// blocks they cover: Tet10 with one quadrature rule of at most 14 points,
+// FP32 element arithmetic; staged whole-block CUDA-core kernels for the
+// rest), staged CUDA-core kernels only, or the colored scatter kernels.
+enum StiffnessPath { STIFFNESS_AUTO = 0, STIFFNESS_CUDA_CORES = 1, STIFFNESS_STAGED = 2 };
 
 struct Model {
   int device = 0;

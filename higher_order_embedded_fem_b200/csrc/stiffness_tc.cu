@@ -654,7 +654,7 @@ void prepare_tc(const Model& m, const Block& blk, cudaStream_t s) {
 }  // namespace
 
 bool stiffness_tc_eligible(const Model& m, const Block& blk) {
-  if (m.stiffness_path == STIFFNESS_CUDA_CORES) return false;
+  if (m.stiffness_path != STIFFNESS_AUTO) return false;
   return blk.kind == HOEFEM_ELEM_TET10 && blk.uniform && !blk.qw.empty() && (int)blk.qw.size() <= TC_PPC * TC_MAXCH &&
          blk.escene.empty() && blk.scene_active == nullptr && blk.ne > 0;
 }

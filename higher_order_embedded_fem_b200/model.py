@@ -81,9 +81,10 @@ class _Model:
         check(lib().hoefem_model_set_spmv_variant(self._h, int(variant)))
 
     def set_stiffness_path(self, path="auto"):
-        """FP32 element stiffness implementation: "auto" (Tet10 blocks on the
-        tensor cores where they qualify) or "cuda_cores"
-        (hoefem_model_set_stiffness_path)."""
+        """Element stiffness / force implementation: "auto" (FP32 Tet10 blocks
+        on the tensor cores where they qualify, the rest staged whole-block
+        CUDA-core kernels), "staged" (no tensor cores) or "cuda_cores" (colored
+        scatter) (hoefem_model_set_stiffness_path)."""
         check(lib().hoefem_model_set_stiffness_path(self._h, _capi.STIFFNESS_PATH[path]))
 
     def set_cg_engine(self, engine="auto", schwarz_fp16=False, phase_profile=False):

@@ -137,16 +137,24 @@ int hoefem_model_autotune(hoefem_model m, int32_t* lanes);
 int hoefem_model_set_spmv_variant(hoefem_model m, int32_t variant);
 /* The SpMV variants in use for FP64 and FP32 operator values. */
 int hoefem_model_get_spmv_variants(hoefem_model m, int32_t* fp64_values, int32_t* fp32_values);
-/* Element stiffness implementation for FP32 element arithmetic
-   (hoefem_assemble_stiffness_into_precision with HOEFEM_PRECISION_MIXED, the
-   mixed-precision Newton steps).  HOEFEM_STIFFNESS_AUTO (default): Tet10
+/* Element stiffness (and force) implementation.  HOEFEM_STIFFNESS_AUTO
+   (default): with FP32 element arithmetic (HOEFEM_PRECISION_MIXED), Tet10
    blocks with one quadrature rule of at most 14 points run on the tensor
    cores (tcgen05 TF32 with a hi / lo split of both operands, three products;
    the element blocks of all elements as one GEMM against the block's
-   reference-gradient operator, then a gather into the CSR values), other
-   blocks on the CUDA-core kernels; HOEFEM_STIFFNESS_CUDA_CORES: the
-   CUDA-core kernels only.  No counterpart in the reference. */
-typedef enum { HOEFEM_STIFFNESS_AUTO = 0, HOEFEM_STIFFNESS_CUDA_CORES = 1 } hoefem_stiffness_path;
+   reference-gradient operator); every other block runs the CUDA-core kernel
+   over the whole block in one launch into staged node-pair blocks; both then
+   gather the blocks into the CSR values (forces likewise, per node).
+   HOEFEM_STIFFNESS_STAGED: the staged CUDA-core kernels for every block (no
+   tensor cores).  HOEFEM_STIFFNESS_CUDA_CORES: one launch per element color
+   with the scatter into the values (the path batched scenes always take).
+   All three add the same values up to the order of the FP64 additions.  No
+   counterpart in the reference. */
+typedef enum {
+  HOEFEM_STIFFNESS_AUTO = 0,
+  HOEFEM_STIFFNESS_CUDA_CORES = 1,
+  HOEFEM_STIFFNESS_STAGED = 2
+} hoefem_stiffness_path;
 int hoefem_model_set_stiffness_path(hoefem_model m, int path);
 int hoefem_model_sizes(hoefem_model m, int64_t* ndof, int64_t* nnz, int64_t* num_elements, int64_t* num_blocks);
 /* row_offsets: ndof+1, column_indices: nnz (SparsityPattern, sparse.rs:297-410) */

@@ -100,14 +100,14 @@ def test_staged_pair_stiffness_matches_oracle_and_colored(scene, mat_kind):
     u = H.scenes.random_normal(11, m.ndof(), 0.01 * h)
     Kr = ref.stiffness(u)
     out = {}
-    for path in ("auto", "cuda_cores"):
+    for path in ("auto", "staged", "cuda_cores"):
         m.set_stiffness_path(path)
         out[path] = (m.assemble_stiffness_into_par(np.zeros(m.nnz), u, mat),
                      m.assemble_stiffness_into_precision(np.zeros(m.nnz), u, mat, True))
     m.set_stiffness_path("auto")
-    (a64, a32), (c64, c32) = out["auto"], out["cuda_cores"]
-    assert rel(a64, Kr) < 1e-10 and rel(a64, c64) < 1e-12
-    assert rel(a32, Kr) < 1e-5 and rel(c32, Kr) < 1e-5
+    (a64, a32), (s64, s32), (c64, c32) = out["auto"], out["staged"], out["cuda_cores"]
+    assert rel(a64, Kr) < 1e-10 and rel(a64, c64) < 1e-12 and np.array_equal(a64, s64)
+    assert rel(a32, Kr) < 1e-5 and rel(s32, Kr) < 1e-5 and rel(c32, Kr) < 1e-5
     # adds into the values
     init = H.scenes.random_normal(12, m.nnz, 1.0)
     K = m.assemble_stiffness_into_par(init.copy(), u, mat)
