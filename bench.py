@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--min-elements", type=float, default=1e3, help="batched: smallest scene (elements)")
     ap.add_argument("--max-elements", type=float, default=5e4, help="batched: largest scene (elements)")
     ap.add_argument("--no-sequential", action="store_true", help="batched: skip the one-scene-at-a-time comparison")
+    ap.add_argument("--batch-cg-engine", default="auto", choices=["auto", "chunked", "streamed"],
+                    help="batched: CG engine (graphs, persistent launch, or the autotuner's choice)")
     ap.add_argument("--roofline-only", action="store_true",
                     help="cylinder: autotune the SpMV, then only the roofline launches (for a DRAM-traffic capture)")
     return ap.parse_args()
@@ -546,6 +548,7 @@ def run_batched(args):
                                       [x["bc"] for x in sc])
     setup_s = time.perf_counter() - t0
     B.set_tolerances(args.cg_tol, args.cg_max_iter, 100)
+    B.set_cg_engine(args.batch_cg_engine)
     stream = torch.cuda.current_stream(dev)
     B.set_stream(stream.cuda_stream)
     u0 = torch.from_numpy(np.concatenate([x["u0"] for x in sc])).to(dev)
@@ -613,6 +616,7 @@ def run_batched(args):
             del it
     newton = [s["newton_iterations"] for s in stats]
     cgit = [s["total_cg_iterations"] for s in stats]
+    eng, per, tune_ms = B.cg_choice()
     line = {
         "metric": "batched Newton step ms (all scenes) on 1 GPU", "value": ms, "unit": "ms", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
@@ -626,6 +630,9 @@ def run_batched(args):
         "newton_iterations": {"min": int(min(newton)), "max": int(max(newton)), "sum": int(sum(newton))},
         "cg_iterations": {"min": int(min(cgit)), "max": int(max(cgit)), "sum": int(sum(cgit))},
         "statuses": sorted({int(s["status"]) for s in stats}),
+        "cg_engine": {"requested": args.batch_cg_engine, "used": eng, "ctas_per_sm": per,
+                      "autotuner_first_solve_ms": [round(t, 3) for t in tune_ms],
+                      "candidates": "chunked graphs, then persistent at 1, 2, 4, ... CTAs/SM"},
         "setup_s": setup_s,
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 16 * int(B.ndof),
                 "d2h_bytes_per_step": 16 * int(B.ndof)},

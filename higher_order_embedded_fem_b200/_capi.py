@@ -145,6 +145,9 @@ SIGNATURES = {
     "hoefem_batch_destroy": (C.c_int, [vp]),
     "hoefem_batch_set_stream": (C.c_int, [vp, vp]),
     "hoefem_batch_set_tolerances": (C.c_int, [vp, dbl, i64, i64]),
+    "hoefem_batch_set_cg_engine": (C.c_int, [vp, C.c_int32, C.c_int32]),
+    "hoefem_batch_cg_choice": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), vp,
+                                         C.POINTER(C.c_int32)]),
     "hoefem_batch_sizes": (C.c_int, [vp, pi64, pi64, pi64, vp]),
     "hoefem_batch_step": (C.c_int, [vp, vp, vp, dbl, dbl, C.c_int]),
     "hoefem_batch_scene_stats": (C.c_int, [vp, C.c_int32, C.POINTER(StepStats), C.POINTER(C.c_int32)]),

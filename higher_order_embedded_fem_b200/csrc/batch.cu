@@ -17,7 +17,10 @@
 // reductions are segmented (one block per scene over its contiguous node
 // range, fixed order) so each scene's result is deterministic and independent
 // of the others.  Converged scenes are masked out of further updates.  The CG
-// iterations of all scenes advance together in CUDA-graph chunks.
+// iterations of all scenes advance together, either in CUDA-graph chunks of
+// per-phase kernels or inside one persistent cooperative launch per solve;
+// an autotuner times both (the persistent one at each grid size) on the first
+// solve.  The engines share every arithmetic step, so they give the same bits.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,6 +30,7 @@
 #include "internal.h"
 #include "kernels_common.cuh"
 #include "solver.h"
+#include "stream_pipe.cuh"
 
 namespace hoefem {
 
@@ -78,11 +82,11 @@ __device__ __forceinline__ void for_chunk_nodes(int lo, int hi, F&& body) {
 }
 
 template <int K>
-__device__ __forceinline__ void chunk_store(double (&acc)[K], double* __restrict__ cpart, int nch) {
+__device__ __forceinline__ void chunk_store(double (&acc)[K], double* __restrict__ cpart, int nch, int c) {
   block_sum<K>(acc);
   if (threadIdx.x == 0)
 #pragma unroll
-    for (int k = 0; k < K; ++k) cpart[(size_t)k * nch + blockIdx.x] = acc[k];
+    for (int k = 0; k < K; ++k) cpart[(size_t)k * nch + c] = acc[k];
 }
 
 // per-scene sums of the chunk partials (block per scene, fixed order)
@@ -100,22 +104,27 @@ __device__ __forceinline__ void scene_sum(const Chunks ch, const double* __restr
   for (int k = 0; k < K; ++k) out[k] = acc[k];
 }
 
-// mode 0: init (b.b, r.r) ; 1: zTr init ; 2: pAp -> alpha ; 3: (r.r, z.r) -> convergence, beta.
-// Scenes already finished (or masked out) keep their state.
-__global__ void k_seg_finalize(int mode, const Chunks ch, const double* __restrict__ cpart, SegCg* st, double tol,
-                               long long max_iter) {
-  const int s = blockIdx.x;
-  SegCg& c = st[s];
-  if (c.done) {
-    if (mode == 1 && threadIdx.x == 0) {
-      c.iters = 0;
-      c.status = HOEFEM_OK;
-    }
-    return;
-  }
-  double v[2];
-  scene_sum<2>(ch, cpart, s, v);
-  if (threadIdx.x != 0) return;
+// The same sums by one warp (lane-strided over the scene's chunks, then the
+// xor tree): the CG scalars of both engines come from here.
+template <int K>
+__device__ __forceinline__ void scene_sum_warp(const Chunks ch, const double* __restrict__ cpart, int s,
+                                               double (&out)[K]) {
+  const int lane = threadIdx.x & 31;
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0.0;
+  for (int c = ch.cs_off[s] + lane; c < ch.cs_off[s + 1]; c += 32)
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] += cpart[(size_t)k * ch.n + c];
+#pragma unroll
+  for (int k = 0; k < K; ++k) out[k] = warp_sum_d(acc[k]);
+}
+
+// The scalar step of a running scene (cg.rs:376-482 per scene) from its sums v.
+// mode 0: init (b.b, r.r) ; 1: zTr init ; 2: pAp -> alpha ; 3: (r.r, z.r) ->
+// convergence, beta.
+__device__ __forceinline__ void scene_update(int mode, SegCg& c, const double (&v)[2], double tol,
+                                             long long max_iter) {
   if (mode == 0) {
     c.bnorm = sqrt(v[0]);
     c.rr = v[1];
@@ -143,7 +152,177 @@ __global__ void k_seg_finalize(int mode, const Chunks ch, const double* __restri
   }
 }
 
+// Scenes already finished (or masked out) keep their state; mode 1 resets
+// their iteration count and status.
+__device__ __forceinline__ void scene_finalize_warp(int mode, const Chunks ch, const double* __restrict__ cpart,
+                                                    SegCg& c, int s, double tol, long long max_iter) {
+  const int lane = threadIdx.x & 31;
+  if (c.done) {
+    if (mode == 1 && lane == 0) {
+      c.iters = 0;
+      c.status = HOEFEM_OK;
+    }
+    return;
+  }
+  double v[2];
+  scene_sum_warp<2>(ch, cpart, s, v);
+  if (lane == 0) scene_update(mode, c, v, tol, max_iter);
+}
+
+// one warp per scene
+__global__ void k_seg_finalize(int mode, const Chunks ch, const double* __restrict__ cpart, SegCg* st, double tol,
+                               long long max_iter) {
+  const int s = blockIdx.x;
+  scene_finalize_warp(mode, ch, cpart, st[s], s, tol, max_iter);
+}
+
+// The operand x of the node-row products: a vector, or the next search
+// direction z + beta p formed on the fly (p = z in the first iteration).
+struct XVec {
+  const double* __restrict__ v;
+  __device__ __forceinline__ double operator()(long long k) const { return v[k]; }
+};
+struct XDir {
+  const double* __restrict__ z;
+  const double* __restrict__ p;
+  double beta;
+  int first;
+  __device__ __forceinline__ double operator()(long long k) const { return first ? z[k] : fma(beta, p[k], z[k]); }
+};
+
+// node_row_dot (the same traversals and sums) with the operand read through
+// an accessor.
+template <int L, class X>
+__device__ __forceinline__ void node_row_dot_x(const NodeRows& A, const double* __restrict__ vals, const X& x, int a,
+                                               int sl, double& s0, double& s1, double& s2) {
+  constexpr int LNS = LaneCfg<L>::lanes;
+  s0 = s1 = s2 = 0.0;
+  if (a >= 0) {
+    const long long b = A.base[a];
+    if (A.diag_only && A.diag_only[a]) {
+      if (sl == 0) {
+        s0 = vals[b] * x(3LL * a);
+        s1 = vals[b + 1] * x(3LL * a + 1);
+        s2 = vals[b + 2] * x(3LL * a + 2);
+      }
+    } else if constexpr (LaneCfg<L>::stream) {
+      const int o = A.adj_off[a], d = A.adj_off[a + 1] - o;
+      const int rl = 3 * d;
+      const double* r0 = vals + b;
+#pragma unroll 4
+      for (int c = sl; c < rl; c += LNS) {
+        const int s = c / 3, j = c - 3 * s;
+        const double xv = x(3LL * A.adj[o + s] + j);
+        s0 += r0[c] * xv;
+        s1 += r0[rl + c] * xv;
+        s2 += r0[2 * rl + c] * xv;
+      }
+    } else {
+      const int o = A.adj_off[a], d = A.adj_off[a + 1] - o;
+      const long long rl = 3LL * d;
+#pragma unroll 2
+      for (int s = sl; s < d; s += LNS) {
+        const long long nb = A.adj[o + s];
+        const double x0 = x(3 * nb), x1 = x(3 * nb + 1), x2 = x(3 * nb + 2);
+        const double* r0 = vals + b + 3 * s;
+        s0 += r0[0] * x0 + r0[1] * x1 + r0[2] * x2;
+        const double* r1 = r0 + rl;
+        s1 += r1[0] * x0 + r1[1] * x1 + r1[2] * x2;
+        const double* r2 = r1 + rl;
+        s2 += r2[0] * x0 + r2[1] * x1 + r2[2] * x2;
+      }
+    }
+  }
+#pragma unroll
+  for (int off = LNS / 2; off > 0; off >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+  }
+}
+
+// ---- per-chunk CG steps (chunk c of a running scene, the whole CTA) --------------
+
 // r = b - A x ; chunk partials b.b, r.r
+template <int L>
+__device__ __forceinline__ void chunk_init(const NodeRows& A, const double* __restrict__ vals,
+                                           const double* __restrict__ x, const double* __restrict__ b,
+                                           double* __restrict__ r, const Chunks ch, double* __restrict__ cpart, int c) {
+  double acc[2] = {0.0, 0.0};
+  const XVec xv{x};
+  for_chunk_nodes<L>(ch.lo[c], ch.lo[c + 1], [&](int a, int sl) {
+    double s[3];
+    node_row_dot_x<L>(A, vals, xv, a, sl, s[0], s[1], s[2]);
+    if (a >= 0 && sl == 0) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        double bi = b[3 * a + i], ri = bi - s[i];
+        r[3 * a + i] = ri;
+        acc[0] = fma(bi, bi, acc[0]);
+        acc[1] = fma(ri, ri, acc[1]);
+      }
+    }
+  });
+  chunk_store<2>(acc, cpart, ch.n, c);
+}
+
+// z = d r (and p = z when p is given) ; chunk partials z.r
+__device__ __forceinline__ void chunk_prec0(const Chunks ch, const double* __restrict__ d,
+                                            const double* __restrict__ r, double* __restrict__ z,
+                                            double* __restrict__ p, double* __restrict__ cpart, int c) {
+  double acc[2] = {0.0, 0.0};
+  for (int k = 3 * ch.lo[c] + threadIdx.x; k < 3 * ch.lo[c + 1]; k += blockDim.x) {
+    double zi = d[k] * r[k];
+    z[k] = zi;
+    if (p) p[k] = zi;
+    acc[0] = fma(zi, r[k], acc[0]);
+  }
+  chunk_store<2>(acc, cpart, ch.n, c);
+}
+
+// Ap = A p with p read through `pa` (and written to pout when given) ;
+// chunk partials p.Ap
+template <int L, class X>
+__device__ __forceinline__ void chunk_Ap(const NodeRows& A, const double* __restrict__ vals, const X& pa,
+                                         double* __restrict__ pout, double* __restrict__ Ap, const Chunks ch,
+                                         double* __restrict__ cpart, int c) {
+  double acc[2] = {0.0, 0.0};
+  for_chunk_nodes<L>(ch.lo[c], ch.lo[c + 1], [&](int a, int sl) {
+    double s[3];
+    node_row_dot_x<L>(A, vals, pa, a, sl, s[0], s[1], s[2]);
+    if (a >= 0 && sl == 0) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const double pi = pa(3LL * a + i);
+        if (pout) pout[3 * a + i] = pi;
+        Ap[3 * a + i] = s[i];
+        acc[0] = fma(pi, s[i], acc[0]);
+      }
+    }
+  });
+  chunk_store<2>(acc, cpart, ch.n, c);
+}
+
+// x += alpha p ; r -= alpha Ap ; z = d r ; chunk partials r.r, z.r
+__device__ __forceinline__ void chunk_update(const Chunks ch, double al, const double* __restrict__ d,
+                                             double* __restrict__ x, double* __restrict__ r,
+                                             const double* __restrict__ p, const double* __restrict__ Ap,
+                                             double* __restrict__ z, double* __restrict__ cpart, int c) {
+  double acc[2] = {0.0, 0.0};
+  for (int k = 3 * ch.lo[c] + threadIdx.x; k < 3 * ch.lo[c + 1]; k += blockDim.x) {
+    x[k] = fma(al, p[k], x[k]);
+    const double ri = fma(-al, Ap[k], r[k]);
+    r[k] = ri;
+    const double zi = d[k] * ri;
+    z[k] = zi;
+    acc[0] = fma(ri, ri, acc[0]);
+    acc[1] = fma(zi, ri, acc[1]);
+  }
+  chunk_store<2>(acc, cpart, ch.n, c);
+}
+
+// ---- graph engine: one kernel per phase, one CTA per chunk ------------------------
+
 template <int L>
 __global__ void __launch_bounds__(TPB) k_seg_init(NodeRows A, const double* __restrict__ vals,
                                                   const double* __restrict__ x, const double* __restrict__ b,
@@ -151,63 +330,27 @@ __global__ void __launch_bounds__(TPB) k_seg_init(NodeRows A, const double* __re
                                                   double* __restrict__ cpart) {
   const int c = blockIdx.x;
   if (st[ch.scene[c]].done) return;
-  double acc[2] = {0.0, 0.0};
-  for_chunk_nodes<L>(ch.lo[c], ch.lo[c + 1], [&](int a, int sl) {
-    double s[3];
-    node_row_dot<L>(A, vals, x, a, sl, s[0], s[1], s[2]);
-    if (a >= 0 && sl == 0) {
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        double bi = b[3 * a + i], ri = bi - s[i];
-        r[3 * a + i] = ri;
-        acc[0] += bi * bi;
-        acc[1] += ri * ri;
-      }
-    }
-  });
-  chunk_store<2>(acc, cpart, ch.n);
+  chunk_init<L>(A, vals, x, b, r, ch, cpart, c);
 }
 
-// z = d r, p = z ; chunk partials z.r
 __global__ void __launch_bounds__(TPB) k_seg_prec0(const Chunks ch, const SegCg* __restrict__ st,
                                                    const double* __restrict__ d, const double* __restrict__ r,
                                                    double* __restrict__ z, double* __restrict__ p,
                                                    double* __restrict__ cpart) {
   const int c = blockIdx.x;
   if (st[ch.scene[c]].done) return;
-  double acc[2] = {0.0, 0.0};
-  for (int k = 3 * ch.lo[c] + threadIdx.x; k < 3 * ch.lo[c + 1]; k += blockDim.x) {
-    double zi = d[k] * r[k];
-    z[k] = zi;
-    p[k] = zi;
-    acc[0] += zi * r[k];
-  }
-  chunk_store<2>(acc, cpart, ch.n);
+  chunk_prec0(ch, d, r, z, p, cpart, c);
 }
 
-// Ap = A p ; chunk partials p.Ap
 template <int L>
 __global__ void __launch_bounds__(TPB) k_seg_Ap(NodeRows A, const double* __restrict__ vals,
                                                 const double* __restrict__ p, double* __restrict__ Ap, const Chunks ch,
                                                 const SegCg* __restrict__ st, double* __restrict__ cpart) {
   const int c = blockIdx.x;
   if (st[ch.scene[c]].done) return;
-  double acc[2] = {0.0, 0.0};
-  for_chunk_nodes<L>(ch.lo[c], ch.lo[c + 1], [&](int a, int sl) {
-    double s[3];
-    node_row_dot<L>(A, vals, p, a, sl, s[0], s[1], s[2]);
-    if (a >= 0 && sl == 0) {
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        Ap[3 * a + i] = s[i];
-        acc[0] += p[3 * a + i] * s[i];
-      }
-    }
-  });
-  chunk_store<2>(acc, cpart, ch.n);
+  chunk_Ap<L>(A, vals, XVec{p}, nullptr, Ap, ch, cpart, c);
 }
 
-// x += alpha p ; r -= alpha Ap ; z = d r ; chunk partials r.r, z.r
 __global__ void __launch_bounds__(TPB) k_seg_update(const Chunks ch, const SegCg* __restrict__ st,
                                                     const double* __restrict__ d, double* __restrict__ x,
                                                     double* __restrict__ r, const double* __restrict__ p,
@@ -216,18 +359,7 @@ __global__ void __launch_bounds__(TPB) k_seg_update(const Chunks ch, const SegCg
   const int c = blockIdx.x;
   const SegCg& sc = st[ch.scene[c]];
   if (sc.done) return;
-  const double al = sc.alpha;
-  double acc[2] = {0.0, 0.0};
-  for (int k = 3 * ch.lo[c] + threadIdx.x; k < 3 * ch.lo[c + 1]; k += blockDim.x) {
-    x[k] = x[k] + al * p[k];
-    double ri = r[k] - al * Ap[k];
-    r[k] = ri;
-    double zi = d[k] * ri;
-    z[k] = zi;
-    acc[0] += ri * ri;
-    acc[1] += zi * ri;
-  }
-  chunk_store<2>(acc, cpart, ch.n);
+  chunk_update(ch, sc.alpha, d, x, r, p, Ap, z, cpart, c);
 }
 
 // p = z + beta p
@@ -237,7 +369,146 @@ __global__ void __launch_bounds__(TPB) k_seg_p(const Chunks ch, const SegCg* __r
   const SegCg& sc = st[ch.scene[c]];
   if (sc.done) return;
   const double be = sc.beta;
-  for (int k = 3 * ch.lo[c] + threadIdx.x; k < 3 * ch.lo[c + 1]; k += blockDim.x) p[k] = z[k] + be * p[k];
+  for (int k = 3 * ch.lo[c] + threadIdx.x; k < 3 * ch.lo[c + 1]; k += blockDim.x) p[k] = fma(be, p[k], z[k]);
+}
+
+// ---- persistent engine: one cooperative launch per solve --------------------------
+// CTA g takes chunks g, g + G, ... in every phase (the work of the scenes still
+// running spreads over all CTAs).  Between phases a grid barrier: the last CTA
+// to arrive applies the scene updates (one warp per scene, the same sums and
+// steps as k_seg_finalize) and counts the scenes still running before it
+// releases the others.  The search direction is double-buffered and formed on
+// the fly inside A p (z + beta p_old), which drops the third barrier of the
+// graph engine's iteration.  Every wait is bounded (2 s): a wait that runs
+// out raises `abort`, and every CTA returns.
+struct SegGrid {
+  unsigned count;  // CTAs arrived at the current barrier
+  unsigned gen;    // barrier generation
+  int active;      // scenes still running after the last scene update
+  int abort;       // a wait ran out
+};
+
+struct PersistArgs {
+  NodeRows A;
+  const double* vals;
+  const double* d;
+  const double* b;
+  double* x;
+  double* r;
+  double* z;
+  double* p0;
+  double* p1;
+  double* Ap;
+  double* cpart;
+  Chunks ch;
+  SegCg* st;
+  int nscene;
+  double tol;
+  long long max_iter;
+  long long max_loop;  // bound on the kernel's own iterations
+  SegGrid* g;
+};
+
+__device__ void persist_scene_updates(const PersistArgs& P, int mode) {
+  __shared__ int s_cnt;
+  if (threadIdx.x == 0) s_cnt = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int cnt = 0;
+  for (int s = w; s < P.nscene; s += nw) {
+    SegCg& c = P.st[s];
+    scene_finalize_warp(mode, P.ch, P.cpart, c, s, P.tol, P.max_iter);
+    __syncwarp();
+    if (lane == 0 && !c.done) ++cnt;
+  }
+  if (lane == 0 && cnt) atomicAdd(&s_cnt, cnt);
+  __syncthreads();
+  if (threadIdx.x == 0) P.g->active = s_cnt;
+}
+
+// Grid barrier with the scene updates of `mode`; false if a wait ran out.
+__device__ bool persist_sync(const PersistArgs& P, int mode) {
+  __shared__ int s_last, s_ok;
+  __shared__ unsigned s_gen;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_gen = *(volatile unsigned*)&P.g->gen;
+    __threadfence();
+    s_last = atomicAdd(&P.g->count, 1u) == gridDim.x - 1u;
+    s_ok = 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    persist_scene_updates(P, mode);
+    if (threadIdx.x == 0) {
+      P.g->count = 0u;
+      __threadfence();
+      atomicAdd(&P.g->gen, 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    const uint64_t t0 = pipe::clock_ns();
+    for (;;) {
+      if (*(volatile unsigned*)&P.g->gen != s_gen) break;
+      if (*(volatile int*)&P.g->abort) {
+        s_ok = 0;
+        break;
+      }
+      if (pipe::clock_ns() - t0 > pipe::HOEFEM_WAIT_NS) {
+        atomicExch(&P.g->abort, 1);
+        s_ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <int L>
+__global__ void __launch_bounds__(TPB) k_seg_persistent(const PersistArgs P) {
+  const Chunks ch = P.ch;
+  const int G = gridDim.x;
+  for (int c = blockIdx.x; c < ch.n; c += G)
+    if (!P.st[ch.scene[c]].done) chunk_init<L>(P.A, P.vals, P.x, P.b, P.r, ch, P.cpart, c);
+  if (!persist_sync(P, 0)) return;
+  for (int c = blockIdx.x; c < ch.n; c += G)
+    if (!P.st[ch.scene[c]].done) chunk_prec0(ch, P.d, P.r, P.z, nullptr, P.cpart, c);
+  if (!persist_sync(P, 1)) return;
+  for (long long it = 0; it < P.max_loop; ++it) {
+    if (*(volatile int*)&P.g->active == 0) break;
+    const double* pold = (it & 1) ? P.p1 : P.p0;
+    double* pnew = (it & 1) ? P.p0 : P.p1;
+    for (int c = blockIdx.x; c < ch.n; c += G) {
+      const SegCg& sc = P.st[ch.scene[c]];
+      if (sc.done) continue;
+      const XDir pa{P.z, pold, sc.beta, it == 0 ? 1 : 0};
+      chunk_Ap<L>(P.A, P.vals, pa, pnew, P.Ap, ch, P.cpart, c);
+    }
+    if (!persist_sync(P, 2)) return;
+    for (int c = blockIdx.x; c < ch.n; c += G) {
+      const SegCg& sc = P.st[ch.scene[c]];
+      if (sc.done) continue;
+      chunk_update(ch, sc.alpha, P.d, P.x, P.r, pnew, P.Ap, P.z, P.cpart, c);
+    }
+    if (!persist_sync(P, 3)) return;
+  }
+}
+
+template <int L>
+int persistent_blocks_per_sm() {
+  int occ = 0;
+  HOEFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_seg_persistent<L>, TPB, 0));
+  return occ;
+}
+
+template <int L>
+void launch_persistent(const PersistArgs& args, int G, cudaStream_t s) {
+  PersistArgs a = args;
+  void* kargs[] = {&a};
+  note_launch();
+  HOEFEM_CUDA(cudaLaunchCooperativeKernel((const void*)k_seg_persistent<L>, G, TPB, kargs, 0, s));
 }
 
 // per-scene sum of squares of a vector into out[s]: chunk partials, then scenes
@@ -246,7 +517,7 @@ __global__ void __launch_bounds__(TPB) k_chunk_norm2(const Chunks ch, const doub
   const int c = blockIdx.x;
   double acc[1] = {0.0};
   for (int k = 3 * ch.lo[c] + threadIdx.x; k < 3 * ch.lo[c + 1]; k += blockDim.x) acc[0] += v[k] * v[k];
-  chunk_store<1>(acc, cpart, ch.n);
+  chunk_store<1>(acc, cpart, ch.n, c);
 }
 
 __global__ void k_seg_norm2(const Chunks ch, const double* __restrict__ cpart, double* __restrict__ out) {
@@ -445,6 +716,13 @@ struct Batch {
   std::vector<SegCg> h_st;
   cudaGraphExec_t graph = nullptr;
   long long graph_kernels = 0;
+  // CG engine: requested (HOEFEM_CG_ENGINE_*, CTAs per multiprocessor for the
+  // persistent engine, 0 = as many as fit) and the autotuner's choice
+  int cg_engine = HOEFEM_CG_ENGINE_AUTO, cg_ctas = 0;
+  int tuned_engine = -1, tuned_ctas = 0, persist_occ = 0;
+  std::vector<float> tune_ms;
+  DBuf<double> p2;  // second search-direction buffer of the persistent engine
+  DBuf<SegGrid> sgrid;
   // per-scene results of the last step
   std::vector<i64> st_newton, st_cg_solves, st_cg_total, st_cg_max, st_substeps;
   std::vector<int> status, st_cg_last;
@@ -549,40 +827,49 @@ struct Batch {
     const Chunks ch = chunks();
     HOEFEM_LANES_DISPATCH(A.lanes, (note_launch(), k_seg_Ap<LN><<<nch, TPB, 0, s>>>(A, J.p, p.p, Ap.p, ch, st.p,
                                                                                    cpart.p)));
-    (note_launch(), k_seg_finalize<<<nscene, TPB, 0, s>>>(2, ch, cpart.p, st.p, cg_tol, cg_max));
+    (note_launch(), k_seg_finalize<<<nscene, 32, 0, s>>>(2, ch, cpart.p, st.p, cg_tol, cg_max));
     (note_launch(), k_seg_update<<<nch, TPB, 0, s>>>(ch, st.p, diag.p, x.p, r.p, p.p, Ap.p, z.p, cpart.p));
-    (note_launch(), k_seg_finalize<<<nscene, TPB, 0, s>>>(3, ch, cpart.p, st.p, cg_tol, cg_max));
+    (note_launch(), k_seg_finalize<<<nscene, 32, 0, s>>>(3, ch, cpart.p, st.p, cg_tol, cg_max));
     (note_launch(), k_seg_p<<<nch, TPB, 0, s>>>(ch, st.p, z.p, p.p));
   }
 
-  // batched PCG with the diagonal preconditioner on J for the active scenes
-  void cg(const std::vector<unsigned char>& active) {
+  void ensure_graph() {
+    if (graph) return;
+    cudaStream_t cs;
+    HOEFEM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    HOEFEM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    g_capture_count = 0;
+    for (int k = 0; k < chunk; ++k) enqueue_iter(cs);
+    graph_kernels = g_capture_count;
+    g_capture_count = -1;
+    HOEFEM_CUDA(cudaStreamEndCapture(cs, &g));
+    HOEFEM_CUDA(cudaGraphInstantiate(&graph, g, 0));
+    cudaGraphDestroy(g);
+    cudaStreamDestroy(cs);
+  }
+
+  // the active scenes start from x = 0, the others are marked finished
+  void cg_start(const std::vector<unsigned char>& active) {
     cudaStream_t s = m.stream;
-    NodeRows A = m.rows();
     HOEFEM_CUDA(cudaMemcpyAsync(d_active.p, active.data(), nscene, cudaMemcpyHostToDevice, s));
     (note_launch(), k_seg_mask_done<<<(nscene + 127) / 128, 128, 0, s>>>(nscene, d_active.p, st.p));
     HOEFEM_CUDA(cudaMemsetAsync(x.p, 0, sizeof(double) * m.ndof, s));
+  }
+
+  // graph engine: the set-up kernels, then graphs of `chunk` iterations until
+  // every scene has finished (the host reads the scene states between graphs)
+  void cg_graphs() {
+    cudaStream_t s = m.stream;
+    NodeRows A = m.rows();
     const Chunks ch = chunks();
     HOEFEM_LANES_DISPATCH(A.lanes, (note_launch(), k_seg_init<LN><<<nch, TPB, 0, s>>>(A, J.p, x.p, b.p, r.p, ch,
                                                                                      st.p, cpart.p)));
-    (note_launch(), k_seg_finalize<<<nscene, TPB, 0, s>>>(0, ch, cpart.p, st.p, cg_tol, cg_max));
+    (note_launch(), k_seg_finalize<<<nscene, 32, 0, s>>>(0, ch, cpart.p, st.p, cg_tol, cg_max));
     (note_launch(), k_seg_prec0<<<nch, TPB, 0, s>>>(ch, st.p, diag.p, r.p, z.p, p.p, cpart.p));
-    (note_launch(), k_seg_finalize<<<nscene, TPB, 0, s>>>(1, ch, cpart.p, st.p, cg_tol, cg_max));
+    (note_launch(), k_seg_finalize<<<nscene, 32, 0, s>>>(1, ch, cpart.p, st.p, cg_tol, cg_max));
     HOEFEM_CUDA(cudaGetLastError());
-    if (!graph) {
-      cudaStream_t cs;
-      HOEFEM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-      cudaGraph_t g;
-      HOEFEM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-      g_capture_count = 0;
-      for (int k = 0; k < chunk; ++k) enqueue_iter(cs);
-      graph_kernels = g_capture_count;
-      g_capture_count = -1;
-      HOEFEM_CUDA(cudaStreamEndCapture(cs, &g));
-      HOEFEM_CUDA(cudaGraphInstantiate(&graph, g, 0));
-      cudaGraphDestroy(g);
-      cudaStreamDestroy(cs);
-    }
+    ensure_graph();
     h_st.resize(nscene);
     const i64 max_chunks = (cg_max >= 0 ? cg_max : 10 * m.ndof) / chunk + 2;
     for (i64 c = 0; c <= max_chunks; ++c) {
@@ -595,6 +882,101 @@ struct Batch {
       g_launch_count.fetch_add(graph_kernels, std::memory_order_relaxed);
     }
     // zero-rhs scenes: x = 0 already (x was zeroed and never updated)
+  }
+
+  int persistent_occupancy() {
+    if (persist_occ == 0) {
+      HOEFEM_LANES_DISPATCH(m.rows().lanes, persist_occ = persistent_blocks_per_sm<LN>());
+      HOEFEM_REQUIRE(persist_occ >= 1, HOEFEM_ERR_CUDA, "persistent batched CG kernel does not fit on a multiprocessor");
+    }
+    return persist_occ;
+  }
+
+  // persistent engine: one cooperative launch runs the whole solve of every
+  // active scene with `per` CTAs per multiprocessor (0: as many as fit)
+  void cg_persistent(int per) {
+    cudaStream_t s = m.stream;
+    NodeRows A = m.rows();
+    const int occ = persistent_occupancy();
+    per = per <= 0 ? occ : std::min(per, occ);
+    const int G = std::max(1, std::min(nch, per * device_sms()));
+    if (!p2.p) p2.alloc(m.ndof);
+    if (!sgrid.p) sgrid.alloc(1);
+    HOEFEM_CUDA(cudaMemsetAsync(sgrid.p, 0, sizeof(SegGrid), s));
+    PersistArgs a;
+    a.A = A;
+    a.vals = J.p;
+    a.d = diag.p;
+    a.b = b.p;
+    a.x = x.p;
+    a.r = r.p;
+    a.z = z.p;
+    a.p0 = p.p;
+    a.p1 = p2.p;
+    a.Ap = Ap.p;
+    a.cpart = cpart.p;
+    a.ch = chunks();
+    a.st = st.p;
+    a.nscene = nscene;
+    a.tol = cg_tol;
+    a.max_iter = cg_max;
+    a.max_loop = (cg_max >= 0 ? cg_max : 10 * m.ndof) + 2;
+    a.g = sgrid.p;
+    HOEFEM_LANES_DISPATCH(A.lanes, launch_persistent<LN>(a, G, s));
+    h_st.resize(nscene);
+    SegGrid hg;
+    HOEFEM_CUDA(cudaMemcpyAsync(h_st.data(), st.p, sizeof(SegCg) * nscene, cudaMemcpyDeviceToHost, s));
+    HOEFEM_CUDA(cudaMemcpyAsync(&hg, sgrid.p, sizeof(SegGrid), cudaMemcpyDeviceToHost, s));
+    HOEFEM_CUDA(cudaStreamSynchronize(s));
+    if (hg.abort) throw Error(HOEFEM_ERR_DEVICE_TIMEOUT, "persistent batched CG: device wait ran out");
+  }
+
+  void run_cg(const std::vector<unsigned char>& active, int engine, int per) {
+    cg_start(active);
+    if (engine == HOEFEM_CG_ENGINE_STREAMED) cg_persistent(per);
+    else cg_graphs();
+  }
+
+  // Autotuner: the first solve runs once per candidate (the graph engine, then
+  // the persistent engine at 1, 2, 4, ... CTAs per multiprocessor up to the
+  // occupancy limit) and the fastest is kept.  Every candidate is a complete
+  // solve of the same system with the same arithmetic, so the last one leaves
+  // the result.
+  void tune(const std::vector<unsigned char>& active) {
+    cudaStream_t s = m.stream;
+    ensure_graph();
+    std::vector<std::pair<int, int>> cand = {{HOEFEM_CG_ENGINE_CHUNKED, 0}};
+    const int occ = persistent_occupancy();
+    for (int k = 1; k < occ; k *= 2) cand.push_back({HOEFEM_CG_ENGINE_STREAMED, k});
+    cand.push_back({HOEFEM_CG_ENGINE_STREAMED, occ});
+    cudaEvent_t e0, e1;
+    HOEFEM_CUDA(cudaEventCreate(&e0));
+    HOEFEM_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    tune_ms.clear();
+    for (auto& c : cand) {
+      HOEFEM_CUDA(cudaEventRecord(e0, s));
+      run_cg(active, c.first, c.second);
+      HOEFEM_CUDA(cudaEventRecord(e1, s));
+      HOEFEM_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      HOEFEM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      tune_ms.push_back(ms);
+      if (ms < best) {
+        best = ms;
+        tuned_engine = c.first;
+        tuned_ctas = c.second;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+
+  // batched PCG with the diagonal preconditioner on J for the active scenes
+  void cg(const std::vector<unsigned char>& active) {
+    if (cg_engine != HOEFEM_CG_ENGINE_AUTO) return run_cg(active, cg_engine, cg_ctas);
+    if (tuned_engine < 0) return tune(active);
+    run_cg(active, tuned_engine, tuned_ctas);
   }
 
   // One backward-Euler step of the scenes in `part` (newton.rs:131-170 per
@@ -747,7 +1129,9 @@ struct Batch {
         try {
           be_step(sdt, part);
         } catch (Error& err2) {
-          if (err2.code == HOEFEM_ERR_CUDA || err2.code == HOEFEM_ERR_OUT_OF_MEMORY) throw;
+          if (err2.code == HOEFEM_ERR_CUDA || err2.code == HOEFEM_ERR_OUT_OF_MEMORY ||
+              err2.code == HOEFEM_ERR_DEVICE_TIMEOUT)
+            throw;
           for (int q = 0; q < nscene; ++q)
             if (part[q]) status[q] = err2.code;
         }
@@ -897,6 +1281,25 @@ Batch* batch_build(const std::vector<const Model*>& scenes, const std::vector<Ma
 void batch_delete(Batch* b) { delete b; }
 Model& batch_model(Batch* b) { return b->m; }
 int batch_step(Batch* b, double* u, double* v, double dt) { return b->step(u, v, dt); }
+void batch_set_cg_engine(Batch* b, int engine, int ctas_per_sm) {
+  HOEFEM_REQUIRE(engine >= HOEFEM_CG_ENGINE_AUTO && engine <= HOEFEM_CG_ENGINE_STREAMED && ctas_per_sm >= 0,
+                 HOEFEM_ERR_INVALID_ARGUMENT, "bad CG engine");
+  b->cg_engine = engine;
+  b->cg_ctas = ctas_per_sm;
+  b->tuned_engine = -1;
+  b->tuned_ctas = 0;
+  b->tune_ms.clear();
+}
+void batch_cg_choice(Batch* b, int* engine, int* ctas_per_sm, std::vector<float>* tune_ms) {
+  if (b->cg_engine != HOEFEM_CG_ENGINE_AUTO) {
+    *engine = b->cg_engine;
+    *ctas_per_sm = b->cg_ctas;
+  } else {
+    *engine = b->tuned_engine < 0 ? HOEFEM_CG_ENGINE_AUTO : b->tuned_engine;
+    *ctas_per_sm = b->tuned_ctas;
+  }
+  if (tune_ms) *tune_ms = b->tune_ms;
+}
 void batch_set_tolerances(Batch* b, double tol, i64 cg_max, i64 newton_max) {
   b->cg_tol = tol;
   b->cg_max = cg_max;

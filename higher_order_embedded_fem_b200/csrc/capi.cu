@@ -39,6 +39,8 @@ void batch_delete(Batch* b);
 Model& batch_model(Batch* b);
 int batch_step(Batch* b, double* u, double* v, double dt);
 void batch_set_tolerances(Batch* b, double tol, i64 cg_max, i64 newton_max);
+void batch_set_cg_engine(Batch* b, int engine, int ctas_per_sm);
+void batch_cg_choice(Batch* b, int* engine, int* ctas_per_sm, std::vector<float>* tune_ms);
 const std::vector<int>& batch_node_offsets(Batch* b);
 void batch_scene_stats(Batch* b, int k, hoefem_step_stats* out, int* status);
 void greedy_coloring(const i64* conn, i64 ne, int nn, i64 nv, std::vector<i64>& color_off,
@@ -1007,6 +1009,31 @@ int hoefem_batch_set_tolerances(hoefem_batch b, double cg_tol, int64_t cg_max_it
   API_BEGIN
   HOEFEM_REQUIRE(b && cg_tol >= 0.0 && newton_max_iter >= 0, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
   batch_set_tolerances(b->b, cg_tol, cg_max_iter, newton_max_iter);
+  API_END
+}
+
+int hoefem_batch_set_cg_engine(hoefem_batch b, int32_t engine, int32_t ctas_per_sm) {
+  API_BEGIN
+  HOEFEM_REQUIRE(b, HOEFEM_ERR_INVALID_ARGUMENT, "null batch");
+  batch_set_cg_engine(b->b, engine, ctas_per_sm);
+  API_END
+}
+
+int hoefem_batch_cg_choice(hoefem_batch b, int32_t* engine, int32_t* ctas_per_sm, float* tune_ms,
+                           int32_t* num_candidates) {
+  API_BEGIN
+  HOEFEM_REQUIRE(b && engine && ctas_per_sm, HOEFEM_ERR_INVALID_ARGUMENT, "bad arguments");
+  int e = 0, c = 0;
+  std::vector<float> t;
+  batch_cg_choice(b->b, &e, &c, &t);
+  *engine = e;
+  *ctas_per_sm = c;
+  if (num_candidates) {
+    const int cap = *num_candidates;
+    *num_candidates = (int32_t)t.size();
+    if (tune_ms)
+      for (int k = 0; k < cap && k < (int)t.size(); ++k) tune_ms[k] = t[k];
+  }
   API_END
 }
 

@@ -355,6 +355,21 @@ class BatchedNewtonCgIntegrator3d:
     def set_tolerances(self, cg_tol=1e-5, cg_max_iter=500, newton_max_iter=100):
         check(lib().hoefem_batch_set_tolerances(self._h, cg_tol, cg_max_iter, newton_max_iter))
 
+    def set_cg_engine(self, engine="auto", ctas_per_sm=0):
+        """'chunked': CUDA graphs of per-phase kernels; 'streamed': one
+        persistent launch per solve (ctas_per_sm CTAs per multiprocessor, 0 =
+        as many as fit); 'auto': the autotuner times both on the first solve
+        (see hoefem_batch_set_cg_engine).  Results do not depend on it."""
+        check(lib().hoefem_batch_set_cg_engine(self._h, _capi.CG_ENGINE[engine], int(ctas_per_sm)))
+
+    def cg_choice(self):
+        """(engine name, CTAs per multiprocessor, autotuner ms per candidate)."""
+        e, c, n = C.c_int32(), C.c_int32(), C.c_int32(16)
+        t = (C.c_float * 16)()
+        check(lib().hoefem_batch_cg_choice(self._h, C.byref(e), C.byref(c), C.cast(t, C.c_void_p), C.byref(n)))
+        names = {v: k for k, v in _capi.CG_ENGINE.items()}
+        return names[e.value], c.value, [t[k] for k in range(min(n.value, 16))]
+
     def split(self, x):
         """Per-scene views of a concatenated DOF vector."""
         o = self.dof_offsets

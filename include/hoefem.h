@@ -474,7 +474,8 @@ int hoefem_integrator_set_learned(hoefem_integrator it, hoefem_learned l, int mo
    substepping.  All scenes share every kernel launch: the scenes' elements
    are merged per element kind (per-element Lame parameters), colored once
    (each scene keeps its own greedy coloring) and the CG iterations of all
-   scenes run together in CUDA-graph chunks with per-scene stopping tests.
+   scenes run together with per-scene stopping tests, in CUDA-graph chunks or
+   in one persistent launch per solve (hoefem_batch_set_cg_engine).
    models: num_scenes models (not necessarily finalized; their vertices,
    blocks and quadrature are copied); materials: one per scene, all of one
    kind; bc_offsets (num_scenes+1) / bc_nodes: Dirichlet nodes per scene, local
@@ -489,6 +490,23 @@ int hoefem_batch_destroy(hoefem_batch b);
 int hoefem_batch_set_stream(hoefem_batch b, void* stream);
 /* Defaults as hoefem_integrator_set_tolerances: 1e-5, 500, 100. */
 int hoefem_batch_set_tolerances(hoefem_batch b, double cg_tol, int64_t cg_max_iter, int64_t newton_max_iter);
+/* CG engine of the batch (no counterpart in the reference).
+   HOEFEM_CG_ENGINE_CHUNKED: CUDA graphs of 8 iterations of per-phase kernels
+   (one CTA per 256-node chunk), the host reads the scene states between
+   graphs.  HOEFEM_CG_ENGINE_STREAMED: one persistent cooperative launch per
+   solve runs every iteration of every scene (grid barriers with bounded waits;
+   a wait that runs out gives HOEFEM_ERR_DEVICE_TIMEOUT) with ctas_per_sm CTAs
+   per multiprocessor (0: as many as fit).  HOEFEM_CG_ENGINE_AUTO (default):
+   the autotuner runs the first solve once per candidate (the graphs, then the
+   persistent launch at 1, 2, 4, ... CTAs per multiprocessor) and keeps the
+   fastest.  All engines give bitwise the same results. */
+int hoefem_batch_set_cg_engine(hoefem_batch b, int32_t engine, int32_t ctas_per_sm);
+/* The engine in use (HOEFEM_CG_ENGINE_AUTO while the autotuner has not run
+   yet) and its CTAs per multiprocessor; tune_ms (capacity *num_candidates,
+   may be NULL) receives the autotuner's time per candidate in the order above,
+   *num_candidates their number (0 before tuning). */
+int hoefem_batch_cg_choice(hoefem_batch b, int32_t* engine, int32_t* ctas_per_sm, float* tune_ms,
+                           int32_t* num_candidates);
 /* dof_offsets: num_scenes+1 (may be NULL). */
 int hoefem_batch_sizes(hoefem_batch b, int64_t* num_scenes, int64_t* ndof, int64_t* nnz, int64_t* dof_offsets);
 /* One time step of every scene; u, v (total ndof) updated in place for every

@@ -2,7 +2,8 @@
 
 Every scene of a batch must end where the oracle's backward-Euler Newton-CG
 step (diagonal preconditioner) takes it alone: displacement and velocity
-within 1e-8 relative, the same number of Newton iterations.
+within 1e-8 relative, the same number of Newton iterations.  The CG engines
+of the batch (graphs, persistent launch, autotuned) give the same bits.
 """
 import numpy as np
 import pytest
@@ -133,3 +134,34 @@ def test_batch_failure_is_per_scene(batch_inputs):
     integ.set_tolerances(1e-5, 500, 0)
     with pytest.raises(H.HoefemError):
         integ.step(parts[1].copy(), np.zeros_like(parts[1]), 0.0, 1e-3)
+
+
+@pytest.mark.parametrize("cg_tol,cg_max", [(1e-5, 500), (1e-9, 60)])
+def test_batch_cg_engines_give_the_same_bits(batch_inputs, cg_tol, cg_max):
+    # The graph engine, the persistent launch at several grid sizes and the
+    # autotuned choice run the same arithmetic: identical states and statistics
+    # (also when the iteration cap ends solves early).
+    models = [x[1] for x in batch_inputs]
+    mats = [x[2] for x in batch_inputs]
+    bcs = [x[4] for x in batch_inputs]
+    u0 = np.concatenate([x[5] for x in batch_inputs])
+    out = {}
+    for key in [("chunked", 0), ("streamed", 0), ("streamed", 1), ("streamed", 2), ("auto", 0)]:
+        B = H.BatchedNewtonCgIntegrator3d(models, mats, 1000.0, bcs)
+        B.set_tolerances(cg_tol, cg_max, 100)
+        B.set_cg_engine(*key)
+        u, v = u0.copy(), np.zeros_like(u0)
+        stats = []
+        for _ in range(2):
+            stats.append(B.step(u, v, 0.0, 1e-3, raise_on_failure=False))
+        drop = ("ms_total",)
+        stats = [[{k: x for k, x in d.items() if k not in drop} for d in st] for st in stats]
+        out[key] = (u, v, stats, B.cg_choice())
+    ua, va, sa, _ = out[("chunked", 0)]
+    for key, (u, v, st, choice) in out.items():
+        assert np.array_equal(u, ua) and np.array_equal(v, va), key
+        assert st == sa, key
+    eng, per, times = out[("auto", 0)][3]
+    print("autotuner: %s, %d CTAs/SM, candidates (ms) %s" % (eng, per, ["%.2f" % t for t in times]))
+    assert eng in ("chunked", "streamed") and len(times) >= 2
+    assert out[("streamed", 1)][3][:2] == ("streamed", 1)
