@@ -373,8 +373,8 @@ __global__ void __launch_bounds__(TPB) k_seg_p(const Chunks ch, const SegCg* __r
 }
 
 // ---- persistent engine: one cooperative launch per solve --------------------------
-// CTA g takes chunks g, g + G, ... in every phase (the work of the scenes still
-// running spreads over all CTAs).  Between phases a grid barrier: the last CTA
+// In every phase the CTAs claim chunks from a shared counter (the work of the
+// scenes still running spreads over all CTAs).  Between phases a grid barrier: the last CTA
 // to arrive applies the scene updates (one warp per scene, the same sums and
 // steps as k_seg_finalize) and counts the scenes still running before it
 // releases the others.  The search direction is double-buffered and formed on
@@ -386,6 +386,7 @@ struct SegGrid {
   unsigned gen;    // barrier generation
   int active;      // scenes still running after the last scene update
   int abort;       // a wait ran out
+  int next;        // next chunk to claim in the current phase
 };
 
 struct PersistArgs {
@@ -409,17 +410,50 @@ struct PersistArgs {
   SegGrid* g;
 };
 
+// The last CTA's scene updates: each warp takes SPW scenes at a time and issues
+// all their loads before the sums (the same lane-strided sums and xor trees as
+// scene_finalize_warp, so the same bits), then the count of running scenes.
 __device__ void persist_scene_updates(const PersistArgs& P, int mode) {
+  constexpr int SPW = 4;
   __shared__ int s_cnt;
   if (threadIdx.x == 0) s_cnt = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const Chunks ch = P.ch;
   int cnt = 0;
-  for (int s = w; s < P.nscene; s += nw) {
-    SegCg& c = P.st[s];
-    scene_finalize_warp(mode, P.ch, P.cpart, c, s, P.tol, P.max_iter);
-    __syncwarp();
-    if (lane == 0 && !c.done) ++cnt;
+  for (int s0 = w * SPW; s0 < P.nscene; s0 += nw * SPW) {
+    int lo[SPW], hi[SPW], run[SPW];
+#pragma unroll
+    for (int j = 0; j < SPW; ++j) {
+      const int s = s0 + j;
+      run[j] = s < P.nscene ? (P.st[s].done == 0) : 0;
+      lo[j] = s < P.nscene ? ch.cs_off[s] : 0;
+      hi[j] = s < P.nscene ? ch.cs_off[s + 1] : 0;
+    }
+    double acc[SPW][2];
+#pragma unroll
+    for (int j = 0; j < SPW; ++j) {
+      acc[j][0] = acc[j][1] = 0.0;
+      if (run[j])
+        for (int c = lo[j] + lane; c < hi[j]; c += 32) {
+          acc[j][0] += P.cpart[c];
+          acc[j][1] += P.cpart[(size_t)ch.n + c];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < SPW; ++j) {
+      const double v[2] = {warp_sum_d(acc[j][0]), warp_sum_d(acc[j][1])};
+      const int s = s0 + j;
+      if (lane == 0 && s < P.nscene) {
+        SegCg& c = P.st[s];
+        if (run[j]) scene_update(mode, c, v, P.tol, P.max_iter);
+        else if (mode == 1) {
+          c.iters = 0;
+          c.status = HOEFEM_OK;
+        }
+        if (!c.done) ++cnt;
+      }
+    }
   }
   if (lane == 0 && cnt) atomicAdd(&s_cnt, cnt);
   __syncthreads();
@@ -427,6 +461,7 @@ __device__ void persist_scene_updates(const PersistArgs& P, int mode) {
 }
 
 // Grid barrier with the scene updates of `mode`; false if a wait ran out.
+// The last CTA also resets the chunk counter of the next phase.
 __device__ bool persist_sync(const PersistArgs& P, int mode) {
   __shared__ int s_last, s_ok;
   __shared__ unsigned s_gen;
@@ -443,6 +478,7 @@ __device__ bool persist_sync(const PersistArgs& P, int mode) {
     persist_scene_updates(P, mode);
     if (threadIdx.x == 0) {
       P.g->count = 0u;
+      P.g->next = 0;
       __threadfence();
       atomicAdd(&P.g->gen, 1u);
     }
@@ -459,6 +495,7 @@ __device__ bool persist_sync(const PersistArgs& P, int mode) {
         s_ok = 0;
         break;
       }
+      __nanosleep(128);
     }
     __threadfence();
   }
@@ -466,32 +503,42 @@ __device__ bool persist_sync(const PersistArgs& P, int mode) {
   return s_ok != 0;
 }
 
+// The chunks of a phase, claimed one at a time from the shared counter
+// (dynamic balance: chunk costs differ by element kind and scenes finish at
+// different iterations); body(c) for every claimed chunk of a running scene.
+template <class F>
+__device__ __forceinline__ void persist_chunks(const PersistArgs& P, F&& body) {
+  __shared__ int s_chunk;
+  for (;;) {
+    if (threadIdx.x == 0) s_chunk = atomicAdd(&P.g->next, 1);
+    __syncthreads();
+    const int c = s_chunk;
+    __syncthreads();
+    if (c >= P.ch.n) break;
+    const SegCg& sc = P.st[P.ch.scene[c]];
+    if (!sc.done) body(c, sc);
+  }
+}
+
 template <int L>
-__global__ void __launch_bounds__(TPB) k_seg_persistent(const PersistArgs P) {
+__global__ void __launch_bounds__(TPB, 5) k_seg_persistent(const PersistArgs P) {
   const Chunks ch = P.ch;
-  const int G = gridDim.x;
-  for (int c = blockIdx.x; c < ch.n; c += G)
-    if (!P.st[ch.scene[c]].done) chunk_init<L>(P.A, P.vals, P.x, P.b, P.r, ch, P.cpart, c);
+  persist_chunks(P, [&](int c, const SegCg&) { chunk_init<L>(P.A, P.vals, P.x, P.b, P.r, ch, P.cpart, c); });
   if (!persist_sync(P, 0)) return;
-  for (int c = blockIdx.x; c < ch.n; c += G)
-    if (!P.st[ch.scene[c]].done) chunk_prec0(ch, P.d, P.r, P.z, nullptr, P.cpart, c);
+  persist_chunks(P, [&](int c, const SegCg&) { chunk_prec0(ch, P.d, P.r, P.z, nullptr, P.cpart, c); });
   if (!persist_sync(P, 1)) return;
   for (long long it = 0; it < P.max_loop; ++it) {
     if (*(volatile int*)&P.g->active == 0) break;
     const double* pold = (it & 1) ? P.p1 : P.p0;
     double* pnew = (it & 1) ? P.p0 : P.p1;
-    for (int c = blockIdx.x; c < ch.n; c += G) {
-      const SegCg& sc = P.st[ch.scene[c]];
-      if (sc.done) continue;
+    persist_chunks(P, [&](int c, const SegCg& sc) {
       const XDir pa{P.z, pold, sc.beta, it == 0 ? 1 : 0};
       chunk_Ap<L>(P.A, P.vals, pa, pnew, P.Ap, ch, P.cpart, c);
-    }
+    });
     if (!persist_sync(P, 2)) return;
-    for (int c = blockIdx.x; c < ch.n; c += G) {
-      const SegCg& sc = P.st[ch.scene[c]];
-      if (sc.done) continue;
+    persist_chunks(P, [&](int c, const SegCg& sc) {
       chunk_update(ch, sc.alpha, P.d, P.x, P.r, pnew, P.Ap, P.z, P.cpart, c);
-    }
+    });
     if (!persist_sync(P, 3)) return;
   }
 }
