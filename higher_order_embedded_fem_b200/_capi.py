@@ -58,7 +58,8 @@ class StepStats(C.Structure):
 class CgEngineStats(C.Structure):
     _fields_ = [("launches", C.c_int64), ("iterations", C.c_int64), ("device_ms", C.c_double),
                 ("operator_bytes", C.c_int64), ("schwarz_bytes", C.c_int64), ("phase_us", C.c_double * 12),
-                ("auto_us_per_iteration", C.c_double * 2), ("auto_choice", C.c_int32)]
+                ("auto_us_per_iteration", C.c_double * 2), ("auto_choice", C.c_int32),
+                ("phase_us_max", C.c_double * 12), ("busy_us", C.c_double * 2)]
 
 
 CG_ENGINE = {"auto": 0, "chunked": 1, "streamed": 2}

@@ -729,7 +729,7 @@ static void engine_stats(CgWork& w, const Precond* P, hoefem_cg_engine_stats* ou
   out->device_ms = w.stream_ms_total;
   out->operator_bytes = w.sop32.vsize && w.last_f32 ? w.sop32.bytes : w.sop64.bytes;
   out->schwarz_bytes = (P && P->kind == PREC_SCHWARZ) ? w.ssw.bytes : 0;
-  cg_stream_phase_us(w, out->phase_us);
+  cg_stream_phase_us(w, out->phase_us, out->phase_us_max, out->busy_us);
   const CgWork::EngineTune& et = w.etune[w.last_tune];
   out->auto_us_per_iteration[0] = et.us_per_it[0];
   out->auto_us_per_iteration[1] = et.us_per_it[1];

@@ -766,6 +766,105 @@ void split_items(const std::vector<CgsItem>& items, int G, std::vector<int>& off
   while (g <= G) off[g++] = (int)items.size();
 }
 
+// CTA ranges for an operator + Schwarz stream.  The operator tiles and the
+// Schwarz rows of an iteration run in two phases that each end at a grid
+// barrier, so an iteration costs about max_g A_g + max_g B_g (A_g: operator
+// bytes of range g; B_g: its Schwarz bytes at the operator's value size,
+// times kappa, their measured cost per byte relative to the operator tiles).
+// For caps T1 on A from 1.0 to 1.6 times the mean, the smallest cap T2 on B
+// for which the greedy cut (each range extended while both sums stay within
+// the caps; it needs the fewest ranges of any cut under these caps) fits in G
+// ranges is found by bisection, and the pair with the smallest T1 + T2 is
+// kept.  If the cut uses fewer than G ranges, the heaviest ranges are halved.
+void split_items_phases(const std::vector<CgsItem>& items, const std::vector<long long>& swb, double kappa, int G,
+                        std::vector<int>& off) {
+  const size_t n = items.size();
+  if (n == 0 || G <= 1) return split_items(items, G, off, &swb);
+  std::vector<double> a(n), b(n);
+  double sa = 0.0, sb = 0.0, ma = 0.0, mb = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    a[i] = (double)items[i].bytes;
+    b[i] = kappa * (double)swb[i];
+    sa += a[i];
+    sb += b[i];
+    ma = std::max(ma, a[i]);
+    mb = std::max(mb, b[i]);
+  }
+  auto ranges = [&](double T1, double T2) {
+    int g = 1;
+    double x = 0.0, y = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+      if (x + a[i] > T1 || y + b[i] > T2) {
+        if (++g > G) return g;
+        x = y = 0.0;
+      }
+      x += a[i];
+      y += b[i];
+    }
+    return g;
+  };
+  const double mA = sa / G, mB = sb / G;
+  double best = -1.0, bT1 = 0.0, bT2 = 0.0;
+  for (int k = 0; k <= 40; ++k) {
+    const double T1 = std::max(ma, mA * (1.0 + 0.015 * k));
+    double lo = std::max(mb, mB), hi = 4.0 * lo + sb / 16.0;
+    if (ranges(T1, hi) > G) continue;
+    for (int it = 0; it < 30; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      if (ranges(T1, mid) > G) lo = mid;
+      else hi = mid;
+    }
+    if (best < 0.0 || T1 + hi < best) {
+      best = T1 + hi;
+      bT1 = T1;
+      bT2 = hi;
+    }
+  }
+  if (best < 0.0) return split_items(items, G, off, &swb);
+  off.assign(1, 0);
+  {
+    double x = 0.0, y = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+      if (x + a[i] > bT1 || y + b[i] > bT2) {
+        off.push_back((int)i);
+        x = y = 0.0;
+      }
+      x += a[i];
+      y += b[i];
+    }
+    off.push_back((int)n);
+  }
+  while ((int)off.size() - 1 < G) {
+    int r = -1;
+    double worst = -1.0;
+    for (size_t q = 0; q + 1 < off.size(); ++q) {
+      if (off[q + 1] - off[q] < 2) continue;
+      double x = 0.0, y = 0.0;
+      for (int i = off[q]; i < off[q + 1]; ++i) {
+        x += a[i];
+        y += b[i];
+      }
+      const double wq = std::max(x / bT1, y / bT2);
+      if (wq > worst) {
+        worst = wq;
+        r = (int)q;
+      }
+    }
+    if (r < 0) break;
+    double tot = 0.0;
+    for (int i = off[r]; i < off[r + 1]; ++i) tot += a[i] / bT1 + b[i] / bT2;
+    double c = 0.0;
+    int cut = off[r] + 1;
+    for (int i = off[r]; i < off[r + 1] - 1; ++i) {
+      c += a[i] / bT1 + b[i] / bT2;
+      cut = i + 1;
+      if (c >= 0.5 * tot) break;
+    }
+    off.insert(off.begin() + r + 1, cut);
+  }
+  while ((int)off.size() < G + 1) off.push_back((int)n);
+}
+
 // Packs consecutive records (byte sizes rec[r], each 16-aligned) into items of
 // at most STAGE bytes with a header; item.a = first record, item.b = records;
 // the records' absolute offsets go to rec_off.  False if one record alone
@@ -894,9 +993,10 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
     ++tile_id;
   }
   std::vector<int> off, nrange(G + 1);
-  // CTA ranges of about equal operator + Schwarz bytes (the Schwarz rows at
-  // the operator's value size): the producer streams both through one ring,
-  // so a CTA's iteration costs about their sum
+  // CTA ranges balanced for the two phases (split_items_phases): Schwarz
+  // bytes counted at the operator's value size cost 1.30 times the operator
+  // tile bytes per byte with FP32 values and 0.84 times with FP64 values
+  // (phase times per CTA on the benchmark cylinder)
   std::vector<long long> swb;
   if (sw) {
     swb.assign(items.size(), 0);
@@ -905,7 +1005,8 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
         for (int k = pair_off[q]; k < pair_off[q + 1]; ++k)
           swb[j] += 9LL * (P->sub_off[slot_sub[k] + 1] - P->sub_off[slot_sub[k]]) * vsize;
   }
-  split_items(items, G, off, sw ? &swb : nullptr);
+  if (sw) split_items_phases(items, swb, vsize == 8 ? 0.84 : 1.30, G, off);
+  else split_items(items, G, off, nullptr);
   for (int g = 0; g <= G; ++g) nrange[g] = off[g] < (int)items.size() ? items[off[g]].c : (int)nv;
   // segments: halo-local neighbour indices (sorted halo, times 3), own halo index
   std::vector<CgsSeg> segs;
@@ -1245,8 +1346,9 @@ bool cg_stream_prepare(CgWork& w, const double* A64, bool f32, const Precond* P,
   return true;
 }
 
-void cg_stream_phase_us(CgWork& w, double* out) {
-  for (int i = 0; i < 12; ++i) out[i] = 0.0;
+void cg_stream_phase_us(CgWork& w, double* out, double* out_max, double* busy) {
+  for (int i = 0; i < 12; ++i) out[i] = out_max[i] = 0.0;
+  busy[0] = busy[1] = 0.0;
   if (!w.phase_profile || !w.sprof.p) return;
   std::vector<unsigned long long> h(w.sprof.n);
   HOEFEM_CUDA(cudaMemcpy(h.data(), w.sprof.p, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
@@ -1260,11 +1362,26 @@ void cg_stream_phase_us(CgWork& w, double* out) {
     w.sclock_khz = khz > 0 ? khz : 1.0;
   }
   if (its > 0) {
+    const double us = 1.0 / (double)its / (w.sclock_khz * 1e-3);
     for (int i = 0; i < 12; ++i) {
-      double sum = 0.0;
-      for (int c = 0; c < G; ++c) sum += (double)h[16 * c + i];
-      out[i] = sum / G / (double)its / (w.sclock_khz * 1e-3);
+      double sum = 0.0, mx = 0.0;
+      for (int c = 0; c < G; ++c) {
+        sum += (double)h[16 * c + i];
+        mx = std::max(mx, (double)h[16 * c + i]);
+      }
+      out[i] = sum / G * us;
+      out_max[i] = mx * us;
     }
+    // work outside the grid barriers: halo gathers, operator tiles, Schwarz
+    // chunks, own-DOF update
+    double bsum = 0.0, bmax = 0.0;
+    for (int c = 0; c < G; ++c) {
+      const double b = (double)(h[16 * c + 0] + h[16 * c + 1] + h[16 * c + 4] + h[16 * c + 5] + h[16 * c + 8]);
+      bsum += b;
+      bmax = std::max(bmax, b);
+    }
+    busy[0] = bsum / G * us;
+    busy[1] = bmax * us;
   }
   HOEFEM_CUDA(cudaMemset(w.sprof.p, 0, w.sprof.n * sizeof(unsigned long long)));
 }

@@ -256,7 +256,7 @@ bool cg_stream_prepare(CgWork& w, const double* A64, bool f32, const Precond* P,
 void cg_stream_iterate(CgWork& w, bool f32, const Precond* P, bool p32, bool reliable, cudaStream_t s);
 // Per-phase microseconds per iteration of the streamed CG since the last
 // reset (zeros without HOEFEM_CG_PHASE_PROFILE); resets the counters.
-void cg_stream_phase_us(CgWork& w, double* out12);
+void cg_stream_phase_us(CgWork& w, double* out12, double* max12, double* busy2);
 // Sets the residual-replacement reference rr_ref = rr (current state) and
 // delta^2, clears the replacement flag.
 void cg_stream_arm(CgWork& w, double delta, cudaStream_t s);

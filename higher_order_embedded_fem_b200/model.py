@@ -103,7 +103,8 @@ class _Model:
         check(lib().hoefem_model_cg_engine_stats(self._h, C.byref(s)))
         out = {f: getattr(s, f) for f, _ in s._fields_}
         out["phase_us"] = list(out["phase_us"])
-        out["auto_us_per_iteration"] = list(out["auto_us_per_iteration"])
+        for k in ("auto_us_per_iteration", "phase_us_max", "busy_us"):
+            out[k] = list(out[k])
         return out
 
     def set_stream(self, stream):

@@ -391,7 +391,10 @@ int hoefem_model_set_cg_engine(hoefem_model m, int engine, int options);
    producer lifetime.  Automatic engine choice for the last solve's operator
    precision and preconditioner kind: the sampled whole-solve microseconds per
    iteration of the chunked and the streamed engine (0 until sampled) and the choice
-   (-1 undecided, 0 chunked, 1 streamed). */
+   (-1 undecided, 0 chunked, 1 streamed).  With the phase profile also the
+   largest value of each phase over the CTAs, and the mean and largest time per
+   iteration a CTA spends outside the grid barriers ([0] + [1] + [4] + [5] +
+   [8]): their ratio is the load imbalance the barriers wait for. */
 typedef struct {
   int64_t launches, iterations;
   double device_ms;
@@ -399,6 +402,8 @@ typedef struct {
   double phase_us[12];
   double auto_us_per_iteration[2];
   int32_t auto_choice;
+  double phase_us_max[12];
+  double busy_us[2];
 } hoefem_cg_engine_stats;
 int hoefem_integrator_cg_engine_stats(hoefem_integrator it, hoefem_cg_engine_stats* out);
 int hoefem_model_cg_engine_stats(hoefem_model m, hoefem_cg_engine_stats* out);
