@@ -51,6 +51,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <vector>
 
@@ -775,9 +776,16 @@ void split_items(const std::vector<CgsItem>& items, int G, std::vector<int>& off
 // for which the greedy cut (each range extended while both sums stay within
 // the caps; it needs the fewest ranges of any cut under these caps) fits in G
 // ranges is found by bisection, and the pair with the smallest T1 + T2 is
-// kept.  If the cut uses fewer than G ranges, the heaviest ranges are halved.
+// kept.  Then the cut also keeps every range within one segment (`fit`: its
+// halo and Schwarz incidences within the segment bounds, so that no CTA
+// gathers two overlapping halos), with both caps relaxed by 1% steps until
+// the cut fits in G ranges (without it if none does).  If the cut uses fewer
+// than G ranges, the heaviest ranges are halved (a part of a range fits
+// wherever the range does).  Fit: start(i) opens a range at item i, add(i)
+// extends it if the item fits.
+template <class Fit>
 void split_items_phases(const std::vector<CgsItem>& items, const std::vector<long long>& swb, double kappa, int G,
-                        std::vector<int>& off) {
+                        std::vector<int>& off, Fit& fit) {
   const size_t n = items.size();
   if (n == 0 || G <= 1) return split_items(items, G, off, &swb);
   std::vector<double> a(n), b(n);
@@ -790,17 +798,24 @@ void split_items_phases(const std::vector<CgsItem>& items, const std::vector<lon
     ma = std::max(ma, a[i]);
     mb = std::max(mb, b[i]);
   }
-  auto ranges = [&](double T1, double T2) {
+  // the greedy cut under caps (T1, T2), with or without the segment bound;
+  // stops counting past G ranges
+  auto cut = [&](double T1, double T2, bool seg, std::vector<int>* out) {
     int g = 1;
     double x = 0.0, y = 0.0;
+    if (out) out->assign(1, 0);
+    if (seg) fit.start(0);
     for (size_t i = 0; i < n; ++i) {
-      if (x + a[i] > T1 || y + b[i] > T2) {
-        if (++g > G) return g;
+      if (i > 0 && (x + a[i] > T1 || y + b[i] > T2 || (seg && !fit.add((int)i)))) {
+        if (++g > G && !out) return g;
+        if (out) out->push_back((int)i);
+        if (seg) fit.start((int)i);
         x = y = 0.0;
       }
       x += a[i];
       y += b[i];
     }
+    if (out) out->push_back((int)n);
     return g;
   };
   const double mA = sa / G, mB = sb / G;
@@ -808,10 +823,10 @@ void split_items_phases(const std::vector<CgsItem>& items, const std::vector<lon
   for (int k = 0; k <= 40; ++k) {
     const double T1 = std::max(ma, mA * (1.0 + 0.015 * k));
     double lo = std::max(mb, mB), hi = 4.0 * lo + sb / 16.0;
-    if (ranges(T1, hi) > G) continue;
+    if (cut(T1, hi, false, nullptr) > G) continue;
     for (int it = 0; it < 30; ++it) {
       const double mid = 0.5 * (lo + hi);
-      if (ranges(T1, mid) > G) lo = mid;
+      if (cut(T1, mid, false, nullptr) > G) lo = mid;
       else hi = mid;
     }
     if (best < 0.0 || T1 + hi < best) {
@@ -821,19 +836,17 @@ void split_items_phases(const std::vector<CgsItem>& items, const std::vector<lon
     }
   }
   if (best < 0.0) return split_items(items, G, off, &swb);
-  off.assign(1, 0);
-  {
-    double x = 0.0, y = 0.0;
-    for (size_t i = 0; i < n; ++i) {
-      if (x + a[i] > bT1 || y + b[i] > bT2) {
-        off.push_back((int)i);
-        x = y = 0.0;
-      }
-      x += a[i];
-      y += b[i];
+  bool seg = false;
+  for (int k = 0; k <= 30; ++k) {
+    const double f = 1.0 + 0.01 * k;
+    if (cut(bT1 * f, bT2 * f, true, nullptr) <= G) {
+      bT1 *= f;
+      bT2 *= f;
+      seg = true;
+      break;
     }
-    off.push_back((int)n);
   }
+  cut(bT1, bT2, seg, &off);
   while ((int)off.size() - 1 < G) {
     int r = -1;
     double worst = -1.0;
@@ -854,13 +867,13 @@ void split_items_phases(const std::vector<CgsItem>& items, const std::vector<lon
     double tot = 0.0;
     for (int i = off[r]; i < off[r + 1]; ++i) tot += a[i] / bT1 + b[i] / bT2;
     double c = 0.0;
-    int cut = off[r] + 1;
+    int at = off[r] + 1;
     for (int i = off[r]; i < off[r + 1] - 1; ++i) {
       c += a[i] / bT1 + b[i] / bT2;
-      cut = i + 1;
+      at = i + 1;
       if (c >= 0.5 * tot) break;
     }
-    off.insert(off.begin() + r + 1, cut);
+    off.insert(off.begin() + r + 1, at);
   }
   while ((int)off.size() < G + 1) off.push_back((int)n);
 }
@@ -1005,7 +1018,34 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
         for (int k = pair_off[q]; k < pair_off[q + 1]; ++k)
           swb[j] += 9LL * (P->sub_off[slot_sub[k] + 1] - P->sub_off[slot_sub[k]]) * vsize;
   }
-  if (sw) split_items_phases(items, swb, vsize == 8 ? 0.84 : 1.30, G, off);
+  // one segment per CTA range where possible: halo and Schwarz incidences of
+  // the range within the segment bounds (stamps of the range being built)
+  struct SegFit {
+    const Model& m;
+    const std::vector<CgsItem>& items;
+    std::vector<int> stamp;
+    std::function<int(i64)> incid;
+    int id = 0, uniq = 0, inc = 0;
+    void start(int i) {
+      ++id;
+      uniq = inc = 0;
+      add(i);
+    }
+    bool add(int i) {
+      int tinc = 0;
+      for (i64 q = items[i].c; q < items[i].c + items[i].b; ++q) {
+        tinc += incid(q);
+        for (int e = m.adj_off[q]; e < m.adj_off[q + 1]; ++e)
+          if (stamp[m.adj[e]] != id) {
+            stamp[m.adj[e]] = id;
+            ++uniq;
+          }
+      }
+      inc += tinc;
+      return uniq <= HALO_MAX && 3 * inc <= ZMAX;
+    }
+  } fit{m, items, std::vector<int>(nv, 0), incid};
+  if (sw) split_items_phases(items, swb, vsize == 8 ? 0.84 : 1.30, G, off, fit);
   else split_items(items, G, off, nullptr);
   for (int g = 0; g <= G; ++g) nrange[g] = off[g] < (int)items.size() ? items[off[g]].c : (int)nv;
   // segments: halo-local neighbour indices (sorted halo, times 3), own halo index
