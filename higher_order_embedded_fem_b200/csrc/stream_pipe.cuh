@@ -107,13 +107,16 @@ __device__ __forceinline__ void named_sync(int id, int nthreads) {
 // Grid barrier of a cooperative launch (one leader thread per CTA, after the
 // CTA's participating threads have synchronised): the leader adds to a
 // counter whose top bit flips once every CTA has arrived (block 0 adds
-// 2^31 - (G - 1), the others 1), then waits for the flip.  Returns false if
-// the flip did not come within the bound or *abort was raised (in which case
-// it raises *abort itself so that every CTA winds down).
+// 2^31 - (G - 1), the others 1), then waits for the flip.  The add is a
+// release at GPU scope (it orders the CTA's writes before the barrier, which
+// the CTA barrier has ordered before the leader's add) and an acquire fence
+// follows the flip, instead of two sequentially consistent fences.  Returns
+// false if the flip did not come within the bound or *abort was raised (in
+// which case it raises *abort itself so that every CTA winds down).
 __device__ __forceinline__ bool grid_barrier_leader(unsigned* counter, int* abort_flag) {
   const unsigned inc = blockIdx.x == 0 ? (0x80000000u - (gridDim.x - 1u)) : 1u;
-  __threadfence();
-  const unsigned old = atomicAdd(counter, inc);
+  unsigned old;
+  asm volatile("atom.add.release.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(counter), "r"(inc) : "memory");
   const uint64_t t0 = clock_ns();
   bool ok = true;
   for (;;) {
@@ -129,7 +132,7 @@ __device__ __forceinline__ bool grid_barrier_leader(unsigned* counter, int* abor
       break;
     }
   }
-  __threadfence();
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
   return ok;
 }
 
