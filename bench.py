@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--cg-engine", default="auto", choices=["auto", "chunked", "streamed"],
                     help="CG engine of the Jacobian solves (hoefem_integrator_set_cg_engine)")
     ap.add_argument("--schwarz-fp16", action="store_true", help="mixed variants: FP16 Schwarz blocks in the streamed CG")
+    ap.add_argument("--cg-phase-profile", action="store_true",
+                    help="streamed CG: per-phase times (mean and largest over CTAs) in each variant's cg_engine")
     ap.add_argument("--variants", default="plain,mixed,learned", help="comma list: plain, mixed, learned")
     ap.add_argument("--train-states", type=int, default=16, help="learned: training initial states (seeded)")
     ap.add_argument("--train-steps", type=int, default=2000, help="learned: Adam steps")
@@ -272,7 +274,7 @@ def run_hoefem(args):
     P = comp.build(model)
     integ = H.NewtonCgIntegrator3d(model, mat, 1000.0, bc, preconditioner=P)
     integ.set_tolerances(args.cg_tol, args.cg_max_iter, 100)
-    integ.set_cg_engine(args.cg_engine, args.schwarz_fp16)
+    integ.set_cg_engine(args.cg_engine, args.schwarz_fp16, phase_profile=args.cg_phase_profile)
 
     u0d = torch.from_numpy(u0).to(dev)
     v0d = torch.from_numpy(v0).to(dev)
