@@ -666,9 +666,11 @@ def run_tet10(args):
     model.set_stream(stream.cuda_stream)
     integ = H.NewtonCgIntegrator3d(model, mat, 1000.0, bc)
     integ.set_tolerances(args.cg_tol, args.cg_max_iter, 100)
+    integ.set_cg_engine(args.cg_engine, False, phase_profile=args.cg_phase_profile)
     u0d, v0d = torch.from_numpy(u0).to(dev), torch.from_numpy(v0).to(dev)
     out = {}
-    for vname in ("plain", "mixed"):
+    names = [v for v in ("plain", "mixed") if v in [x.strip() for x in args.variants.split(",")]] or ["plain", "mixed"]
+    for vname in names:
         integ.set_precision(vname == "mixed", args.delta)
         for _ in range(args.warmup):
             integ.step(u0d.clone(), v0d.clone(), 0.0, DT)
@@ -684,9 +686,12 @@ def run_tet10(args):
                       "newton_iterations": int(st["newton_iterations"]),
                       "phase_ms": {"forces": st["ms_assemble_forces"], "stiffness": st["ms_assemble_stiffness"],
                                    "cg": st["ms_cg"], "total": st["ms_total"]},
-                      "u": ud.cpu().numpy()}
-    up, um = out["plain"].pop("u"), out["mixed"].pop("u")
-    out["mixed"]["rel_diff_u_vs_plain"] = float(np.abs(um - up).max() / np.abs(up).max())
+                      "cg_engine": integ.cg_engine_stats(), "u": ud.cpu().numpy()}
+    if "plain" in out and "mixed" in out:
+        up, um = out["plain"].pop("u"), out["mixed"].pop("u")
+        out["mixed"]["rel_diff_u_vs_plain"] = float(np.abs(um - up).max() / np.abs(up).max())
+    for v in out.values():
+        v.pop("u", None)
     # the element stiffness alone (device arrays; adds into K); CUDA events on
     # the model's stream
     stiff = {}
@@ -740,12 +745,13 @@ def run_tet10(args):
                      "stiffness_fp32_vs_oracle": float(np.abs(K32 - Kr).max() / np.abs(Kr).max()),
                      "forces_fp64_vs_oracle": float(np.abs(f64 - fr).max() / np.abs(fr).max())})
     line = {"metric": "Newton-step ms, plain FP64 vs mixed, Tet10 box 201,600 elements, 1 GPU",
-            "value": out["mixed"]["ms_per_step"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "value": out[names[-1]]["ms_per_step"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": False, "dtype": "f64/f32", "data": "synthetic (seeded)",
             "config": {"workload": "Tet10 box 40x40x21 cells h=0.025 x6 tets, SNH E=1e6 nu=0.4, u0 ~ N(0,(0.02h)^2), "
                                    "one BE Newton step dt=1e-3, diagonal PCG to %g" % args.cg_tol,
                        "elements": int(model.num_elements), "ndof": int(model.ndof()), "nnz": int(model.nnz)},
-            "variants": out, "speedup_mixed_vs_plain": out["plain"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+            "variants": out, "speedup_mixed_vs_plain": (out["plain"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+                                                        if len(out) == 2 else None),
             "stiffness_ms": stiff, "errors": errs}
     print(json.dumps(line), flush=True)
 
