@@ -232,6 +232,106 @@ __global__ void k_cg_init_check(CgState* st) {
   if (st->max_iter >= 0 && st->iters >= st->max_iter) { st->done = 1; st->status = HOEFEM_CG_MAX_ITERATIONS; }
 }
 
+// Three row sums of node a in FP32: FP32 values times the FP32 copy of the
+// operand (one 16-byte entry per node), FP32 sums, the same traversals as
+// node_row_dot; the products carry the values' own rounding (as the streamed
+// engine's FP32 tiles).
+template <int L>
+__device__ __forceinline__ void node_row_dot_f32(const NodeRows& A, const float* __restrict__ vals,
+                                                 const float4* __restrict__ x4, int a, int sl, float& s0, float& s1,
+                                                 float& s2) {
+  constexpr int LNS = LaneCfg<L>::lanes;
+  s0 = s1 = s2 = 0.f;
+  if (a >= 0) {
+    const long long b = A.base[a];
+    if (A.diag_only && A.diag_only[a]) {
+      if (sl == 0) {
+        const float4 xv = x4[a];
+        s0 = vals[b] * xv.x;
+        s1 = vals[b + 1] * xv.y;
+        s2 = vals[b + 2] * xv.z;
+      }
+    } else if constexpr (LaneCfg<L>::stream) {
+      const int o = A.adj_off[a], d = A.adj_off[a + 1] - o;
+      const int rl = 3 * d;
+      const float* r0 = vals + b;
+      const float* xf = reinterpret_cast<const float*>(x4);
+#pragma unroll 4
+      for (int c = sl; c < rl; c += LNS) {
+        const int s = c / 3, j = c - 3 * s;
+        const float xv = xf[4 * A.adj[o + s] + j];
+        s0 += r0[c] * xv;
+        s1 += r0[rl + c] * xv;
+        s2 += r0[2 * rl + c] * xv;
+      }
+    } else {
+      const int o = A.adj_off[a], d = A.adj_off[a + 1] - o;
+      const long long rl = 3LL * d;
+#pragma unroll 2
+      for (int s = sl; s < d; s += LNS) {
+        const float4 xv = x4[A.adj[o + s]];
+        const float* r0 = vals + b + 3 * s;
+        s0 += r0[0] * xv.x + r0[1] * xv.y + r0[2] * xv.z;
+        const float* r1 = r0 + rl;
+        s1 += r1[0] * xv.x + r1[1] * xv.y + r1[2] * xv.z;
+        const float* r2 = r1 + rl;
+        s2 += r2[0] * xv.x + r2[1] * xv.y + r2[2] * xv.z;
+      }
+    }
+  }
+#pragma unroll
+  for (int off = LNS / 2; off > 0; off >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+  }
+}
+
+// Ap = A p with FP32 values and the FP32 copy of p ; pAp with the FP64 p ;
+// checks ; alpha
+template <int L>
+__global__ void __launch_bounds__(TPB) k_cg_Ap32(NodeRows A, const float* __restrict__ vals,
+                                                 const float4* __restrict__ p4, const double* __restrict__ p,
+                                                 double* __restrict__ Ap, double* part, CgState* st) {
+  if (st->done) return;
+  for_each_node_reduce<L, 1>(A, part, [&](int a, int sl, double (&acc)[1]) {
+    float f[3];
+    node_row_dot_f32<L>(A, vals, p4, a, sl, f[0], f[1], f[2]);
+    if (a >= 0 && sl == 0) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const double si = (double)f[i];
+        Ap[3 * a + i] = si;
+        acc[0] += p[3 * a + i] * si;
+      }
+    }
+  });
+  double extra[1] = {0.0}, tot[1];
+  if (node_reduce_finish<L, 1>(A, part, extra, tot) && threadIdx.x == 0) {
+    double pAp = tot[0];
+    st->pAp = pAp;
+    if (pAp <= 0.0) { st->done = 1; st->status = HOEFEM_CG_INDEFINITE_OPERATOR; }
+    else if (st->zTr <= 0.0) { st->done = 1; st->status = HOEFEM_CG_INDEFINITE_PRECONDITIONER; }
+    else st->alpha = st->zTr / pAp;
+  }
+}
+
+// p = z + beta p (beta = 0: p = z) and its FP32 copy, one node per thread
+__global__ void __launch_bounds__(TPB) k_cg_p4(int nv, const double* __restrict__ z, double* __restrict__ p,
+                                               float4* __restrict__ p4, const CgState* st, int copy) {
+  if (!copy && st->done) return;
+  const double beta = copy ? 0.0 : st->beta;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nv; a += gridDim.x * blockDim.x) {
+    double q[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      q[k] = copy ? z[3 * a + k] : z[3 * a + k] + beta * p[3 * a + k];
+      p[3 * a + k] = q[k];
+    }
+    p4[a] = make_float4((float)q[0], (float)q[1], (float)q[2], 0.f);
+  }
+}
+
 // Ap = A p ; pAp ; checks ; alpha
 template <int L, class VA>
 __global__ void __launch_bounds__(TPB) k_cg_Ap(NodeRows A, const VA* __restrict__ vals,
@@ -452,10 +552,21 @@ void enqueue_Ap(CgWork& w, Operator A, cudaStream_t s) {
   HOEFEM_LANES_DISPATCH(R.lanes, {
     const int sg = spmv_grid(R.count(), LN);
     if (A.v32)
-      (note_launch(), k_cg_Ap<LN, float><<<sg, TPB, 0, s>>>(R, A.v32, w.p.p, w.Ap.p, w.partials.p, w.st.p));
+      (note_launch(), k_cg_Ap32<LN><<<sg, TPB, 0, s>>>(R, A.v32, w.p32.p, w.p.p, w.Ap.p, w.partials.p, w.st.p));
     else
       (note_launch(), k_cg_Ap<LN, double><<<sg, TPB, 0, s>>>(R, A.v64, w.p.p, w.Ap.p, w.partials.p, w.st.p));
   });
+}
+
+// p = z + beta p (copy: p = z), with the FP32 copy when the operator is FP32
+void enqueue_p(CgWork& w, bool f32, bool copy, cudaStream_t s) {
+  const int n = (int)w.n;
+  if (f32)
+    (note_launch(), k_cg_p4<<<vec_grid(n / 3), TPB, 0, s>>>(n / 3, w.z.p, w.p.p, w.p32.p, w.st.p, copy ? 1 : 0));
+  else if (copy)
+    (note_launch(), k_cg_copy<<<vec_grid(n), TPB, 0, s>>>(n, w.z.p, w.p.p));
+  else
+    (note_launch(), k_cg_p<<<vec_grid(n), TPB, 0, s>>>(n, w.z.p, w.p.p, w.st.p));
 }
 
 // update (block apply only): fuse this iteration's x / r step into the apply
@@ -513,7 +624,7 @@ void enqueue_iteration(CgWork& w, Operator A, const Precond* P, bool p32, cudaSt
     (note_launch(), k_cg_update<<<vg, TPB, 0, s>>>(n, mode, kind == PREC_DIAGONAL ? P->diag.p : nullptr, w.x.p, w.r.p,
                                                    w.p.p, w.Ap.p, w.z.p, w.partials.p, w.counter.p, w.st.p));
   }
-  (note_launch(), k_cg_p<<<vg, TPB, 0, s>>>(n, w.z.p, w.p.p, w.st.p));
+  enqueue_p(w, A.v32 != nullptr, false, s);
 }
 
 CgWork::Graph& graph_for(CgWork& w, Operator A, const Precond* P, bool p32) {
@@ -613,7 +724,8 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
     });
   }
   prec_init();
-  (note_launch(), k_cg_copy<<<vg, TPB, 0, s>>>(n, w.z.p, w.p.p));
+  if (A.v32 && !w.p32.p) w.p32.alloc(n / 3);
+  enqueue_p(w, A.v32 != nullptr, true, s);
   (note_launch(), k_cg_init_check<<<1, 1, 0, s>>>(w.st.p));
   HOEFEM_CUDA(cudaGetLastError());
   HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
@@ -765,7 +877,7 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
         true_residual(A64);
         prec_init();
         (note_launch(), k_cg_reliable<<<1, 1, 0, s>>>(w.st.p, conv ? 1 : 0));
-        if (conv) (note_launch(), k_cg_p<<<vg, TPB, 0, s>>>(n, w.z.p, w.p.p, w.st.p));
+        if (conv) enqueue_p(w, A.v32 != nullptr, false, s);
         HOEFEM_CUDA(cudaGetLastError());
         HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
         HOEFEM_CUDA(cudaStreamSynchronize(s));

@@ -155,6 +155,9 @@ struct CgWork {
   Model* m = nullptr;
   i64 n = 0;
   DBuf<double> x, b, r, z, p, Ap, partials;
+  // FP32 copy of the search direction (one 16-byte entry per node) for the
+  // FP32 operator products of the mixed form's chunked engine
+  DBuf<float4> p32;
   DBuf<CgState> st;
   DBuf<unsigned> counter;
   CgState* h_st = nullptr;  // pinned
