@@ -72,6 +72,8 @@ def parse():
                          "batch; tet10: 201,600-element Tet10 box, plain vs mixed precision; embed: embedded "
                          "quadrature construction (classification, cut-cell rules, simplification)")
     ap.add_argument("--scenes", type=int, default=64, help="batched: number of scenes")
+    ap.add_argument("--tet10-grid", default="40,40,21",
+                    help="tet10: hex cells per axis (6 Tet10 each); the benchmark box is 40,40,21")
     ap.add_argument("--min-elements", type=float, default=1e3, help="batched: smallest scene (elements)")
     ap.add_argument("--max-elements", type=float, default=5e4, help="batched: largest scene (elements)")
     ap.add_argument("--no-sequential", action="store_true", help="batched: skip the one-scene-at-a-time comparison")
@@ -655,7 +657,8 @@ def run_tet10(args):
     dev = torch.device("cuda", 0)
     import higher_order_embedded_fem_b200 as H
 
-    s = H.scenes.tet10_box(0.025, 40, 40, 21, 1)
+    nx, ny, nz = (int(v) for v in args.tet10_grid.split(","))
+    s = H.scenes.tet10_box(0.025, nx, ny, nz, 1)
     b = s.blocks[0]
     model = H.NodalModel3d(s.vertices, b.connectivity, (b.weights, b.points))
     mat = H.StableNeoHookeanMaterial(H.YoungPoisson(1e6, 0.4))
@@ -744,11 +747,11 @@ def run_tet10(args):
         errs.update({"stiffness_fp64_vs_oracle": float(np.abs(K64 - Kr).max() / np.abs(Kr).max()),
                      "stiffness_fp32_vs_oracle": float(np.abs(K32 - Kr).max() / np.abs(Kr).max()),
                      "forces_fp64_vs_oracle": float(np.abs(f64 - fr).max() / np.abs(fr).max())})
-    line = {"metric": "Newton-step ms, plain FP64 vs mixed, Tet10 box 201,600 elements, 1 GPU",
+    line = {"metric": "Newton-step ms, plain FP64 vs mixed, Tet10 box %d elements, 1 GPU" % model.num_elements,
             "value": out[names[-1]]["ms_per_step"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": False, "dtype": "f64/f32", "data": "synthetic (seeded)",
-            "config": {"workload": "Tet10 box 40x40x21 cells h=0.025 x6 tets, SNH E=1e6 nu=0.4, u0 ~ N(0,(0.02h)^2), "
-                                   "one BE Newton step dt=1e-3, diagonal PCG to %g" % args.cg_tol,
+            "config": {"workload": "Tet10 box %dx%dx%d cells h=0.025 x6 tets, SNH E=1e6 nu=0.4, u0 ~ N(0,(0.02h)^2), "
+                                   "one BE Newton step dt=1e-3, diagonal PCG to %g" % (nx, ny, nz, args.cg_tol),
                        "elements": int(model.num_elements), "ndof": int(model.ndof()), "nnz": int(model.nnz)},
             "variants": out, "speedup_mixed_vs_plain": (out["plain"]["ms_per_step"] / out["mixed"]["ms_per_step"]
                                                         if len(out) == 2 else None),
