@@ -796,8 +796,8 @@ int run_pcg(CgWork& w, Operator A, const Precond* P, bool p32, double tol, i64 m
           ++nrep_s;
           if (conv) {
             // the recurrence claimed convergence: the true residual usually
-            // confirms it, so wait for the verdict instead of launching a
-            // kernel that would return at once
+            // confirms it, so read the outcome instead of launching a kernel
+            // that would return at once
             HOEFEM_CUDA(cudaMemcpyAsync(w.h_st, w.st.p, sizeof(CgState), cudaMemcpyDeviceToHost, s));
             HOEFEM_CUDA(cudaStreamSynchronize(s));
             if (w.h_st->done) break;
