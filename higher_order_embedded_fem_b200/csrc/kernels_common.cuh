@@ -241,6 +241,8 @@ template <int L>
 struct NodeChunk {
   static constexpr int G = 32 / LaneCfg<L>::lanes;
   static constexpr int NF = G >= 4 ? 16 : 8;
+  // the CG's partial-sum buffer holds one entry per chunk of at least 8 nodes
+  static_assert(NF >= 8, "node chunks smaller than the partial-sum buffer allows");
 };
 __host__ __device__ inline int node_chunk_count(int count, int nf) { return (count + nf - 1) / nf; }
 
