@@ -180,3 +180,12 @@ def test_compute_without_device_fails_loudly():
     with pytest.raises(H.HoefemError) as ei:
         m.assemble_stiffness(np.zeros(m.ndof()), H.StVKMaterial(H.YoungPoisson(1e6, 0.3)))
     assert ei.value.status == "NO_DEVICE"
+
+
+def test_batch_engine_entry_points_check_arguments():
+    L = _capi.lib()
+    invalid = [k for k, v in _capi.STATUS.items() if v == "INVALID_ARGUMENT"][0]
+    e, c, n = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(0)
+    assert L.hoefem_batch_set_cg_engine(None, 0, 0) == invalid
+    assert L.hoefem_batch_cg_choice(None, ctypes.byref(e), ctypes.byref(c), None, ctypes.byref(n)) == invalid
+    assert _capi.CG_ENGINE == {"auto": 0, "chunked": 1, "streamed": 2}
