@@ -58,6 +58,7 @@
 #include "internal.h"
 #include "kernels_common.cuh"
 #include "solver.h"
+#include "stream_partition.h"
 #include "stream_pipe.cuh"
 
 namespace hoefem {
@@ -750,132 +751,12 @@ __global__ void k_cg_stream_arm(CgState* st, double delta2) {
   st->rcur = 0;
 }
 
-// Splits items into G contiguous groups of about equal weight (the item's
-// bytes, plus extra[i] when given): off[0..G].
-void split_items(const std::vector<CgsItem>& items, int G, std::vector<int>& off,
-                 const std::vector<long long>* extra = nullptr) {
-  auto weight = [&](size_t i) { return (long long)items[i].bytes + (extra ? (*extra)[i] : 0LL); };
-  long long total = 0;
-  for (size_t i = 0; i < items.size(); ++i) total += weight(i);
-  off.assign(G + 1, 0);
-  long long cum = 0;
-  int g = 1;
-  for (size_t i = 0; i < items.size(); ++i) {
-    cum += weight(i);
-    while (g < G && cum * (long long)G >= total * (long long)g) off[g++] = (int)(i + 1);
-  }
-  while (g <= G) off[g++] = (int)items.size();
-}
-
-// CTA ranges for an operator + Schwarz stream.  The operator tiles and the
-// Schwarz rows of an iteration run in two phases that each end at a grid
-// barrier, so an iteration costs about max_g A_g + max_g B_g (A_g: operator
-// bytes of range g; B_g: its Schwarz bytes at the operator's value size,
-// times kappa, their measured cost per byte relative to the operator tiles).
-// For caps T1 on A from 1.0 to 1.6 times the mean, the smallest cap T2 on B
-// for which the greedy cut (each range extended while both sums stay within
-// the caps; it needs the fewest ranges of any cut under these caps) fits in G
-// ranges is found by bisection, and the pair with the smallest T1 + T2 is
-// kept.  Then the cut also keeps every range within one segment (`fit`: its
-// halo and Schwarz incidences within the segment bounds, so that no CTA
-// gathers two overlapping halos), with both caps relaxed by 1% steps until
-// the cut fits in G ranges (without it if none does).  If the cut uses fewer
-// than G ranges, the heaviest ranges are halved (a part of a range fits
-// wherever the range does).  Fit: start(i) opens a range at item i, add(i)
-// extends it if the item fits.
-template <class Fit>
-void split_items_phases(const std::vector<CgsItem>& items, const std::vector<long long>& swb, double kappa, int G,
-                        std::vector<int>& off, Fit& fit) {
-  const size_t n = items.size();
-  if (n == 0 || G <= 1) return split_items(items, G, off, &swb);
-  std::vector<double> a(n), b(n);
-  double sa = 0.0, sb = 0.0, ma = 0.0, mb = 0.0;
-  for (size_t i = 0; i < n; ++i) {
-    a[i] = (double)items[i].bytes;
-    b[i] = kappa * (double)swb[i];
-    sa += a[i];
-    sb += b[i];
-    ma = std::max(ma, a[i]);
-    mb = std::max(mb, b[i]);
-  }
-  // the greedy cut under caps (T1, T2), with or without the segment bound;
-  // stops counting past G ranges
-  auto cut = [&](double T1, double T2, bool seg, std::vector<int>* out) {
-    int g = 1;
-    double x = 0.0, y = 0.0;
-    if (out) out->assign(1, 0);
-    if (seg) fit.start(0);
-    for (size_t i = 0; i < n; ++i) {
-      if (i > 0 && (x + a[i] > T1 || y + b[i] > T2 || (seg && !fit.add((int)i)))) {
-        if (++g > G && !out) return g;
-        if (out) out->push_back((int)i);
-        if (seg) fit.start((int)i);
-        x = y = 0.0;
-      }
-      x += a[i];
-      y += b[i];
-    }
-    if (out) out->push_back((int)n);
-    return g;
-  };
-  const double mA = sa / G, mB = sb / G;
-  double best = -1.0, bT1 = 0.0, bT2 = 0.0;
-  for (int k = 0; k <= 40; ++k) {
-    const double T1 = std::max(ma, mA * (1.0 + 0.015 * k));
-    double lo = std::max(mb, mB), hi = 4.0 * lo + sb / 16.0;
-    if (cut(T1, hi, false, nullptr) > G) continue;
-    for (int it = 0; it < 30; ++it) {
-      const double mid = 0.5 * (lo + hi);
-      if (cut(T1, mid, false, nullptr) > G) lo = mid;
-      else hi = mid;
-    }
-    if (best < 0.0 || T1 + hi < best) {
-      best = T1 + hi;
-      bT1 = T1;
-      bT2 = hi;
-    }
-  }
-  if (best < 0.0) return split_items(items, G, off, &swb);
-  bool seg = false;
-  for (int k = 0; k <= 30; ++k) {
-    const double f = 1.0 + 0.01 * k;
-    if (cut(bT1 * f, bT2 * f, true, nullptr) <= G) {
-      bT1 *= f;
-      bT2 *= f;
-      seg = true;
-      break;
-    }
-  }
-  cut(bT1, bT2, seg, &off);
-  while ((int)off.size() - 1 < G) {
-    int r = -1;
-    double worst = -1.0;
-    for (size_t q = 0; q + 1 < off.size(); ++q) {
-      if (off[q + 1] - off[q] < 2) continue;
-      double x = 0.0, y = 0.0;
-      for (int i = off[q]; i < off[q + 1]; ++i) {
-        x += a[i];
-        y += b[i];
-      }
-      const double wq = std::max(x / bT1, y / bT2);
-      if (wq > worst) {
-        worst = wq;
-        r = (int)q;
-      }
-    }
-    if (r < 0) break;
-    double tot = 0.0;
-    for (int i = off[r]; i < off[r + 1]; ++i) tot += a[i] / bT1 + b[i] / bT2;
-    double c = 0.0;
-    int at = off[r] + 1;
-    for (int i = off[r]; i < off[r + 1] - 1; ++i) {
-      c += a[i] / bT1 + b[i] / bT2;
-      at = i + 1;
-      if (c >= 0.5 * tot) break;
-    }
-    off.insert(off.begin() + r + 1, at);
-  }
-  while ((int)off.size() < G + 1) off.push_back((int)n);
+// Item weights for the range splits of stream_partition.h: the item's bytes,
+// plus extra[i] when given.
+std::vector<long long> item_weights(const std::vector<CgsItem>& items, const std::vector<long long>* extra) {
+  std::vector<long long> w(items.size());
+  for (size_t i = 0; i < items.size(); ++i) w[i] = (long long)items[i].bytes + (extra ? (*extra)[i] : 0LL);
+  return w;
 }
 
 // Packs consecutive records (byte sizes rec[r], each 16-aligned) into items of
@@ -1006,7 +887,7 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
     ++tile_id;
   }
   std::vector<int> off, nrange(G + 1);
-  // CTA ranges balanced for the two phases (split_items_phases): Schwarz
+  // CTA ranges balanced for the two phases (split_two_phase): Schwarz
   // bytes counted at the operator's value size cost 1.30 times the operator
   // tile bytes per byte with FP32 values and 0.84 times with FP64 values
   // (phase times per CTA on the benchmark cylinder)
@@ -1045,8 +926,17 @@ bool build_op_layout(CgStreamOp& L, Model& m, int vsize, int G, const Precond* P
       return uniq <= HALO_MAX && 3 * inc <= ZMAX;
     }
   } fit{m, items, std::vector<int>(nv, 0), incid};
-  if (sw) split_items_phases(items, swb, vsize == 8 ? 0.84 : 1.30, G, off, fit);
-  else split_items(items, G, off, nullptr);
+  if (sw) {
+    const double kappa = vsize == 8 ? 0.84 : 1.30;
+    std::vector<double> wa(items.size()), wb(items.size());
+    for (size_t i = 0; i < items.size(); ++i) {
+      wa[i] = (double)items[i].bytes;
+      wb[i] = kappa * (double)swb[i];
+    }
+    if (!split_two_phase(wa, wb, G, off, fit)) split_weighted(item_weights(items, &swb), G, off);
+  } else {
+    split_weighted(item_weights(items, nullptr), G, off);
+  }
   for (int g = 0; g <= G; ++g) nrange[g] = off[g] < (int)items.size() ? items[off[g]].c : (int)nv;
   // segments: halo-local neighbour indices (sorted halo, times 3), own halo index
   std::vector<CgsSeg> segs;
