@@ -189,3 +189,16 @@ def test_batch_engine_entry_points_check_arguments():
     assert L.hoefem_batch_set_cg_engine(None, 0, 0) == invalid
     assert L.hoefem_batch_cg_choice(None, ctypes.byref(e), ctypes.byref(c), None, ctypes.byref(n)) == invalid
     assert _capi.CG_ENGINE == {"auto": 0, "chunked": 1, "streamed": 2}
+
+
+def test_header_is_plain_c():
+    # the boundary is a C ABI: the header compiles as C99 and as C++11
+    import shutil
+    import subprocess
+
+    hdr = os.path.join(ROOT, "include", "hoefem.h")
+    for cc, lang, std in (("gcc", "c", "-std=c99"), ("g++", "c++", "-std=c++11")):
+        exe = shutil.which(cc)
+        if exe is None:
+            pytest.skip("no host compiler")
+        subprocess.check_call([exe, std, "-Wall", "-Werror", "-fsyntax-only", "-x", lang, hdr])
